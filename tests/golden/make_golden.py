@@ -1,0 +1,154 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference CoMech code itself.
+
+Run in a container where the reference is mounted (default /root/reference, override with COMECH_REF):
+
+    python tests/golden/make_golden.py
+
+Every fixture stores its inputs as well as the reference's outputs, so the tests never need the
+reference (nor the synthetic generator) at run time.  Reference functions used:
+fe/solver.py (element_matrices, element_basis, Grid, assemble, solve, cell_stress),
+fe/gmg.py (GMG, pcg_gmg), rb/splitfe.py (split_connectivity[_fast], KL_family, assemble_cn,
+solve_cn, cell_stress_cn, element_forces_cn), fe/test_patch.py (patch-test set-up).
+"""
+import os
+import sys
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("COMECH_REF", "/root/reference")
+sys.path.insert(0, REPO)
+sys.path.insert(1, REF)
+sys.path.insert(2, os.path.join(REF, "rb"))
+
+from fe import solver as RS          # noqa: E402  (reference)
+from fe import gmg as RG             # noqa: E402
+import splitfe as RSF                # noqa: E402
+from comech_b200 import synth        # noqa: E402  (input generator only)
+
+
+def save(name, **arrs):
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+    print("wrote", name, {k: np.shape(v) for k, v in arrs.items()})
+
+
+def springs_arrays(s):
+    return dict(pair_a=s.pair_a, pair_b=s.pair_b, pair_k=s.pair_k, line_a=s.line_a, line_b=s.line_b,
+                line_d=s.line_d, line_k=s.line_k)
+
+
+def elements():
+    out = {}
+    for i, d in enumerate([(1.0, 1.0, 1.0), (0.5, 0.75, 1.25), (3.0, 1.5, 0.3)]):
+        KL, KM, Bc = RS.element_matrices(np.array(d))
+        out[f"dims{i}"] = np.array(d); out[f"KL{i}"] = KL; out[f"KM{i}"] = KM; out[f"Bc{i}"] = Bc
+        out[f"KB{i}"] = RS.element_basis(np.array(d))
+    g = RS.Grid(np.r_[0, 1, 3, 4, 7, 10], np.r_[0, 2, 5, 10], np.r_[0, 1, 2, 4, 6, 10])
+    out["patch_KLsri"] = RSF.KL_family(g)
+    out["patch_udims"] = g.udims
+    out["patch_dim_id"] = g.dim_id
+    out["patch_cell_nodes"] = g.cell_nodes
+    out["patch_node_xyz"] = g.node_xyz
+    save("elements", **out)
+
+
+def split_cases():
+    out = {}
+    P = synth.hindfoot_problem(28, 20, 16, h=2.8, seed=3)
+    g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    cn, orig, ns = RSF.split_connectivity_fast(g, P["active"], P["part"], P["bone_share"])
+    cn2, orig2, ns2 = RSF.split_connectivity(g, P["active"], P["part"], P["bone_share"])
+    assert (cn == cn2).all() and (orig == orig2).all() and ns == ns2
+    out.update(h_edges_x=g.xe, h_edges_y=g.ye, h_edges_z=g.ze, h_active=P["active"], h_part=P["part"],
+               h_share=P["bone_share"], h_cn=cn, h_orig=orig, h_nsplit=ns)
+    # random parts and shares: many bones, ties in share and in cell counts
+    rng = np.random.default_rng(11)
+    g2 = RS.Grid(np.arange(13.0), np.arange(11.0), np.arange(9.0))
+    act = rng.random(g2.ncell) < 0.9
+    part = rng.integers(0, 5, g2.ncell) * (rng.random(g2.ncell) < 0.7)
+    share = np.round(rng.random((g2.ncell, 5)) * 4) / 4 * (rng.random((g2.ncell, 5)) < 0.5)
+    share[:, 0] = 0
+    cn, orig, ns = RSF.split_connectivity_fast(g2, act, part, share)
+    cn2, orig2, ns2 = RSF.split_connectivity(g2, act, part, share)
+    assert (cn == cn2).all() and (orig == orig2).all() and ns == ns2
+    out.update(r_edges_x=g2.xe, r_edges_y=g2.ye, r_edges_z=g2.ze, r_active=act, r_part=part, r_share=share,
+               r_cn=cn, r_orig=orig, r_nsplit=ns)
+    save("split", **out)
+
+
+def hindfoot_solve():
+    P = synth.hindfoot_problem(24, 18, 16, h=3.0, seed=1)
+    g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    cells = np.flatnonzero(P["active"])
+    K, nmap, nused = RSF.assemble_cn(g, P["lam"], P["mu"], cells, P["cn"])
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((2, K.shape[0]))
+    Ku = np.stack([K @ x for x in u])
+    U, info, R = RSF.solve_cn(g, P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"],
+                              P["extra"], P["node_groups"], tol=1e-10, maxiter=800)
+    sig, vm, eps = RSF.cell_stress_cn(g, P["lam"], P["mu"], U, cells, P["cn"])
+    fcells = cells[::7]
+    F = RSF.element_forces_cn(g, P["lam"], P["mu"], U, fcells, P["cn"])
+    (ln, la, lt), = P["loads"]
+    groups = np.concatenate(P["node_groups"]); glen = np.array([len(x) for x in P["node_groups"]])
+    save("hindfoot_small", xe=g.xe, ye=g.ye, ze=g.ze, lam=P["lam"], mu=P["mu"], active=P["active"], cn=P["cn"],
+         orig=P["orig"], fixed_nodes=P["fixed"][0], fixed_area=P["fixed"][1], load_nodes=ln, load_area=la,
+         load_t=lt, groups=groups, group_len=glen, nused=nused, u=u, Ku=Ku, U=U, R=R, iters=info["iters"],
+         flag=info["flag"], levels=info["levels"], ndof=info["ndof"], sig=sig, vm=vm, eps=eps, fcells=fcells, F=F,
+         **springs_arrays(P["extra"]))
+    # multigrid internals on the assembled operator of this problem
+    kd = np.zeros(K.shape[0])
+    for c in range(3):
+        np.add.at(kd, 3 * nmap[P["fixed"][0]] + c, P["fixed"][1] * 1e6)
+    A = K + RS.sp.diags(kd) + P["extra"](nmap, K.shape[0])
+    mg = RG.GMG(A.tocsr(), P["orig"][nused], g.xe, g.ye, g.ze, min_dofs=600)
+    b = rng.standard_normal(A.shape[0])
+    save("gmg_small", nused=nused, b=b, vcycle=mg.vcycle(b), sizes=np.array([L.A.shape[0] for L in mg.levels]),
+         lmax=np.array([L.lmax for L in mg.levels]))
+
+
+def block_solves():
+    P = synth.block_problem(12, 10, 8, h=1.0, seed=2)
+    g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    (sn, sa, sk), = P["springs"]; (ln, la, lt), = P["loads"]
+    cells = np.arange(g.ncell)
+    out = dict(xe=g.xe, ye=g.ye, ze=g.ze, lam=P["lam"], mu=P["mu"], spring_nodes=sn, spring_area=sa, spring_k=sk,
+               load_nodes=ln, load_area=la, load_t=lt)
+    U, info = RS.solve(g, P["lam"], P["mu"], P["active"], P["springs"], P["loads"], method="gmg", tol=1e-10)
+    sig, vm, eps = RS.cell_stress(g, P["lam"], P["mu"], U, cells)
+    out.update(U_gmg=U, iters_gmg=info["iters"], vm_gmg=vm, sig_gmg=sig)
+    # rank-1 penalty on the mean x translation of the top face, rigid groups, orthotropic coefficients
+    top = cells[g.cK == g.nz - 1]
+    tn, ta = RS.face_node_areas(g, top, "z+")
+    pen = [(tn, ta, 0, 1e5)]
+    coeffs = RS.ortho_coeffs(P["lam"], P["mu"], shear_factor=0.5)
+    half = np.unique(g.cell_nodes[cells[g.cI < g.nx // 2]])
+    U2, info2 = RS.solve(g, P["lam"], P["mu"], P["active"], P["springs"], P["loads"], method="gmg", tol=1e-10,
+                         penalties=pen, coeffs=coeffs, node_groups=[half])
+    sig2, vm2, eps2 = RS.cell_stress(g, P["lam"], P["mu"], U2, cells, coeffs=coeffs)
+    out.update(pen_nodes=tn, pen_w=ta, pen_comp=0, pen_k=1e5, coeffs=coeffs, group=half, U_pen=U2,
+               iters_pen=info2["iters"], vm_pen=vm2, sig_pen=sig2)
+    U3, info3 = RS.solve(g, P["lam"], P["mu"], P["active"], P["springs"], P["loads"], method="cg", tol=1e-10)
+    out.update(U_cg=U3, iters_cg=info3["iters"])
+    save("block_small", **out)
+
+
+def patch():
+    g = RS.Grid(np.r_[0, 1, 3, 4, 7, 10], np.r_[0, 2, 5, 10], np.r_[0, 1, 2, 4, 6, 10])
+    E, nu = 1000.0, 0.3
+    lam, mu = RS.lame(np.full(g.ncell, E), np.full(g.ncell, nu))
+    active = np.ones(g.ncell, bool)
+    bot = np.flatnonzero(g.cK == 0); top = np.flatnonzero(g.cK == g.nz - 1)
+    nb, ab = RS.face_node_areas(g, bot, "z-"); nt, at = RS.face_node_areas(g, top, "z+")
+    U, info = RS.solve(g, lam, mu, active, [(nb, ab, np.array([1e-6, 1e-6, 1e9]))], [(nt, at, np.array([0, 0, -1.0]))],
+                       method="direct")
+    sig, vm, eps = RS.cell_stress(g, lam, mu, U, np.arange(g.ncell))
+    save("patch", xe=g.xe, ye=g.ye, ze=g.ze, E=E, nu=nu, U=U, sig=sig, vm=vm)
+
+
+if __name__ == "__main__":
+    elements()
+    split_cases()
+    hindfoot_solve()
+    block_solves()
+    patch()
