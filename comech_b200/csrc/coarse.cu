@@ -1,0 +1,505 @@
+// Coarse-level kernels: stencil products, structured restriction / prolongation, Galerkin on the device.
+#include "coarse.cuh"
+
+namespace feb {
+
+namespace {
+
+__device__ __forceinline__ double axis_w(const AxisDev& A, int i, int J) {
+  double w = 0.0;
+  if (A.ca[i] == J) w += A.wa[i];
+  if (A.cb[i] == J) w += A.wb[i];
+  return w;
+}
+
+// coarse support of fine node i along one axis: up to 2 (index, weight) pairs
+__device__ __forceinline__ int axis_support(const AxisDev& A, int i, int (&J)[2], double (&w)[2]) {
+  int n = 0;
+  if (A.wa[i] != 0.0) { J[n] = A.ca[i]; w[n] = A.wa[i]; ++n; }
+  if (A.cb[i] != A.ca[i] && A.wb[i] != 0.0) { J[n] = A.cb[i]; w[n] = A.wb[i]; ++n; }
+  return n;
+}
+
+// fine nodes interpolating from coarse node J along one axis: up to 3 (index, weight) pairs
+__device__ __forceinline__ int axis_fan(const AxisDev& A, int J, int (&I)[3], double (&w)[3]) {
+  int n = 0, f = A.cidx[J];
+  for (int i = f - 1; i <= f + 1; ++i) {
+    if (i < 0 || i >= A.nf) continue;
+    double x = axis_w(A, i, J);
+    if (x != 0.0) { I[n] = i; w[n] = x; ++n; }
+  }
+  return n;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_apply(StencilView<T> L, const T* __restrict__ u, T* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= L.n) return;
+  int i = int(n % L.nx), j = int((n / L.nx) % L.ny), k = int(n / ((int64_t)L.nx * L.ny));
+  T acc0 = 0, acc1 = 0, acc2 = 0;
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+    const int ii = i + dx, jj = j + dy, kk = k + dz;
+    if (ii < 0 || jj < 0 || kk < 0 || ii >= L.nx || jj >= L.ny || kk >= L.nz) continue;
+    const int64_t m = n + dx + (int64_t)L.nx * (dy + (int64_t)L.ny * dz);
+    const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+    const T* a = L.A + (size_t)(o * 9) * L.n + n;
+    acc0 += a[0] * u0 + a[L.n] * u1 + a[2 * L.n] * u2;
+    acc1 += a[3 * L.n] * u0 + a[4 * L.n] * u1 + a[5 * L.n] * u2;
+    acc2 += a[6 * L.n] * u0 + a[7 * L.n] * u1 + a[8 * L.n] * u2;
+  }
+  y[3 * n] = acc0; y[3 * n + 1] = acc1; y[3 * n + 2] = acc2;
+}
+
+template <typename T>
+__global__ void k_csr_add(int nrow, const int* __restrict__ row_dof, const int* __restrict__ row_ptr,
+                          const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ u,
+                          T* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nrow) return;
+  T s = 0;
+  for (int q = row_ptr[e]; q < row_ptr[e + 1]; ++q) s += val[q] * u[col[q]];
+  atomic_add(y + row_dof[e], s);
+}
+
+template <typename T>
+__global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __restrict__ rf, T* __restrict__ rc,
+                                const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int cnx = P.ax[0].nc, cny = P.ax[1].nc, cnz = P.ax[2].nc;
+  int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (J >= (int64_t)cnx * cny * cnz) return;
+  int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  int Ix[3], Iy[3], Iz[3];
+  double wx[3], wy[3], wz[3];
+  int nxs = axis_fan(P.ax[0], jx, Ix, wx), nys = axis_fan(P.ax[1], jy, Iy, wy), nzs = axis_fan(P.ax[2], jz, Iz, wz);
+  T s0 = 0, s1 = 0, s2 = 0;
+  for (int c = 0; c < nzs; ++c)
+    for (int b = 0; b < nys; ++b)
+      for (int a = 0; a < nxs; ++a) {
+        int64_t f = Ix[a] + (int64_t)fnx * (Iy[b] + (int64_t)fny * Iz[c]);
+        T w = T(wx[a] * wy[b] * wz[c]);
+        s0 += w * rf[3 * f]; s1 += w * rf[3 * f + 1]; s2 += w * rf[3 * f + 2];
+      }
+  rc[3 * J] = s0; rc[3 * J + 1] = s1; rc[3 * J + 2] = s2;
+}
+
+template <typename T>
+__global__ void k_restrict_copies(TransferDev P, int fnx, int fny, int64_t fnnode, int64_t fntotal,
+                                  const int* __restrict__ orig_copy, const T* __restrict__ rf, T* __restrict__ rc,
+                                  const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t e = fnnode + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= fntotal) return;
+  int64_t o = orig_copy[e - fnnode];
+  int pi = int(o % fnx), pj = int((o / fnx) % fny), pk = int(o / ((int64_t)fnx * fny));
+  int Jx[2], Jy[2], Jz[2];
+  double wx[2], wy[2], wz[2];
+  int nxs = axis_support(P.ax[0], pi, Jx, wx), nys = axis_support(P.ax[1], pj, Jy, wy),
+      nzs = axis_support(P.ax[2], pk, Jz, wz);
+  const int cnx = P.ax[0].nc, cny = P.ax[1].nc;
+  for (int c = 0; c < nzs; ++c)
+    for (int b = 0; b < nys; ++b)
+      for (int a = 0; a < nxs; ++a) {
+        int64_t K = Jx[a] + (int64_t)cnx * (Jy[b] + (int64_t)cny * Jz[c]);
+        T w = T(wx[a] * wy[b] * wz[c]);
+        for (int q = 0; q < 3; ++q) atomic_add(rc + 3 * K + q, w * rf[3 * e + q]);
+      }
+}
+
+template <typename T>
+__global__ void k_prolong_add(TransferDev P, int fnx, int fny, int64_t fnnode, int64_t fntotal,
+                              const int* __restrict__ orig_copy, const uint8_t* __restrict__ used,
+                              const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= fntotal || !used[n]) return;
+  int64_t o = n < fnnode ? n : (int64_t)orig_copy[n - fnnode];
+  int pi = int(o % fnx), pj = int((o / fnx) % fny), pk = int(o / ((int64_t)fnx * fny));
+  int Jx[2], Jy[2], Jz[2];
+  double wx[2], wy[2], wz[2];
+  int nxs = axis_support(P.ax[0], pi, Jx, wx), nys = axis_support(P.ax[1], pj, Jy, wy),
+      nzs = axis_support(P.ax[2], pk, Jz, wz);
+  const int cnx = P.ax[0].nc, cny = P.ax[1].nc;
+  T s0 = 0, s1 = 0, s2 = 0;
+  for (int c = 0; c < nzs; ++c)
+    for (int b = 0; b < nys; ++b)
+      for (int a = 0; a < nxs; ++a) {
+        int64_t K = Jx[a] + (int64_t)cnx * (Jy[b] + (int64_t)cny * Jz[c]);
+        T w = T(wx[a] * wy[b] * wz[c]);
+        s0 += w * xc[3 * K]; s1 += w * xc[3 * K + 1]; s2 += w * xc[3 * K + 2];
+      }
+  xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+}
+
+__global__ void k_kept_mask(TransferDev P, const uint8_t* __restrict__ used_f, uint8_t* __restrict__ kept_c) {
+  const int cnx = P.ax[0].nc, cny = P.ax[1].nc, cnz = P.ax[2].nc;
+  const int fnx = P.ax[0].nf, fny = P.ax[1].nf;
+  int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (J >= (int64_t)cnx * cny * cnz) return;
+  int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  int Ix[3], Iy[3], Iz[3];
+  double wx[3], wy[3], wz[3];
+  int nxs = axis_fan(P.ax[0], jx, Ix, wx), nys = axis_fan(P.ax[1], jy, Iy, wy), nzs = axis_fan(P.ax[2], jz, Iz, wz);
+  uint8_t k = 0;
+  for (int c = 0; c < nzs && !k; ++c)
+    for (int b = 0; b < nys && !k; ++b)
+      for (int a = 0; a < nxs && !k; ++a) k = used_f[Ix[a] + (int64_t)fnx * (Iy[b] + (int64_t)fny * Iz[c])];
+  kept_c[J] = k ? 1 : 0;
+}
+
+// Column q = (corner a, component s) of the coarse-cell matrix sum_{fine cells} P_c^T K_c P_c, obtained by
+// applying the fine element operator to the prolonged unit vector and restricting the result.
+template <int MODE>
+__global__ void __launch_bounds__(192)
+k_galerkin_cells(FineView<double> F, const double* __restrict__ mat_all, TransferDev P, double* __restrict__ KeC,
+                 int ncx, int ncy, int ncz) {
+  constexpr int W = MatWidth<MODE>::value;
+  const int q = threadIdx.x;                     // 0..23
+  const int64_t C = blockIdx.x * (int64_t)blockDim.y + threadIdx.y;
+  if (C >= (int64_t)ncx * ncy * ncz) return;
+  const int CI = int(C % ncx), CJ = int((C / ncx) % ncy), CK = int(C / ((int64_t)ncx * ncy));
+  const int a = q / 3, s = q % 3;
+  const int ax = a & 1, ay = (a >> 1) & 1, az = (a >> 2) & 1;
+  double acc[24];
+#pragma unroll
+  for (int t = 0; t < 24; ++t) acc[t] = 0.0;
+  const AxisDev &X = P.ax[0], &Y = P.ax[1], &Z = P.ax[2];
+  for (int fk = Z.iv_first[CK]; fk < Z.iv_first[CK] + Z.iv_count[CK]; ++fk)
+    for (int fj = Y.iv_first[CJ]; fj < Y.iv_first[CJ] + Y.iv_count[CJ]; ++fj)
+      for (int fi = X.iv_first[CI]; fi < X.iv_first[CI] + X.iv_count[CI]; ++fi) {
+        const double* p = mat_all + (size_t)W * (fi + (int64_t)F.nx * (fj + (int64_t)F.ny * fk));
+        double m[W];
+        bool nz = false;
+#pragma unroll
+        for (int t = 0; t < W; ++t) { m[t] = p[t]; nz |= (m[t] != 0.0); }
+        if (!nz) continue;
+        // weights of the fine corners (2 per axis) toward the coarse corners (2 per axis)
+        double wxt[2][2], wyt[2][2], wzt[2][2];
+#pragma unroll
+        for (int f = 0; f < 2; ++f)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            wxt[f][c] = axis_w(X, fi + f, CI + c);
+            wyt[f][c] = axis_w(Y, fj + f, CJ + c);
+            wzt[f][c] = axis_w(Z, fk + f, CK + c);
+          }
+        double u[3][8], f[3][8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+          double v = wxt[l & 1][ax] * wyt[(l >> 1) & 1][ay] * wzt[(l >> 2) & 1][az];
+          u[0][l] = s == 0 ? v : 0.0;
+          u[1][l] = s == 1 ? v : 0.0;
+          u[2][l] = s == 2 ? v : 0.0;
+        }
+        Material<double> mt = make_material<double, MODE>(m);
+        hex8_apply(u, F.dx[fi], F.dy[fj], F.dz[fk], F.idx[fi], F.idy[fj], F.idz[fk], mt, f);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+#pragma unroll
+          for (int l = 0; l < 8; ++l) {
+            double w = wxt[l & 1][b & 1] * wyt[(l >> 1) & 1][(b >> 1) & 1] * wzt[(l >> 2) & 1][(b >> 2) & 1];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) acc[3 * b + r] += w * f[r][l];
+          }
+        }
+      }
+  double* dst = KeC + (size_t)C * 576 + q;
+#pragma unroll
+  for (int t = 0; t < 24; ++t) dst[24 * t] = acc[t];
+}
+
+// Node stencil of level 1 from the coarse-cell matrices: A1[J][o] = sum over coarse cells holding J and J+o.
+__global__ void k_cells_to_stencil(const double* __restrict__ KeC, double* __restrict__ A, int cnx, int cny, int cnz) {
+  const int o = threadIdx.x;          // 0..26
+  const int64_t n = (int64_t)cnx * cny * cnz;
+  const int64_t J = blockIdx.x * (int64_t)blockDim.y + threadIdx.y;
+  if (J >= n) return;
+  const int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+  const int jc[3] = {jx, jy, jz}, nn[3] = {cnx, cny, cnz};
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int I[3][2], aJ[3][2], aK[3][2], cnt[3];
+  bool ok = true;
+  for (int d = 0; d < 3; ++d) {
+    cnt[d] = 0;
+    int K = jc[d] + od[d];
+    if (K < 0 || K >= nn[d]) { ok = false; break; }
+    for (int iv = jc[d] - 1; iv <= jc[d]; ++iv) {
+      if (iv < 0 || iv >= nn[d] - 1) continue;
+      if (K < iv || K > iv + 1) continue;
+      I[d][cnt[d]] = iv; aJ[d][cnt[d]] = jc[d] - iv; aK[d][cnt[d]] = K - iv; ++cnt[d];
+    }
+  }
+  if (ok) {
+    for (int c = 0; c < cnt[2]; ++c)
+      for (int b = 0; b < cnt[1]; ++b)
+        for (int a = 0; a < cnt[0]; ++a) {
+          int64_t C = I[0][a] + (int64_t)(cnx - 1) * (I[1][b] + (int64_t)(cny - 1) * I[2][c]);
+          int la = aJ[0][a] + 2 * aJ[1][b] + 4 * aJ[2][c];
+          int lb = aK[0][a] + 2 * aK[1][b] + 4 * aK[2][c];
+          const double* src = KeC + (size_t)C * 576;
+          for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) acc[3 * r + q] += src[(3 * la + r) * 24 + 3 * lb + q];
+        }
+  }
+  for (int t = 0; t < 9; ++t) A[(size_t)(o * 9 + t) * n + J] = acc[t];
+}
+
+__device__ __forceinline__ int64_t grid_pos(int64_t node, int64_t fnnode, const int* orig_copy) {
+  return node < fnnode ? node : (int64_t)orig_copy[node - fnnode];
+}
+
+__global__ void k_galerkin_penalty(TransferDev P, int fnx, int fny, int64_t fnnode, const int* __restrict__ orig_copy,
+                                   int npen, const int* __restrict__ pen_node, const double* __restrict__ pen_k,
+                                   double* __restrict__ A, int cnx, int cny, int64_t cn) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= npen) return;
+  int64_t o = grid_pos(pen_node[e], fnnode, orig_copy);
+  int p[3] = {int(o % fnx), int((o / fnx) % fny), int(o / ((int64_t)fnx * fny))};
+  int J[3][2], ns[3];
+  double w[3][2];
+  for (int d = 0; d < 3; ++d) ns[d] = axis_support(P.ax[d], p[d], J[d], w[d]);
+  for (int c1 = 0; c1 < ns[2]; ++c1) for (int b1 = 0; b1 < ns[1]; ++b1) for (int a1 = 0; a1 < ns[0]; ++a1) {
+    int64_t Jn = J[0][a1] + (int64_t)cnx * (J[1][b1] + (int64_t)cny * J[2][c1]);
+    double wJ = w[0][a1] * w[1][b1] * w[2][c1];
+    for (int c2 = 0; c2 < ns[2]; ++c2) for (int b2 = 0; b2 < ns[1]; ++b2) for (int a2 = 0; a2 < ns[0]; ++a2) {
+      int oo = (J[0][a2] - J[0][a1] + 1) + 3 * (J[1][b2] - J[1][b1] + 1) + 9 * (J[2][c2] - J[2][c1] + 1);
+      double wK = w[0][a2] * w[1][b2] * w[2][c2];
+      for (int c = 0; c < 3; ++c) atomicAdd(A + (size_t)(oo * 9 + 4 * c) * cn + Jn, wJ * wK * pen_k[3 * e + c]);
+    }
+  }
+}
+
+__global__ void k_galerkin_local(TransferDev P, int fnx, int fny, int64_t fnnode, const int* __restrict__ orig_copy,
+                                 int nent, const int* __restrict__ rdof, const int* __restrict__ cdof,
+                                 const double* __restrict__ val, double* __restrict__ A, int cnx, int cny, int64_t cn) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  int64_t orow = grid_pos(rdof[e] / 3, fnnode, orig_copy), ocol = grid_pos(cdof[e] / 3, fnnode, orig_copy);
+  int r = rdof[e] % 3, c = cdof[e] % 3;
+  int pr[3] = {int(orow % fnx), int((orow / fnx) % fny), int(orow / ((int64_t)fnx * fny))};
+  int pc[3] = {int(ocol % fnx), int((ocol / fnx) % fny), int(ocol / ((int64_t)fnx * fny))};
+  int Jr[3][2], Jc[3][2], nr[3], nc[3];
+  double wr[3][2], wc[3][2];
+  for (int d = 0; d < 3; ++d) {
+    nr[d] = axis_support(P.ax[d], pr[d], Jr[d], wr[d]);
+    nc[d] = axis_support(P.ax[d], pc[d], Jc[d], wc[d]);
+  }
+  for (int c1 = 0; c1 < nr[2]; ++c1) for (int b1 = 0; b1 < nr[1]; ++b1) for (int a1 = 0; a1 < nr[0]; ++a1) {
+    int64_t Jn = Jr[0][a1] + (int64_t)cnx * (Jr[1][b1] + (int64_t)cny * Jr[2][c1]);
+    double wJ = wr[0][a1] * wr[1][b1] * wr[2][c1];
+    for (int c2 = 0; c2 < nc[2]; ++c2) for (int b2 = 0; b2 < nc[1]; ++b2) for (int a2 = 0; a2 < nc[0]; ++a2) {
+      int dx = Jc[0][a2] - Jr[0][a1], dy = Jc[1][b2] - Jr[1][b1], dz = Jc[2][c2] - Jr[2][c1];
+      if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;   // not local: excluded on the host
+      int oo = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+      double wK = wc[0][a2] * wc[1][b2] * wc[2][c2];
+      atomicAdd(A + (size_t)(oo * 9 + 3 * r + c) * cn + Jn, wJ * wK * val[e]);
+    }
+  }
+}
+
+// A_c[J][o] = sum_{i in fan(J)} sum_{i' in fan(J+o), |i'-i| <= 1} P[i,J] A_f[i][i'-i] P[i',J+o]
+__global__ void k_galerkin_stencil(TransferDev P, const double* __restrict__ Af, int fnx, int fny, int fnz,
+                                   double* __restrict__ Ac, int cnx, int cny, int cnz) {
+  const int o = threadIdx.x;
+  const int64_t nc = (int64_t)cnx * cny * cnz, nf = (int64_t)fnx * fny * fnz;
+  const int64_t J = blockIdx.x * (int64_t)blockDim.y + threadIdx.y;
+  if (J >= nc) return;
+  const int jc[3] = {int(J % cnx), int((J / cnx) % cny), int(J / ((int64_t)cnx * cny))};
+  const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+  const int nn[3] = {cnx, cny, cnz};
+  // per axis: pairs (i, i'-i, weight)
+  int pi[3][9], pd[3][9], np[3];
+  double pw[3][9];
+  bool ok = true;
+  for (int d = 0; d < 3; ++d) {
+    np[d] = 0;
+    int K = jc[d] + od[d];
+    if (K < 0 || K >= nn[d]) { ok = false; break; }
+    int I[3]; double w[3];
+    int nI = axis_fan(P.ax[d], jc[d], I, w);
+    for (int t = 0; t < nI; ++t)
+      for (int dd = -1; dd <= 1; ++dd) {
+        int i2 = I[t] + dd;
+        if (i2 < 0 || i2 >= P.ax[d].nf) continue;
+        double w2 = axis_w(P.ax[d], i2, K);
+        if (w2 == 0.0) continue;
+        pi[d][np[d]] = I[t]; pd[d][np[d]] = dd; pw[d][np[d]] = w[t] * w2; ++np[d];
+      }
+  }
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (ok) {
+    for (int c = 0; c < np[2]; ++c)
+      for (int b = 0; b < np[1]; ++b)
+        for (int a = 0; a < np[0]; ++a) {
+          int64_t f = pi[0][a] + (int64_t)fnx * (pi[1][b] + (int64_t)fny * pi[2][c]);
+          int of = (pd[0][a] + 1) + 3 * (pd[1][b] + 1) + 9 * (pd[2][c] + 1);
+          double w = pw[0][a] * pw[1][b] * pw[2][c];
+          const double* src = Af + (size_t)(of * 9) * nf + f;
+#pragma unroll
+          for (int t = 0; t < 9; ++t) acc[t] += w * src[(size_t)t * nf];
+        }
+  }
+  for (int t = 0; t < 9; ++t) Ac[(size_t)(o * 9 + t) * nc + J] = acc[t];
+}
+
+__global__ void k_stencil_diag(const double* __restrict__ A, int64_t n, double* __restrict__ D) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int t = 0; t < 9; ++t) D[9 * i + t] = A[(size_t)(13 * 9 + t) * n + i];
+}
+
+__global__ void k_add_diag_entries(int nent, const int* __restrict__ rdof, const int* __restrict__ cdof,
+                                   const double* __restrict__ val, double* __restrict__ D) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  int64_t n = rdof[e] / 3;
+  atomicAdd(D + 9 * n + 3 * (rdof[e] % 3) + cdof[e] % 3, val[e]);
+}
+
+__global__ void k_block_inverse(const double* __restrict__ D, int64_t n, double* __restrict__ Di64,
+                                float* __restrict__ Di32) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a[9];
+  for (int t = 0; t < 9; ++t) a[t] = D[9 * i + t];
+  double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+  double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  double inv[9];
+  if (fabs(det) < 1e-30) {
+    for (int t = 0; t < 9; ++t) inv[t] = (t % 4 == 0) ? 1.0 : 0.0;
+  } else {
+    double id = 1.0 / det;
+    inv[0] = c00 * id;
+    inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    inv[3] = c01 * id;
+    inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    inv[6] = c02 * id;
+    inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+  }
+  for (int t = 0; t < 9; ++t) {
+    Di64[(size_t)t * n + i] = inv[t];
+    if (Di32) Di32[(size_t)t * n + i] = float(inv[t]);
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s) {
+  k_stencil_apply<T><<<div_up(L.n, kThreads), kThreads, 0, s>>>(L, u, y, skip);
+  if (L.nrow > 0) launch_csr_add<T>(L.nrow, L.row_dof, L.row_ptr, L.col, L.val, u, y, skip, s);
+}
+
+template <typename T>
+void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,
+                    const int* skip, cudaStream_t s) {
+  if (nrow <= 0) return;
+  k_csr_add<T><<<div_up(nrow, kThreads), kThreads, 0, s>>>(nrow, row_dof, row_ptr, col, val, u, y, skip);
+}
+
+template <typename T>
+void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
+                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s) {
+  int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
+  k_restrict_grid<T><<<div_up(nc, kThreads), kThreads, 0, s>>>(P, fnx, fny, rf, rc, skip);
+  if (fntotal > fnnode)
+    k_restrict_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
+                                                                                 orig_copy, rf, rc, skip);
+  (void)fnz;
+}
+
+template <typename T>
+void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
+                        const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
+                        cudaStream_t s) {
+  k_prolong_add<T><<<div_up(fntotal, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal, orig_copy, used, xc,
+                                                                  xf, skip);
+  (void)fnz;
+}
+
+void launch_kept_mask(const TransferDev& P, const uint8_t* used_f, uint8_t* kept_c, cudaStream_t s) {
+  int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
+  k_kept_mask<<<div_up(nc, kThreads), kThreads, 0, s>>>(P, used_f, kept_c);
+}
+
+template <int MODE>
+void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, const TransferDev& P, double* KeC,
+                           double* A1, int cnx, int cny, int cnz, cudaStream_t s) {
+  int ncx = cnx - 1, ncy = cny - 1, ncz = cnz - 1;
+  int64_t ncell = (int64_t)ncx * ncy * ncz;
+  dim3 blk(24, 8);
+  k_galerkin_cells<MODE><<<div_up(ncell, 8), blk, 0, s>>>(F, mat_all, P, KeC, ncx, ncy, ncz);
+  int64_t n = (int64_t)cnx * cny * cnz;
+  dim3 blk2(27, 8);
+  k_cells_to_stencil<<<div_up(n, 8), blk2, 0, s>>>(KeC, A1, cnx, cny, cnz);
+}
+
+void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
+                             const int* pen_node, const double* pen_k, double* A1, int cnx, int cny, int cnz,
+                             int64_t cn, cudaStream_t s) {
+  if (npen <= 0) return;
+  k_galerkin_penalty<<<div_up(npen, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, orig_copy, npen, pen_node,
+                                                                  pen_k, A1, cnx, cny, cn);
+  (void)cnz;
+}
+
+void launch_galerkin_local(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int nent,
+                           const int* rdof, const int* cdof, const double* val, double* A1, int cnx, int cny, int cnz,
+                           int64_t cn, cudaStream_t s) {
+  if (nent <= 0) return;
+  k_galerkin_local<<<div_up(nent, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, orig_copy, nent, rdof, cdof, val,
+                                                                A1, cnx, cny, cn);
+  (void)cnz;
+}
+
+void launch_galerkin_stencil(const TransferDev& P, const double* Af, int fnx, int fny, int fnz, double* Ac, int cnx,
+                             int cny, int cnz, cudaStream_t s) {
+  int64_t n = (int64_t)cnx * cny * cnz;
+  dim3 blk(27, 8);
+  k_galerkin_stencil<<<div_up(n, 8), blk, 0, s>>>(P, Af, fnx, fny, fnz, Ac, cnx, cny, cnz);
+}
+
+void launch_stencil_diag(const double* A, int64_t n, double* D, cudaStream_t s) {
+  k_stencil_diag<<<div_up(n, kThreads), kThreads, 0, s>>>(A, n, D);
+}
+
+void launch_add_diag_entries(int nent, const int* rdof, const int* cdof, const double* val, double* D, cudaStream_t s) {
+  if (nent <= 0) return;
+  k_add_diag_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, D);
+}
+
+void launch_block_inverse(const double* D, int64_t n, double* Dinv64, float* Dinv32, cudaStream_t s) {
+  k_block_inverse<<<div_up(n, kThreads), kThreads, 0, s>>>(D, n, Dinv64, Dinv32);
+}
+
+template void launch_stencil_apply<float>(const StencilView<float>&, const float*, float*, const int*, cudaStream_t);
+template void launch_stencil_apply<double>(const StencilView<double>&, const double*, double*, const int*, cudaStream_t);
+template void launch_csr_add<float>(int, const int*, const int*, const int*, const float*, const float*, float*,
+                                    const int*, cudaStream_t);
+template void launch_csr_add<double>(int, const int*, const int*, const int*, const double*, const double*, double*,
+                                     const int*, cudaStream_t);
+template void launch_restrict<float>(const TransferDev&, int, int, int, int64_t, int64_t, const int*, const float*,
+                                     float*, const int*, cudaStream_t);
+template void launch_restrict<double>(const TransferDev&, int, int, int, int64_t, int64_t, const int*, const double*,
+                                      double*, const int*, cudaStream_t);
+template void launch_prolong_add<float>(const TransferDev&, int, int, int, int64_t, int64_t, const int*,
+                                        const uint8_t*, const float*, float*, const int*, cudaStream_t);
+template void launch_prolong_add<double>(const TransferDev&, int, int, int, int64_t, int64_t, const int*,
+                                         const uint8_t*, const double*, double*, const int*, cudaStream_t);
+template void launch_galerkin_cells<MAT_ISO_SRI>(const FineView<double>&, const double*, const TransferDev&, double*,
+                                                 double*, int, int, int, cudaStream_t);
+template void launch_galerkin_cells<MAT_ISO_FULL>(const FineView<double>&, const double*, const TransferDev&, double*,
+                                                  double*, int, int, int, cudaStream_t);
+template void launch_galerkin_cells<MAT_ORTHO>(const FineView<double>&, const double*, const TransferDev&, double*,
+                                               double*, int, int, int, cudaStream_t);
+
+}  // namespace feb

@@ -1,0 +1,78 @@
+// Coarse multigrid levels: 27-point 3x3-block stencils on structured node grids, structured transfers,
+// and the Galerkin products P^T A P built on the device.
+#pragma once
+#include "common.cuh"
+#include "fine.cuh"
+
+namespace feb {
+
+// 1-D linear prolongation of one axis from every other node plus the last one (fe/gmg.py:7-26).
+struct AxisDev {
+  int nf, nc;                      // fine / coarse node counts
+  const int* ca; const int* cb;    // per fine node: coarse neighbours a <= b (a == b for coincident nodes)
+  const double* wa; const double* wb;
+  const int* cidx;                 // per coarse node: fine node index
+  const int* iv_first;             // per coarse interval [J, J+1]: first fine cell
+  const int* iv_count;             //   and number of fine cells (1 or 2)
+};
+
+struct TransferDev {
+  AxisDev ax[3];
+};
+
+// Structured level (>= 1): nodes nx*ny*nz (x fastest), stencil A[o*9 + 3r + c][n], o = (dx+1) + 3(dy+1) + 9(dz+1)
+template <typename T>
+struct StencilView {
+  int nx, ny, nz;
+  int64_t n;
+  const T* A;
+  // sparse remainder (entries the stencil cannot hold), CSR over dofs with entries
+  int nrow; const int* row_dof; const int* row_ptr; const int* col; const T* val;
+};
+
+template <typename T>
+void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s);
+
+template <typename T>
+void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,
+                    const int* skip, cudaStream_t s);
+
+// r_c = P^T r_f.  Fine level given by its grid dims; copies (ids >= nnode) are folded through `orig`.
+template <typename T>
+void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
+                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s);
+
+// x_f += P x_c on used fine nodes (copies take their grid node's value).
+template <typename T>
+void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
+                        const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
+                        cudaStream_t s);
+
+// kept[J] = some used fine node interpolates from coarse node J (fe/gmg.py:95)
+void launch_kept_mask(const TransferDev& P, const uint8_t* used_f, uint8_t* kept_c, cudaStream_t s);
+
+// Level-1 stencil from the fine cells (P^T K_cells P), KeC scratch: ncoarse_cells x 576 doubles.
+template <int MODE>
+void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, const TransferDev& P, double* KeC,
+                           double* A1, int cnx, int cny, int cnz, cudaStream_t s);
+
+// Fold diagonal penalties / local extra entries of level 0 into the level-1 stencil.
+void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
+                             const int* pen_node, const double* pen_k, double* A1, int cnx, int cny, int cnz,
+                             int64_t cn, cudaStream_t s);
+void launch_galerkin_local(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int nent,
+                           const int* rdof, const int* cdof, const double* val, double* A1, int cnx, int cny, int cnz,
+                           int64_t cn, cudaStream_t s);
+
+// Stencil Galerkin: A_c = P^T A_f P for structured levels.
+void launch_galerkin_stencil(const TransferDev& P, const double* Af, int fnx, int fny, int fnz, double* Ac, int cnx,
+                             int cny, int cnz, cudaStream_t s);
+
+// Diagonal 3x3 blocks of a stencil into D[n][9].
+void launch_stencil_diag(const double* A, int64_t n, double* D, cudaStream_t s);
+// D[node][3r+c] += v for a list of (dof row, dof col, v) with equal nodes.
+void launch_add_diag_entries(int nent, const int* rdof, const int* cdof, const double* val, double* D, cudaStream_t s);
+// Inverse of every diagonal block, |det| < 1e-30 -> identity (fe/gmg.py:29-44); output SoA [9][n].
+void launch_block_inverse(const double* D, int64_t n, double* Dinv64, float* Dinv32, cudaStream_t s);
+
+}  // namespace feb

@@ -1,0 +1,1309 @@
+// Solver runtime: device-side set-up of the operator and the multigrid hierarchy, V-cycle, CG with
+// device-resident scalars (graph-captured iterations), FP64 iterative refinement, and the C ABI.
+//
+// Reference algorithm: fe/gmg.py (GMG + PCG), rb/gpusolve.py (GPU variant: FP64 CG, FP32 V-cycle,
+// dense FP64 coarse solve, rigid-mode correction), rb/splitfe.py:123-158 (split-node solve).
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <unordered_map>
+#include <vector>
+
+#include "coarse.cuh"
+#include "dense.cuh"
+#include "fine.cuh"
+#include "rigid.cuh"
+#include "vec.cuh"
+
+namespace feb {
+
+static thread_local char g_err[512] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+namespace {
+
+constexpr int kMaxLevels = 8;
+
+// ------------------------------------------------------------------------------------------------ memory
+class Pool {
+ public:
+  explicit Pool(cudaStream_t s) : s_(s) {}
+  ~Pool() { release(); }
+  template <typename T>
+  int alloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return FEB_OK;
+    cudaError_t e = cudaMallocAsync((void**)p, n * sizeof(T), s_);
+    if (e != cudaSuccess) {
+      set_last_error("cudaMallocAsync(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? FEB_ERR_NOMEM : FEB_ERR_CUDA;
+    }
+    ptrs_.push_back((void*)*p);
+    return FEB_OK;
+  }
+  template <typename T>
+  int zeros(T** p, size_t n) {
+    FEB_TRY(alloc(p, n));
+    if (n) FEB_CUDA(cudaMemsetAsync(*p, 0, n * sizeof(T), s_));
+    return FEB_OK;
+  }
+  template <typename T>
+  int upload(T** p, const T* h, size_t n) {
+    FEB_TRY(alloc(p, n));
+    if (n) FEB_CUDA(cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, s_));
+    return FEB_OK;
+  }
+  void free(void* p) {
+    if (!p) return;
+    auto it = std::find(ptrs_.begin(), ptrs_.end(), p);
+    if (it != ptrs_.end()) {
+      cudaFreeAsync(p, s_);
+      ptrs_.erase(it);
+    }
+  }
+  void release() {
+    for (void* p : ptrs_) cudaFreeAsync(p, s_);
+    ptrs_.clear();
+  }
+
+ private:
+  cudaStream_t s_;
+  std::vector<void*> ptrs_;
+};
+
+// ------------------------------------------------------------------------------------------------ host helpers
+struct AxisHost {
+  int nf = 0, nc = 0;
+  std::vector<int> ca, cb, cidx, iv_first, iv_count;
+  std::vector<double> wa, wb, coarse;
+};
+
+// 1-D prolongation from every other node plus the last one with linear weights (fe/gmg.py:7-26)
+AxisHost make_axis(const std::vector<double>& c) {
+  AxisHost A;
+  const int n = (int)c.size();
+  A.nf = n;
+  for (int i = 0; i < n; i += 2) A.cidx.push_back(i);
+  if (A.cidx.back() != n - 1) A.cidx.push_back(n - 1);
+  A.nc = (int)A.cidx.size();
+  A.ca.resize(n); A.cb.resize(n); A.wa.resize(n); A.wb.resize(n);
+  std::vector<int> pos(n, -1);
+  for (int J = 0; J < A.nc; ++J) pos[A.cidx[J]] = J;
+  for (int i = 0; i < n; ++i) {
+    if (pos[i] >= 0) {
+      A.ca[i] = A.cb[i] = pos[i]; A.wa[i] = 1.0; A.wb[i] = 0.0;
+    } else {
+      int a = (i - 1) / 2, b = a + 1;
+      double w = (c[i] - c[A.cidx[a]]) / (c[A.cidx[b]] - c[A.cidx[a]]);
+      A.ca[i] = a; A.cb[i] = b; A.wa[i] = 1.0 - w; A.wb[i] = w;
+    }
+  }
+  for (int J = 0; J + 1 < A.nc; ++J) {
+    A.iv_first.push_back(A.cidx[J]);
+    A.iv_count.push_back(A.cidx[J + 1] - A.cidx[J]);
+  }
+  for (int J = 0; J < A.nc; ++J) A.coarse.push_back(c[A.cidx[J]]);
+  return A;
+}
+
+// host sparse entries on dofs (3 node + comp) of one level
+struct Entries {
+  std::vector<int64_t> r, c;
+  std::vector<double> v;
+  size_t size() const { return v.size(); }
+};
+
+void coo_merge(Entries& E) {
+  std::vector<size_t> idx(E.size());
+  for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return E.r[a] != E.r[b] ? E.r[a] < E.r[b] : E.c[a] < E.c[b]; });
+  Entries M;
+  for (size_t t = 0; t < idx.size(); ++t) {
+    size_t i = idx[t];
+    if (!M.v.empty() && M.r.back() == E.r[i] && M.c.back() == E.c[i]) M.v.back() += E.v[i];
+    else { M.r.push_back(E.r[i]); M.c.push_back(E.c[i]); M.v.push_back(E.v[i]); }
+  }
+  E = std::move(M);
+}
+
+// supports of a node position along each axis
+inline int supp(const AxisHost& A, int i, int (&J)[2], double (&w)[2]) {
+  int n = 0;
+  if (A.wa[i] != 0.0) { J[n] = A.ca[i]; w[n] = A.wa[i]; ++n; }
+  if (A.cb[i] != A.ca[i] && A.wb[i] != 0.0) { J[n] = A.cb[i]; w[n] = A.wb[i]; ++n; }
+  return n;
+}
+
+// P^T E P for entries E of a level whose node `pos` maps to grid positions (fnx, fny)
+Entries project(const Entries& E, const AxisHost (&ax)[3], const std::vector<int64_t>& pos_of_node_copy,
+                int64_t fnnode, int fnx, int fny) {
+  Entries out;
+  const int64_t cnx = ax[0].nc, cny = ax[1].nc;
+  auto position = [&](int64_t node) { return node < fnnode ? node : pos_of_node_copy[node - fnnode]; };
+  for (size_t e = 0; e < E.size(); ++e) {
+    int64_t pr = position(E.r[e] / 3), pc = position(E.c[e] / 3);
+    int ir[3] = {int(pr % fnx), int((pr / fnx) % fny), int(pr / ((int64_t)fnx * fny))};
+    int ic[3] = {int(pc % fnx), int((pc / fnx) % fny), int(pc / ((int64_t)fnx * fny))};
+    int Jr[3][2], Jc[3][2], nr[3], nc[3];
+    double wr[3][2], wc[3][2];
+    for (int d = 0; d < 3; ++d) { nr[d] = supp(ax[d], ir[d], Jr[d], wr[d]); nc[d] = supp(ax[d], ic[d], Jc[d], wc[d]); }
+    for (int a = 0; a < nr[0]; ++a) for (int b = 0; b < nr[1]; ++b) for (int c = 0; c < nr[2]; ++c) {
+      int64_t J = Jr[0][a] + cnx * (Jr[1][b] + cny * Jr[2][c]);
+      double wJ = wr[0][a] * wr[1][b] * wr[2][c];
+      for (int a2 = 0; a2 < nc[0]; ++a2) for (int b2 = 0; b2 < nc[1]; ++b2) for (int c2 = 0; c2 < nc[2]; ++c2) {
+        int64_t K = Jc[0][a2] + cnx * (Jc[1][b2] + cny * Jc[2][c2]);
+        out.r.push_back(3 * J + E.r[e] % 3);
+        out.c.push_back(3 * K + E.c[e] % 3);
+        out.v.push_back(wJ * wc[0][a2] * wc[1][b2] * wc[2][c2] * E.v[e]);
+      }
+    }
+  }
+  coo_merge(out);
+  return out;
+}
+
+// symmetric pseudo-inverse by cyclic Jacobi (numpy.linalg.pinv semantics: cutoff 1e-15 * max |eig|)
+std::vector<double> sym_pinv(const std::vector<double>& A0, int n) {
+  std::vector<double> A(A0), V(n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) { tot += A[i * n + j] * A[i * n + j]; if (i != j) off += A[i * n + j] * A[i * n + j]; }
+    if (off <= 1e-30 * tot) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = A[p * n + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+        double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          double akp = A[k * n + p], akq = A[k * n + q];
+          A[k * n + p] = c * akp - s * akq;
+          A[k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double apk = A[p * n + k], aqk = A[q * n + k];
+          A[p * n + k] = c * apk - s * aqk;
+          A[q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          double vkp = V[k * n + p], vkq = V[k * n + q];
+          V[k * n + p] = c * vkp - s * vkq;
+          V[k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  double mx = 0.0;
+  for (int i = 0; i < n; ++i) mx = std::max(mx, std::fabs(A[i * n + i]));
+  std::vector<double> P(n * n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    double ev = A[k * n + k];
+    if (std::fabs(ev) <= 1e-15 * mx) continue;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) P[i * n + j] += V[i * n + k] * V[j * n + k] / ev;
+  }
+  return P;
+}
+
+// ------------------------------------------------------------------------------------------------ cell set-up
+template <int W>
+__global__ void k_prepare_cells(int nx, int ny, int nz, const double* __restrict__ mat, int mode,
+                                const uint8_t* __restrict__ active, const int64_t* __restrict__ cn,
+                                double* __restrict__ mat_all, double* __restrict__ mat_s64, float* __restrict__ mat_s32,
+                                uint8_t* __restrict__ irr_flag, uint8_t* __restrict__ used) {
+  const int64_t ncell = (int64_t)nx * ny * nz;
+  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= ncell) return;
+  int k = int(r % nz), j = int((r / nz) % ny), i = int(r / ((int64_t)nz * ny));
+  int64_t xc = i + (int64_t)nx * (j + (int64_t)ny * k);
+  const int64_t nx1 = nx + 1, ny1 = ny + 1;
+  bool act = active[r] != 0;
+  bool irr = false;
+  if (act) {
+    for (int l = 0; l < 8; ++l) {
+      int64_t g = (i + (l & 1)) + nx1 * ((j + ((l >> 1) & 1)) + ny1 * (k + ((l >> 2) & 1)));
+      int64_t node = cn ? cn[8 * r + l] : g;
+      irr |= (node != g);
+      used[node] = 1;
+    }
+  }
+  double v[W];
+  for (int q = 0; q < W; ++q) v[q] = (mode == MAT_ORTHO) ? mat[W * r + q] : mat[q * ncell + r];
+  for (int q = 0; q < W; ++q) {
+    double a = act ? v[q] : 0.0, s = (act && !irr) ? v[q] : 0.0;
+    mat_all[W * xc + q] = a;
+    mat_s64[W * xc + q] = s;
+    mat_s32[W * xc + q] = float(s);
+  }
+  irr_flag[r] = (act && irr) ? 1 : 0;
+}
+
+template <int W>
+__global__ void k_build_irregular(int nx, int ny, int nz, const int64_t* __restrict__ irr_ref, int nirr,
+                                  const double* __restrict__ mat, int mode, const int64_t* __restrict__ cn,
+                                  int* __restrict__ irr_cell, int* __restrict__ irr_nodes, double* __restrict__ m64,
+                                  float* __restrict__ m32) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nirr) return;
+  const int64_t ncell = (int64_t)nx * ny * nz;
+  int64_t r = irr_ref[e];
+  int k = int(r % nz), j = int((r / nz) % ny), i = int(r / ((int64_t)nz * ny));
+  irr_cell[e] = int(i + (int64_t)nx * (j + (int64_t)ny * k));
+  for (int l = 0; l < 8; ++l) irr_nodes[8 * e + l] = int(cn[8 * r + l]);
+  for (int q = 0; q < W; ++q) {
+    double v = (mode == MAT_ORTHO) ? mat[W * r + q] : mat[q * ncell + r];
+    m64[W * e + q] = v;
+    m32[W * e + q] = float(v);
+  }
+}
+
+__global__ void k_orig_copy(const int64_t* __restrict__ orig, int64_t nnode, int64_t ntotal, int* __restrict__ out) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= ntotal - nnode) return;
+  out[e] = int(orig[nnode + e]);
+}
+
+__global__ void k_masked_copy(const double* __restrict__ src, const uint8_t* __restrict__ used, int64_t n,
+                              double* __restrict__ dst) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  dst[i] = used[i / 3] ? src[i] : 0.0;
+}
+
+__global__ void k_export(const double* __restrict__ x, const uint8_t* __restrict__ used, int64_t n,
+                         double* __restrict__ U) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  U[i] = used[i / 3] ? x[i] : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+struct Csr {
+  int nrow = 0;
+  int *row_dof = nullptr, *row_ptr = nullptr, *col = nullptr;
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+};
+
+int upload_csr(Pool& pool, const Entries& E, Csr& C) {
+  std::vector<int> rd, rp, cl;
+  std::vector<double> v;
+  std::vector<float> vf;
+  for (size_t e = 0; e < E.size(); ++e) {
+    if (rd.empty() || rd.back() != E.r[e]) { rd.push_back((int)E.r[e]); rp.push_back((int)e); }
+    cl.push_back((int)E.c[e]);
+    v.push_back(E.v[e]);
+    vf.push_back((float)E.v[e]);
+  }
+  rp.push_back((int)E.size());
+  C.nrow = (int)rd.size();
+  if (C.nrow == 0) return FEB_OK;
+  FEB_TRY(pool.upload(&C.row_dof, rd.data(), rd.size()));
+  FEB_TRY(pool.upload(&C.row_ptr, rp.data(), rp.size()));
+  FEB_TRY(pool.upload(&C.col, cl.data(), cl.size()));
+  FEB_TRY(pool.upload(&C.v64, v.data(), v.size()));
+  FEB_TRY(pool.upload(&C.v32, vf.data(), vf.size()));
+  return FEB_OK;
+}
+
+struct Level {
+  int nx = 0, ny = 0, nz = 0;             // node grid of this level
+  int64_t nnode = 0, ntotal = 0;          // grid nodes, grid nodes + copies (level 0)
+  int64_t ndof = 0;                       // 3 x used / kept nodes
+  std::vector<double> coord[3];
+  uint8_t* used = nullptr;
+  double* A64 = nullptr;                  // stencil (levels >= 1)
+  float* A32 = nullptr;
+  Csr sparse;                             // entries the stencil does not hold (levels >= 1)
+  Entries nonlocal;                       // host copy of `sparse` (projected to the next level)
+  double* Dinv64 = nullptr;
+  float* Dinv32 = nullptr;
+  AxisHost ax[3];                         // transfer to the next level
+  TransferDev P{};
+  double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr, *t64 = nullptr;
+  float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr, *t32 = nullptr;
+};
+
+}  // namespace
+}  // namespace feb
+
+using namespace feb;
+
+// own non-blocking stream (stream capture is impossible on the legacy default stream); ordered with the
+// caller's stream by events at every entry point
+static cudaStream_t make_stream() {
+  cudaStream_t st = nullptr;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  return st;
+}
+
+struct FebHandle {
+  explicit FebHandle(cudaStream_t caller_) : caller(caller_), s(make_stream()), pool(s) {
+    cudaEventCreateWithFlags(&ev_sync, cudaEventDisableTiming);
+  }
+  cudaStream_t caller;
+  cudaStream_t s;
+  Pool pool;
+  cudaEvent_t ev_sync = nullptr;
+  // work on s after everything queued so far on the caller's stream
+  int sync_in() {
+    FEB_CUDA(cudaEventRecord(ev_sync, caller));
+    FEB_CUDA(cudaStreamWaitEvent(s, ev_sync, 0));
+    return FEB_OK;
+  }
+  // the caller's stream continues after everything queued on s
+  int sync_out() {
+    FEB_CUDA(cudaEventRecord(ev_sync, s));
+    FEB_CUDA(cudaStreamWaitEvent(caller, ev_sync, 0));
+    return FEB_OK;
+  }
+  FebOptions opt{};
+  int mode = MAT_ISO_SRI;
+  int nx = 0, ny = 0, nz = 0;
+  std::vector<double> xe, ye, ze;
+  int64_t nnode = 0, ntotal = 0, ndof = 0;
+  FineView<double> F64{};
+  FineView<float> F32{};
+  int* orig_copy = nullptr;
+  std::vector<int64_t> orig_copy_h;
+  double *xe_d = nullptr, *ye_d = nullptr, *ze_d = nullptr;
+  // penalties and local extra entries of level 0, for the level-1 Galerkin product
+  int npen = 0;
+  int nlocal = 0;
+  int *loc_r = nullptr, *loc_c = nullptr;
+  double* loc_v = nullptr;
+  double* mat_all = nullptr;
+  std::vector<Level> L;
+  int coarsest = 0;
+  // dense coarsest level
+  int nd = 0;
+  double *Minv = nullptr, *bd = nullptr, *xd = nullptr;
+  int *klist = nullptr, *cmap = nullptr;
+  // scalars
+  LevelParams* lp = nullptr;
+  CgState* st = nullptr;      // outer CG
+  CgState* sti = nullptr;     // inner CG (refinement)
+  double* partials = nullptr;
+  double* sc = nullptr;       // refinement scaling
+  int* status = nullptr;
+  CgState* st_h = nullptr;    // pinned
+  // CG vectors
+  double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *fb = nullptr;
+  float *xf = nullptr, *rf = nullptr, *zf = nullptr, *pf = nullptr, *qf = nullptr;
+  // rigid modes
+  bool has_rigid = false;
+  RigidView Z{};
+  double *Einv = nullptr, *zpart = nullptr, *zr = nullptr, *zcoef = nullptr;
+  // graphs
+  cudaGraphExec_t g_outer = nullptr, g_inner = nullptr;
+  int g_outer_nodes = 0, g_inner_nodes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double t_setup_ms = 0.0;
+  int launches = 0;
+
+  ~FebHandle() {
+    if (g_outer) cudaGraphExecDestroy(g_outer);
+    if (g_inner) cudaGraphExecDestroy(g_inner);
+    if (st_h) cudaFreeHost(st_h);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    pool.release();
+    cudaStreamSynchronize(s);
+    if (ev_sync) cudaEventDestroy(ev_sync);
+    cudaStreamDestroy(s);
+  }
+
+  // ---------------------------------------------------------------------------------------------- operators
+  template <typename T>
+  const FineView<T>& fine() const;
+
+  template <typename T>
+  void apply(int l, const T* u, T* y, const int* skip) {
+    if (l == 0) {
+      const FineView<T>& F = fine<T>();
+      const int zc = 16;
+      switch (mode) {
+        case MAT_ISO_SRI: launch_fine_apply<T, MAT_ISO_SRI>(F, u, y, skip, zc, s); break;
+        case MAT_ISO_FULL: launch_fine_apply<T, MAT_ISO_FULL>(F, u, y, skip, zc, s); break;
+        default: launch_fine_apply<T, MAT_ORTHO>(F, u, y, skip, zc, s); break;
+      }
+    } else {
+      Level& V = L[l];
+      StencilView<T> S{V.nx, V.ny, V.nz, V.nnode, stencil<T>(V), V.sparse.nrow, V.sparse.row_dof, V.sparse.row_ptr,
+                       V.sparse.col, sval<T>(V)};
+      launch_stencil_apply<T>(S, u, y, skip, s);
+    }
+  }
+  template <typename T> static const T* stencil(const Level& V);
+  template <typename T> static const T* sval(const Level& V);
+  template <typename T> static const T* dinv(const Level& V);
+  template <typename T> static T* vb(Level& V);
+  template <typename T> static T* vx(Level& V);
+  template <typename T> static T* vr(Level& V);
+  template <typename T> static T* vd(Level& V);
+  template <typename T> static T* vt(Level& V);
+
+  // ---------------------------------------------------------------------------------------------- V-cycle
+  template <typename T>
+  void smooth(int l, const T* b, T* x, bool zero_start, const int* skip) {
+    Level& V = L[l];
+    const int64_t nn = V.ntotal;
+    T *r = vr<T>(V), *d = vd<T>(V), *t = vt<T>(V);
+    const T* D = dinv<T>(V);
+    if (zero_start) {
+      launch_cheb_first<T>(b, r, d, x, D, lp + l, nn, skip, s);
+    } else {
+      apply<T>(l, x, t, skip);
+      launch_cheb_init<T>(b, t, r, d, x, D, lp + l, nn, skip, s);
+    }
+    for (int k = 0; k + 1 < opt.cheb_degree; ++k) {
+      apply<T>(l, d, t, skip);
+      launch_cheb_step<T>(t, r, d, x, D, lp + l, k, nn, skip, s);
+    }
+  }
+
+  template <typename T>
+  void vcycle(int l, const T* b, T* x, const int* skip) {
+    if (l == coarsest) {
+      Level& V = L[l];
+      launch_dense_solve<T>(Minv, nd, klist, cmap, V.ntotal, b, x, bd, xd, skip, s);
+      return;
+    }
+    Level& V = L[l];
+    Level& C = L[l + 1];
+    smooth<T>(l, b, x, true, skip);
+    T *t = vt<T>(V), *r = vr<T>(V);
+    apply<T>(l, x, t, skip);
+    launch_residual<T>(b, t, r, 3 * V.ntotal, skip, s);
+    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s);
+    vcycle<T>(l + 1, vb<T>(C), vx<T>(C), skip);
+    launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), x, skip, s);
+    smooth<T>(l, b, x, false, skip);
+  }
+
+  // z = M r for the CG of precision T (FP64 CG with an FP64 or FP32 V-cycle, FP32 CG with FP32)
+  template <typename T>
+  void precondition(const T* r_, T* z_, const int* skip) {
+    const int64_t n = 3 * ntotal;
+    if constexpr (std::is_same<T, double>::value) {
+      if (opt.precision == FEB_PREC_FP64) {
+        vcycle<double>(0, r_, z_, skip);
+      } else {
+        launch_convert<double, float>(r_, rf, n, skip, s);
+        vcycle<float>(0, rf, zf, skip);
+        launch_convert<float, double>(zf, z_, n, skip, s);
+      }
+    } else {
+      vcycle<float>(0, r_, z_, skip);
+    }
+    if (has_rigid) launch_rigid_apply<T>(Z, r_, z_, zpart, zr, zcoef, Einv, skip, s);
+  }
+
+  // one CG iteration (SciPy order: z = M r, beta, p, q = A p, alpha, x, r, convergence)
+  template <typename T>
+  void cg_body(CgState* S, T* x_, T* r_, T* z_, T* p_, T* q_) {
+    const int* skip = &S->done;
+    const int64_t n = 3 * ntotal;
+    precondition<T>(r_, z_, skip);
+    launch_dot_partial<T, T>(r_, z_, n, partials, skip, s);
+    launch_finalize(FIN_RZ, partials, S, nullptr, 0, skip, s);
+    launch_update_p<T>(z_, p_, S, n, skip, s);
+    apply<T>(0, p_, q_, skip);
+    launch_dot_partial<T, T>(p_, q_, n, partials, skip, s);
+    launch_finalize(FIN_ALPHA, partials, S, nullptr, 0, skip, s);
+    launch_update_xr<T>(p_, q_, x_, r_, S, n, partials, skip, s);
+    launch_finalize(FIN_CONV, partials, S, nullptr, 0, skip, s);
+  }
+
+  int capture(CgState* S, bool inner, cudaGraphExec_t* exec, int* nodes) {
+    if (*exec) return FEB_OK;
+    cudaGraph_t g;
+    FEB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
+    else cg_body<double>(S, x, r, z, p, q);
+    FEB_CUDA(cudaStreamEndCapture(s, &g));
+    size_t nn = 0;
+    FEB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    *nodes = (int)nn;
+    FEB_CUDA(cudaGraphInstantiate(exec, g, 0));
+    FEB_CUDA(cudaGraphDestroy(g));
+    return FEB_OK;
+  }
+
+  // runs CG iterations until S->done; returns the final host copy of the state
+  int run_cg(CgState* S, bool inner, CgState& out) {
+    cudaGraphExec_t* ex = inner ? &g_inner : &g_outer;
+    int* nn = inner ? &g_inner_nodes : &g_outer_nodes;
+    if (opt.use_graphs) FEB_TRY(capture(S, inner, ex, nn));
+    const int every = std::max(1, opt.check_every);
+    for (int guard = 0; guard < 1000000; ++guard) {
+      FEB_CUDA(cudaMemcpyAsync(st_h, S, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+      FEB_CUDA(cudaStreamSynchronize(s));
+      if (st_h->done) break;
+      for (int k = 0; k < every; ++k) {
+        if (opt.use_graphs) {
+          FEB_CUDA(cudaGraphLaunch(*ex, s));
+          launches += *nn;
+        } else {
+          if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
+          else cg_body<double>(S, x, r, z, p, q);
+        }
+      }
+    }
+    FEB_CUDA(cudaGetLastError());
+    out = *st_h;
+    return FEB_OK;
+  }
+
+  // CG on K x = b in precision T from x (x0 given or zero); thr = tol ||b||
+  template <typename T>
+  int cg_start(CgState* S, const T* b, T* x_, T* r_, bool has_x0, double thr2, int maxiter) {
+    const int64_t n = 3 * ntotal;
+    CgState init{};
+    init.thr2 = thr2;
+    init.maxiter = maxiter;
+    FEB_CUDA(cudaMemcpyAsync(S, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+    if (has_x0) {
+      T* q_ = std::is_same<T, double>::value ? (T*)q : (T*)qf;
+      apply<T>(0, x_, q_, nullptr);
+      launch_residual<T>(b, q_, r_, n, nullptr, s);
+    } else {
+      FEB_CUDA(cudaMemsetAsync(x_, 0, n * sizeof(T), s));
+      FEB_CUDA(cudaMemcpyAsync(r_, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
+    launch_dot_partial<T, T>(r_, r_, n, partials, nullptr, s);
+    launch_finalize(FIN_INIT, partials, S, nullptr, 0, nullptr, s);
+    launches += has_x0 ? 6 : 2;
+    return FEB_OK;
+  }
+
+  double read_dot(const double* a, const double* b, int64_t n, int* st) {
+    launch_dot_partial<double, double>(a, b, n, partials, nullptr, s);
+    std::vector<double> h(kRedBlocks);
+    cudaError_t e = cudaMemcpyAsync(h.data(), partials, kRedBlocks * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_last_error("read_dot: %s", cudaGetErrorString(e)); *st = FEB_ERR_CUDA; return 0.0; }
+    double acc = 0.0;
+    for (double v : h) acc += v;
+    return acc;
+  }
+};
+
+template <> const FineView<double>& FebHandle::fine<double>() const { return F64; }
+template <> const FineView<float>& FebHandle::fine<float>() const { return F32; }
+template <> const double* FebHandle::stencil<double>(const Level& V) { return V.A64; }
+template <> const float* FebHandle::stencil<float>(const Level& V) { return V.A32; }
+template <> const double* FebHandle::sval<double>(const Level& V) { return V.sparse.v64; }
+template <> const float* FebHandle::sval<float>(const Level& V) { return V.sparse.v32; }
+template <> const double* FebHandle::dinv<double>(const Level& V) { return V.Dinv64; }
+template <> const float* FebHandle::dinv<float>(const Level& V) { return V.Dinv32; }
+template <> double* FebHandle::vb<double>(Level& V) { return V.b64; }
+template <> float* FebHandle::vb<float>(Level& V) { return V.b32; }
+template <> double* FebHandle::vx<double>(Level& V) { return V.x64; }
+template <> float* FebHandle::vx<float>(Level& V) { return V.x32; }
+template <> double* FebHandle::vr<double>(Level& V) { return V.r64; }
+template <> float* FebHandle::vr<float>(Level& V) { return V.r32; }
+template <> double* FebHandle::vd<double>(Level& V) { return V.d64; }
+template <> float* FebHandle::vd<float>(Level& V) { return V.d32; }
+template <> double* FebHandle::vt<double>(Level& V) { return V.t64; }
+template <> float* FebHandle::vt<float>(Level& V) { return V.t32; }
+
+
+namespace feb {
+namespace {
+
+__global__ void k_count(const uint8_t* __restrict__ m, int64_t n, unsigned long long* __restrict__ out) {
+  unsigned long long c = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    c += m[i] ? 1ull : 0ull;
+  c = block_sum(c);
+  if (threadIdx.x == 0) atomicAdd(out, c);
+}
+
+int count_mask(FebHandle* h, const uint8_t* m, int64_t n, int64_t* out) {
+  unsigned long long* d = nullptr;
+  FEB_TRY(h->pool.zeros(&d, 1));
+  k_count<<<std::min<int64_t>(div_up(n, kThreads), 4 * kSmCount), kThreads, 0, h->s>>>(m, n, d);
+  unsigned long long v = 0;
+  FEB_CUDA(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, h->s));
+  FEB_CUDA(cudaStreamSynchronize(h->s));
+  h->pool.free(d);
+  *out = (int64_t)v;
+  return FEB_OK;
+}
+
+template <typename T>
+int level_vectors(Pool& pool, Level& V, bool f64, bool f32) {
+  size_t n = 3 * (size_t)V.ntotal;
+  if (f64) {
+    FEB_TRY(pool.zeros(&V.b64, n)); FEB_TRY(pool.zeros(&V.x64, n)); FEB_TRY(pool.zeros(&V.r64, n));
+    FEB_TRY(pool.zeros(&V.d64, n)); FEB_TRY(pool.zeros(&V.t64, n));
+  }
+  if (f32) {
+    FEB_TRY(pool.zeros(&V.b32, n)); FEB_TRY(pool.zeros(&V.x32, n)); FEB_TRY(pool.zeros(&V.r32, n));
+    FEB_TRY(pool.zeros(&V.d32, n)); FEB_TRY(pool.zeros(&V.t32, n));
+  }
+  return FEB_OK;
+}
+
+int upload_transfer(Pool& pool, Level& V) {
+  for (int d = 0; d < 3; ++d) {
+    AxisHost& A = V.ax[d];
+    AxisDev& D = V.P.ax[d];
+    D.nf = A.nf; D.nc = A.nc;
+    int *ca, *cb, *cidx, *ivf, *ivc;
+    double *wa, *wb;
+    FEB_TRY(pool.upload(&ca, A.ca.data(), A.ca.size()));
+    FEB_TRY(pool.upload(&cb, A.cb.data(), A.cb.size()));
+    FEB_TRY(pool.upload(&wa, A.wa.data(), A.wa.size()));
+    FEB_TRY(pool.upload(&wb, A.wb.data(), A.wb.size()));
+    FEB_TRY(pool.upload(&cidx, A.cidx.data(), A.cidx.size()));
+    std::vector<int> f(A.iv_first), c(A.iv_count);
+    if (f.empty()) { f.push_back(0); c.push_back(0); }
+    FEB_TRY(pool.upload(&ivf, f.data(), f.size()));
+    FEB_TRY(pool.upload(&ivc, c.data(), c.size()));
+    D.ca = ca; D.cb = cb; D.wa = wa; D.wb = wb; D.cidx = cidx; D.iv_first = ivf; D.iv_count = ivc;
+  }
+  return FEB_OK;
+}
+
+// 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients
+int power_iteration(FebHandle* h, int l) {
+  Level& V = h->L[l];
+  const int64_t n = 3 * V.ntotal;
+  launch_random_start(V.x64, V.used, V.ntotal, h->opt.seed + 7919ull * (uint64_t)l, h->s);
+  launch_dot_partial<double, double>(V.x64, V.x64, n, h->partials, nullptr, h->s);
+  launch_finalize(FIN_POWER0, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
+  for (int it = 0; it < 12; ++it) {
+    h->apply<double>(l, V.x64, V.t64, nullptr);
+    launch_bj_apply_norm(V.Dinv64, V.t64, V.d64, V.ntotal, h->partials, h->s);
+    launch_finalize(FIN_POWER, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
+    launch_scale(V.d64, V.x64, h->lp + l, n, h->s);
+  }
+  FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+template <int W>
+int setup_level0(FebHandle* h, const FebOperator* op) {
+  FebHandle& H = *h;
+  cudaStream_t s = H.s;
+  const int64_t ncell = (int64_t)H.nx * H.ny * H.nz;
+  Level& V = H.L[0];
+  V.nx = H.nx + 1; V.ny = H.ny + 1; V.nz = H.nz + 1;
+  V.nnode = H.nnode; V.ntotal = H.ntotal;
+  V.coord[0] = H.xe; V.coord[1] = H.ye; V.coord[2] = H.ze;
+  // per-axis widths
+  std::vector<double> w64[3], iw64[3];
+  std::vector<float> w32[3], iw32[3];
+  const std::vector<double>* e[3] = {&H.xe, &H.ye, &H.ze};
+  double* dw64[3]; double* diw64[3]; float* dw32[3]; float* diw32[3];
+  for (int d = 0; d < 3; ++d) {
+    for (size_t i = 0; i + 1 < e[d]->size(); ++i) {
+      double w = (*e[d])[i + 1] - (*e[d])[i];
+      w64[d].push_back(w); iw64[d].push_back(1.0 / w);
+      w32[d].push_back((float)w); iw32[d].push_back((float)(1.0 / w));
+    }
+    FEB_TRY(H.pool.upload(&dw64[d], w64[d].data(), w64[d].size()));
+    FEB_TRY(H.pool.upload(&diw64[d], iw64[d].data(), iw64[d].size()));
+    FEB_TRY(H.pool.upload(&dw32[d], w32[d].data(), w32[d].size()));
+    FEB_TRY(H.pool.upload(&diw32[d], iw32[d].data(), iw32[d].size()));
+  }
+  FEB_TRY(H.pool.upload(&H.xe_d, H.xe.data(), H.xe.size()));
+  FEB_TRY(H.pool.upload(&H.ye_d, H.ye.data(), H.ye.size()));
+  FEB_TRY(H.pool.upload(&H.ze_d, H.ze.data(), H.ze.size()));
+  // cells
+  double *mat_s64;
+  float* mat_s32;
+  uint8_t* irr_flag;
+  FEB_TRY(H.pool.alloc(&H.mat_all, W * ncell));
+  FEB_TRY(H.pool.alloc(&mat_s64, W * ncell));
+  FEB_TRY(H.pool.alloc(&mat_s32, W * ncell));
+  FEB_TRY(H.pool.alloc(&irr_flag, ncell));
+  FEB_TRY(H.pool.zeros(&V.used, H.ntotal));
+  k_prepare_cells<W><<<div_up(ncell, kThreads), kThreads, 0, s>>>(H.nx, H.ny, H.nz, op->mat, H.mode, op->active, op->cn,
+                                                                  H.mat_all, mat_s64, mat_s32, irr_flag, V.used);
+  FEB_CUDA(cudaGetLastError());
+  // irregular cells, in ascending cell-id order
+  int nirr = 0;
+  int *irr_cell = nullptr, *irr_nodes = nullptr;
+  double* irr_m64 = nullptr;
+  float* irr_m32 = nullptr;
+  if (op->cn) {
+    int64_t* sel = nullptr;
+    int* nsel = nullptr;
+    FEB_TRY(H.pool.alloc(&sel, ncell));
+    FEB_TRY(H.pool.alloc(&nsel, 1));
+    size_t tb = 0;
+    thrust::counting_iterator<int64_t> cnt(0);
+    FEB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, cnt, irr_flag, sel, nsel, ncell, s));
+    uint8_t* tmp = nullptr;
+    FEB_TRY(H.pool.alloc(&tmp, tb));
+    FEB_CUDA(cub::DeviceSelect::Flagged(tmp, tb, cnt, irr_flag, sel, nsel, ncell, s));
+    FEB_CUDA(cudaMemcpyAsync(&nirr, nsel, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEB_CUDA(cudaStreamSynchronize(s));
+    if (nirr > 0) {
+      FEB_TRY(H.pool.alloc(&irr_cell, nirr));
+      FEB_TRY(H.pool.alloc(&irr_nodes, 8 * (size_t)nirr));
+      FEB_TRY(H.pool.alloc(&irr_m64, W * (size_t)nirr));
+      FEB_TRY(H.pool.alloc(&irr_m32, W * (size_t)nirr));
+      k_build_irregular<W><<<div_up(nirr, kThreads), kThreads, 0, s>>>(H.nx, H.ny, H.nz, sel, nirr, op->mat, H.mode,
+                                                                        op->cn, irr_cell, irr_nodes, irr_m64, irr_m32);
+      FEB_CUDA(cudaGetLastError());
+    }
+    H.pool.free(tmp); H.pool.free(sel); H.pool.free(nsel);
+  }
+  H.pool.free(irr_flag);
+  // copies
+  if (H.ntotal > H.nnode) {
+    if (!op->orig) { set_last_error("feb_create: nnode_total > grid nodes needs orig"); return FEB_ERR_ARG; }
+    FEB_TRY(H.pool.alloc(&H.orig_copy, H.ntotal - H.nnode));
+    k_orig_copy<<<div_up(H.ntotal - H.nnode, kThreads), kThreads, 0, s>>>(op->orig, H.nnode, H.ntotal, H.orig_copy);
+    std::vector<int> oc(H.ntotal - H.nnode);
+    FEB_CUDA(cudaMemcpyAsync(oc.data(), H.orig_copy, oc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEB_CUDA(cudaStreamSynchronize(s));
+    H.orig_copy_h.assign(oc.begin(), oc.end());
+  }
+  std::vector<uint8_t> used_h(H.ntotal);
+  FEB_CUDA(cudaMemcpyAsync(used_h.data(), V.used, H.ntotal, cudaMemcpyDeviceToHost, s));
+  FEB_CUDA(cudaStreamSynchronize(s));
+  // penalties (entries on unused nodes are dropped, fe/solver.py:213-215)
+  std::vector<int> pn;
+  std::vector<double> pk;
+  std::vector<float> pkf;
+  for (int64_t e2 = 0; e2 < op->npen; ++e2) {
+    int64_t node = op->pen_node[e2];
+    if (node < 0 || node >= H.ntotal) { set_last_error("penalty node %lld out of range", (long long)node); return FEB_ERR_ARG; }
+    if (!used_h[node]) continue;
+    pn.push_back((int)node);
+    for (int c = 0; c < 3; ++c) { pk.push_back(op->pen_k[3 * e2 + c]); pkf.push_back((float)op->pen_k[3 * e2 + c]); }
+  }
+  H.npen = (int)pn.size();
+  int* pen_node = nullptr;
+  double* pen_k64 = nullptr;
+  float* pen_k32 = nullptr;
+  FEB_TRY(H.pool.upload(&pen_node, pn.data(), pn.size()));
+  FEB_TRY(H.pool.upload(&pen_k64, pk.data(), pk.size()));
+  FEB_TRY(H.pool.upload(&pen_k32, pkf.data(), pkf.size()));
+  // extra matrix: all entries applied on level 0; local ones folded into the level-1 stencil on the
+  // device, non-local ones projected through the levels on the host
+  Entries ex;
+  for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
+    int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
+    if (rr < 0 || cc < 0 || rr >= 3 * H.ntotal || cc >= 3 * H.ntotal) {
+      set_last_error("extra entry (%lld, %lld) out of range", (long long)rr, (long long)cc);
+      return FEB_ERR_ARG;
+    }
+    if (!used_h[rr / 3] || !used_h[cc / 3]) continue;
+    ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
+  }
+  coo_merge(ex);
+  Csr c0;
+  FEB_TRY(upload_csr(H.pool, ex, c0));
+  Entries loc;
+  const int gx = H.nx + 1, gy = H.ny + 1;
+  auto pos = [&](int64_t node) { return node < H.nnode ? node : H.orig_copy_h[node - H.nnode]; };
+  for (size_t e2 = 0; e2 < ex.size(); ++e2) {
+    int64_t a = pos(ex.r[e2] / 3), b = pos(ex.c[e2] / 3);
+    int da = int(a % gx) - int(b % gx), db = int((a / gx) % gy) - int((b / gx) % gy), dc = int(a / ((int64_t)gx * gy)) - int(b / ((int64_t)gx * gy));
+    bool local = std::abs(da) <= 1 && std::abs(db) <= 1 && std::abs(dc) <= 1;
+    Entries& dst = local ? loc : V.nonlocal;
+    dst.r.push_back(ex.r[e2]); dst.c.push_back(ex.c[e2]); dst.v.push_back(ex.v[e2]);
+  }
+  H.nlocal = (int)loc.size();
+  if (H.nlocal) {
+    std::vector<int> lr(loc.r.begin(), loc.r.end()), lc(loc.c.begin(), loc.c.end());
+    FEB_TRY(H.pool.upload(&H.loc_r, lr.data(), lr.size()));
+    FEB_TRY(H.pool.upload(&H.loc_c, lc.data(), lc.size()));
+    FEB_TRY(H.pool.upload(&H.loc_v, loc.v.data(), loc.v.size()));
+  }
+  // device views
+  FineView<double>& F = H.F64;
+  FineView<float>& G = H.F32;
+  F.nx = G.nx = H.nx; F.ny = G.ny = H.ny; F.nz = G.nz = H.nz;
+  F.nxn = G.nxn = H.nx + 1; F.nyn = G.nyn = H.ny + 1; F.nzn = G.nzn = H.nz + 1;
+  F.nnode = G.nnode = H.nnode; F.ntotal = G.ntotal = H.ntotal;
+  F.dx = dw64[0]; F.dy = dw64[1]; F.dz = dw64[2]; F.idx = diw64[0]; F.idy = diw64[1]; F.idz = diw64[2];
+  G.dx = dw32[0]; G.dy = dw32[1]; G.dz = dw32[2]; G.idx = diw32[0]; G.idy = diw32[1]; G.idz = diw32[2];
+  F.mat = mat_s64; G.mat = mat_s32;
+  F.nirr = G.nirr = nirr; F.irr_cell = G.irr_cell = irr_cell; F.irr_nodes = G.irr_nodes = irr_nodes;
+  F.irr_mat = irr_m64; G.irr_mat = irr_m32;
+  F.npen = G.npen = H.npen; F.pen_node = G.pen_node = pen_node; F.pen_k = pen_k64; G.pen_k = pen_k32;
+  F.nrow = G.nrow = c0.nrow; F.row_dof = G.row_dof = c0.row_dof; F.row_ptr = G.row_ptr = c0.row_ptr;
+  F.col = G.col = c0.col; F.val = c0.v64; G.val = c0.v32;
+  // used nodes, diagonal blocks
+  FEB_TRY(count_mask(h, V.used, H.ntotal, &H.ndof));
+  H.ndof *= 3;
+  V.ndof = H.ndof;
+  double* D = nullptr;
+  FEB_TRY(H.pool.alloc(&D, 9 * (size_t)H.ntotal));
+  switch (H.mode) {
+    case MAT_ISO_SRI: launch_fine_diag<MAT_ISO_SRI>(F, D, s); break;
+    case MAT_ISO_FULL: launch_fine_diag<MAT_ISO_FULL>(F, D, s); break;
+    default: launch_fine_diag<MAT_ORTHO>(F, D, s); break;
+  }
+  FEB_TRY(H.pool.alloc(&V.Dinv64, 9 * (size_t)H.ntotal));
+  FEB_TRY(H.pool.alloc(&V.Dinv32, 9 * (size_t)H.ntotal));
+  launch_block_inverse(D, H.ntotal, V.Dinv64, V.Dinv32, s);
+  FEB_CUDA(cudaGetLastError());
+  H.pool.free(D);
+  return FEB_OK;
+}
+
+int build_dense(FebHandle* h) {
+  FebHandle& H = *h;
+  Level& V = H.L[H.coarsest];
+  const int64_t n = V.ntotal;
+  std::vector<uint8_t> mask(n);
+  FEB_CUDA(cudaMemcpyAsync(mask.data(), V.used, n, cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  std::vector<int> cmap(n, -1), klist;
+  for (int64_t i = 0; i < n; ++i)
+    if (mask[i]) { cmap[i] = (int)klist.size(); klist.push_back((int)i); }
+  H.nd = 3 * (int)klist.size();
+  if (H.nd == 0) { set_last_error("empty coarsest level"); return FEB_ERR_ARG; }
+  FEB_TRY(H.pool.upload(&H.cmap, cmap.data(), cmap.size()));
+  FEB_TRY(H.pool.upload(&H.klist, klist.data(), klist.size()));
+  FEB_TRY(H.pool.zeros(&H.Minv, (size_t)H.nd * H.nd));
+  FEB_TRY(H.pool.alloc(&H.bd, H.nd));
+  FEB_TRY(H.pool.alloc(&H.xd, H.nd));
+  if (H.coarsest == 0) {
+    switch (H.mode) {
+      case MAT_ISO_SRI: launch_dense_from_fine<MAT_ISO_SRI>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
+      case MAT_ISO_FULL: launch_dense_from_fine<MAT_ISO_FULL>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
+      default: launch_dense_from_fine<MAT_ORTHO>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
+    }
+  } else {
+    launch_dense_from_stencil(V.A64, V.nx, V.ny, V.nz, H.cmap, H.Minv, H.nd, H.s);
+    if (V.nonlocal.size()) {
+      std::vector<int> rr(V.nonlocal.r.begin(), V.nonlocal.r.end()), cc(V.nonlocal.c.begin(), V.nonlocal.c.end());
+      int *dr, *dc;
+      double* dv;
+      FEB_TRY(H.pool.upload(&dr, rr.data(), rr.size()));
+      FEB_TRY(H.pool.upload(&dc, cc.data(), cc.size()));
+      FEB_TRY(H.pool.upload(&dv, V.nonlocal.v.data(), V.nonlocal.v.size()));
+      launch_dense_add_entries((int)rr.size(), dr, dc, dv, H.cmap, H.Minv, H.nd, H.s);
+    }
+  }
+  double* scratch = nullptr;
+  FEB_TRY(H.pool.alloc(&scratch, dense_scratch_doubles(H.nd)));
+  FEB_CUDA(cudaMemsetAsync(H.status, 0, sizeof(int), H.s));
+  launch_dense_invert(H.Minv, H.nd, scratch, H.status, H.s);
+  FEB_CUDA(cudaGetLastError());
+  int st = 0;
+  FEB_CUDA(cudaMemcpyAsync(&st, H.status, sizeof(int), cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  H.pool.free(scratch);
+  if (st != 0) { set_last_error("coarsest-level matrix (%d dofs) is not positive definite", H.nd); return FEB_ERR_COARSE; }
+  return FEB_OK;
+}
+
+int build_hierarchy(FebHandle* h) {
+  FebHandle& H = *h;
+  const bool f32 = H.opt.precision != FEB_PREC_FP64;
+  if (H.opt.max_levels <= 0) {   // operator only: K.u is available, no multigrid (feb_solve refuses)
+    H.coarsest = -1;
+    return FEB_OK;
+  }
+  const int maxl = std::min(H.opt.max_levels, kMaxLevels);
+  int l = 0;
+  while (true) {
+    Level& V = H.L[l];
+    if (V.ndof <= H.opt.min_dofs || l == maxl - 1) { H.coarsest = l; break; }
+    // transfer l -> l+1
+    for (int d = 0; d < 3; ++d) V.ax[d] = make_axis(V.coord[d]);
+    FEB_TRY(upload_transfer(H.pool, V));
+    H.L.emplace_back();
+    Level& C = H.L.back();
+    Level& F = H.L[l];   // reference again after emplace_back
+    C.nx = F.ax[0].nc; C.ny = F.ax[1].nc; C.nz = F.ax[2].nc;
+    C.nnode = C.ntotal = (int64_t)C.nx * C.ny * C.nz;
+    for (int d = 0; d < 3; ++d) C.coord[d] = F.ax[d].coarse;
+    FEB_TRY(H.pool.alloc(&C.used, C.ntotal));
+    launch_kept_mask(F.P, F.used, C.used, H.s);
+    int64_t kept = 0;
+    FEB_TRY(count_mask(h, C.used, C.ntotal, &kept));
+    C.ndof = 3 * kept;
+    FEB_TRY(H.pool.zeros(&C.A64, 243 * (size_t)C.ntotal));
+    if (l == 0) {
+      double* KeC = nullptr;
+      FEB_TRY(H.pool.alloc(&KeC, 576 * (size_t)(C.nx - 1) * (C.ny - 1) * (C.nz - 1)));
+      switch (H.mode) {
+        case MAT_ISO_SRI: launch_galerkin_cells<MAT_ISO_SRI>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+        case MAT_ISO_FULL: launch_galerkin_cells<MAT_ISO_FULL>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+        default: launch_galerkin_cells<MAT_ORTHO>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+      }
+      FEB_CUDA(cudaGetLastError());
+      H.pool.free(KeC);
+      launch_galerkin_penalty(F.P, F.nx, F.ny, F.nnode, H.orig_copy, H.npen, H.F64.pen_node, H.F64.pen_k, C.A64, C.nx,
+                              C.ny, C.nz, C.ntotal, H.s);
+      launch_galerkin_local(F.P, F.nx, F.ny, F.nnode, H.orig_copy, H.nlocal, H.loc_r, H.loc_c, H.loc_v, C.A64, C.nx,
+                            C.ny, C.nz, C.ntotal, H.s);
+    } else {
+      launch_galerkin_stencil(F.P, F.A64, F.nx, F.ny, F.nz, C.A64, C.nx, C.ny, C.nz, H.s);
+    }
+    FEB_CUDA(cudaGetLastError());
+    C.nonlocal = project(F.nonlocal, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
+    FEB_TRY(upload_csr(H.pool, C.nonlocal, C.sparse));
+    if (f32) {
+      FEB_TRY(H.pool.alloc(&C.A32, 243 * (size_t)C.ntotal));
+      launch_convert<double, float>(C.A64, C.A32, 243 * (int64_t)C.ntotal, nullptr, H.s);
+    }
+    l += 1;
+    bool last = (C.ndof <= H.opt.min_dofs) || (l == maxl - 1);
+    if (!last) {
+      double* D = nullptr;
+      FEB_TRY(H.pool.alloc(&D, 9 * (size_t)C.ntotal));
+      launch_stencil_diag(C.A64, C.ntotal, D, H.s);
+      std::vector<int> dr, dc;
+      std::vector<double> dv;
+      for (size_t e = 0; e < C.nonlocal.size(); ++e)
+        if (C.nonlocal.r[e] / 3 == C.nonlocal.c[e] / 3) {
+          dr.push_back((int)C.nonlocal.r[e]); dc.push_back((int)C.nonlocal.c[e]); dv.push_back(C.nonlocal.v[e]);
+        }
+      if (!dr.empty()) {
+        int *ddr, *ddc;
+        double* ddv;
+        FEB_TRY(H.pool.upload(&ddr, dr.data(), dr.size()));
+        FEB_TRY(H.pool.upload(&ddc, dc.data(), dc.size()));
+        FEB_TRY(H.pool.upload(&ddv, dv.data(), dv.size()));
+        launch_add_diag_entries((int)dr.size(), ddr, ddc, ddv, D, H.s);
+      }
+      FEB_TRY(H.pool.alloc(&C.Dinv64, 9 * (size_t)C.ntotal));
+      if (f32) FEB_TRY(H.pool.alloc(&C.Dinv32, 9 * (size_t)C.ntotal));
+      launch_block_inverse(D, C.ntotal, C.Dinv64, C.Dinv32, H.s);
+      FEB_CUDA(cudaGetLastError());
+      H.pool.free(D);
+    }
+  }
+  // work vectors and smoother parameters
+  for (int k = 0; k <= H.coarsest; ++k) {
+    Level& V = H.L[k];
+    FEB_TRY(level_vectors<double>(H.pool, V, true, f32));
+  }
+  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(power_iteration(h, k));
+  FEB_TRY(build_dense(h));
+  return FEB_OK;
+}
+
+int env_flag(const char* name) {
+  const char* v = std::getenv(name);
+  return v && *v && std::strcmp(v, "0") != 0;
+}
+
+}  // namespace
+}  // namespace feb
+
+// ================================================================================================== C ABI
+extern "C" {
+
+const char* feb_last_error(void) { return g_err; }
+
+void feb_default_options(FebOptions* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = FEB_PREC_FP64;
+  o->maxiter = 800;
+  o->tol = 1e-6;
+  o->min_dofs = 6000;
+  o->max_levels = 6;
+  o->cheb_degree = 3;
+  o->check_every = 1;
+  o->inner_tol = 1e-3;
+  o->inner_maxiter = 200;
+  o->use_graphs = 1;
+  o->seed = 0;
+}
+
+int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt, void* stream, FebHandle** out) {
+  if (!grid || !op || !out || !grid->xe || !grid->ye || !grid->ze || !op->mat || !op->active) {
+    set_last_error("feb_create: null argument");
+    return FEB_ERR_ARG;
+  }
+  *out = nullptr;
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) { set_last_error("feb_create: empty grid"); return FEB_ERR_ARG; }
+  if (op->mat_mode < 0 || op->mat_mode > 2) { set_last_error("feb_create: bad mat_mode"); return FEB_ERR_ARG; }
+  FebHandle* h = new FebHandle((cudaStream_t)stream);
+  if (opt) h->opt = *opt; else feb_default_options(&h->opt);
+  if (h->opt.cheb_degree < 1 || h->opt.cheb_degree > 9) { delete h; set_last_error("cheb_degree must be 1..9"); return FEB_ERR_ARG; }
+  h->mode = op->mat_mode;
+  h->nx = grid->nx; h->ny = grid->ny; h->nz = grid->nz;
+  h->xe.assign(grid->xe, grid->xe + grid->nx + 1);
+  h->ye.assign(grid->ye, grid->ye + grid->ny + 1);
+  h->ze.assign(grid->ze, grid->ze + grid->nz + 1);
+  h->nnode = (int64_t)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1);
+  h->ntotal = op->nnode_total > 0 ? op->nnode_total : h->nnode;
+  if (h->ntotal < h->nnode || h->ntotal > INT32_MAX / 3) { delete h; set_last_error("feb_create: bad nnode_total"); return FEB_ERR_ARG; }
+  cudaEventCreate(&h->ev0);
+  cudaEventCreate(&h->ev1);
+  if (h->sync_in() != FEB_OK) { delete h; return FEB_ERR_CUDA; }
+  cudaEventRecord(h->ev0, h->s);
+  int st = FEB_OK;
+  do {
+    h->L.reserve(kMaxLevels);
+    h->L.emplace_back();
+    if ((st = h->pool.alloc(&h->lp, kMaxLevels)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->st, 1)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->sti, 1)) != FEB_OK) break;
+    if ((st = h->pool.alloc(&h->partials, kRedBlocks)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->sc, 4)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->status, 1)) != FEB_OK) break;
+    if (cudaMallocHost(&h->st_h, sizeof(CgState)) != cudaSuccess) { st = FEB_ERR_CUDA; set_last_error("cudaMallocHost"); break; }
+    st = (h->mode == MAT_ORTHO) ? setup_level0<6>(h, op) : setup_level0<2>(h, op);
+    if (st != FEB_OK) break;
+    st = build_hierarchy(h);
+    if (st != FEB_OK) break;
+    const size_t n = 3 * (size_t)h->ntotal;
+    if ((st = h->pool.zeros(&h->x, n)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->r, n)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->z, n)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->p, n)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->q, n)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->fb, n)) != FEB_OK) break;
+    if (h->opt.precision != FEB_PREC_FP64) {
+      if ((st = h->pool.zeros(&h->xf, n)) != FEB_OK) break;
+      if ((st = h->pool.zeros(&h->rf, n)) != FEB_OK) break;
+      if ((st = h->pool.zeros(&h->zf, n)) != FEB_OK) break;
+      if ((st = h->pool.zeros(&h->pf, n)) != FEB_OK) break;
+      if ((st = h->pool.zeros(&h->qf, n)) != FEB_OK) break;
+    }
+    h->pool.free(h->mat_all);
+    h->mat_all = nullptr;
+  } while (0);
+  if (st == FEB_OK) {
+    cudaEventRecord(h->ev1, h->s);
+    if (cudaEventSynchronize(h->ev1) != cudaSuccess) { st = FEB_ERR_CUDA; set_last_error("feb_create: %s", cudaGetErrorString(cudaGetLastError())); }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->t_setup_ms = ms;
+  }
+  if (st != FEB_OK) {
+    delete h;
+    return st;
+  }
+  h->sync_out();
+  *out = h;
+  return FEB_OK;
+}
+
+int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, const int64_t* nodes) {
+  if (!h || ngroups < 0 || (ngroups > 0 && (!offsets || !nodes))) { set_last_error("feb_set_rigid_groups: bad argument"); return FEB_ERR_ARG; }
+  FebHandle& H = *h;
+  FEB_TRY(H.sync_in());
+  H.has_rigid = false;
+  if (H.g_outer) { cudaGraphExecDestroy(H.g_outer); H.g_outer = nullptr; }
+  if (H.g_inner) { cudaGraphExecDestroy(H.g_inner); H.g_inner = nullptr; }
+  if (ngroups == 0) return FEB_OK;
+  // keep used nodes of every group, drop groups with fewer than 4 (rb/splitfe.py:105-112)
+  const int64_t total = offsets[ngroups];
+  std::vector<int64_t> nh(total);
+  FEB_CUDA(cudaMemcpyAsync(nh.data(), nodes, total * sizeof(int64_t), cudaMemcpyDeviceToHost, H.s));
+  std::vector<uint8_t> used(H.ntotal);
+  FEB_CUDA(cudaMemcpyAsync(used.data(), H.L[0].used, H.ntotal, cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  std::vector<int> off(1, 0);
+  std::vector<int64_t> kept;
+  for (int g = 0; g < ngroups; ++g) {
+    std::vector<int64_t> gn;
+    for (int64_t e = offsets[g]; e < offsets[g + 1]; ++e) {
+      int64_t n = nh[e];
+      if (n < 0 || n >= H.ntotal) { set_last_error("group node %lld out of range", (long long)n); return FEB_ERR_ARG; }
+      if (used[n]) gn.push_back(n);
+    }
+    if (gn.size() < 4) continue;
+    kept.insert(kept.end(), gn.begin(), gn.end());
+    off.push_back((int)kept.size());
+  }
+  const int G = (int)off.size() - 1;
+  if (G == 0) return FEB_OK;
+  int* doff;
+  int64_t* dnodes;
+  double* cen;
+  FEB_TRY(H.pool.upload(&doff, off.data(), off.size()));
+  FEB_TRY(H.pool.upload(&dnodes, kept.data(), kept.size()));
+  FEB_TRY(H.pool.alloc(&cen, 3 * (size_t)G));
+  RigidView& Z = H.Z;
+  Z.ngroups = G; Z.off = doff; Z.nodes = dnodes; Z.cen = cen;
+  Z.nxn = H.nx + 1; Z.nyn = H.ny + 1; Z.nnode = H.nnode; Z.orig_copy = H.orig_copy;
+  Z.xe = H.xe_d; Z.ye = H.ye_d; Z.ze = H.ze_d;
+  launch_centroids(Z, cen, H.s);
+  const int nc = 6 * G;
+  FEB_TRY(H.pool.alloc(&H.zpart, (size_t)rigid_blocks(Z) * G * 6));
+  FEB_TRY(H.pool.alloc(&H.zr, nc));
+  FEB_TRY(H.pool.alloc(&H.zcoef, nc));
+  // Ec = Z^T K Z column by column (FP64 matrix-free K)
+  std::vector<double> Ec((size_t)nc * nc);
+  double *col, *kcol;
+  FEB_TRY(H.pool.alloc(&col, 3 * (size_t)H.ntotal));
+  FEB_TRY(H.pool.alloc(&kcol, 3 * (size_t)H.ntotal));
+  for (int c = 0; c < nc; ++c) {
+    FEB_CUDA(cudaMemsetAsync(col, 0, 3 * (size_t)H.ntotal * sizeof(double), H.s));
+    launch_z_column(Z, c, col, H.s);
+    H.apply<double>(0, col, kcol, nullptr);
+    launch_ztr(Z, kcol, H.zpart, H.zr, H.s);
+    FEB_CUDA(cudaMemcpyAsync(&Ec[(size_t)c * nc], H.zr, nc * sizeof(double), cudaMemcpyDeviceToHost, H.s));
+  }
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  H.pool.free(col);
+  H.pool.free(kcol);
+  std::vector<double> Es((size_t)nc * nc);
+  for (int i = 0; i < nc; ++i)
+    for (int j = 0; j < nc; ++j) Es[(size_t)i * nc + j] = 0.5 * (Ec[(size_t)i * nc + j] + Ec[(size_t)j * nc + i]);
+  std::vector<double> Ei = sym_pinv(Es, nc);
+  FEB_TRY(H.pool.upload(&H.Einv, Ei.data(), Ei.size()));
+  H.has_rigid = true;
+  return H.sync_out();
+}
+
+int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, FebInfo* info) {
+  if (!h || !f || !xout) { set_last_error("feb_solve: null argument"); return FEB_ERR_ARG; }
+  static int fail_once_used = 0;
+  if (env_flag("FEB_TEST_FAIL")) { set_last_error("injected failure (FEB_TEST_FAIL)"); return FEB_ERR_INJECTED; }
+  if (env_flag("FEB_TEST_FAIL_ONCE") && !fail_once_used) {
+    fail_once_used = 1;
+    set_last_error("injected transient failure (FEB_TEST_FAIL_ONCE)");
+    return FEB_ERR_INJECTED;
+  }
+  FebHandle& H = *h;
+  if (H.coarsest < 0) { set_last_error("feb_solve: handle built with max_levels = 0 (operator only)"); return FEB_ERR_ARG; }
+  const int64_t n = 3 * H.ntotal;
+  FEB_TRY(H.sync_in());
+  H.launches = 0;
+  FebInfo inf{};
+  FEB_CUDA(cudaEventRecord(H.ev0, H.s));
+  // loads and start values on nodes no active cell uses are dropped (fe/solver.py:216-219)
+  k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(f, H.L[0].used, H.ntotal, H.fb);
+  f = H.fb;
+  if (x0) {
+    k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(x0, H.L[0].used, H.ntotal, H.z);
+    x0 = H.z;
+  }
+  int st = FEB_OK;
+  int err = FEB_OK;
+  const double fn2 = H.read_dot(f, f, n, &err);
+  if (err) return err;
+  const double fnorm = std::sqrt(fn2);
+  const double thr2 = fn2 > 0 ? H.opt.tol * H.opt.tol * fn2 : 1.0;
+  if (fn2 == 0.0) {
+    FEB_CUDA(cudaMemsetAsync(xout, 0, n * sizeof(double), H.s));
+    inf.flag = 0; inf.iters = 0; inf.relres = 0.0;
+  } else if (H.opt.precision != FEB_PREC_REFINE) {
+    if (x0) FEB_CUDA(cudaMemcpyAsync(H.x, x0, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+    FEB_TRY(H.cg_start<double>(H.st, f, H.x, H.r, x0 != nullptr, thr2, H.opt.maxiter));
+    CgState out{};
+    FEB_TRY(H.run_cg(H.st, false, out));
+    inf.iters = out.it; inf.flag = out.flag; inf.sweeps = 1;
+    st = out.status;
+    FEB_CUDA(cudaMemcpyAsync(xout, H.x, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+  } else {
+    // FP64 iterative refinement: r = f - K x (FP64), e = FP32 GMG-PCG(r / ||r||), x += ||r|| e
+    if (x0) FEB_CUDA(cudaMemcpyAsync(H.x, x0, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+    else FEB_CUDA(cudaMemsetAsync(H.x, 0, n * sizeof(double), H.s));
+    int total = 0, sweeps = 0;
+    inf.flag = H.opt.maxiter;
+    for (; sweeps < 1000; ++sweeps) {
+      H.apply<double>(0, H.x, H.q, nullptr);
+      launch_residual<double>(f, H.q, H.r, n, nullptr, H.s);
+      double rr = H.read_dot(H.r, H.r, n, &err);
+      if (err) return err;
+      if (!std::isfinite(rr)) { st = FEB_ERR_NAN; break; }
+      if (rr < thr2) { inf.flag = 0; break; }
+      if (total >= H.opt.maxiter) break;
+      double scale[2] = {std::sqrt(rr), 1.0 / std::sqrt(rr)};
+      FEB_CUDA(cudaMemcpyAsync(H.sc, scale, 2 * sizeof(double), cudaMemcpyHostToDevice, H.s));
+      launch_scale_to_float(H.r, H.rf, H.sc + 1, n, nullptr, H.s);
+      // the inner CG starts from r32 as its right-hand side (stored in qf's partner pf? use bf = zf temp)
+      FEB_CUDA(cudaMemcpyAsync(H.L[0].b32, H.rf, n * sizeof(float), cudaMemcpyDeviceToDevice, H.s));
+      int budget = std::min(H.opt.inner_maxiter, H.opt.maxiter - total);
+      FEB_TRY(H.cg_start<float>(H.sti, H.L[0].b32, H.xf, H.rf, false, H.opt.inner_tol * H.opt.inner_tol, budget));
+      CgState out{};
+      FEB_TRY(H.run_cg(H.sti, true, out));
+      total += out.it;
+      if (out.status == FEB_ERR_NAN) { st = FEB_ERR_NAN; break; }
+      launch_add_scaled(H.xf, H.x, H.sc, n, nullptr, H.s);
+      H.launches += 6;
+      if (out.it == 0) break;
+    }
+    inf.iters = total; inf.sweeps = sweeps + 1;
+    FEB_CUDA(cudaMemcpyAsync(xout, H.x, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+  }
+  // true FP64 residual of the result
+  if (fn2 > 0) {
+    H.apply<double>(0, xout, H.q, nullptr);
+    launch_residual<double>(f, H.q, H.r, n, nullptr, H.s);
+    double rr = H.read_dot(H.r, H.r, n, &err);
+    if (err) return err;
+    inf.relres = std::sqrt(rr) / fnorm;
+  }
+  FEB_CUDA(cudaEventRecord(H.ev1, H.s));
+  FEB_CUDA(cudaEventSynchronize(H.ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, H.ev0, H.ev1);
+  inf.t_solve_ms = ms;
+  inf.t_setup_ms = H.t_setup_ms;
+  inf.levels = H.coarsest + 1;
+  inf.ndof = H.ndof;
+  inf.coarse_n = H.nd;
+  std::vector<LevelParams> lp(kMaxLevels);
+  FEB_CUDA(cudaMemcpy(lp.data(), H.lp, kMaxLevels * sizeof(LevelParams), cudaMemcpyDeviceToHost));
+  for (int l = 0; l <= H.coarsest && l < 8; ++l) {
+    inf.level_dofs[l] = H.L[l].ndof;
+    inf.lmax[l] = l < H.coarsest ? lp[l].lmax : 0.0;
+  }
+  inf.kernel_launches = H.launches;
+  if (info) *info = inf;
+  FEB_TRY(H.sync_out());
+  if (st != FEB_OK) {
+    set_last_error(st == FEB_ERR_BREAKDOWN ? "CG breakdown: p^T K p <= 0" : "non-finite residual");
+    return st;
+  }
+  return FEB_OK;
+}
+
+int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y) {
+  if (!h || !u || !y) { set_last_error("feb_apply: null argument"); return FEB_ERR_ARG; }
+  FEB_TRY(h->sync_in());
+  if (prec == 0) h->apply<double>(0, (const double*)u, (double*)y, nullptr);
+  else h->apply<float>(0, (const float*)u, (float*)y, nullptr);
+  FEB_CUDA(cudaGetLastError());
+  return h->sync_out();
+}
+
+int feb_export_solution(FebHandle* h, const double* x, double* U) {
+  if (!h || !x || !U) { set_last_error("feb_export_solution: null argument"); return FEB_ERR_ARG; }
+  FEB_TRY(h->sync_in());
+  k_export<<<div_up(3 * h->ntotal, kThreads), kThreads, 0, h->s>>>(x, h->L[0].used, h->ntotal, U);
+  FEB_CUDA(cudaGetLastError());
+  return h->sync_out();
+}
+
+int feb_used_nodes(FebHandle* h, int64_t* nused, uint8_t* mask) {
+  if (!h) { set_last_error("feb_used_nodes: null handle"); return FEB_ERR_ARG; }
+  if (nused) *nused = h->ndof / 3;
+  if (mask) {
+    FEB_TRY(h->sync_in());
+    FEB_CUDA(cudaMemcpyAsync(mask, h->L[0].used, h->ntotal, cudaMemcpyDeviceToDevice, h->s));
+    return h->sync_out();
+  }
+  return FEB_OK;
+}
+
+int feb_destroy(FebHandle* h) {
+  if (!h) return FEB_OK;
+  delete h;
+  return FEB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,357 @@
+// Vector kernels: deterministic two-stage reductions, CG updates, Chebyshev smoother steps.
+#include "vec.cuh"
+
+namespace feb {
+
+namespace {
+
+template <typename Ta, typename Tb>
+__global__ void __launch_bounds__(kThreads)
+k_dot_partial(const Ta* __restrict__ a, const Tb* __restrict__ b, int64_t n, double* __restrict__ partials,
+              const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+    s += double(a[i]) * double(b[i]);
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// Sums the partials in a fixed order (deterministic) and runs the scalar step of the caller.
+__global__ void __launch_bounds__(kThreads)
+k_finalize(int kind, const double* __restrict__ partials, int np, CgState* st, LevelParams* lp, int deg,
+           const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += kThreads) s += partials[i];
+  s = block_sum(s);
+  if (threadIdx.x != 0) return;
+  switch (kind) {
+    case FIN_RZ:
+      st->rz = s;
+      st->beta = (st->it == 0) ? 0.0 : s / st->rz_old;
+      break;
+    case FIN_ALPHA:
+      st->pq = s;
+      if (!(s > 0.0) || !isfinite(s)) {
+        st->status = isfinite(s) ? FEB_ERR_BREAKDOWN : FEB_ERR_NAN;
+        st->done = 1;
+        st->flag = st->maxiter;
+      } else {
+        st->alpha = st->rz / s;
+      }
+      break;
+    case FIN_CONV:
+      st->rr = s;
+      st->rz_old = st->rz;
+      st->it += 1;
+      if (!isfinite(s)) {
+        st->status = FEB_ERR_NAN; st->done = 1; st->flag = st->maxiter;
+      } else if (s < st->thr2) {
+        st->done = 1; st->flag = 0;
+      } else if (st->it >= st->maxiter) {
+        st->done = 1; st->flag = st->maxiter;
+      }
+      break;
+    case FIN_INIT:
+      st->rr = s;
+      if (!isfinite(s)) { st->status = FEB_ERR_NAN; st->done = 1; st->flag = st->maxiter; }
+      else if (s < st->thr2) { st->done = 1; st->flag = 0; }
+      else if (st->maxiter <= 0) { st->done = 1; st->flag = st->maxiter; }
+      break;
+    case FIN_POWER0:
+      lp->xnorm = sqrt(s);
+      break;
+    case FIN_POWER: {
+      double ny = sqrt(s);
+      lp->lam = ny / lp->xnorm;
+      lp->inv = 1.0 / ny;
+      lp->xnorm = 1.0;
+      double lmax = 1.1 * lp->lam, lmin = lmax / 30.0;
+      double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+      double rho = 1.0 / sigma;
+      lp->lmax = lmax; lp->lmin = lmin;
+      lp->c_init = 1.0 / theta;
+      for (int k = 0; k < deg - 1 && k < 8; ++k) {
+        double rn = 1.0 / (2.0 * sigma - rho);
+        lp->a1[k] = rn * rho;
+        lp->a2[k] = 2.0 * rn / delta;
+        rho = rn;
+      }
+      break;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_update_p(const T* __restrict__ z, T* __restrict__ p, const CgState* __restrict__ st, int64_t n,
+                           const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const T beta = T(st->beta);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_update_xr(const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x, T* __restrict__ r,
+            const CgState* __restrict__ st, int64_t n, double* __restrict__ partials, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const T alpha = T(st->alpha);
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    x[i] += alpha * p[i];
+    T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    s += double(ri) * double(ri);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+template <typename T>
+__device__ __forceinline__ void bj(const T* __restrict__ D, int64_t nn, int64_t i, T r0, T r1, T r2, T& z0, T& z1,
+                                   T& z2) {
+  z0 = D[i] * r0 + D[nn + i] * r1 + D[2 * nn + i] * r2;
+  z1 = D[3 * nn + i] * r0 + D[4 * nn + i] * r1 + D[5 * nn + i] * r2;
+  z2 = D[6 * nn + i] * r0 + D[7 * nn + i] * r1 + D[8 * nn + i] * r2;
+}
+
+template <typename T>
+__global__ void k_cheb_first(const T* __restrict__ b, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
+                             const T* __restrict__ D, const LevelParams* __restrict__ lp, int64_t nn,
+                             const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const T c = T(lp->c_init);
+  T r0 = b[3 * i], r1 = b[3 * i + 1], r2 = b[3 * i + 2], z0, z1, z2;
+  bj(D, nn, i, r0, r1, r2, z0, z1, z2);
+  r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+  z0 *= c; z1 *= c; z2 *= c;
+  d[3 * i] = z0; d[3 * i + 1] = z1; d[3 * i + 2] = z2;
+  x[3 * i] = z0; x[3 * i + 1] = z1; x[3 * i + 2] = z2;
+}
+
+template <typename T>
+__global__ void k_cheb_init(const T* __restrict__ b, const T* __restrict__ Ax, T* __restrict__ r, T* __restrict__ d,
+                            T* __restrict__ x, const T* __restrict__ D, const LevelParams* __restrict__ lp, int64_t nn,
+                            const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const T c = T(lp->c_init);
+  T r0 = b[3 * i] - Ax[3 * i], r1 = b[3 * i + 1] - Ax[3 * i + 1], r2 = b[3 * i + 2] - Ax[3 * i + 2], z0, z1, z2;
+  bj(D, nn, i, r0, r1, r2, z0, z1, z2);
+  r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+  z0 *= c; z1 *= c; z2 *= c;
+  d[3 * i] = z0; d[3 * i + 1] = z1; d[3 * i + 2] = z2;
+  x[3 * i] += z0; x[3 * i + 1] += z1; x[3 * i + 2] += z2;
+}
+
+template <typename T>
+__global__ void k_cheb_step(const T* __restrict__ Ad, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
+                            const T* __restrict__ D, const LevelParams* __restrict__ lp, int k, int64_t nn,
+                            const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const T a1 = T(lp->a1[k]), a2 = T(lp->a2[k]);
+  T r0 = r[3 * i] - Ad[3 * i], r1 = r[3 * i + 1] - Ad[3 * i + 1], r2 = r[3 * i + 2] - Ad[3 * i + 2], z0, z1, z2;
+  bj(D, nn, i, r0, r1, r2, z0, z1, z2);
+  r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+  T d0 = a1 * d[3 * i] + a2 * z0, d1 = a1 * d[3 * i + 1] + a2 * z1, d2 = a1 * d[3 * i + 2] + a2 * z2;
+  d[3 * i] = d0; d[3 * i + 1] = d1; d[3 * i + 2] = d2;
+  x[3 * i] += d0; x[3 * i + 1] += d1; x[3 * i + 2] += d2;
+}
+
+template <typename T>
+__global__ void k_residual(const T* __restrict__ b, const T* __restrict__ Ax, T* __restrict__ r, int64_t n,
+                           const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    r[i] = b[i] - Ax[i];
+}
+
+__device__ __forceinline__ uint64_t splitmix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// standard normal start vector of the power iteration (Box-Muller on a counter-based hash), 0 where masked out
+__global__ void k_random_start(double* __restrict__ x, const uint8_t* __restrict__ mask, int64_t nn, uint64_t seed) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 3 * nn) return;
+  uint64_t h = splitmix(seed ^ splitmix((uint64_t)i));
+  double u1 = ((h >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+  double u2 = (splitmix(h) >> 11) * (1.0 / 9007199254740992.0);
+  double g = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  x[i] = (mask == nullptr || mask[i / 3]) ? g : 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_bj_apply_norm(const double* __restrict__ D, const double* __restrict__ v, double* __restrict__ y, int64_t nn,
+                double* __restrict__ partials) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < nn; i += (int64_t)gridDim.x * kThreads) {
+    double z0, z1, z2;
+    bj(D, nn, i, v[3 * i], v[3 * i + 1], v[3 * i + 2], z0, z1, z2);
+    y[3 * i] = z0; y[3 * i + 1] = z1; y[3 * i + 2] = z2;
+    s += z0 * z0 + z1 * z1 + z2 * z2;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_scale(const double* __restrict__ y, double* __restrict__ x, const LevelParams* __restrict__ lp,
+                        int64_t n) {
+  const double inv = lp->inv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = y[i] * inv;
+}
+
+template <typename Ts, typename Td>
+__global__ void k_convert(const Ts* __restrict__ a, Td* __restrict__ b, int64_t n, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = Td(a[i]);
+}
+
+template <typename T>
+__global__ void k_axpy_dev(const T* __restrict__ x, T* __restrict__ y, int64_t n, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+__global__ void k_add_scaled(const float* __restrict__ e, double* __restrict__ x, const double* __restrict__ scale,
+                             int64_t n, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const double s = *scale;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += s * double(e[i]);
+}
+
+__global__ void k_scale_to_float(const double* __restrict__ r, float* __restrict__ rf,
+                                 const double* __restrict__ scale_inv, int64_t n, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const double s = *scale_inv;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    rf[i] = float(r[i] * s);
+}
+
+__global__ void k_mask_vector(double* __restrict__ v, const uint8_t* __restrict__ used, int64_t nn, double fill) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 3 * nn) return;
+  if (!used[i / 3]) v[i] = fill;
+}
+
+inline int grid_for(int64_t n) { return int(std::min<int64_t>((n + kThreads - 1) / kThreads, 8 * kSmCount)); }
+
+}  // namespace
+
+template <typename Ta, typename Tb>
+void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s) {
+  k_dot_partial<Ta, Tb><<<kRedBlocks, kThreads, 0, s>>>(a, b, n, partials, skip);
+}
+
+void launch_finalize(int kind, const double* partials, CgState* st, LevelParams* lp, int deg, const int* skip,
+                     cudaStream_t s) {
+  k_finalize<<<1, kThreads, 0, s>>>(kind, partials, kRedBlocks, st, lp, deg, skip);
+}
+
+template <typename T>
+void launch_update_p(const T* z, T* p, const CgState* st, int64_t n, const int* skip, cudaStream_t s) {
+  k_update_p<T><<<grid_for(n), kThreads, 0, s>>>(z, p, st, n, skip);
+}
+
+template <typename T>
+void launch_update_xr(const T* p, const T* q, T* x, T* r, const CgState* st, int64_t n, double* partials,
+                      const int* skip, cudaStream_t s) {
+  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, st, n, partials, skip);
+}
+
+template <typename T>
+void launch_cheb_first(const T* b, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
+                       const int* skip, cudaStream_t s) {
+  k_cheb_first<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, r, d, x, Dinv, lp, nn, skip);
+}
+
+template <typename T>
+void launch_cheb_init(const T* b, const T* Ax, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
+                      const int* skip, cudaStream_t s) {
+  k_cheb_init<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, Ax, r, d, x, Dinv, lp, nn, skip);
+}
+
+template <typename T>
+void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int k, int64_t nn,
+                      const int* skip, cudaStream_t s) {
+  k_cheb_step<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(Ad, r, d, x, Dinv, lp, k, nn, skip);
+}
+
+template <typename T>
+void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s) {
+  k_residual<T><<<grid_for(n), kThreads, 0, s>>>(b, Ax, r, n, skip);
+}
+
+void launch_random_start(double* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s) {
+  k_random_start<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(x, mask, nn, seed);
+}
+
+void launch_bj_apply_norm(const double* Dinv, const double* v, double* y, int64_t nn, double* partials,
+                          cudaStream_t s) {
+  k_bj_apply_norm<<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials);
+}
+
+void launch_scale(const double* y, double* x, const LevelParams* lp, int64_t n, cudaStream_t s) {
+  k_scale<<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n);
+}
+
+template <typename Ts, typename Td>
+void launch_convert(const Ts* src, Td* dst, int64_t n, const int* skip, cudaStream_t s) {
+  k_convert<Ts, Td><<<grid_for(n), kThreads, 0, s>>>(src, dst, n, skip);
+}
+
+template <typename T>
+void launch_axpy_dev(const T* x, T* y, int64_t n, const int* skip, cudaStream_t s) {
+  k_axpy_dev<T><<<grid_for(n), kThreads, 0, s>>>(x, y, n, skip);
+}
+
+void launch_add_scaled(const float* e, double* x, const double* scale, int64_t n, const int* skip, cudaStream_t s) {
+  k_add_scaled<<<grid_for(n), kThreads, 0, s>>>(e, x, scale, n, skip);
+}
+
+void launch_scale_to_float(const double* r, float* rf, const double* scale_inv, int64_t n, const int* skip,
+                           cudaStream_t s) {
+  k_scale_to_float<<<grid_for(n), kThreads, 0, s>>>(r, rf, scale_inv, n, skip);
+}
+
+void launch_mask_vector(double* v, const uint8_t* used, int64_t nn, double fill, cudaStream_t s) {
+  k_mask_vector<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(v, used, nn, fill);
+}
+
+#define INST_T(T)                                                                                              \
+  template void launch_update_p<T>(const T*, T*, const CgState*, int64_t, const int*, cudaStream_t);          \
+  template void launch_update_xr<T>(const T*, const T*, T*, T*, const CgState*, int64_t, double*, const int*,   \
+                                    cudaStream_t);                                                             \
+  template void launch_cheb_first<T>(const T*, T*, T*, T*, const T*, const LevelParams*, int64_t, const int*,   \
+                                     cudaStream_t);                                                            \
+  template void launch_cheb_init<T>(const T*, const T*, T*, T*, T*, const T*, const LevelParams*, int64_t,      \
+                                    const int*, cudaStream_t);                                                 \
+  template void launch_cheb_step<T>(const T*, T*, T*, T*, const T*, const LevelParams*, int, int64_t,           \
+                                    const int*, cudaStream_t);                                                 \
+  template void launch_residual<T>(const T*, const T*, T*, int64_t, const int*, cudaStream_t);                 \
+  template void launch_axpy_dev<T>(const T*, T*, int64_t, const int*, cudaStream_t);
+INST_T(float)
+INST_T(double)
+#undef INST_T
+template void launch_dot_partial<double, double>(const double*, const double*, int64_t, double*, const int*,
+                                                 cudaStream_t);
+template void launch_dot_partial<float, float>(const float*, const float*, int64_t, double*, const int*,
+                                               cudaStream_t);
+template void launch_convert<double, float>(const double*, float*, int64_t, const int*, cudaStream_t);
+template void launch_convert<float, double>(const float*, double*, int64_t, const int*, cudaStream_t);
+
+}  // namespace feb

@@ -1,0 +1,68 @@
+// Vector kernels of the CG iteration and the Chebyshev smoother; all scalars live in device memory so
+// a whole iteration can be captured in a CUDA graph with no host round trip.
+#pragma once
+#include "common.cuh"
+
+namespace feb {
+
+constexpr int kRedBlocks = 2 * kSmCount;   // partial sums per reduction
+
+// CG state (one per solve); SciPy cg semantics (stop when ||r|| < tol ||b|| before an iteration).
+struct CgState {
+  double rz, rz_old, pq, alpha, beta, rr, thr2;
+  int it, done, flag, status, maxiter, pad;
+};
+
+// Per-level smoother parameters written by the power iteration.
+struct LevelParams {
+  double lam, lmax, lmin;
+  double xnorm;              // power iteration: ||x|| of the current iterate
+  double inv;                // power iteration: 1 / ||y||
+  double c_init;             // Chebyshev: 1 / theta
+  double a1[8], a2[8];       // Chebyshev step k: d = a1[k] d + a2[k] M r
+};
+
+template <typename Ta, typename Tb>
+void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s);
+
+// kinds of the single-block finalisation kernel
+enum FinKind : int { FIN_RZ = 0, FIN_ALPHA = 1, FIN_CONV = 2, FIN_INIT = 3, FIN_POWER0 = 4, FIN_POWER = 5 };
+void launch_finalize(int kind, const double* partials, CgState* st, LevelParams* lp, int deg, const int* skip,
+                     cudaStream_t s);
+
+template <typename T>
+void launch_update_p(const T* z, T* p, const CgState* st, int64_t n, const int* skip, cudaStream_t s);
+template <typename T>
+void launch_update_xr(const T* p, const T* q, T* x, T* r, const CgState* st, int64_t n, double* partials,
+                      const int* skip, cudaStream_t s);
+
+// Chebyshev smoother pieces (Dinv SoA [9][nn], vectors AoS [3 nn])
+template <typename T>
+void launch_cheb_first(const T* b, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
+                       const int* skip, cudaStream_t s);
+template <typename T>
+void launch_cheb_init(const T* b, const T* Ax, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
+                      const int* skip, cudaStream_t s);
+template <typename T>
+void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int k, int64_t nn,
+                      const int* skip, cudaStream_t s);
+template <typename T>
+void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s);
+
+// power iteration
+void launch_random_start(double* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s);
+void launch_bj_apply_norm(const double* Dinv, const double* v, double* y, int64_t nn, double* partials,
+                          cudaStream_t s);
+void launch_scale(const double* y, double* x, const LevelParams* lp, int64_t n, cudaStream_t s);
+
+// conversions and small helpers
+template <typename Ts, typename Td>
+void launch_convert(const Ts* src, Td* dst, int64_t n, const int* skip, cudaStream_t s);
+template <typename T>
+void launch_axpy_dev(const T* x, T* y, int64_t n, const int* skip, cudaStream_t s);   // y += x
+void launch_add_scaled(const float* e, double* x, const double* scale, int64_t n, const int* skip, cudaStream_t s);
+void launch_scale_to_float(const double* r, float* rf, const double* scale_inv, int64_t n, const int* skip,
+                           cudaStream_t s);
+void launch_mask_vector(double* v, const uint8_t* used, int64_t nn, double fill, cudaStream_t s);
+
+}  // namespace feb

@@ -1,0 +1,349 @@
+"""Host layer over libfeb200: the reference's solve entry points with their signatures and results.
+
+* ``solve_cn``        -- rb/splitfe.py:123  (split-node engine solve; the engine's hot path)
+* ``solve``           -- fe/solver.py:202   (single-connectivity solve: springs, loads, rank-1 penalties,
+                                            orthotropic coefficients, rigid groups, warm start)
+* ``cell_stress_cn``  -- rb/splitfe.py:161,  ``cell_stress`` -- fe/solver.py:257
+* ``element_forces_cn`` -- rb/splitfe.py:178
+
+Inputs arrive as NumPy arrays (the reference's types); they are copied to the current CUDA device with
+torch (used only as the carrier of device memory and streams), the operator and the multigrid hierarchy
+are built and solved by the C ABI of libfeb200.so, and the results come back as NumPy arrays.  There
+is no CPU fallback: without a CUDA device or the library every call raises.
+
+Extra keyword-only arguments (not in the reference): ``precision`` ('fp64', 'mixed', 'refine'),
+``x0`` (warm start, full node layout), ``options`` (dict of FebOptions fields) and ``keep_device``
+(return device tensors in ``info['device']`` for a following stress call without a round trip).
+"""
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from .grid import CORNERS
+
+K_GROUND = 1e6      # ground penalty per unit area of rb/splitfe.py:143
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("comech_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def _dev(a, dtype):
+    torch = _torch()
+    t = torch.from_numpy(np.ascontiguousarray(a, dtype=dtype))
+    return t.to("cuda", non_blocking=False)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream():
+    return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+def _grid_struct(g):
+    xe, ye, ze = (np.ascontiguousarray(e, dtype=np.float64) for e in (g.xe, g.ye, g.ze))
+    s = _lib.FebGrid(len(xe) - 1, len(ye) - 1, len(ze) - 1, xe.ctypes.data, ye.ctypes.data, ze.ctypes.data)
+    s._keep = (xe, ye, ze)
+    return s
+
+
+def _options(precision, tol, maxiter, options):
+    o = _lib.default_options()
+    o.precision = _lib.PREC[precision]
+    o.tol = float(tol)
+    o.maxiter = int(maxiter)
+    for k, v in (options or {}).items():
+        setattr(o, k, v)
+    return o
+
+
+class Problem:
+    """A level-0 operator on the device with its multigrid hierarchy (one FebHandle)."""
+
+    def __init__(self, g, mat_mode, mat, active, cn=None, orig=None, pen_node=None, pen_k=None, extra_coo=None,
+                 precision="fp64", tol=1e-6, maxiter=800, options=None):
+        _lib.load()
+        torch = _torch()
+        self.g = g
+        self.grid = _grid_struct(g)
+        self.ncell = g.nx * g.ny * g.nz
+        self.nnode = (g.nx + 1) * (g.ny + 1) * (g.nz + 1)
+        self.ntotal = len(orig) if orig is not None else self.nnode
+        self.mat_mode = mat_mode
+        self.mat = _dev(mat, np.float64)
+        self.active = _dev(np.asarray(active, dtype=bool).view(np.uint8), np.uint8)
+        self.cn = _dev(cn, np.int64) if cn is not None else None
+        self.orig = _dev(orig, np.int64) if (orig is not None and self.ntotal > self.nnode) else None
+        pen_node = np.ascontiguousarray(pen_node if pen_node is not None else np.zeros(0), dtype=np.int64)
+        pen_k = np.ascontiguousarray(pen_k if pen_k is not None else np.zeros((0, 3)), dtype=np.float64)
+        if extra_coo is None:
+            er = ec = np.zeros(0, np.int64); ev = np.zeros(0)
+        else:
+            er, ec, ev = (np.ascontiguousarray(a, dtype=t) for a, t in zip(extra_coo, (np.int64, np.int64, np.float64)))
+        op = _lib.FebOperator(mat_mode, self.mat.data_ptr(), self.active.data_ptr(),
+                              self.cn.data_ptr() if self.cn is not None else None, self.ntotal,
+                              self.orig.data_ptr() if self.orig is not None else None, len(pen_node),
+                              pen_node.ctypes.data, pen_k.ctypes.data, len(ev), er.ctypes.data, ec.ctypes.data,
+                              ev.ctypes.data)
+        self.opt = _options(precision, tol, maxiter, options)
+        h = C.c_void_p()
+        _lib.check(_lib.load().feb_create(C.byref(self.grid), C.byref(op), C.byref(self.opt), _stream(), C.byref(h)))
+        self.h = h
+        self.torch = torch
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().feb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_rigid_groups(self, node_groups):
+        if not node_groups:
+            return
+        groups = [np.asarray(gr, dtype=np.int64) for gr in node_groups]
+        off = np.zeros(len(groups) + 1, np.int64)
+        off[1:] = np.cumsum([len(gr) for gr in groups])
+        nodes = _dev(np.concatenate(groups) if groups else np.zeros(0), np.int64)
+        _lib.check(_lib.load().feb_set_rigid_groups(self.h, len(groups), off.ctypes.data, _ptr(nodes)))
+
+    def rhs(self, loads):
+        """Nodal load vector (full layout) from (nodes, area, traction) lists (rb/splitfe.py:144-147)."""
+        f = self.torch.zeros(3 * self.ntotal, dtype=self.torch.float64, device="cuda")
+        for nodes, area, t in loads:
+            nodes = np.asarray(nodes, dtype=np.int64)
+            vals = np.asarray(area, dtype=np.float64)[:, None] * np.asarray(t, dtype=np.float64)[None, :]
+            nd, vd = _dev(nodes, np.int64), _dev(vals, np.float64)
+            _lib.check(_lib.load().feb_accumulate_nodal(len(nodes), _ptr(nd), _ptr(vd), _ptr(f), _stream()))
+        return f
+
+    def solve(self, f, x0=None):
+        x = self.torch.empty_like(f)
+        info = _lib.FebInfo()
+        _lib.check(_lib.load().feb_solve(self.h, _ptr(f), _ptr(x0), _ptr(x), C.byref(info)))
+        return x, info
+
+    def apply(self, u):
+        y = self.torch.empty_like(u)
+        prec = 0 if u.dtype == self.torch.float64 else 1
+        _lib.check(_lib.load().feb_apply(self.h, prec, _ptr(u), _ptr(y)))
+        return y
+
+    def export(self, x):
+        U = self.torch.empty_like(x)
+        _lib.check(_lib.load().feb_export_solution(self.h, _ptr(x), _ptr(U)))
+        return U
+
+    def used_mask(self):
+        m = self.torch.empty(self.ntotal, dtype=self.torch.uint8, device="cuda")
+        n = C.c_int64()
+        _lib.check(_lib.load().feb_used_nodes(self.h, C.byref(n), _ptr(m)))
+        return m, int(n.value)
+
+
+def _info_dict(info, t0, extra=None):
+    d = dict(iters=int(info.iters), flag=int(info.flag), relres=float(info.relres), levels=int(info.levels),
+             ndof=int(info.ndof), sweeps=int(info.sweeps), t_setup=round(info.t_setup_ms / 1e3, 4),
+             t_gpu=round(info.t_solve_ms / 1e3, 4), coarse="dense-inverse", coarse_n=int(info.coarse_n),
+             level_dofs=[int(info.level_dofs[i]) for i in range(int(info.levels))],
+             lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
+             kernel_launches=int(info.kernel_launches), device=f"cuda:{_torch().cuda.current_device()}",
+             t_wall=round(time.perf_counter() - t0, 4))
+    if extra:
+        d.update(extra)
+    return d
+
+
+def _extra_entries(extra, used_nodes_fn, ntotal):
+    """Full-layout COO of the reference's ``extra(nmap, n)`` hook; objects exposing ``node_coo()`` skip the
+    compact numbering (no device->host round trip of the used-node map)."""
+    if extra is None:
+        return None
+    if hasattr(extra, "node_coo"):
+        nr, cr, nc, cc, v = extra.node_coo()
+        return 3 * np.asarray(nr, np.int64) + cr, 3 * np.asarray(nc, np.int64) + cc, np.asarray(v, np.float64)
+    nused = used_nodes_fn()
+    nmap = -np.ones(ntotal, np.int64)
+    nmap[nused] = np.arange(len(nused))
+    M = extra(nmap, 3 * len(nused)).tocoo()
+    return 3 * nused[M.row // 3] + M.row % 3, 3 * nused[M.col // 3] + M.col % 3, M.data
+
+
+def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups=None, tol=1e-6, maxiter=800,
+             aniso=None, *, precision="fp64", x0=None, options=None, keep_device=False):
+    """Split-node solve on the GPU (rb/splitfe.py:123-158): returns (U (nnew, 3) with NaN on unused nodes,
+    info, reactions R)."""
+    if aniso is not None:
+        raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
+    t0 = time.perf_counter()
+    ncell = g.nx * g.ny * g.nz
+    orig = np.asarray(orig)
+    ntotal = len(orig)
+    fn, fa = fixed
+    fn = np.asarray(fn, np.int64)
+    fa = np.asarray(fa, np.float64)
+    pen_k = np.repeat((fa * K_GROUND)[:, None], 3, axis=1)
+    active = np.asarray(active, bool)
+
+    def used_nodes():
+        return np.unique(np.asarray(cn)[np.flatnonzero(active)])
+
+    coo = _extra_entries(extra, used_nodes, ntotal)
+    mat = np.concatenate([np.asarray(lam, np.float64).ravel(), np.asarray(mu, np.float64).ravel()])
+    P = Problem(g, _lib.MAT_ISO_SRI, mat, active, cn=cn, orig=orig, pen_node=fn, pen_k=pen_k, extra_coo=coo,
+                precision=precision, tol=tol, maxiter=maxiter, options=options)
+    try:
+        P.set_rigid_groups(node_groups)
+        f = P.rhs(loads)
+        x0d = _dev(np.nan_to_num(np.asarray(x0, np.float64)).ravel(), np.float64) if x0 is not None else None
+        x, info = P.solve(f, x0d)
+        Ud = P.export(x)
+        U = Ud.view(ntotal, 3).cpu().numpy()
+        R = np.zeros((ntotal, 3))
+        np.add.at(R, fn, -(fa[:, None] * K_GROUND) * U[fn])
+        d = _info_dict(info, t0)
+        if keep_device:
+            d["device"] = dict(U=Ud, mat=P.mat, cn=P.cn, problem=P)
+        return U, d, R
+    finally:
+        if not keep_device:
+            P.close()
+
+
+def _used_from_grid(g, active):
+    nx1, ny1 = g.nx + 1, g.ny + 1
+    cells = np.flatnonzero(active)
+    k = cells % g.nz; j = (cells // g.nz) % g.ny; i = cells // (g.nz * g.ny)
+    used = np.zeros((g.nx + 1) * (g.ny + 1) * (g.nz + 1), bool)
+    for a, b, c in CORNERS:
+        used[(i + a) + nx1 * ((j + b) + ny1 * (k + c))] = True
+    return used
+
+
+def solve(grid, lam, mu, active, springs, loads, method="cg", tol=1e-8, x0=None, maxiter=20000, penalties=(),
+          coeffs=None, node_groups=None, U0=None, *, precision="fp64", options=None):
+    """Single-connectivity solve on the GPU (fe/solver.py:202-254).  Every method ('gmg', 'direct', 'cg')
+    runs the device GMG-PCG; 'direct' tightens the tolerance to 1e-12.  Returns (U (nnode, 3) with NaN on
+    unused nodes, info)."""
+    t0 = time.perf_counter()
+    g = grid
+    active = np.asarray(active, bool)
+    used = _used_from_grid(g, active)
+    nnode = len(used)
+    if method == "direct":
+        tol = min(tol, 1e-12)
+    # diagonal springs on used nodes (fe/solver.py:212-215)
+    pn, pk = [], []
+    for nodes, area, kvec in springs:
+        nodes = np.asarray(nodes, np.int64); ok = used[nodes]
+        pn.append(nodes[ok]); pk.append(np.asarray(area, np.float64)[ok][:, None] * np.asarray(kvec, np.float64)[None])
+    pen_node = np.concatenate(pn) if pn else np.zeros(0, np.int64)
+    pen_k = np.concatenate(pk) if pk else np.zeros((0, 3))
+    # rank-1 penalties k w w^T, w normalised to unit sum over used nodes (fe/solver.py:224-232)
+    er, ec, ev = [], [], []
+    for nodes, weights, comp, k in penalties:
+        nodes = np.asarray(nodes, np.int64); ok = used[nodes]
+        dof = 3 * nodes[ok] + int(comp)
+        w = np.asarray(weights, np.float64)[ok]
+        ud, inv = np.unique(dof, return_inverse=True)
+        wv = np.bincount(inv, weights=w)
+        wv /= wv.sum()
+        er.append(np.repeat(ud, len(ud))); ec.append(np.tile(ud, len(ud))); ev.append(k * np.outer(wv, wv).ravel())
+    coo = (np.concatenate(er), np.concatenate(ec), np.concatenate(ev)) if er else None
+    if coeffs is not None:
+        mode, mat = _lib.MAT_ORTHO, np.asarray(coeffs, np.float64).reshape(-1, 6)
+    else:
+        mode, mat = _lib.MAT_ISO_FULL, np.concatenate([np.asarray(lam, np.float64), np.asarray(mu, np.float64)])
+    P = Problem(g, mode, mat, active, pen_node=pen_node, pen_k=pen_k, extra_coo=coo, precision=precision, tol=tol,
+                maxiter=maxiter, options=options)
+    try:
+        P.set_rigid_groups(node_groups)
+        lo = []
+        for nodes, area, t in loads:
+            nodes = np.asarray(nodes, np.int64); ok = used[nodes]
+            lo.append((nodes[ok], np.asarray(area, np.float64)[ok], t))
+        f = P.rhs(lo)
+        if U0 is not None:
+            x0 = np.where(used[:, None], np.nan_to_num(np.asarray(U0, np.float64)), 0.0)
+        elif x0 is not None:
+            full = np.zeros((nnode, 3)); full[used] = np.asarray(x0, np.float64).reshape(-1, 3)
+            x0 = full
+        x0d = _dev(np.asarray(x0).ravel(), np.float64) if x0 is not None else None
+        x, info = P.solve(f, x0d)
+        U = P.export(x).view(nnode, 3).cpu().numpy()
+        usedn = np.flatnonzero(used)
+        fh = f.view(nnode, 3).cpu().numpy()[usedn].ravel()
+        return U, _info_dict(info, t0, dict(K=None, f=fh, used=usedn))
+    finally:
+        P.close()
+
+
+def _stress(g, mode, mat, U, cells, cn, nan_to_zero):
+    torch = _torch()
+    cells = np.asarray(cells, np.int64)
+    n = len(cells)
+    Ud = U if isinstance(U, torch.Tensor) else _dev(np.asarray(U, np.float64).ravel(), np.float64)
+    matd = mat if isinstance(mat, torch.Tensor) else _dev(mat, np.float64)
+    cnd = cn if (cn is None or isinstance(cn, torch.Tensor)) else _dev(cn, np.int64)
+    cd = _dev(cells, np.int64)
+    sig = torch.empty(6 * n, dtype=torch.float64, device="cuda")
+    vm = torch.empty(n, dtype=torch.float64, device="cuda")
+    eps = torch.empty(6 * n, dtype=torch.float64, device="cuda")
+    gs = _grid_struct(g)
+    _lib.check(_lib.load().feb_cell_stress(C.byref(gs), mode, _ptr(matd), _ptr(Ud), n, _ptr(cd), _ptr(cnd),
+                                           int(nan_to_zero), _ptr(sig), _ptr(vm), _ptr(eps), _stream()))
+    return sig.view(n, 6).cpu().numpy(), vm.cpu().numpy(), eps.view(n, 6).cpu().numpy()
+
+
+def cell_stress_cn(g, lam, mu, U, cells, cn, aniso=None, *, device=None):
+    """Centre-point strain, stress, von Mises of the split-node model (rb/splitfe.py:161-175); NaN
+    displacements count as 0.  ``device``: the ``info['device']`` of a ``solve_cn(..., keep_device=True)``
+    call with the same lam, mu, cn and U, to skip their upload."""
+    if aniso is not None:
+        raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
+    if device is not None:
+        return _stress(g, _lib.MAT_ISO_SRI, device["mat"], device["U"], cells, device["cn"], True)
+    mat = np.concatenate([np.asarray(lam, np.float64), np.asarray(mu, np.float64)])
+    return _stress(g, _lib.MAT_ISO_SRI, mat, U, cells, cn, True)
+
+
+def cell_stress(grid, lam, mu, U, cells, coeffs=None):
+    """Centre-point strain, stress, von Mises (fe/solver.py:257-272); NaN displacements propagate."""
+    if coeffs is not None:
+        return _stress(grid, _lib.MAT_ORTHO, np.asarray(coeffs, np.float64).reshape(-1, 6), U, cells, None, False)
+    mat = np.concatenate([np.asarray(lam, np.float64), np.asarray(mu, np.float64)])
+    return _stress(grid, _lib.MAT_ISO_SRI, mat, U, cells, None, False)
+
+
+def element_forces_cn(g, lam, mu, U, cells, cn, aniso=None):
+    """Internal nodal forces K_e u_e (SRI lambda term) of listed cells (rb/splitfe.py:178-193)."""
+    if aniso is not None:
+        raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
+    torch = _torch()
+    cells = np.asarray(cells, np.int64)
+    n = len(cells)
+    mat = _dev(np.concatenate([np.asarray(lam, np.float64), np.asarray(mu, np.float64)]), np.float64)
+    Ud = _dev(np.asarray(U, np.float64).ravel(), np.float64)
+    cd, cnd = _dev(cells, np.int64), _dev(cn, np.int64)
+    out = torch.empty(24 * n, dtype=torch.float64, device="cuda")
+    gs = _grid_struct(g)
+    _lib.check(_lib.load().feb_element_forces(C.byref(gs), _ptr(mat), _ptr(Ud), n, _ptr(cd), _ptr(cnd), _ptr(out),
+                                              _stream()))
+    return out.view(n, 8, 3).cpu().numpy()

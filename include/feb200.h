@@ -1,0 +1,157 @@
+/* feb200 -- C ABI of the B200-native voxel linear-elastic FE solver.
+ *
+ * Drop-in engine for the solve call of CoMech's data engine.  The reference is pure Python; the entry
+ * points below are the C boundary under the Python host layer (comech_b200/), which keeps the
+ * reference signatures.  Each function names the reference interface it serves.
+ *
+ * Conventions
+ *   - grid: node id = i + (nx+1) (j + (ny+1) k); cell id = (i ny + j) nz + k (fe/solver.py:93-128);
+ *     split copies have ids >= (nx+1)(ny+1)(nz+1) (rb/splitfe.py:261-305).
+ *   - "full layout" vectors hold 3 doubles per node id (all grid nodes, then all copies); the reference's
+ *     compact dof numbering (dof = 3 nmap[node] + comp over used nodes, rb/splitfe.py:72-76) is the
+ *     restriction of it to the used nodes.
+ *   - pointers marked [dev] are CUDA device pointers, [host] are host pointers.
+ *   - every function returns FEB_OK (0) or a negative status; feb_last_error() describes the failure.
+ *     No function aborts, and none falls back to a CPU implementation.
+ */
+#ifndef FEB200_H
+#define FEB200_H
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FEB_API __attribute__((visibility("default")))
+#else
+#define FEB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEB_OK 0
+#define FEB_ERR_ARG (-1)
+#define FEB_ERR_CUDA (-2)
+#define FEB_ERR_BREAKDOWN (-3)   /* p^T A p <= 0 in CG */
+#define FEB_ERR_NAN (-4)         /* non-finite residual */
+#define FEB_ERR_COARSE (-5)      /* coarsest-level matrix not positive definite */
+#define FEB_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */
+#define FEB_ERR_INJECTED (-7)    /* failure injected on the host for tests (FEB_TEST_FAIL) */
+#define FEB_ERR_NOMEM (-8)
+
+#define FEB_MAT_ISO_SRI 0        /* lambda at the cell centre, mu 2x2x2 (rb/splitfe.py:58-69)      */
+#define FEB_MAT_ISO_FULL 1       /* lambda and mu 2x2x2 (fe/solver.py:77-90)                       */
+#define FEB_MAT_ORTHO 2          /* six orthotropic pattern coefficients (fe/solver.py:43-74)      */
+
+#define FEB_PREC_FP64 0          /* FP64 PCG, FP64 V-cycle                                         */
+#define FEB_PREC_MIXED 1         /* FP64 PCG, FP32 V-cycle (rb/gpusolve.py:206-262 mg_dtype=float32) */
+#define FEB_PREC_REFINE 2        /* FP64 iterative refinement around an all-FP32 GMG-PCG           */
+
+typedef struct FebHandle FebHandle;
+
+typedef struct FebGrid {
+  int32_t nx, ny, nz;            /* cells per axis */
+  const double* xe;              /* [host] nx+1 edges */
+  const double* ye;              /* [host] ny+1 edges */
+  const double* ze;              /* [host] nz+1 edges */
+} FebGrid;
+
+/* Level-0 operator K = sum_cells K_e + diag(kd) + E, E a sparse symmetric extra matrix
+ * (rb/splitfe.py:123-150, fe/solver.py:202-232). */
+typedef struct FebOperator {
+  int32_t mat_mode;              /* FEB_MAT_* */
+  const double* mat;             /* [dev] ISO: lam[ncell] followed by mu[ncell]; ORTHO: coeffs[ncell][6]; cell-id order */
+  const uint8_t* active;         /* [dev] ncell flags */
+  const int64_t* cn;             /* [dev] ncell x 8 node ids (split connectivity), NULL = grid connectivity */
+  int64_t nnode_total;           /* grid nodes + split copies */
+  const int64_t* orig;           /* [dev] grid node of every node id (nnode_total), NULL when there are no copies */
+  int64_t npen;                  /* diagonal penalties: kd[3 node + c] += k[3 i + c] */
+  const int64_t* pen_node;       /* [host] npen node ids */
+  const double* pen_k;           /* [host] npen x 3 */
+  int64_t nextra;                /* extra matrix entries (COO, duplicates summed), full-layout dofs */
+  const int64_t* extra_row;      /* [host] */
+  const int64_t* extra_col;      /* [host] */
+  const double* extra_val;       /* [host] */
+} FebOperator;
+
+typedef struct FebOptions {
+  int32_t precision;             /* FEB_PREC_* */
+  int32_t maxiter;               /* CG iterations (all refinement sweeps together) */
+  double tol;                    /* stop when ||f - K x|| < tol ||f|| */
+  int32_t min_dofs;              /* coarsening stops at <= min_dofs dofs (fe/gmg.py:80: 6000) */
+  int32_t max_levels;            /* (fe/gmg.py:80: 6); 0 = operator only (feb_apply, no feb_solve) */
+  int32_t cheb_degree;           /* Chebyshev degree (fe/gmg.py:61: 3) */
+  int32_t check_every;           /* host polls convergence every k iterations (>= 1) */
+  double inner_tol;              /* REFINE: relative residual reduction of each FP32 sweep */
+  int32_t inner_maxiter;         /* REFINE: CG iterations per sweep */
+  int32_t use_graphs;            /* capture the CG iteration in a CUDA graph */
+  uint64_t seed;                 /* power-iteration start vectors */
+} FebOptions;
+
+typedef struct FebInfo {
+  int32_t iters;                 /* CG iterations (sum over refinement sweeps) */
+  int32_t flag;                  /* 0 converged, else maxiter (SciPy cg convention) */
+  int32_t levels;                /* multigrid levels incl. the coarsest */
+  int32_t sweeps;                /* refinement sweeps (1 for FP64 / MIXED) */
+  double relres;                 /* FP64 ||f - K x|| / ||f|| of the returned x */
+  double t_setup_ms;             /* device time of feb_create's multigrid set-up */
+  double t_solve_ms;             /* device time of feb_solve */
+  int64_t ndof;                  /* 3 x used nodes */
+  int64_t level_dofs[8];
+  double lmax[8];
+  int32_t coarse_n;              /* dofs of the dense coarsest level */
+  int32_t kernel_launches;       /* kernels launched by feb_solve */
+} FebInfo;
+
+/* Default options (tol 1e-6, maxiter 800 as rb/splitfe.py:123; GMG parameters of fe/gmg.py:80). */
+FEB_API void feb_default_options(FebOptions* opt);
+
+/* Builds the operator and the multigrid hierarchy on the device (replaces the CPU/SciPy assembly,
+ * fe/solver.py:137-162, rb/splitfe.py:72-91, rb/gpusolve.py:306-346, and the hierarchy set-up,
+ * fe/gmg.py:79-102, rb/gpusolve.py:39-171).  `stream` is a cudaStream_t (NULL = default). */
+FEB_API int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt, void* stream, FebHandle** out);
+
+/* Per-group rigid-body modes for the additive coarse correction Z pinv(Z^T K Z) Z^T
+ * (fe/solver.py:177-199, rb/splitfe.py:105-120, fe/gmg.py:127-135).  Group g is
+ * nodes[offsets[g] .. offsets[g+1]) (node ids, [dev] int64); unused nodes are dropped and groups with
+ * fewer than 4 used nodes are skipped, as in the reference. */
+FEB_API int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, const int64_t* nodes);
+
+/* Solve K x = f by GMG-preconditioned CG (fe/gmg.py:120-137, rb/gpusolve.py:206-292).
+ * f, x: [dev] full layout (3 nnode_total doubles); x0: [dev] start or NULL (zero start).
+ * Unused nodes of x are left 0. */
+FEB_API int feb_solve(FebHandle* h, const double* f, const double* x0, double* x, FebInfo* info);
+
+/* y = K u on the level-0 operator (full layout), prec = 0 FP64 / 1 FP32 (test and benchmark hook). */
+FEB_API int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y);
+
+/* U[node][c] = x for used nodes, NaN for unused ones (the reference's U, rb/splitfe.py:154). */
+FEB_API int feb_export_solution(FebHandle* h, const double* x, double* U);
+
+/* Number of used nodes and the used-node mask ([dev] uint8 nnode_total). */
+FEB_API int feb_used_nodes(FebHandle* h, int64_t* nused, uint8_t* mask);
+
+/* Releases every device buffer of the handle. */
+FEB_API int feb_destroy(FebHandle* h);
+
+/* dst[3 node[i] + c] += vals[3 i + c]; nodes/vals [dev], dst [dev] (nodal loads, rb/splitfe.py:144-147). */
+FEB_API int feb_accumulate_nodal(int64_t n, const int64_t* nodes, const double* vals, double* dst, void* stream);
+
+/* Centre-point strain, stress and von Mises of listed cells (fe/solver.py:257-272,
+ * rb/splitfe.py:161-175).  mat as in FebOperator (ISO uses lam/mu; ORTHO uses D = sum c_k P_k);
+ * U [dev] nnode_total x 3 (NaN treated as 0 when nan_to_zero); cells [dev] int64 cell ids;
+ * cn [dev] connectivity or NULL; outputs [dev] sig ncells x 6, vm ncells, eps ncells x 6 (eps may be NULL). */
+FEB_API int feb_cell_stress(const FebGrid* grid, int32_t mat_mode, const double* mat, const double* U, int64_t ncells,
+                    const int64_t* cells, const int64_t* cn, int32_t nan_to_zero, double* sig, double* vm,
+                    double* eps, void* stream);
+
+/* Internal nodal forces K_e u_e of listed cells with the SRI lambda term (rb/splitfe.py:178-193);
+ * out [dev] ncells x 8 x 3. */
+FEB_API int feb_element_forces(const FebGrid* grid, const double* mat, const double* U, int64_t ncells,
+                       const int64_t* cells, const int64_t* cn, double* out, void* stream);
+
+FEB_API const char* feb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,215 @@
+"""Parity of the CUDA path (through the C ABI) with the reference: golden vectors made by running the
+reference itself (tests/golden/) and, at larger sizes, the CPU oracle and size-independent properties.
+
+Tolerances: FP64 operator products 1e-12 relative; solutions at CG tolerance 1e-10 within 1e-7 relative
+L2 of the reference's; mixed / refined precision at rel-res 1e-8 within 1e-6 (displacement) and 1e-5
+(von Mises), the bar of the task statement."""
+import os
+
+import numpy as np
+import pytest
+
+from comech_b200 import engine, _lib
+from comech_b200.grid import Grid, face_node_areas, lame
+from comech_b200.synth import SpringSet
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _springs(z):
+    return SpringSet(pair_a=z["pair_a"], pair_b=z["pair_b"], pair_k=z["pair_k"], line_a=z["line_a"],
+                     line_b=z["line_b"], line_d=z["line_d"], line_k=z["line_k"])
+
+
+def _groups(z):
+    return np.split(z["groups"], np.cumsum(z["group_len"])[:-1])
+
+
+def _hindfoot(golden):
+    z = golden("hindfoot_small")
+    g = Grid(z["xe"], z["ye"], z["ze"])
+    return z, g
+
+
+def test_fine_operator_matches_reference_assembly(golden):
+    import torch
+    z, g = _hindfoot(golden)
+    mat = np.concatenate([z["lam"], z["mu"]])
+    nused = z["nused"]
+    with engine.Problem(g, _lib.MAT_ISO_SRI, mat, z["active"], cn=z["cn"], orig=z["orig"],
+                        options=dict(max_levels=0)) as P:
+        m, n = P.used_mask()
+        assert n == len(nused)
+        assert (np.flatnonzero(m.cpu().numpy()) == nused).all()
+        for u, ku in zip(z["u"], z["Ku"]):
+            uf = np.zeros((P.ntotal, 3)); uf[nused] = u.reshape(-1, 3)
+            y = P.apply(torch.from_numpy(uf.ravel()).cuda()).cpu().numpy().reshape(-1, 3)
+            assert np.abs(y[nused].ravel() - ku).max() <= 1e-12 * np.abs(ku).max()
+            unused = np.ones(P.ntotal, bool); unused[nused] = False
+            assert np.abs(y[unused]).max(initial=0.0) == 0.0
+            y32 = P.apply(torch.from_numpy(uf.ravel().astype(np.float32)).cuda()).cpu().numpy().reshape(-1, 3)
+            assert rel(y32[nused].ravel(), ku) < 2e-6
+
+
+def test_solve_cn_matches_reference(golden):
+    z, g = _hindfoot(golden)
+    U, info, R = engine.solve_cn(g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"],
+                                 (z["fixed_nodes"], z["fixed_area"]),
+                                 [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z),
+                                 tol=1e-10, maxiter=800)
+    ok = ~np.isnan(z["U"])
+    assert (np.isnan(U) == ~ok).all()
+    assert rel(U[ok], z["U"][ok]) < 1e-7
+    assert info["flag"] == 0 and info["relres"] < 1e-10
+    assert info["ndof"] == int(z["ndof"]) and info["levels"] == int(z["levels"])
+    assert abs(info["iters"] - int(z["iters"])) <= 3
+    assert rel(R, z["R"]) < 1e-7
+    cells = np.flatnonzero(z["active"])
+    sig, vm, eps = engine.cell_stress_cn(g, z["lam"], z["mu"], U, cells, z["cn"])
+    assert rel(vm, z["vm"]) < 1e-6
+
+
+def test_stress_and_element_forces_exact(golden):
+    z, g = _hindfoot(golden)
+    cells = np.flatnonzero(z["active"])
+    sig, vm, eps = engine.cell_stress_cn(g, z["lam"], z["mu"], z["U"], cells, z["cn"])
+    np.testing.assert_allclose(sig, z["sig"], rtol=0, atol=1e-10 * np.abs(z["sig"]).max())
+    np.testing.assert_allclose(vm, z["vm"], rtol=0, atol=1e-10 * np.abs(z["vm"]).max())
+    np.testing.assert_allclose(eps, z["eps"], rtol=0, atol=1e-10 * np.abs(z["eps"]).max())
+    F = engine.element_forces_cn(g, z["lam"], z["mu"], z["U"], z["fcells"], z["cn"])
+    np.testing.assert_allclose(F, z["F"], rtol=0, atol=1e-10 * np.abs(z["F"]).max())
+
+
+@pytest.mark.parametrize("precision", ["mixed", "refine"])
+def test_reduced_precision_solve_cn(golden, precision):
+    z, g = _hindfoot(golden)
+    U, info, R = engine.solve_cn(g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"],
+                                 (z["fixed_nodes"], z["fixed_area"]),
+                                 [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z),
+                                 tol=1e-8, maxiter=800, precision=precision)
+    ok = ~np.isnan(z["U"])
+    assert info["flag"] == 0 and info["relres"] < 1e-8
+    assert rel(U[ok], z["U"][ok]) < 1e-6
+    cells = np.flatnonzero(z["active"])
+    _, vm, _ = engine.cell_stress_cn(g, z["lam"], z["mu"], U, cells, z["cn"])
+    assert rel(vm, z["vm"]) < 1e-5
+
+
+def _block(golden):
+    z = golden("block_small")
+    g = Grid(z["xe"], z["ye"], z["ze"])
+    springs = [(z["spring_nodes"], z["spring_area"], z["spring_k"])]
+    loads = [(z["load_nodes"], z["load_area"], z["load_t"])]
+    return z, g, springs, loads
+
+
+def test_solve_gmg_matches_reference(golden):
+    z, g, springs, loads = _block(golden)
+    act = np.ones(g.ncell, bool)
+    U, info = engine.solve(g, z["lam"], z["mu"], act, springs, loads, method="gmg", tol=1e-10)
+    assert rel(U, z["U_gmg"]) < 1e-7
+    _, vm, _ = engine.cell_stress(g, z["lam"], z["mu"], U, np.arange(g.ncell))
+    assert rel(vm, z["vm_gmg"]) < 1e-6
+
+
+def test_solve_penalty_ortho_groups_matches_reference(golden):
+    z, g, springs, loads = _block(golden)
+    act = np.ones(g.ncell, bool)
+    pen = [(z["pen_nodes"], z["pen_w"], int(z["pen_comp"]), float(z["pen_k"]))]
+    U, info = engine.solve(g, z["lam"], z["mu"], act, springs, loads, method="gmg", tol=1e-10, penalties=pen,
+                           coeffs=z["coeffs"], node_groups=[z["group"]])
+    assert rel(U, z["U_pen"]) < 1e-7
+    _, vm, _ = engine.cell_stress(g, z["lam"], z["mu"], U, np.arange(g.ncell), coeffs=z["coeffs"])
+    assert rel(vm, z["vm_pen"]) < 1e-6
+
+
+def test_solve_cg_method_same_solution(golden):
+    z, g, springs, loads = _block(golden)
+    act = np.ones(g.ncell, bool)
+    U, info = engine.solve(g, z["lam"], z["mu"], act, springs, loads, method="cg", tol=1e-10)
+    assert rel(U, z["U_cg"]) < 1e-7
+
+
+def test_patch_test(golden):
+    z = golden("patch")
+    g = Grid(z["xe"], z["ye"], z["ze"])
+    E, nu = float(z["E"]), float(z["nu"])
+    lam, mu = lame(np.full(g.ncell, E), np.full(g.ncell, nu))
+    act = np.ones(g.ncell, bool)
+    nb, ab = face_node_areas(g, g.cell_nodes, np.flatnonzero(g.cK == 0), "z-")
+    nt, at = face_node_areas(g, g.cell_nodes, np.flatnonzero(g.cK == g.nz - 1), "z+")
+    U, info = engine.solve(g, lam, mu, act, [(nb, ab, np.array([1e-6, 1e-6, 1e9]))], [(nt, at, np.array([0, 0, -1.0]))],
+                           method="direct")
+    # uniaxial compression: u_z(top) = -10/E, sigma_zz = -1 everywhere (fe/test_patch.py)
+    assert abs(np.nanmin(U[:, 2]) + 10.0 / E) < 1e-9
+    sig, vm, _ = engine.cell_stress(g, lam, mu, U, np.arange(g.ncell))
+    assert np.abs(sig[:, 2] + 1.0).max() < 1e-8
+    assert np.abs(U[:, 2] - z["U"][:, 2]).max() < 1e-10
+
+
+def test_non_convergence_flag_and_injected_failure(golden, monkeypatch):
+    z, g = _hindfoot(golden)
+    args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
+            [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z))
+    U, info, R = engine.solve_cn(*args, tol=1e-12, maxiter=1)
+    assert info["flag"] == 1 and info["iters"] == 1 and info["relres"] > 1e-12
+    monkeypatch.setenv("FEB_TEST_FAIL", "1")
+    with pytest.raises(_lib.FebError) as e:
+        engine.solve_cn(*args, tol=1e-8)
+    assert e.value.code == -7
+
+
+def test_block_config1_against_oracle():
+    """48x32x24 two-material block (121,275 dofs) at rel-res 1e-8: FP64, mixed and refined precision
+    against the CPU oracle (a restatement of fe/solver.py:202 solve(method='gmg'))."""
+    from oracle import fe_oracle as O
+    from comech_b200 import synth
+    P = synth.block_problem(48, 32, 24, h=1.0, seed=0)
+    g = P["grid"]
+    og = O.OGrid(g.xe, g.ye, g.ze)
+    Uo, io = O.solve(og, P["lam"], P["mu"], P["active"], P["springs"], P["loads"], method="gmg", tol=1e-10)
+    cells = np.arange(g.ncell)
+    _, vmo, _ = O.cell_stress(og, P["lam"], P["mu"], Uo, cells)
+    for precision in ("fp64", "mixed", "refine"):
+        U, info = engine.solve(g, P["lam"], P["mu"], P["active"], P["springs"], P["loads"], method="gmg", tol=1e-8,
+                               precision=precision)
+        assert info["flag"] == 0 and info["relres"] < 1e-8, (precision, info)
+        assert rel(U, Uo) < 1e-6, precision
+        _, vm, _ = engine.cell_stress(g, P["lam"], P["mu"], U, cells)
+        assert rel(vm, vmo) < 1e-5, precision
+
+
+def test_operator_symmetry_and_rigid_nullspace():
+    """At a larger size: u^T K v == v^T K u and K annihilates rigid translations / rotations when no
+    penalty is present (FP64, size-independent properties)."""
+    import torch
+    from comech_b200 import synth
+    P = synth.hindfoot_problem(64, 48, 40, h=1.25, seed=4)
+    g = P["grid"]
+    mat = np.concatenate([P["lam"], P["mu"]])
+    with engine.Problem(g, _lib.MAT_ISO_SRI, mat, P["active"], cn=P["cn"], orig=P["orig"],
+                        options=dict(max_levels=0)) as Pr:
+        m, n = Pr.used_mask()
+        used = m.cpu().numpy().astype(bool)
+        rng = np.random.default_rng(0)
+        u = rng.standard_normal((Pr.ntotal, 3)) * used[:, None]
+        v = rng.standard_normal((Pr.ntotal, 3)) * used[:, None]
+        Ku = Pr.apply(torch.from_numpy(u.ravel()).cuda()).cpu().numpy()
+        Kv = Pr.apply(torch.from_numpy(v.ravel()).cuda()).cpu().numpy()
+        a, b = v.ravel() @ Ku, u.ravel() @ Kv
+        assert abs(a - b) <= 1e-12 * np.sqrt((Ku @ Ku) * (v.ravel() @ v.ravel()))
+        xyz = g.node_xyz[P["orig"]]
+        for mode in range(6):
+            w = np.zeros((Pr.ntotal, 3))
+            if mode < 3:
+                w[:, mode] = 1.0
+            else:
+                ax = mode - 3
+                w = np.cross(np.eye(3)[ax], xyz - xyz.mean(0))
+            w *= used[:, None]
+            Kw = Pr.apply(torch.from_numpy(w.ravel()).cuda()).cpu().numpy()
+            assert np.linalg.norm(Kw) <= 1e-10 * np.linalg.norm(Ku) * np.linalg.norm(w) / np.linalg.norm(u)
