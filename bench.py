@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Seconds per solve to rel-res 1e-8 of the synthetic ~5M-DOF hindfoot (160x112x96 voxels, h = 0.5 mm) on
+one B200, mixed precision (FP64 refinement around an FP32 GMG-PCG) next to the plain FP64 GMG-PCG.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one solve of the same inputs: device set-up of the operator and the multigrid hierarchy
+(Galerkin products, power iterations, coarse inverse), CG to rel-res 1e-8, displacement export and
+cell stress / von Mises.  ``value`` is timed with CUDA events from device-resident inputs; ``e2e``
+times the public API (``engine.solve_cn`` + ``engine.cell_stress_cn``) from pinned host arrays to host
+results.  ``--impl reference`` times the CPU oracle (a NumPy/SciPy restatement of the reference's
+``rb/splitfe.solve_cn`` + ``cell_stress_cn``) on a bounded sample of the same generator, scaled to the
+metric's problem size by the dof ratio.  Under torchrun every rank solves its own seeded instance
+(independent units, weak scaling); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "s/solve to 1e-8 rel. residual, 5M DOF: learned+mixed vs plain FP64, one B200"
+WORKLOAD = dict(nx=160, ny=112, nz=96, h=0.5)
+SAMPLE_BIG = dict(nx=64, ny=45, nz=38, h=1.25)     # CPU sample (~25 s of oracle work on 1 core)
+SAMPLE_SMALL = dict(nx=40, ny=28, nz=24, h=2.0)    # CPU sample for long reference runs (~5 s)
+TOL = 1e-8
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i, v in enumerate(r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_problem(seed, dims=WORKLOAD):
+    from comech_b200 import synth
+    return synth.hindfoot_problem(dims["nx"], dims["ny"], dims["nz"], h=dims["h"], seed=seed)
+
+
+def cpu_oracle_step(dims, seed=0):
+    """One solve_cn + cell_stress of the CPU oracle; returns (seconds, ndof)."""
+    from oracle import fe_oracle as O
+    P = make_problem(seed, dims)
+    g = O.OGrid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    t = time.perf_counter()
+    U, info, R = O.solve_cn(g, P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"], P["extra"],
+                            P["node_groups"], tol=TOL)
+    O.cell_stress(g, P["lam"], P["mu"], U, np.flatnonzero(P["active"]), P["cn"], nan_to_zero=True)
+    return time.perf_counter() - t, info["ndof"], info["iters"]
+
+
+def workload_ndof():
+    # used nodes of the metric's workload (3 dofs each) -- counted once on the generator output
+    P = make_problem(0)
+    used = np.unique(P["cn"][np.flatnonzero(P["active"])])
+    return 3 * len(used)
+
+
+def device_inputs(P):
+    """Upload the big per-cell / per-node arrays once (value is timed from device-resident inputs)."""
+    import torch
+    from comech_b200.synth import SpringSet  # noqa: F401
+    d = {}
+    d["mat"] = torch.from_numpy(np.concatenate([P["lam"], P["mu"]])).cuda()
+    d["active"] = torch.from_numpy(P["active"].astype(np.uint8)).cuda()
+    d["cn"] = torch.from_numpy(np.ascontiguousarray(P["cn"], dtype=np.int64)).cuda()
+    d["orig"] = torch.from_numpy(np.ascontiguousarray(P["orig"], dtype=np.int64)).cuda()
+    groups = P["node_groups"]
+    d["g_off"] = np.r_[0, np.cumsum([len(x) for x in groups])].astype(np.int64)
+    d["g_nodes"] = torch.from_numpy(np.concatenate(groups).astype(np.int64)).cuda()
+    (ln, la, lt), = P["loads"]
+    d["l_nodes"] = torch.from_numpy(np.asarray(ln, np.int64)).cuda()
+    d["l_vals"] = torch.from_numpy(np.asarray(la, np.float64)[:, None] * lt[None, :]).cuda()
+    d["cells"] = torch.from_numpy(np.flatnonzero(P["active"]).astype(np.int64)).cuda()
+    fn, fa = P["fixed"]
+    d["pen_node"] = np.asarray(fn, np.int64)
+    d["pen_k"] = np.repeat((np.asarray(fa) * 1e6)[:, None], 3, axis=1)
+    nr, cr, nc, cc, v = P["extra"].node_coo()
+    d["extra"] = (3 * nr + cr, 3 * nc + cc, v)
+    return d
+
+
+def device_solve(P, d, precision, x0=None):
+    """One solve from device-resident inputs (same work as engine.solve_cn + cell_stress_cn)."""
+    from comech_b200 import engine, _lib
+    g = P["grid"]
+    pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
+                        pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], precision=precision, tol=TOL,
+                        maxiter=800)
+    try:
+        pr.set_rigid_groups(d["g_nodes"], offsets=d["g_off"])
+        f = pr.rhs([(d["l_nodes"], d["l_vals"])])
+        x, info = pr.solve(f, x0)
+        U = pr.export(x)
+        sig, vm, eps = engine._stress(g, _lib.MAT_ISO_SRI, d["mat"], U, d["cells"], d["cn"], True, to_host=False)
+        return U, vm, info
+    finally:
+        pr.close()
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from comech_b200 import engine, _lib
+    lib = _lib.load()
+    dev = torch.cuda.current_device()
+    P = make_problem(seed=rank)
+    d = device_inputs(P)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    prec = args.precision
+    for _ in range(args.warmup):
+        device_solve(P, d, prec)
+    torch.cuda.synchronize()
+    # ---------------------------------------------------------------- timed: device-resident inputs
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    launches0 = lib.feb_launch_count()
+    with Clocks(dev) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush_l2(flush)
+            ev0.record()
+            U, vm, info = device_solve(P, d, prec)
+            ev1.record()
+            torch.cuda.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+    launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
+    t_total = sum(step_ms) / 1e3
+    if dist:
+        t = torch.tensor([t_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    value = t_total / (args.steps * world)
+    mixed_info = info
+    U_mixed = U.cpu().numpy()
+    # ---------------------------------------------------------------- plain FP64 GMG-PCG, same inputs
+    device_solve(P, d, "fp64")
+    torch.cuda.synchronize()
+    fp64_ms = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush_l2(flush)
+        ev0.record()
+        U64, vm64, info64 = device_solve(P, d, "fp64")
+        ev1.record()
+        torch.cuda.synchronize()
+        fp64_ms.append(ev0.elapsed_time(ev1))
+    U64h = U64.cpu().numpy()
+    ok = ~np.isnan(U64h)
+    disp_rel = float(np.linalg.norm(U_mixed[ok] - U64h[ok]) / np.linalg.norm(U64h[ok]))
+    vm_rel = float(torch.linalg.norm(vm - vm64).item() / torch.linalg.norm(vm64).item())
+    # ---------------------------------------------------------------- e2e through the public API
+    pinned = {}
+    for k in ("lam", "mu", "cn", "orig"):
+        a = np.ascontiguousarray(P[k])
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        pinned[k] = t.numpy()
+    act = torch.empty(P["active"].shape, dtype=torch.bool, pin_memory=True)
+    act.numpy()[...] = P["active"]
+    pinned["active"] = act.numpy()
+    cells_h = np.flatnonzero(P["active"])
+    g = P["grid"]
+
+    def e2e_step():
+        t_a = time.perf_counter()
+        U, inf, R = engine.solve_cn(g, pinned["lam"], pinned["mu"], pinned["active"], pinned["cn"], pinned["orig"],
+                                    P["fixed"], P["loads"], P["extra"], P["node_groups"], tol=TOL, maxiter=800,
+                                    precision=prec, keep_device=True)
+        t_b = time.perf_counter()
+        sig, vmh, eps = engine.cell_stress_cn(g, pinned["lam"], pinned["mu"], U, cells_h, pinned["cn"],
+                                              device=inf["device"])
+        inf["device"]["problem"].close()
+        inf["t_host"]["stress"] = round(time.perf_counter() - t_b, 4)
+        inf["t_host"]["solve_cn_total"] = round(t_b - t_a, 4)
+        return U, vmh, inf
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Ue, vme, infe = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s.append(time.perf_counter() - t0)
+    ncell, ntotal, nact = g.ncell, len(P["orig"]), len(cells_h)
+    h2d = (2 * ncell * 8 + ncell + ncell * 64 + ntotal * 8 + 8 * sum(len(x) for x in P["node_groups"])
+           + P["loads"][0][0].size * 32 + nact * 8 + P["fixed"][0].size * 32 + P["extra"].node_coo()[4].size * 24)
+    d2h = ntotal * 24 + nact * 13 * 8
+    e2e_val = max(e2e_s)
+    if dist:
+        t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = float(t.item())
+    e2e_val /= world
+    # ---------------------------------------------------------------- roofline of the K.u operator
+    pk, pk_kind = peaks()
+    pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"], pen_node=d["pen_node"],
+                        pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
+    import ctypes as C
+    roof = {}
+    try:
+        used = pr.used_mask()[1]
+        n_irr = int(np.count_nonzero((P["cn"][cells_h] != g.cell_nodes[cells_h]).any(1)))
+        n_pen = len(P["fixed"][0])
+        n_extra = P["extra"].node_coo()[4].size
+        for name, dt, sv in (("fp32", torch.float32, 4), ("fp64", torch.float64, 8)):
+            u = torch.randn(3 * ntotal, dtype=dt, device="cuda")
+            y = torch.empty_like(u)
+            ms = C.c_float()
+            _lib.check(lib.feb_benchmark_apply(pr.h, 0 if sv == 8 else 1, C.c_void_p(u.data_ptr()),
+                                               C.c_void_p(y.data_ptr()), 5, C.byref(ms)))
+            _lib.check(lib.feb_benchmark_apply(pr.h, 0 if sv == 8 else 1, C.c_void_p(u.data_ptr()),
+                                               C.c_void_p(y.data_ptr()), 50, C.byref(ms)))
+            alg = (3 * ntotal * sv * 2 + nact * 2 * sv + n_irr * (32 + 2 * sv) + n_pen * (4 + 3 * sv)
+                   + n_extra * (8 + sv))
+            roof[name] = dict(ms=ms.value, bytes=alg, gbs=alg / (ms.value * 1e-3) / 1e9)
+    finally:
+        pr.close()
+    traffic = None
+    tfile = os.path.join(HERE, "profiles", "ku_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                traffic = json.load(f).get("fp32_bytes_per_launch")
+        except Exception:
+            traffic = None
+    r32 = roof["fp32"]
+    roofline = {"bound": "hbm", "achieved": round(r32["gbs"], 1), "peak": pk, "unit": "GB/s",
+                "frac": round(r32["gbs"] / pk, 4), "traffic": traffic, "kernel": "K.u FP32 (k_fine_struct + sparse pass)",
+                "peak_kind": pk_kind, "ms_per_launch": round(r32["ms"], 4), "algorithmic_bytes": r32["bytes"],
+                "fp64": {"achieved": round(roof["fp64"]["gbs"], 1), "frac": round(roof["fp64"]["gbs"] / pk, 4),
+                         "ms_per_launch": round(roof["fp64"]["ms"], 4)}}
+    # ---------------------------------------------------------------- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        secs, nd, iters = cpu_oracle_step(SAMPLE_BIG)
+        scale = mixed_info.ndof / nd
+        cpu = {"value": round(secs * scale, 2), "unit": "s/solve", "cores": 1, "kind": "port",
+               "sample": (f"oracle solve_cn + cell_stress, hindfoot {SAMPLE_BIG['nx']}x{SAMPLE_BIG['ny']}x"
+                          f"{SAMPLE_BIG['nz']} h={SAMPLE_BIG['h']} ({nd} dofs, {iters} iters, {secs:.1f} s), scaled "
+                          f"x{scale:.2f} by dofs to the workload")}
+    return dict(
+        metric=METRIC, value=round(value, 5), unit="s/solve", n_gpus=world, steps=args.steps, warmup=args.warmup,
+        ms_per_step=round(1e3 * t_total / args.steps, 3), higher_is_better=False, scaling="weak", vs_baseline=None,
+        dtype="f32 inner / f64 refinement" if prec == "refine" else ("f64" if prec == "fp64" else "f64 CG / f32 V-cycle"),
+        data="synthetic (seeded hindfoot generator)",
+        config={"workload": "hindfoot 160x112x96 h=0.5mm (C2 generator)", "ndof": int(mixed_info.ndof),
+                "precision": prec, "warm_start": "zero (learned warm start not used)", "tol": TOL,
+                "iters": int(mixed_info.iters), "sweeps": int(mixed_info.sweeps), "relres": mixed_info.relres,
+                "levels": int(mixed_info.levels), "l2": "flushed (256 MB write) before every step",
+                "parallelism": f"independent solves x{world}"},
+        plain_fp64={"s_per_solve": round(min(fp64_ms) / 1e3, 5), "iters": int(info64.iters),
+                    "relres": info64.relres},
+        speedup_vs_plain_fp64=round(min(fp64_ms) / 1e3 / value, 3) if world == 1 else None,
+        parity_vs_fp64={"disp_rel_l2": disp_rel, "vm_rel_l2": vm_rel},
+        stage_ms={"setup": round(mixed_info.t_setup_ms, 3), "solve": round(mixed_info.t_solve_ms, 3)},
+        e2e={"value": round(e2e_val, 5), "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
+             "d2h_bytes_per_step": int(d2h), "iters": int(infe["iters"]), "relres": infe["relres"],
+             "t_host": infe["t_host"]},
+        roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk.summary(),
+    )
+
+
+def run_profile(args):
+    """Profiling workloads: one device solve (solve-once) or 3 FP32 + 3 FP64 K.u products (ku)."""
+    import ctypes as C
+    import torch
+    from comech_b200 import engine, _lib
+    P = make_problem(seed=0)
+    d = device_inputs(P)
+    if args.mode == "solve-once":
+        for _ in range(args.warmup):
+            device_solve(P, d, args.precision)
+        U, vm, info = device_solve(P, d, args.precision)
+        torch.cuda.synchronize()
+        return {"mode": "solve-once", "iters": int(info.iters), "relres": info.relres, "t_setup_ms": info.t_setup_ms,
+                "t_solve_ms": info.t_solve_ms, "ndof": int(info.ndof)}
+    pr = engine.Problem(P["grid"], _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
+                        pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
+    out = {"mode": "ku"}
+    try:
+        ntotal = len(P["orig"])
+        for name, dt, prec in (("fp32", torch.float32, 1), ("fp64", torch.float64, 0)):
+            u = torch.randn(3 * ntotal, dtype=dt, device="cuda")
+            y = torch.empty_like(u)
+            ms = C.c_float()
+            _lib.check(_lib.load().feb_benchmark_apply(pr.h, prec, C.c_void_p(u.data_ptr()), C.c_void_p(y.data_ptr()),
+                                                       3, C.byref(ms)))
+            out[name + "_ms"] = ms.value
+    finally:
+        pr.close()
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    dims = SAMPLE_BIG if args.steps <= 4 else SAMPLE_SMALL
+    for _ in range(args.warmup):
+        cpu_oracle_step(SAMPLE_SMALL)
+    secs = []
+    nd = it = None
+    for _ in range(args.steps):
+        s, nd, it = cpu_oracle_step(dims)
+        secs.append(s)
+    full = workload_ndof()
+    scale = full / nd
+    value = sum(secs) / len(secs) * scale
+    desc = (f"oracle (NumPy/SciPy restatement of rb/splitfe.solve_cn + cell_stress_cn) on hindfoot "
+            f"{dims['nx']}x{dims['ny']}x{dims['nz']} h={dims['h']} ({nd} dofs, {it} iters), mean of {len(secs)} steps, "
+            f"scaled x{scale:.2f} by dofs to the {full}-dof workload")
+    return dict(metric=METRIC, value=round(value, 3), unit="s/solve", n_gpus=world, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(1e3 * sum(secs) / len(secs), 1), higher_is_better=False,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic (seeded hindfoot generator)",
+                config={"workload": "hindfoot 160x112x96 h=0.5mm (C2 generator)", "tol": TOL,
+                        "parallelism": "CPU, 1 process"},
+                impl="reference",
+                cpu_baseline={"value": round(value, 3), "unit": "s/solve", "cores": 1, "kind": "port", "sample": desc},
+                e2e={"value": round(value, 3), "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="refine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["full", "solve-once", "ku"], default="full",
+                    help="solve-once / ku: one device solve or a few K.u products of the workload (profiling)")
+    ap.add_argument("--size", default=None, help="override the workload grid, e.g. 96x64x56x0.833 (profiling)")
+    args = ap.parse_args()
+    if args.size:
+        nx, ny, nz, h = args.size.split("x")
+        WORKLOAD.update(nx=int(nx), ny=int(ny), nz=int(nz), h=float(h))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        import torch
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        if world > 1:
+            import datetime
+            import torch.distributed as tdist
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                     device_id=torch.device("cuda", local))
+            dist = tdist
+        if args.mode == "full":
+            out = run_ours(args, rank, world, dist)
+        else:
+            out = run_profile(args)
+        if dist:
+            dist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -395,7 +395,7 @@ __global__ void k_block_inverse(const double* __restrict__ D, int64_t n, double*
 
 template <typename T>
 void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s) {
-  k_stencil_apply<T><<<div_up(L.n, kThreads), kThreads, 0, s>>>(L, u, y, skip);
+  k_stencil_apply<T><<<div_up(L.n, kThreads), kThreads, 0, s>>>(L, u, y, skip); note_launch();
   if (L.nrow > 0) launch_csr_add<T>(L.nrow, L.row_dof, L.row_ptr, L.col, L.val, u, y, skip, s);
 }
 
@@ -403,17 +403,17 @@ template <typename T>
 void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,
                     const int* skip, cudaStream_t s) {
   if (nrow <= 0) return;
-  k_csr_add<T><<<div_up(nrow, kThreads), kThreads, 0, s>>>(nrow, row_dof, row_ptr, col, val, u, y, skip);
+  k_csr_add<T><<<div_up(nrow, kThreads), kThreads, 0, s>>>(nrow, row_dof, row_ptr, col, val, u, y, skip); note_launch();
 }
 
 template <typename T>
 void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                      const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s) {
   int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
-  k_restrict_grid<T><<<div_up(nc, kThreads), kThreads, 0, s>>>(P, fnx, fny, rf, rc, skip);
+  k_restrict_grid<T><<<div_up(nc, kThreads), kThreads, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
   if (fntotal > fnnode)
     k_restrict_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
-                                                                                 orig_copy, rf, rc, skip);
+                                                                                 orig_copy, rf, rc, skip); note_launch();
   (void)fnz;
 }
 
@@ -422,13 +422,13 @@ void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
                         cudaStream_t s) {
   k_prolong_add<T><<<div_up(fntotal, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal, orig_copy, used, xc,
-                                                                  xf, skip);
+                                                                  xf, skip); note_launch();
   (void)fnz;
 }
 
 void launch_kept_mask(const TransferDev& P, const uint8_t* used_f, uint8_t* kept_c, cudaStream_t s) {
   int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
-  k_kept_mask<<<div_up(nc, kThreads), kThreads, 0, s>>>(P, used_f, kept_c);
+  k_kept_mask<<<div_up(nc, kThreads), kThreads, 0, s>>>(P, used_f, kept_c); note_launch();
 }
 
 template <int MODE>
@@ -437,10 +437,10 @@ void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, con
   int ncx = cnx - 1, ncy = cny - 1, ncz = cnz - 1;
   int64_t ncell = (int64_t)ncx * ncy * ncz;
   dim3 blk(24, 8);
-  k_galerkin_cells<MODE><<<div_up(ncell, 8), blk, 0, s>>>(F, mat_all, P, KeC, ncx, ncy, ncz);
+  k_galerkin_cells<MODE><<<div_up(ncell, 8), blk, 0, s>>>(F, mat_all, P, KeC, ncx, ncy, ncz); note_launch();
   int64_t n = (int64_t)cnx * cny * cnz;
   dim3 blk2(27, 8);
-  k_cells_to_stencil<<<div_up(n, 8), blk2, 0, s>>>(KeC, A1, cnx, cny, cnz);
+  k_cells_to_stencil<<<div_up(n, 8), blk2, 0, s>>>(KeC, A1, cnx, cny, cnz); note_launch();
 }
 
 void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
@@ -448,7 +448,7 @@ void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnn
                              int64_t cn, cudaStream_t s) {
   if (npen <= 0) return;
   k_galerkin_penalty<<<div_up(npen, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, orig_copy, npen, pen_node,
-                                                                  pen_k, A1, cnx, cny, cn);
+                                                                  pen_k, A1, cnx, cny, cn); note_launch();
   (void)cnz;
 }
 
@@ -457,7 +457,7 @@ void launch_galerkin_local(const TransferDev& P, int fnx, int fny, int64_t fnnod
                            int64_t cn, cudaStream_t s) {
   if (nent <= 0) return;
   k_galerkin_local<<<div_up(nent, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, orig_copy, nent, rdof, cdof, val,
-                                                                A1, cnx, cny, cn);
+                                                                A1, cnx, cny, cn); note_launch();
   (void)cnz;
 }
 
@@ -465,20 +465,20 @@ void launch_galerkin_stencil(const TransferDev& P, const double* Af, int fnx, in
                              int cny, int cnz, cudaStream_t s) {
   int64_t n = (int64_t)cnx * cny * cnz;
   dim3 blk(27, 8);
-  k_galerkin_stencil<<<div_up(n, 8), blk, 0, s>>>(P, Af, fnx, fny, fnz, Ac, cnx, cny, cnz);
+  k_galerkin_stencil<<<div_up(n, 8), blk, 0, s>>>(P, Af, fnx, fny, fnz, Ac, cnx, cny, cnz); note_launch();
 }
 
 void launch_stencil_diag(const double* A, int64_t n, double* D, cudaStream_t s) {
-  k_stencil_diag<<<div_up(n, kThreads), kThreads, 0, s>>>(A, n, D);
+  k_stencil_diag<<<div_up(n, kThreads), kThreads, 0, s>>>(A, n, D); note_launch();
 }
 
 void launch_add_diag_entries(int nent, const int* rdof, const int* cdof, const double* val, double* D, cudaStream_t s) {
   if (nent <= 0) return;
-  k_add_diag_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, D);
+  k_add_diag_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, D); note_launch();
 }
 
 void launch_block_inverse(const double* D, int64_t n, double* Dinv64, float* Dinv32, cudaStream_t s) {
-  k_block_inverse<<<div_up(n, kThreads), kThreads, 0, s>>>(D, n, Dinv64, Dinv32);
+  k_block_inverse<<<div_up(n, kThreads), kThreads, 0, s>>>(D, n, Dinv64, Dinv32); note_launch();
 }
 
 template void launch_stencil_apply<float>(const StencilView<float>&, const float*, float*, const int*, cudaStream_t);

@@ -31,6 +31,9 @@ void set_last_error(const char* fmt, ...);
     if (s_ != FEB_OK) return s_;   \
   } while (0)
 
+// host-side count of kernel launches issued by the library (feb_launch_count)
+void note_launch(int n = 1);
+
 constexpr int kThreads = 256;
 constexpr int kSmCount = 148;
 

@@ -191,26 +191,26 @@ void launch_dense_from_stencil(const double* A, int nx, int ny, int nz, const in
                                cudaStream_t s) {
   int64_t n = (int64_t)nx * ny * nz;
   dim3 blk(27, 8);
-  k_dense_from_stencil<<<div_up(n, 8), blk, 0, s>>>(A, nx, ny, nz, cmap, M, nd);
+  k_dense_from_stencil<<<div_up(n, 8), blk, 0, s>>>(A, nx, ny, nz, cmap, M, nd); note_launch();
 }
 
 void launch_dense_add_entries(int nent, const int* rdof, const int* cdof, const double* val, const int* cmap,
                               double* M, int nd, cudaStream_t s) {
-  if (nent > 0) k_dense_add_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, cmap, M, nd);
+  if (nent > 0) k_dense_add_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, cmap, M, nd); note_launch();
 }
 
 void launch_dense_invert(double* M, int nd, double* scratch, int* status, cudaStream_t s) {
-  k_symmetrize<<<div_up((int64_t)nd * nd, kThreads), kThreads, 0, s>>>(M, nd);
+  k_symmetrize<<<div_up((int64_t)nd * nd, kThreads), kThreads, 0, s>>>(M, nd); note_launch();
   double* Dinv = scratch;
   double* Trow = scratch + GJ_B * GJ_B;
   for (int k0 = 0; k0 < nd; k0 += GJ_B) {
     int bs = std::min(GJ_B, nd - k0);
-    k_gj_pivot<<<1, 256, 0, s>>>(M, nd, k0, bs, Dinv, status);
+    k_gj_pivot<<<1, 256, 0, s>>>(M, nd, k0, bs, Dinv, status); note_launch();
     dim3 g1(div_up(nd, 128), bs);
-    k_gj_row<<<g1, 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow);
+    k_gj_row<<<g1, 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow); note_launch();
     dim3 g2(div_up(nd, GJ_T), div_up(nd, GJ_T));
-    k_gj_update<<<g2, 256, 0, s>>>(M, nd, k0, bs, Trow);
-    k_gj_finish<<<div_up(nd, 128), 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow);
+    k_gj_update<<<g2, 256, 0, s>>>(M, nd, k0, bs, Trow); note_launch();
+    k_gj_finish<<<div_up(nd, 128), 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow); note_launch();
   }
 }
 
@@ -220,9 +220,9 @@ template <typename T>
 void launch_dense_solve(const double* Minv, int nd, const int* klist, const int* cmap, int64_t n, const T* b, T* x,
                         double* bd, double* xd, const int* skip, cudaStream_t s) {
   int nk = nd / 3;
-  k_dense_gather<T><<<div_up(nd, kThreads), kThreads, 0, s>>>(b, klist, nk, bd, skip);
-  k_dense_gemv<<<div_up(nd, 8), 256, 0, s>>>(Minv, bd, xd, nd, skip);
-  k_dense_scatter<T><<<div_up(3 * n, kThreads), kThreads, 0, s>>>(xd, cmap, n, x, skip);
+  k_dense_gather<T><<<div_up(nd, kThreads), kThreads, 0, s>>>(b, klist, nk, bd, skip); note_launch();
+  k_dense_gemv<<<div_up(nd, 8), 256, 0, s>>>(Minv, bd, xd, nd, skip); note_launch();
+  k_dense_scatter<T><<<div_up(3 * n, kThreads), kThreads, 0, s>>>(xd, cmap, n, x, skip); note_launch();
 }
 
 template void launch_dense_solve<float>(const double*, int, const int*, const int*, int64_t, const float*, float*,

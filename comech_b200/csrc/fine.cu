@@ -315,9 +315,9 @@ template <int MODE>
 void launch_dense_from_fine(const FineView<double>& F, const int* cmap, double* M, int nd, cudaStream_t s) {
   int64_t n = (int64_t)F.nx * F.ny * F.nz + F.nirr;
   dim3 blk(24, 8);
-  k_dense_from_fine<MODE><<<div_up(n, 8), blk, 0, s>>>(F, cmap, M, nd);
-  if (F.npen) k_dense_penalty<<<div_up(F.npen, kThreads), kThreads, 0, s>>>(F, cmap, M, nd);
-  if (F.nrow) k_dense_csr<<<div_up(F.nrow, kThreads), kThreads, 0, s>>>(F, cmap, M, nd);
+  k_dense_from_fine<MODE><<<div_up(n, 8), blk, 0, s>>>(F, cmap, M, nd); note_launch();
+  if (F.npen) k_dense_penalty<<<div_up(F.npen, kThreads), kThreads, 0, s>>>(F, cmap, M, nd); note_launch();
+  if (F.nrow) k_dense_csr<<<div_up(F.nrow, kThreads), kThreads, 0, s>>>(F, cmap, M, nd); note_launch();
 }
 template void launch_dense_from_fine<MAT_ISO_SRI>(const FineView<double>&, const int*, double*, int, cudaStream_t);
 template void launch_dense_from_fine<MAT_ISO_FULL>(const FineView<double>&, const int*, double*, int, cudaStream_t);
@@ -327,21 +327,21 @@ template <typename T, int MODE>
 void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, int zchunk, cudaStream_t s) {
   dim3 block(TX, TY);
   dim3 grid(div_up(F.nxn, TX - 1), div_up(F.nyn, TY - 1), div_up(F.nzn, zchunk));
-  k_fine_struct<T, MODE><<<grid, block, 0, s>>>(F, u, y, skip, zchunk);
+  k_fine_struct<T, MODE><<<grid, block, 0, s>>>(F, u, y, skip, zchunk); note_launch();
   if (F.ntotal > F.nnode) {
     int64_t n = 3 * (F.ntotal - F.nnode);
-    k_zero_tail<T><<<div_up(n, kThreads), kThreads, 0, s>>>(y, 3 * F.nnode, 3 * F.ntotal, skip);
+    k_zero_tail<T><<<div_up(n, kThreads), kThreads, 0, s>>>(y, 3 * F.nnode, 3 * F.ntotal, skip); note_launch();
   }
   int b_irr = div_up(F.nirr, kThreads), b_pen = div_up(F.npen, kThreads), b_row = div_up(F.nrow, kThreads);
   if (b_irr + b_pen + b_row > 0)
-    k_fine_sparse<T, MODE><<<b_irr + b_pen + b_row, kThreads, 0, s>>>(F, u, y, skip, b_irr, b_pen);
+    k_fine_sparse<T, MODE><<<b_irr + b_pen + b_row, kThreads, 0, s>>>(F, u, y, skip, b_irr, b_pen); note_launch();
 }
 
 template <int MODE>
 void launch_fine_diag(const FineView<double>& F, double* D, cudaStream_t s) {
-  k_fine_diag_grid<MODE><<<div_up(F.ntotal, kThreads), kThreads, 0, s>>>(F, D);
+  k_fine_diag_grid<MODE><<<div_up(F.ntotal, kThreads), kThreads, 0, s>>>(F, D); note_launch();
   int n = max(F.nirr, max(F.npen, F.nrow));
-  if (n > 0) k_fine_diag_sparse<MODE><<<div_up(n, kThreads), kThreads, 0, s>>>(F, D);
+  if (n > 0) k_fine_diag_sparse<MODE><<<div_up(n, kThreads), kThreads, 0, s>>>(F, D); note_launch();
 }
 
 #define INST(T, M) template void launch_fine_apply<T, M>(const FineView<T>&, const T*, T*, const int*, int, cudaStream_t);

@@ -132,7 +132,7 @@ __global__ void k_z_column(RigidView Z, int col, double* __restrict__ v) {
 int rigid_blocks(const RigidView& Z) { (void)Z; return 2 * kSmCount / 4; }
 
 void launch_centroids(const RigidView& Z, double* cen, cudaStream_t s) {
-  k_centroids<<<Z.ngroups, kThreads, 0, s>>>(Z, cen);
+  k_centroids<<<Z.ngroups, kThreads, 0, s>>>(Z, cen); note_launch();
 }
 
 template <typename T>
@@ -140,21 +140,21 @@ void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, doub
                         const double* Einv, const int* skip, cudaStream_t s) {
   int nb = rigid_blocks(Z);
   dim3 g(nb, Z.ngroups);
-  k_ztr_partial<T><<<g, kThreads, 0, s>>>(Z, r, part, skip);
-  k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, Einv, zr, coef, skip);
-  if (Einv) k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip);
+  k_ztr_partial<T><<<g, kThreads, 0, s>>>(Z, r, part, skip); note_launch();
+  k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, Einv, zr, coef, skip); note_launch();
+  if (Einv) k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip); note_launch();
 }
 
 void launch_ztr(const RigidView& Z, const double* r, double* part, double* zr, cudaStream_t s) {
   int nb = rigid_blocks(Z);
   dim3 g(nb, Z.ngroups);
-  k_ztr_partial<double><<<g, kThreads, 0, s>>>(Z, r, part, nullptr);
-  k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, nullptr, zr, nullptr, nullptr);
+  k_ztr_partial<double><<<g, kThreads, 0, s>>>(Z, r, part, nullptr); note_launch();
+  k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, nullptr, zr, nullptr, nullptr); note_launch();
 }
 
 void launch_z_column(const RigidView& Z, int col, double* v, cudaStream_t s) {
   dim3 g(rigid_blocks(Z));
-  k_z_column<<<g, kThreads, 0, s>>>(Z, col, v);
+  k_z_column<<<g, kThreads, 0, s>>>(Z, col, v); note_launch();
 }
 
 template void launch_rigid_apply<float>(const RigidView&, const float*, float*, double*, double*, double*,

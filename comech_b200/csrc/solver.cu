@@ -7,6 +7,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -24,6 +25,9 @@
 namespace feb {
 
 static thread_local char g_err[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_last_error(const char* fmt, ...) {
   va_list ap;
@@ -530,10 +534,12 @@ struct FebHandle {
   int capture(CgState* S, bool inner, cudaGraphExec_t* exec, int* nodes) {
     if (*exec) return FEB_OK;
     cudaGraph_t g;
+    const long long before = g_launches.load();
     FEB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
     else cg_body<double>(S, x, r, z, p, q);
     FEB_CUDA(cudaStreamEndCapture(s, &g));
+    g_launches.store(before);   // captured kernels are counted when the graph runs
     size_t nn = 0;
     FEB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
     *nodes = (int)nn;
@@ -556,6 +562,7 @@ struct FebHandle {
         if (opt.use_graphs) {
           FEB_CUDA(cudaGraphLaunch(*ex, s));
           launches += *nn;
+          note_launch(*nn);
         } else {
           if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
           else cg_body<double>(S, x, r, z, p, q);
@@ -635,7 +642,7 @@ __global__ void k_count(const uint8_t* __restrict__ m, int64_t n, unsigned long 
 int count_mask(FebHandle* h, const uint8_t* m, int64_t n, int64_t* out) {
   unsigned long long* d = nullptr;
   FEB_TRY(h->pool.zeros(&d, 1));
-  k_count<<<std::min<int64_t>(div_up(n, kThreads), 4 * kSmCount), kThreads, 0, h->s>>>(m, n, d);
+  k_count<<<std::min<int64_t>(div_up(n, kThreads), 4 * kSmCount), kThreads, 0, h->s>>>(m, n, d); note_launch();
   unsigned long long v = 0;
   FEB_CUDA(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, h->s));
   FEB_CUDA(cudaStreamSynchronize(h->s));
@@ -734,7 +741,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   FEB_TRY(H.pool.alloc(&irr_flag, ncell));
   FEB_TRY(H.pool.zeros(&V.used, H.ntotal));
   k_prepare_cells<W><<<div_up(ncell, kThreads), kThreads, 0, s>>>(H.nx, H.ny, H.nz, op->mat, H.mode, op->active, op->cn,
-                                                                  H.mat_all, mat_s64, mat_s32, irr_flag, V.used);
+                                                                  H.mat_all, mat_s64, mat_s32, irr_flag, V.used); note_launch();
   FEB_CUDA(cudaGetLastError());
   // irregular cells, in ascending cell-id order
   int nirr = 0;
@@ -760,7 +767,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
       FEB_TRY(H.pool.alloc(&irr_m64, W * (size_t)nirr));
       FEB_TRY(H.pool.alloc(&irr_m32, W * (size_t)nirr));
       k_build_irregular<W><<<div_up(nirr, kThreads), kThreads, 0, s>>>(H.nx, H.ny, H.nz, sel, nirr, op->mat, H.mode,
-                                                                        op->cn, irr_cell, irr_nodes, irr_m64, irr_m32);
+                                                                        op->cn, irr_cell, irr_nodes, irr_m64, irr_m32); note_launch();
       FEB_CUDA(cudaGetLastError());
     }
     H.pool.free(tmp); H.pool.free(sel); H.pool.free(nsel);
@@ -770,7 +777,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   if (H.ntotal > H.nnode) {
     if (!op->orig) { set_last_error("feb_create: nnode_total > grid nodes needs orig"); return FEB_ERR_ARG; }
     FEB_TRY(H.pool.alloc(&H.orig_copy, H.ntotal - H.nnode));
-    k_orig_copy<<<div_up(H.ntotal - H.nnode, kThreads), kThreads, 0, s>>>(op->orig, H.nnode, H.ntotal, H.orig_copy);
+    k_orig_copy<<<div_up(H.ntotal - H.nnode, kThreads), kThreads, 0, s>>>(op->orig, H.nnode, H.ntotal, H.orig_copy); note_launch();
     std::vector<int> oc(H.ntotal - H.nnode);
     FEB_CUDA(cudaMemcpyAsync(oc.data(), H.orig_copy, oc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
     FEB_CUDA(cudaStreamSynchronize(s));
@@ -1184,10 +1191,10 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   FebInfo inf{};
   FEB_CUDA(cudaEventRecord(H.ev0, H.s));
   // loads and start values on nodes no active cell uses are dropped (fe/solver.py:216-219)
-  k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(f, H.L[0].used, H.ntotal, H.fb);
+  k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(f, H.L[0].used, H.ntotal, H.fb); note_launch();
   f = H.fb;
   if (x0) {
-    k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(x0, H.L[0].used, H.ntotal, H.z);
+    k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(x0, H.L[0].used, H.ntotal, H.z); note_launch();
     x0 = H.z;
   }
   int st = FEB_OK;
@@ -1284,7 +1291,7 @@ int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y) {
 int feb_export_solution(FebHandle* h, const double* x, double* U) {
   if (!h || !x || !U) { set_last_error("feb_export_solution: null argument"); return FEB_ERR_ARG; }
   FEB_TRY(h->sync_in());
-  k_export<<<div_up(3 * h->ntotal, kThreads), kThreads, 0, h->s>>>(x, h->L[0].used, h->ntotal, U);
+  k_export<<<div_up(3 * h->ntotal, kThreads), kThreads, 0, h->s>>>(x, h->L[0].used, h->ntotal, U); note_launch();
   FEB_CUDA(cudaGetLastError());
   return h->sync_out();
 }
@@ -1298,6 +1305,24 @@ int feb_used_nodes(FebHandle* h, int64_t* nused, uint8_t* mask) {
     return h->sync_out();
   }
   return FEB_OK;
+}
+
+int64_t feb_launch_count(void) { return g_launches.load(); }
+
+int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms) {
+  if (!h || !u || !y || nrep < 1 || !ms) { set_last_error("feb_benchmark_apply: bad argument"); return FEB_ERR_ARG; }
+  FEB_TRY(h->sync_in());
+  FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+  for (int i = 0; i < nrep; ++i) {
+    if (prec == 0) h->apply<double>(0, (const double*)u, (double*)y, nullptr);
+    else h->apply<float>(0, (const float*)u, (float*)y, nullptr);
+  }
+  FEB_CUDA(cudaEventRecord(h->ev1, h->s));
+  FEB_CUDA(cudaEventSynchronize(h->ev1));
+  float t = 0.f;
+  FEB_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+  *ms = t / nrep;
+  return h->sync_out();
 }
 
 int feb_destroy(FebHandle* h) {

@@ -140,7 +140,7 @@ extern "C" int feb_cell_stress(const FebGrid* grid, int32_t mat_mode, const doub
   FEB_TRY(make_geom(grid, G, &buf, s));
   int64_t nct = (int64_t)grid->nx * grid->ny * grid->nz;
   k_cell_stress<<<div_up(ncells, kThreads), kThreads, 0, s>>>(G, mat_mode, mat, nct, U, ncells, cells, cn,
-                                                              nan_to_zero, sig, vm, eps);
+                                                              nan_to_zero, sig, vm, eps); note_launch();
   FEB_CUDA(cudaGetLastError());
   FEB_CUDA(cudaFreeAsync(buf, s));
   return FEB_OK;
@@ -158,7 +158,7 @@ extern "C" int feb_element_forces(const FebGrid* grid, const double* mat, const 
   double* buf = nullptr;
   FEB_TRY(make_geom(grid, G, &buf, s));
   int64_t nct = (int64_t)grid->nx * grid->ny * grid->nz;
-  k_element_forces<<<div_up(ncells, kThreads), kThreads, 0, s>>>(G, mat, nct, U, ncells, cells, cn, out);
+  k_element_forces<<<div_up(ncells, kThreads), kThreads, 0, s>>>(G, mat, nct, U, ncells, cells, cn, out); note_launch();
   FEB_CUDA(cudaGetLastError());
   FEB_CUDA(cudaFreeAsync(buf, s));
   return FEB_OK;
@@ -170,7 +170,7 @@ extern "C" int feb_accumulate_nodal(int64_t n, const int64_t* nodes, const doubl
     return FEB_ERR_ARG;
   }
   if (n == 0) return FEB_OK;
-  k_accumulate_nodal<<<div_up(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(n, nodes, vals, dst);
+  k_accumulate_nodal<<<div_up(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(n, nodes, vals, dst); note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
 }

@@ -254,82 +254,82 @@ inline int grid_for(int64_t n) { return int(std::min<int64_t>((n + kThreads - 1)
 
 template <typename Ta, typename Tb>
 void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s) {
-  k_dot_partial<Ta, Tb><<<kRedBlocks, kThreads, 0, s>>>(a, b, n, partials, skip);
+  k_dot_partial<Ta, Tb><<<kRedBlocks, kThreads, 0, s>>>(a, b, n, partials, skip); note_launch();
 }
 
 void launch_finalize(int kind, const double* partials, CgState* st, LevelParams* lp, int deg, const int* skip,
                      cudaStream_t s) {
-  k_finalize<<<1, kThreads, 0, s>>>(kind, partials, kRedBlocks, st, lp, deg, skip);
+  k_finalize<<<1, kThreads, 0, s>>>(kind, partials, kRedBlocks, st, lp, deg, skip); note_launch();
 }
 
 template <typename T>
 void launch_update_p(const T* z, T* p, const CgState* st, int64_t n, const int* skip, cudaStream_t s) {
-  k_update_p<T><<<grid_for(n), kThreads, 0, s>>>(z, p, st, n, skip);
+  k_update_p<T><<<grid_for(n), kThreads, 0, s>>>(z, p, st, n, skip); note_launch();
 }
 
 template <typename T>
 void launch_update_xr(const T* p, const T* q, T* x, T* r, const CgState* st, int64_t n, double* partials,
                       const int* skip, cudaStream_t s) {
-  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, st, n, partials, skip);
+  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, st, n, partials, skip); note_launch();
 }
 
 template <typename T>
 void launch_cheb_first(const T* b, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
                        const int* skip, cudaStream_t s) {
-  k_cheb_first<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, r, d, x, Dinv, lp, nn, skip);
+  k_cheb_first<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, r, d, x, Dinv, lp, nn, skip); note_launch();
 }
 
 template <typename T>
 void launch_cheb_init(const T* b, const T* Ax, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
                       const int* skip, cudaStream_t s) {
-  k_cheb_init<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, Ax, r, d, x, Dinv, lp, nn, skip);
+  k_cheb_init<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, Ax, r, d, x, Dinv, lp, nn, skip); note_launch();
 }
 
 template <typename T>
 void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int k, int64_t nn,
                       const int* skip, cudaStream_t s) {
-  k_cheb_step<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(Ad, r, d, x, Dinv, lp, k, nn, skip);
+  k_cheb_step<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(Ad, r, d, x, Dinv, lp, k, nn, skip); note_launch();
 }
 
 template <typename T>
 void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s) {
-  k_residual<T><<<grid_for(n), kThreads, 0, s>>>(b, Ax, r, n, skip);
+  k_residual<T><<<grid_for(n), kThreads, 0, s>>>(b, Ax, r, n, skip); note_launch();
 }
 
 void launch_random_start(double* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s) {
-  k_random_start<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(x, mask, nn, seed);
+  k_random_start<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(x, mask, nn, seed); note_launch();
 }
 
 void launch_bj_apply_norm(const double* Dinv, const double* v, double* y, int64_t nn, double* partials,
                           cudaStream_t s) {
-  k_bj_apply_norm<<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials);
+  k_bj_apply_norm<<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials); note_launch();
 }
 
 void launch_scale(const double* y, double* x, const LevelParams* lp, int64_t n, cudaStream_t s) {
-  k_scale<<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n);
+  k_scale<<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n); note_launch();
 }
 
 template <typename Ts, typename Td>
 void launch_convert(const Ts* src, Td* dst, int64_t n, const int* skip, cudaStream_t s) {
-  k_convert<Ts, Td><<<grid_for(n), kThreads, 0, s>>>(src, dst, n, skip);
+  k_convert<Ts, Td><<<grid_for(n), kThreads, 0, s>>>(src, dst, n, skip); note_launch();
 }
 
 template <typename T>
 void launch_axpy_dev(const T* x, T* y, int64_t n, const int* skip, cudaStream_t s) {
-  k_axpy_dev<T><<<grid_for(n), kThreads, 0, s>>>(x, y, n, skip);
+  k_axpy_dev<T><<<grid_for(n), kThreads, 0, s>>>(x, y, n, skip); note_launch();
 }
 
 void launch_add_scaled(const float* e, double* x, const double* scale, int64_t n, const int* skip, cudaStream_t s) {
-  k_add_scaled<<<grid_for(n), kThreads, 0, s>>>(e, x, scale, n, skip);
+  k_add_scaled<<<grid_for(n), kThreads, 0, s>>>(e, x, scale, n, skip); note_launch();
 }
 
 void launch_scale_to_float(const double* r, float* rf, const double* scale_inv, int64_t n, const int* skip,
                            cudaStream_t s) {
-  k_scale_to_float<<<grid_for(n), kThreads, 0, s>>>(r, rf, scale_inv, n, skip);
+  k_scale_to_float<<<grid_for(n), kThreads, 0, s>>>(r, rf, scale_inv, n, skip); note_launch();
 }
 
 void launch_mask_vector(double* v, const uint8_t* used, int64_t nn, double fill, cudaStream_t s) {
-  k_mask_vector<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(v, used, nn, fill);
+  k_mask_vector<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(v, used, nn, fill); note_launch();
 }
 
 #define INST_T(T)                                                                                              \

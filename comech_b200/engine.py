@@ -33,8 +33,17 @@ def _torch():
     return torch
 
 
+_TDT = {np.float64: "float64", np.int64: "int64", np.uint8: "uint8", np.float32: "float32"}
+
+
 def _dev(a, dtype):
+    """Device tensor of ``a`` (CUDA tensors of the right dtype pass through untouched)."""
     torch = _torch()
+    if isinstance(a, torch.Tensor):
+        want = getattr(torch, _TDT[dtype])
+        if a.is_cuda and a.dtype == want and a.is_contiguous():
+            return a
+        return a.to(device="cuda", dtype=want).contiguous()
     t = torch.from_numpy(np.ascontiguousarray(a, dtype=dtype))
     return t.to("cuda", non_blocking=False)
 
@@ -78,7 +87,10 @@ class Problem:
         self.ntotal = len(orig) if orig is not None else self.nnode
         self.mat_mode = mat_mode
         self.mat = _dev(mat, np.float64)
-        self.active = _dev(np.asarray(active, dtype=bool).view(np.uint8), np.uint8)
+        if isinstance(active, torch.Tensor):
+            self.active = _dev(active, np.uint8)
+        else:
+            self.active = _dev(np.asarray(active, dtype=bool).view(np.uint8), np.uint8)
         self.cn = _dev(cn, np.int64) if cn is not None else None
         self.orig = _dev(orig, np.int64) if (orig is not None and self.ntotal > self.nnode) else None
         pen_node = np.ascontiguousarray(pen_node if pen_node is not None else np.zeros(0), dtype=np.int64)
@@ -115,22 +127,34 @@ class Problem:
     def __exit__(self, *a):
         self.close()
 
-    def set_rigid_groups(self, node_groups):
-        if not node_groups:
+    def set_rigid_groups(self, node_groups, offsets=None):
+        """node_groups: list of node-id arrays, or (with ``offsets``) one concatenated array / device tensor."""
+        if node_groups is None or (offsets is None and len(node_groups) == 0):
             return
-        groups = [np.asarray(gr, dtype=np.int64) for gr in node_groups]
-        off = np.zeros(len(groups) + 1, np.int64)
-        off[1:] = np.cumsum([len(gr) for gr in groups])
-        nodes = _dev(np.concatenate(groups) if groups else np.zeros(0), np.int64)
+        if offsets is None:
+            groups = [np.asarray(gr, dtype=np.int64) for gr in node_groups]
+            off = np.zeros(len(groups) + 1, np.int64)
+            off[1:] = np.cumsum([len(gr) for gr in groups])
+            nodes = _dev(np.concatenate(groups), np.int64)
+        else:
+            off = np.ascontiguousarray(offsets, dtype=np.int64)
+            groups = [None] * (len(off) - 1)
+            nodes = _dev(node_groups, np.int64)
         _lib.check(_lib.load().feb_set_rigid_groups(self.h, len(groups), off.ctypes.data, _ptr(nodes)))
 
     def rhs(self, loads):
-        """Nodal load vector (full layout) from (nodes, area, traction) lists (rb/splitfe.py:144-147)."""
+        """Nodal load vector (full layout) from (nodes, area, traction) lists (rb/splitfe.py:144-147), or from
+        (nodes, values (n, 3)) pairs already on the device."""
         f = self.torch.zeros(3 * self.ntotal, dtype=self.torch.float64, device="cuda")
-        for nodes, area, t in loads:
-            nodes = np.asarray(nodes, dtype=np.int64)
-            vals = np.asarray(area, dtype=np.float64)[:, None] * np.asarray(t, dtype=np.float64)[None, :]
-            nd, vd = _dev(nodes, np.int64), _dev(vals, np.float64)
+        for item in loads:
+            if len(item) == 2:
+                nd, vd = _dev(item[0], np.int64), _dev(item[1], np.float64)
+                nodes = nd
+            else:
+                nodes, area, t = item
+                nodes = np.asarray(nodes, dtype=np.int64)
+                vals = np.asarray(area, dtype=np.float64)[:, None] * np.asarray(t, dtype=np.float64)[None, :]
+                nd, vd = _dev(nodes, np.int64), _dev(vals, np.float64)
             _lib.check(_lib.load().feb_accumulate_nodal(len(nodes), _ptr(nd), _ptr(vd), _ptr(f), _stream()))
         return f
 
@@ -193,6 +217,7 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
     if aniso is not None:
         raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
     t0 = time.perf_counter()
+    stamps = [("start", t0)]
     ncell = g.nx * g.ny * g.nz
     orig = np.asarray(orig)
     ntotal = len(orig)
@@ -207,18 +232,24 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
 
     coo = _extra_entries(extra, used_nodes, ntotal)
     mat = np.concatenate([np.asarray(lam, np.float64).ravel(), np.asarray(mu, np.float64).ravel()])
+    stamps.append(("host_inputs", time.perf_counter()))
     P = Problem(g, _lib.MAT_ISO_SRI, mat, active, cn=cn, orig=orig, pen_node=fn, pen_k=pen_k, extra_coo=coo,
                 precision=precision, tol=tol, maxiter=maxiter, options=options)
+    stamps.append(("create", time.perf_counter()))
     try:
         P.set_rigid_groups(node_groups)
+        stamps.append(("rigid", time.perf_counter()))
         f = P.rhs(loads)
         x0d = _dev(np.nan_to_num(np.asarray(x0, np.float64)).ravel(), np.float64) if x0 is not None else None
         x, info = P.solve(f, x0d)
+        stamps.append(("solve", time.perf_counter()))
         Ud = P.export(x)
         U = Ud.view(ntotal, 3).cpu().numpy()
+        stamps.append(("download", time.perf_counter()))
         R = np.zeros((ntotal, 3))
         np.add.at(R, fn, -(fa[:, None] * K_GROUND) * U[fn])
-        d = _info_dict(info, t0)
+        stamps.append(("reactions", time.perf_counter()))
+        d = _info_dict(info, t0, dict(t_host={b[0]: round(b[1] - a[1], 4) for a, b in zip(stamps, stamps[1:])}))
         if keep_device:
             d["device"] = dict(U=Ud, mat=P.mat, cn=P.cn, problem=P)
         return U, d, R
@@ -295,9 +326,8 @@ def solve(grid, lam, mu, active, springs, loads, method="cg", tol=1e-8, x0=None,
         P.close()
 
 
-def _stress(g, mode, mat, U, cells, cn, nan_to_zero):
+def _stress(g, mode, mat, U, cells, cn, nan_to_zero, to_host=True):
     torch = _torch()
-    cells = np.asarray(cells, np.int64)
     n = len(cells)
     Ud = U if isinstance(U, torch.Tensor) else _dev(np.asarray(U, np.float64).ravel(), np.float64)
     matd = mat if isinstance(mat, torch.Tensor) else _dev(mat, np.float64)
@@ -309,6 +339,8 @@ def _stress(g, mode, mat, U, cells, cn, nan_to_zero):
     gs = _grid_struct(g)
     _lib.check(_lib.load().feb_cell_stress(C.byref(gs), mode, _ptr(matd), _ptr(Ud), n, _ptr(cd), _ptr(cnd),
                                            int(nan_to_zero), _ptr(sig), _ptr(vm), _ptr(eps), _stream()))
+    if not to_host:
+        return sig.view(n, 6), vm, eps.view(n, 6)
     return sig.view(n, 6).cpu().numpy(), vm.cpu().numpy(), eps.view(n, 6).cpu().numpy()
 
 

@@ -149,6 +149,12 @@ FEB_API int feb_cell_stress(const FebGrid* grid, int32_t mat_mode, const double*
 FEB_API int feb_element_forces(const FebGrid* grid, const double* mat, const double* U, int64_t ncells,
                        const int64_t* cells, const int64_t* cn, double* out, void* stream);
 
+/* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
+FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
+
+/* Kernels launched by this library since it was loaded (graph launches count their kernel nodes). */
+FEB_API int64_t feb_launch_count(void);
+
 FEB_API const char* feb_last_error(void);
 
 #ifdef __cplusplus
