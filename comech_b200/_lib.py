@@ -17,7 +17,7 @@ PREC = {"fp64": 0, "mixed": 1, "refine": 2}
 
 EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_solve", "feb_apply",
            "feb_export_solution", "feb_used_nodes", "feb_destroy", "feb_accumulate_nodal", "feb_cell_stress",
-           "feb_element_forces", "feb_benchmark_apply", "feb_launch_count", "feb_last_error"]
+           "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_launch_count", "feb_last_error"]
 
 
 class FebGrid(C.Structure):
@@ -75,6 +75,7 @@ def load():
     lib.feb_destroy.argtypes = [P]
     lib.feb_accumulate_nodal.argtypes = [C.c_int64, P, P, P, P]
     lib.feb_cell_stress.argtypes = [C.POINTER(FebGrid), C.c_int32, P, P, C.c_int64, P, P, C.c_int32, P, P, P, P]
+    lib.feb_cell_stress_noalloc.argtypes = lib.feb_cell_stress.argtypes
     lib.feb_element_forces.argtypes = [C.POINTER(FebGrid), P, P, C.c_int64, P, P, P, P]
     lib.feb_benchmark_apply.argtypes = [P, C.c_int32, P, P, C.c_int32, C.POINTER(C.c_float)]
     lib.feb_launch_count.argtypes = []

@@ -1,5 +1,7 @@
 // Stress / von Mises recovery and element forces (fe/solver.py:257-272, rb/splitfe.py:161-193),
 // nodal accumulation of loads (rb/splitfe.py:144-147).
+#include <mutex>
+
 #include "element.cuh"
 
 namespace feb {
@@ -171,6 +173,107 @@ extern "C" int feb_accumulate_nodal(int64_t n, const int64_t* nodes, const doubl
   }
   if (n == 0) return FEB_OK;
   k_accumulate_nodal<<<div_up(n, kThreads), kThreads, 0, (cudaStream_t)stream>>>(n, nodes, vals, dst); note_launch();
+  FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Allocation-free variant of feb_cell_stress.
+//
+// feb_cell_stress keeps the per-axis cell widths in a scratch buffer that it allocates on every call.
+// Some callers cannot allocate device memory at the point where they need stresses: a host framework
+// that hands the library a fixed memory arena and forbids allocations inside its step, an enqueue
+// callback of a plugin interface, or a latency-critical loop in which cudaMalloc's implicit device
+// synchronisation is unacceptable.  For them this variant keeps the scratch (grid edges and cell
+// widths) in one file-scope device array of fixed size, so the call allocates nothing.
+//
+// Limits and contract:
+//   * at most kNoAllocMaxCells cells along each axis (192 KB of device memory, held by every GPU that
+//     loads the library until the process exits); larger grids are rejected with FEB_ERR_ARG;
+//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+//     device current, and caches it per device: make that first call before any stream capture;
+//   * all calls share the one array and it keeps the last call's contents (every call overwrites all
+//     of it that it reads), so calls whose work overlaps on the GPU race: order them on one stream.
+namespace feb {
+namespace {
+
+constexpr int kNoAllocMaxCells = 4096;
+constexpr int kNoAllocEdges = kNoAllocMaxCells + 1;
+static __device__ __align__(256) double g_noalloc_scratch[3 * kNoAllocEdges + 3 * kNoAllocMaxCells];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kMaxDevices] = {};
+
+// device address of g_noalloc_scratch on the current device (looked up once per device)
+int noalloc_scratch(double** out) {
+  int dev = -1;
+  FEB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_last_error("feb_cell_stress_noalloc: device %d out of range", dev);
+    return FEB_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_last_error("feb_cell_stress_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return FEB_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return FEB_OK;
+}
+
+// widths[a][i] = edges[a][i+1] - edges[a][i] inside the scratch array
+__global__ void k_noalloc_widths(const double* __restrict__ edges, double* __restrict__ widths, int nx, int ny,
+                                 int nz) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a) {
+    if (t < n[a]) {
+      const double* e = edges + a * kNoAllocEdges;
+      widths[a * kNoAllocMaxCells + t] = e[t + 1] - e[t];
+    }
+  }
+}
+
+}  // namespace
+}  // namespace feb
+
+extern "C" int feb_cell_stress_noalloc(const FebGrid* grid, int32_t mat_mode, const double* mat, const double* U,
+                                       int64_t ncells, const int64_t* cells, const int64_t* cn, int32_t nan_to_zero,
+                                       double* sig, double* vm, double* eps, void* stream) {
+  if (!grid || !grid->xe || !grid->ye || !grid->ze || !mat || !U || !cells || !sig || !vm || ncells < 0) {
+    set_last_error("feb_cell_stress_noalloc: null argument");
+    return FEB_ERR_ARG;
+  }
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->nx > kNoAllocMaxCells || grid->ny > kNoAllocMaxCells ||
+      grid->nz > kNoAllocMaxCells) {
+    set_last_error("feb_cell_stress_noalloc: grid %d x %d x %d cells; this entry point supports 1..%d cells per axis",
+                   grid->nx, grid->ny, grid->nz, kNoAllocMaxCells);
+    return FEB_ERR_ARG;
+  }
+  double* scratch = nullptr;
+  FEB_TRY(noalloc_scratch(&scratch));
+  if (ncells == 0) return FEB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  double* edges = scratch;
+  double* widths = scratch + 3 * kNoAllocEdges;
+  const double* src[3] = {grid->xe, grid->ye, grid->ze};
+  const int n[3] = {grid->nx, grid->ny, grid->nz};
+  for (int a = 0; a < 3; ++a)
+    FEB_CUDA(cudaMemcpyAsync(edges + a * kNoAllocEdges, src[a], (n[a] + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+  int mx = std::max(n[0], std::max(n[1], n[2]));
+  k_noalloc_widths<<<div_up(mx, kThreads), kThreads, 0, s>>>(edges, widths, n[0], n[1], n[2]); note_launch();
+  GridGeom G;
+  G.nx = n[0]; G.ny = n[1]; G.nz = n[2];
+  G.dx = widths; G.dy = widths + kNoAllocMaxCells; G.dz = widths + 2 * kNoAllocMaxCells;
+  int64_t nct = (int64_t)n[0] * n[1] * n[2];
+  k_cell_stress<<<div_up(ncells, kThreads), kThreads, 0, s>>>(G, mat_mode, mat, nct, U, ncells, cells, cn,
+                                                              nan_to_zero, sig, vm, eps); note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
 }

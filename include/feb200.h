@@ -144,6 +144,18 @@ FEB_API int feb_cell_stress(const FebGrid* grid, int32_t mat_mode, const double*
                     const int64_t* cells, const int64_t* cn, int32_t nan_to_zero, double* sig, double* vm,
                     double* eps, void* stream);
 
+/* feb_cell_stress without any device allocation, for callers that cannot allocate device memory at the
+ * point of the call (a fixed memory arena owned by a host framework, a plugin's enqueue callback, a
+ * latency-critical loop that must not synchronise on cudaMalloc).  Same arguments and results as
+ * feb_cell_stress.  Its scratch (grid edges and cell widths) is one fixed file-scope device array:
+ * at most 4096 cells per axis (larger grids: FEB_ERR_ARG), 192 KB held on every GPU that loads the
+ * library until exit.  The first call on a device looks up that array's address with the device
+ * current; make it before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race, so order them on one stream.  No counterpart in the reference (its stress recovery is NumPy). */
+FEB_API int feb_cell_stress_noalloc(const FebGrid* grid, int32_t mat_mode, const double* mat, const double* U,
+                                    int64_t ncells, const int64_t* cells, const int64_t* cn, int32_t nan_to_zero,
+                                    double* sig, double* vm, double* eps, void* stream);
+
 /* Internal nodal forces K_e u_e of listed cells with the SRI lambda term (rb/splitfe.py:178-193);
  * out [dev] ncells x 8 x 3. */
 FEB_API int feb_element_forces(const FebGrid* grid, const double* mat, const double* U, int64_t ncells,
