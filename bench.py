@@ -1,6 +1,7 @@
 #!/usr/bin/env python
 """Seconds per solve to rel-res 1e-8 of the synthetic ~5M-DOF hindfoot (160x112x96 voxels, h = 0.5 mm) on
-one B200, mixed precision (FP64 refinement around an FP32 GMG-PCG) next to the plain FP64 GMG-PCG.
+one B200, mixed precision (FP64 CG around an FP32 multigrid V-cycle; --precision refine: FP64 iterative
+refinement around an all-FP32 GMG-PCG) next to the plain FP64 GMG-PCG.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -137,13 +138,16 @@ def device_inputs(P):
     return d
 
 
+SOLVER_OPTIONS = {}
+
+
 def device_solve(P, d, precision, x0=None):
     """One solve from device-resident inputs (same work as engine.solve_cn + cell_stress_cn)."""
     from comech_b200 import engine, _lib
     g = P["grid"]
     pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], precision=precision, tol=TOL,
-                        maxiter=800)
+                        maxiter=800, options=SOLVER_OPTIONS)
     try:
         pr.set_rigid_groups(d["g_nodes"], offsets=d["g_off"])
         f = pr.rhs([(d["l_nodes"], d["l_vals"])])
@@ -340,8 +344,10 @@ def run_profile(args):
             device_solve(P, d, args.precision)
         U, vm, info = device_solve(P, d, args.precision)
         torch.cuda.synchronize()
-        return {"mode": "solve-once", "iters": int(info.iters), "relres": info.relres, "t_setup_ms": info.t_setup_ms,
-                "t_solve_ms": info.t_solve_ms, "ndof": int(info.ndof)}
+        return {"mode": "solve-once", "precision": args.precision, "options": SOLVER_OPTIONS, "iters": int(info.iters),
+                "sweeps": int(info.sweeps), "relres": info.relres, "t_setup_ms": round(info.t_setup_ms, 2),
+                "t_solve_ms": round(info.t_solve_ms, 2), "ndof": int(info.ndof), "ku_shape": list(info.ku_shape),
+                "t_stage_ms": [round(float(v), 2) for v in info.t_stage_ms]}
     pr = engine.Problem(P["grid"], _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
     out = {"mode": "ku"}
@@ -392,12 +398,18 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="refine")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["full", "solve-once", "ku"], default="full",
                     help="solve-once / ku: one device solve or a few K.u products of the workload (profiling)")
     ap.add_argument("--size", default=None, help="override the workload grid, e.g. 96x64x56x0.833 (profiling)")
+    ap.add_argument("--inner-tol", type=float, default=None, help="refinement: FP32 sweep tolerance")
+    ap.add_argument("--use-graphs", type=int, default=None, help="0 direct, 1 graph per iteration, 2 device loop")
     args = ap.parse_args()
+    if args.inner_tol is not None:
+        SOLVER_OPTIONS["inner_tol"] = args.inner_tol
+    if args.use_graphs is not None:
+        SOLVER_OPTIONS["use_graphs"] = args.use_graphs
     if args.size:
         nx, ny, nz, h = args.size.split("x")
         WORKLOAD.update(nx=int(nx), ny=int(ny), nz=int(nz), h=float(h))

@@ -43,7 +43,8 @@ class FebInfo(C.Structure):
     _fields_ = [("iters", C.c_int32), ("flag", C.c_int32), ("levels", C.c_int32), ("sweeps", C.c_int32),
                 ("relres", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("ndof", C.c_int64), ("level_dofs", C.c_int64 * 8), ("lmax", C.c_double * 8),
-                ("coarse_n", C.c_int32), ("kernel_launches", C.c_int32)]
+                ("coarse_n", C.c_int32), ("kernel_launches", C.c_int32), ("ku_shape", C.c_int32 * 4),
+                ("t_stage_ms", C.c_double * 8)]
 
 
 class FebError(RuntimeError):

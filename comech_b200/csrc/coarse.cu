@@ -1,5 +1,6 @@
 // Coarse-level kernels: stencil products, structured restriction / prolongation, Galerkin on the device.
 #include "coarse.cuh"
+#include "vec.cuh"
 
 namespace feb {
 
@@ -70,10 +71,10 @@ template <typename T>
 __global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __restrict__ rf, T* __restrict__ rc,
                                 const int* __restrict__ skip) {
   if (skip && *skip) return;
-  const int cnx = P.ax[0].nc, cny = P.ax[1].nc, cnz = P.ax[2].nc;
-  int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (J >= (int64_t)cnx * cny * cnz) return;
-  int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  const int cnx = P.ax[0].nc, cny = P.ax[1].nc;
+  const int jx = blockIdx.x * blockDim.x + threadIdx.x, jy = blockIdx.y, jz = blockIdx.z;
+  if (jx >= cnx) return;
+  const int64_t J = jx + (int64_t)cnx * (jy + (int64_t)cny * jz);
   int Ix[3], Iy[3], Iz[3];
   double wx[3], wy[3], wz[3];
   int nxs = axis_fan(P.ax[0], jx, Ix, wx), nys = axis_fan(P.ax[1], jy, Iy, wy), nzs = axis_fan(P.ax[2], jz, Iz, wz);
@@ -95,8 +96,8 @@ __global__ void k_restrict_copies(TransferDev P, int fnx, int fny, int64_t fnnod
   if (skip && *skip) return;
   int64_t e = fnnode + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= fntotal) return;
-  int64_t o = orig_copy[e - fnnode];
-  int pi = int(o % fnx), pj = int((o / fnx) % fny), pk = int(o / ((int64_t)fnx * fny));
+  const int o = orig_copy[e - fnnode];
+  const int pi = o % fnx, pj = (o / fnx) % fny, pk = o / (fnx * fny);
   int Jx[2], Jy[2], Jz[2];
   double wx[2], wy[2], wz[2];
   int nxs = axis_support(P.ax[0], pi, Jx, wx), nys = axis_support(P.ax[1], pj, Jy, wy),
@@ -112,20 +113,14 @@ __global__ void k_restrict_copies(TransferDev P, int fnx, int fny, int64_t fnnod
 }
 
 template <typename T>
-__global__ void k_prolong_add(TransferDev P, int fnx, int fny, int64_t fnnode, int64_t fntotal,
-                              const int* __restrict__ orig_copy, const uint8_t* __restrict__ used,
-                              const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
-  if (skip && *skip) return;
-  int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= fntotal || !used[n]) return;
-  int64_t o = n < fnnode ? n : (int64_t)orig_copy[n - fnnode];
-  int pi = int(o % fnx), pj = int((o / fnx) % fny), pk = int(o / ((int64_t)fnx * fny));
+__device__ __forceinline__ void prolong_at(const TransferDev& P, int pi, int pj, int pk, const T* __restrict__ xc,
+                                           T& s0, T& s1, T& s2) {
   int Jx[2], Jy[2], Jz[2];
   double wx[2], wy[2], wz[2];
   int nxs = axis_support(P.ax[0], pi, Jx, wx), nys = axis_support(P.ax[1], pj, Jy, wy),
       nzs = axis_support(P.ax[2], pk, Jz, wz);
   const int cnx = P.ax[0].nc, cny = P.ax[1].nc;
-  T s0 = 0, s1 = 0, s2 = 0;
+  s0 = s1 = s2 = T(0);
   for (int c = 0; c < nzs; ++c)
     for (int b = 0; b < nys; ++b)
       for (int a = 0; a < nxs; ++a) {
@@ -133,6 +128,32 @@ __global__ void k_prolong_add(TransferDev P, int fnx, int fny, int64_t fnnode, i
         T w = T(wx[a] * wy[b] * wz[c]);
         s0 += w * xc[3 * K]; s1 += w * xc[3 * K + 1]; s2 += w * xc[3 * K + 2];
       }
+}
+
+template <typename T>
+__global__ void k_prolong_grid(TransferDev P, int fnx, int fny, const uint8_t* __restrict__ used,
+                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
+  if (pi >= fnx) return;
+  const int64_t n = pi + (int64_t)fnx * (pj + (int64_t)fny * pk);
+  if (!used[n]) return;
+  T s0, s1, s2;
+  prolong_at(P, pi, pj, pk, xc, s0, s1, s2);
+  xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+}
+
+template <typename T>
+__global__ void k_prolong_copies(TransferDev P, int fnx, int fny, int64_t fnnode, int64_t fntotal,
+                                 const int* __restrict__ orig_copy, const T* __restrict__ xc, T* __restrict__ xf,
+                                 const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t n = fnnode + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= fntotal) return;
+  const int o = orig_copy[n - fnnode];
+  const int pi = o % fnx, pj = (o / fnx) % fny, pk = o / (fnx * fny);
+  T s0, s1, s2;
+  prolong_at(P, pi, pj, pk, xc, s0, s1, s2);
   xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
 }
 
@@ -391,7 +412,123 @@ __global__ void k_block_inverse(const double* __restrict__ D, int64_t n, double*
   }
 }
 
+template <typename T>
+__global__ void k_stencil_to_sym(const double* __restrict__ A, int64_t n, T* __restrict__ S) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int o = 13; o < 27; ++o)
+    for (int t = 0; t < 9; ++t) S[(size_t)((o - 13) * 9 + t) * n + i] = T(A[(size_t)(o * 9 + t) * n + i]);
+}
+
+// One thread per node on a (x-blocks, y, z) grid: no integer division.  Rows that also hold entries
+// the stencil cannot (projected springs) are summed cooperatively by the whole warp.
+template <typename T, int EPI>
+__global__ void __launch_bounds__(128)
+k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
+      T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
+      const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  const bool valid = i < L.nx;
+  const int64_t n = i + (int64_t)L.nx * (j + (int64_t)L.ny * k);
+  const int64_t N = L.n;
+  T a0 = 0, a1 = 0, a2 = 0;
+  const T* S = L.S;
+  if (valid) {
+    {
+      const T u0 = u[3 * n], u1 = u[3 * n + 1], u2 = u[3 * n + 2];
+      a0 += S[n] * u0 + S[N + n] * u1 + S[2 * N + n] * u2;
+      a1 += S[3 * N + n] * u0 + S[4 * N + n] * u1 + S[5 * N + n] * u2;
+      a2 += S[6 * N + n] * u0 + S[7 * N + n] * u1 + S[8 * N + n] * u2;
+    }
+#pragma unroll
+    for (int q = 1; q < 14; ++q) {
+      const int o = 13 + q;
+      const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+      const int64_t off = dx + (int64_t)L.nx * (dy + (int64_t)L.ny * dz);
+      const T* B = S + (size_t)(q * 9) * N;
+      if (i + dx >= 0 && i + dx < L.nx && j + dy >= 0 && j + dy < L.ny && k + dz < L.nz) {
+        const int64_t m = n + off;
+        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+        a0 += B[n] * u0 + B[N + n] * u1 + B[2 * N + n] * u2;
+        a1 += B[3 * N + n] * u0 + B[4 * N + n] * u1 + B[5 * N + n] * u2;
+        a2 += B[6 * N + n] * u0 + B[7 * N + n] * u1 + B[8 * N + n] * u2;
+      }
+      if (i - dx >= 0 && i - dx < L.nx && j - dy >= 0 && j - dy < L.ny && k - dz >= 0) {
+        const int64_t m = n - off;
+        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+        a0 += B[m] * u0 + B[3 * N + m] * u1 + B[6 * N + m] * u2;
+        a1 += B[N + m] * u0 + B[4 * N + m] * u1 + B[7 * N + m] * u2;
+        a2 += B[2 * N + m] * u0 + B[5 * N + m] * u1 + B[8 * N + m] * u2;
+      }
+    }
+  }
+  if (L.node_ptr) {
+    const int lane = threadIdx.x & 31;
+    int beg = 0, end = 0;
+    if (valid) { beg = L.node_ptr[n]; end = L.node_ptr[n + 1]; }
+    unsigned todo = __ballot_sync(0xffffffffu, end > beg);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int b0 = __shfl_sync(0xffffffffu, beg, src), b1 = __shfl_sync(0xffffffffu, end, src);
+      T s0 = 0, s1 = 0, s2 = 0;
+      for (int e = b0 + lane; e < b1; e += 32) {
+        const T v = L.ent_v[e] * u[L.ent_col[e]];
+        const int rr = L.ent_r[e];
+        s0 += rr == 0 ? v : T(0);
+        s1 += rr == 1 ? v : T(0);
+        s2 += rr == 2 ? v : T(0);
+      }
+      s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
+      if (lane == src) { a0 += s0; a1 += s1; a2 += s2; }
+    }
+  }
+  if (!valid) return;
+  if constexpr (EPI == EPI_APPLY) {
+    y[3 * n] = a0; y[3 * n + 1] = a1; y[3 * n + 2] = a2;
+  } else if constexpr (EPI == EPI_RESID) {
+    r[3 * n] = b[3 * n] - a0; r[3 * n + 1] = b[3 * n + 1] - a1; r[3 * n + 2] = b[3 * n + 2] - a2;
+  } else {
+    const T c1 = T(lp->a1[kstep]), c2 = T(lp->a2[kstep]);
+    const T r0 = r[3 * n] - a0, r1 = r[3 * n + 1] - a1, r2 = r[3 * n + 2] - a2;
+    r[3 * n] = r0; r[3 * n + 1] = r1; r[3 * n + 2] = r2;
+    const T* D = L.Dinv;
+    const T z0 = D[n] * r0 + D[N + n] * r1 + D[2 * N + n] * r2;
+    const T z1 = D[3 * N + n] * r0 + D[4 * N + n] * r1 + D[5 * N + n] * r2;
+    const T z2 = D[6 * N + n] * r0 + D[7 * N + n] * r1 + D[8 * N + n] * r2;
+    const T e0 = c1 * u[3 * n] + c2 * z0, e1 = c1 * u[3 * n + 1] + c2 * z1, e2 = c1 * u[3 * n + 2] + c2 * z2;
+    d_out[3 * n] = e0; d_out[3 * n + 1] = e1; d_out[3 * n + 2] = e2;
+    x[3 * n] += e0; x[3 * n + 1] += e1; x[3 * n + 2] += e2;
+  }
+}
+
 }  // namespace
+
+template <typename T>
+void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
+                const LevelParams* lp, int k, const int* skip, cudaStream_t s) {
+  const dim3 g(div_up(L.nx, 128), L.ny, L.nz);
+  if (epi == EPI_APPLY) {
+    k_sym<T, EPI_APPLY><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+  } else if (epi == EPI_RESID) {
+    k_sym<T, EPI_RESID><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+  } else {
+    k_sym<T, EPI_CHEB><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+  }
+}
+
+template <typename T>
+void launch_stencil_to_sym(const double* A, int64_t n, T* S, cudaStream_t s) {
+  k_stencil_to_sym<T><<<div_up(n, kThreads), kThreads, 0, s>>>(A, n, S); note_launch();
+}
+
+template void launch_sym<float>(const SymView<float>&, int, const float*, float*, const float*, float*, float*,
+                                float*, const LevelParams*, int, const int*, cudaStream_t);
+template void launch_sym<double>(const SymView<double>&, int, const double*, double*, const double*, double*,
+                                 double*, double*, const LevelParams*, int, const int*, cudaStream_t);
+template void launch_stencil_to_sym<float>(const double*, int64_t, float*, cudaStream_t);
+template void launch_stencil_to_sym<double>(const double*, int64_t, double*, cudaStream_t);
 
 template <typename T>
 void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s) {
@@ -410,7 +547,7 @@ template <typename T>
 void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                      const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s) {
   int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
-  k_restrict_grid<T><<<div_up(nc, kThreads), kThreads, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
+  k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
   if (fntotal > fnnode)
     k_restrict_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
                                                                                  orig_copy, rf, rc, skip); note_launch();
@@ -421,9 +558,11 @@ template <typename T>
 void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
                         cudaStream_t s) {
-  k_prolong_add<T><<<div_up(fntotal, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal, orig_copy, used, xc,
-                                                                  xf, skip); note_launch();
-  (void)fnz;
+  k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip); note_launch();
+  if (fntotal > fnnode) {
+    k_prolong_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
+                                                                               orig_copy, xc, xf, skip); note_launch();
+  }
 }
 
 void launch_kept_mask(const TransferDev& P, const uint8_t* used_f, uint8_t* kept_c, cudaStream_t s) {

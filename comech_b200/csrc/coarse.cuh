@@ -33,6 +33,33 @@ struct StencilView {
 template <typename T>
 void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s);
 
+// Symmetric half storage of a stencil level: blocks of the offsets o = 13..26 (self and the 13 "forward"
+// neighbours) as S[(o-13)*9 + 3r + c][n]; the block of a backward offset o' < 13 is the transpose of the
+// forward block stored at the neighbour.  Entries the stencil cannot hold are a per-node CSR:
+// entries node_ptr[n] .. node_ptr[n+1] with row component ent_r, column dof ent_col, value ent_v.
+template <typename T>
+struct SymView {
+  int nx, ny, nz;
+  int64_t n;
+  const T* S;
+  const int* node_ptr;     // nullptr when there are no such entries
+  const int8_t* ent_r;
+  const int* ent_col;
+  const T* ent_v;
+  const T* Dinv;           // block-Jacobi inverse, SoA [9][n]
+};
+
+// Fused level kernels: EPI_APPLY y = A u; EPI_RESID r = b - A u; EPI_CHEB Chebyshev step with ping-pong
+// directions: t = A d_in, r -= t, d_out = a1 d_in + a2 Dinv r, x += d_out.
+enum SymEpi : int { EPI_APPLY = 0, EPI_RESID = 1, EPI_CHEB = 2 };
+struct LevelParams;
+template <typename T>
+void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
+                const LevelParams* lp, int k, const int* skip, cudaStream_t s);
+// full [243][n] FP64 stencil -> half storage in T
+template <typename T>
+void launch_stencil_to_sym(const double* A, int64_t n, T* S, cudaStream_t s);
+
 template <typename T>
 void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,
                     const int* skip, cudaStream_t s);

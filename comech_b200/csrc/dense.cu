@@ -93,16 +93,25 @@ __global__ void k_gj_row(const double* __restrict__ M, int nd, int k0, int bs, c
   Trow[(size_t)r * nd + j] = s;
 }
 
-// M[i][j] -= M[i][k-block] Trow[:, j] for i, j outside the pivot block (64x64 tiles, 4x4 per thread)
+// Tcol[i][q] = M[i][k0+q]: the pivot-block columns before the sweep changes them
+__global__ void k_gj_colcopy(const double* __restrict__ M, int nd, int k0, int bs, double* __restrict__ Tcol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int q = blockIdx.y;
+  if (i >= nd || q >= bs) return;
+  Tcol[(size_t)i * GJ_B + q] = M[(size_t)i * nd + k0 + q];
+}
+
+// M[i][j] -= Tcol[i][:] Trow[:, j] for i, j outside the pivot block (64x64 tiles, 4x4 per thread)
 __global__ void __launch_bounds__(256)
-k_gj_update(double* __restrict__ M, int nd, int k0, int bs, const double* __restrict__ Trow) {
+k_gj_update(double* __restrict__ M, int nd, int k0, int bs, const double* __restrict__ Tcol,
+            const double* __restrict__ Trow) {
   __shared__ double As[GJ_T][GJ_B + 1];
   __shared__ double Bs[GJ_B][GJ_T + 1];
   const int i0 = blockIdx.y * GJ_T, j0 = blockIdx.x * GJ_T;
   const int t = threadIdx.x;
   for (int e = t; e < GJ_T * GJ_B; e += 256) {
     int ii = e / GJ_B, q = e % GJ_B;
-    As[ii][q] = (i0 + ii < nd && q < bs) ? M[(size_t)(i0 + ii) * nd + k0 + q] : 0.0;
+    As[ii][q] = (i0 + ii < nd && q < bs) ? Tcol[(size_t)(i0 + ii) * GJ_B + q] : 0.0;
     int q2 = e / GJ_T, jj = e % GJ_T;
     Bs[q2][jj] = (j0 + jj < nd && q2 < bs) ? Trow[(size_t)q2 * nd + j0 + jj] : 0.0;
   }
@@ -131,25 +140,21 @@ k_gj_update(double* __restrict__ M, int nd, int k0, int bs, const double* __rest
   }
 }
 
-// M[i][k-block] <- -M[i][k-block] Dinv (i outside), M[k-block][j] <- Trow (j outside), M[kk] <- Dinv
+// pivot rows: M[k-block][j] <- Trow (j outside the block); pivot columns: M[i][k-block] <- -Tcol[i] Dinv
+// (i outside), M[kk] <- Dinv.  One thread per element of the pivot rows and of the pivot columns.
 __global__ void k_gj_finish(double* __restrict__ M, int nd, int k0, int bs, const double* __restrict__ Dinv,
-                            const double* __restrict__ Trow) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nd) return;
-  if (i >= k0 && i < k0 + bs) {
-    int r = i - k0;
-    for (int j = 0; j < nd; ++j) {
-      if (j >= k0 && j < k0 + bs) M[(size_t)i * nd + j] = Dinv[r * bs + (j - k0)];
-      else M[(size_t)i * nd + j] = Trow[(size_t)r * nd + j];
-    }
-  } else {
-    double row[GJ_B];
-    for (int q = 0; q < bs; ++q) row[q] = M[(size_t)i * nd + k0 + q];
-    for (int c = 0; c < bs; ++c) {
-      double s = 0.0;
-      for (int q = 0; q < bs; ++q) s += row[q] * Dinv[q * bs + c];
-      M[(size_t)i * nd + k0 + c] = -s;
-    }
+                            const double* __restrict__ Trow, const double* __restrict__ Tcol) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (j >= nd || r >= bs) return;
+  // element (k0 + r, j) of the pivot rows
+  if (j >= k0 && j < k0 + bs) M[(size_t)(k0 + r) * nd + j] = Dinv[r * bs + (j - k0)];
+  else M[(size_t)(k0 + r) * nd + j] = Trow[(size_t)r * nd + j];
+  // element (j, k0 + r) of the pivot columns (row j outside the block)
+  if (j < k0 || j >= k0 + bs) {
+    double s = 0.0;
+    for (int q = 0; q < bs; ++q) s += Tcol[(size_t)j * GJ_B + q] * Dinv[q * bs + r];
+    M[(size_t)j * nd + k0 + r] = -s;
   }
 }
 
@@ -203,18 +208,20 @@ void launch_dense_invert(double* M, int nd, double* scratch, int* status, cudaSt
   k_symmetrize<<<div_up((int64_t)nd * nd, kThreads), kThreads, 0, s>>>(M, nd); note_launch();
   double* Dinv = scratch;
   double* Trow = scratch + GJ_B * GJ_B;
+  double* Tcol = Trow + (size_t)GJ_B * nd;
   for (int k0 = 0; k0 < nd; k0 += GJ_B) {
     int bs = std::min(GJ_B, nd - k0);
     k_gj_pivot<<<1, 256, 0, s>>>(M, nd, k0, bs, Dinv, status); note_launch();
     dim3 g1(div_up(nd, 128), bs);
     k_gj_row<<<g1, 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow); note_launch();
+    k_gj_colcopy<<<g1, 128, 0, s>>>(M, nd, k0, bs, Tcol); note_launch();
     dim3 g2(div_up(nd, GJ_T), div_up(nd, GJ_T));
-    k_gj_update<<<g2, 256, 0, s>>>(M, nd, k0, bs, Trow); note_launch();
-    k_gj_finish<<<div_up(nd, 128), 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow); note_launch();
+    k_gj_update<<<g2, 256, 0, s>>>(M, nd, k0, bs, Tcol, Trow); note_launch();
+    k_gj_finish<<<g1, 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow, Tcol); note_launch();
   }
 }
 
-size_t dense_scratch_doubles(int nd) { return (size_t)GJ_B * GJ_B + (size_t)GJ_B * nd; }
+size_t dense_scratch_doubles(int nd) { return (size_t)GJ_B * GJ_B + 2 * (size_t)GJ_B * nd; }
 
 template <typename T>
 void launch_dense_solve(const double* Minv, int nd, const int* klist, const int* cmap, int64_t n, const T* b, T* x,

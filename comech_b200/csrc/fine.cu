@@ -1,14 +1,11 @@
 // Level-0 operator kernels: structured matrix-free K.u, sparse pass, diagonal blocks.
+#include <algorithm>
+
 #include "fine.cuh"
 
 namespace feb {
 
 namespace {
-
-constexpr int TX = 32;        // cells per tile along x (one warp)
-constexpr int TY = 8;         // cells per tile along y (warps)
-constexpr int PX = TX + 1;    // node columns staged per plane
-constexpr int PY = TY + 1;
 
 template <typename T, int W>
 __device__ __forceinline__ bool load_material(const T* __restrict__ p, T (&m)[W]) {
@@ -21,99 +18,207 @@ __device__ __forceinline__ bool load_material(const T* __restrict__ p, T (&m)[W]
   return nz;
 }
 
-// Matrix-free K.u over the regular cells.  A CTA owns a (TX-1) x (TY-1) column of grid nodes over
-// `zchunk` node planes.  It computes the TX x TY cells touching those nodes (the first row/column of
-// cells is shared with the neighbouring CTAs and recomputed there), marching upward one cell layer
-// at a time:
-//   * the node plane above the layer is staged in shared memory (two-plane ring);
-//   * every thread computes one cell's 24 nodal forces in registers (modal hex8 operator);
-//   * forces of the x-neighbour arrive by warp shuffle, those of the y-neighbour row through shared
-//     memory; each owned node sums its 4 cells of the layer below (kept in registers from the
-//     previous step) and the 4 cells of the layer above, then stores its 3 components once.
-// No global atomics: every output is written by exactly one thread.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(TX * TY)
+// Matrix-free K.u over the regular cells, sum-factorised across cells.
+//
+// A CTA of 32 x TY threads owns a 30 x (TY-2) column of grid nodes over `zchunk` node planes and computes
+// the 31 x (TY-1) cells touching them (the outermost row / column of cells is shared with the neighbouring
+// CTAs).  Thread (tx, ty) holds node (tx, ty) of the node planes, prefetched two planes ahead, and works
+// on the xy-face and x-edge that start at its node:
+//   forward   x-edge butterfly of its node and its +x neighbour (warp shuffle), xy-face butterfly with the
+//             edge of the row above (shared memory) -- once per plane, shared by the two cells above and
+//             below the face; the z butterfly between the faces of planes k and k+1 completes the modal
+//             transform of cell layer k;
+//   core      the element operator in the modal basis (hex8_modal);
+//   backward  the transposed butterflies in reverse: z (into the faces of planes k and k+1, the upper one
+//             carried in registers to the next layer), y (into the edge of this row and, through shared
+//             memory, of the row above), x (into this node and, by shuffle, its +x neighbour).
+// Each owned node therefore sums its 8 cells with no global atomics and stores its 3 components once.
+// One barrier per cell layer: both shared-memory exchanges are double-buffered.
+template <typename T, int MODE, int TY>
+__global__ void __launch_bounds__(32 * TY)
 k_fine_struct(FineView<T> F, const T* __restrict__ u, T* __restrict__ y, const int* __restrict__ skip, int zchunk) {
   if (skip && *skip) return;
   constexpr int W = MatWidth<MODE>::value;
-  __shared__ T plane[2][PY * PX * 3];
-  __shared__ T rowp[TY][TX][6];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int pi0 = blockIdx.x * (TX - 1) - 1;
-  const int pj0 = blockIdx.y * (TY - 1) - 1;
-  const int ci = pi0 + tx, cj = pj0 + ty;       // this thread's cell, and the node it owns
+  constexpr bool HAS12 = (MODE != MAT_ISO_SRI);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T (*sE)[TY][32][6] = reinterpret_cast<T (*)[TY][32][6]>(smem_raw);                               // [2]
+  T (*sB)[TY][32][6] = reinterpret_cast<T (*)[TY][32][6]>(smem_raw + sizeof(T) * 2 * TY * 32 * 6);  // [2]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int ni = blockIdx.x * 30 - 1 + tx;
+  const int nj = blockIdx.y * (TY - 2) - 1 + ty;
   const int K0 = blockIdx.z * zchunk;
   const int K1 = min(K0 + zchunk, F.nzn);
-  const bool cell_xy = (ci >= 0) && (ci < F.nx) && (cj >= 0) && (cj < F.ny);
-  const bool owner = (tx >= 1) && (ty >= 1) && (ci < F.nxn) && (cj < F.nyn);
+  const bool node_in = ni >= 0 && ni < F.nxn && nj >= 0 && nj < F.nyn;
+  const bool cell_xy = tx < 31 && ty < TY - 1 && ni >= 0 && ni < F.nx && nj >= 0 && nj < F.ny;
+  const bool owner = tx >= 1 && tx <= 30 && ty >= 1 && ty <= TY - 2 && ni < F.nxn && nj < F.nyn;
+  const bool has_above = ty + 1 < TY;
+  const int64_t plane = (int64_t)F.nxn * F.nyn;
+  const int64_t nbase = node_in ? (ni + (int64_t)F.nxn * nj) : 0;
+  const int64_t cplane = (int64_t)F.nx * F.ny;
+  const int64_t cbase = cell_xy ? (ni + (int64_t)F.nx * nj) : 0;
   T a = T(1), b = T(1), ia = T(1), ib = T(1);
-  if (cell_xy) { a = F.dx[ci]; ia = F.idx[ci]; b = F.dy[cj]; ib = F.idy[cj]; }
+  if (cell_xy) { a = F.dx[ni]; ia = F.idx[ni]; b = F.dy[nj]; ib = F.idy[nj]; }
 
-  auto stage = [&](int k, int slot) {
-    T* dst = plane[slot];
-    const bool kin = (k >= 0) && (k < F.nzn);
-    for (int e = tid; e < PY * PX * 3; e += TX * TY) {
-      int row = e / (PX * 3), w = e - row * (PX * 3);
-      int ni = pi0 + w / 3, nj = pj0 + row;
-      T v = T(0);
-      if (kin && ni >= 0 && ni < F.nxn && nj >= 0 && nj < F.nyn)
-        v = u[3 * ((int64_t)ni + (int64_t)F.nxn * (nj + (int64_t)F.nyn * k)) + (w % 3)];
-      dst[e] = v;
+  auto load_node = [&](int k, T (&v)[3]) {
+    if (node_in && k >= 0 && k < F.nzn) {
+      const T* p = u + 3 * (nbase + plane * k);
+      v[0] = p[0]; v[1] = p[1]; v[2] = p[2];
+    } else {
+      v[0] = v[1] = v[2] = T(0);
     }
   };
+  auto load_mat = [&](int k, T (&m)[W]) {
+    if (cell_xy && k >= 0 && k < F.nz) {
+      const T* p = F.mat + (size_t)W * (cbase + cplane * k);
+#pragma unroll
+      for (int q = 0; q < W; ++q) m[q] = p[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < W; ++q) m[q] = T(0);
+    }
+  };
+  // x-edge butterfly of this node and its +x neighbour: E[c] = (sum, difference)
+  auto edge = [&](const T (&v)[3], T (&E)[3][2]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T w = __shfl_down_sync(0xffffffffu, v[c], 1);
+      E[c][0] = v[c] + w;
+      E[c][1] = w - v[c];
+    }
+  };
+  auto put6 = [&](T* d, const T (&E)[3][2]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { d[2 * c] = E[c][0]; d[2 * c + 1] = E[c][1]; }
+  };
+  auto get6 = [&](const T* s, T (&E)[3][2]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { E[c][0] = s[2 * c]; E[c][1] = s[2 * c + 1]; }
+  };
+  auto slot = [](int p) { return (p + 2) & 1; };
 
-  T acc[3] = {T(0), T(0), T(0)};
-  stage(K0 - 1, (K0 - 1) & 1);
-  for (int k = K0 - 1; k < K1; ++k) {
-    stage(k + 1, (k + 1) & 1);
-    T m[W];
-    bool act = false;
-    if (cell_xy && k >= 0 && k < F.nz)
-      act = load_material<T, W>(F.mat + (size_t)W * ((int64_t)ci + (int64_t)F.nx * (cj + (int64_t)F.ny * k)), m);
+  T vn[3], vp[3], vq[3], mc[W], mn[W];
+  T Fk[3][4], topc[3][4], plo[3][2];
+  // prologue: face of plane K0-1
+  {
+    T v0[3], E[3][2], A[3][2] = {};
+    load_node(K0 - 1, v0);
+    load_node(K0, vn);
+    load_node(K0 + 1, vp);
+    load_mat(K0 - 1, mc);
+    edge(v0, E);
+    put6(sE[slot(K0 - 1)][ty][tx], E);
     __syncthreads();
-    T f[3][8];
-    if (act) {
-      T uc[3][8];
+    if (has_above) get6(sE[slot(K0 - 1)][ty + 1][tx], A);
 #pragma unroll
-      for (int l = 0; l < 8; ++l) {
-        const T* src = plane[(k + ((l >> 2) & 1)) & 1] + ((ty + ((l >> 1) & 1)) * PX + tx + (l & 1)) * 3;
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) uc[c][l] = src[c];
+      for (int ax = 0; ax < 2; ++ax) {
+        Fk[c][ax] = E[c][ax] + A[c][ax];
+        Fk[c][ax + 2] = A[c][ax] - E[c][ax];
+        topc[c][ax] = topc[c][ax + 2] = T(0);
       }
-      T cz = F.dz[k], icz = F.idz[k];
-      Material<T> mat = make_material<T, MODE>(m);
-      hex8_apply(uc, a, b, cz, ia, ib, icz, mat, f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) plo[c][0] = plo[c][1] = T(0);
+  }
+  for (int k = K0 - 1; k < K1; ++k) {
+    // (a) x-edge of plane k+1; prefetch plane k+3 and the material of layer k+1
+    T E[3][2];
+    edge(vn, E);
+    put6(sE[slot(k + 1)][ty][tx], E);
+    load_node(k + 3, vq);
+    load_mat(k + 1, mn);
+    __syncthreads();
+    // (c) finish plane k-1: edge = this face's lower share + the row below's upper share; x back-transform
+    if (k > K0 - 1) {
+      T up[3][2] = {};
+      if (ty >= 1) get6(sB[slot(k - 1)][ty - 1][tx], up);
+      T out[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T m = plo[c][0] + up[c][0], d = plo[c][1] + up[c][1];
+        const T left = __shfl_up_sync(0xffffffffu, m + d, 1);
+        out[c] = (m - d) + (tx ? left : T(0));
+      }
+      if (owner && k - 1 >= K0) {
+        T* dst = y + 3 * (nbase + plane * (k - 1));
+        dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2];
+      }
+    }
+    // (d) xy-face of plane k+1, (e) z butterfly -> modal coefficients of cell layer k
+    T A[3][2] = {};
+    if (has_above) get6(sE[slot(k + 1)][ty + 1][tx], A);
+    T Fk1[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int ax = 0; ax < 2; ++ax) {
+        Fk1[c][ax] = E[c][ax] + A[c][ax];
+        Fk1[c][ax + 2] = A[c][ax] - E[c][ax];
+      }
+    bool act = false;
+#pragma unroll
+    for (int q = 0; q < W; ++q) act |= (mc[q] != T(0));
+    T G[3][4];
+    if (act) {
+      T X[8], Y[8], Z[8];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        X[l] = Fk[0][l] + Fk1[0][l]; X[l + 4] = Fk1[0][l] - Fk[0][l];
+        Y[l] = Fk[1][l] + Fk1[1][l]; Y[l + 4] = Fk1[1][l] - Fk[1][l];
+        Z[l] = Fk[2][l] + Fk1[2][l]; Z[l + 4] = Fk1[2][l] - Fk[2][l];
+      }
+      Material<T> mt = make_material<T, MODE>(mc);
+      const T cz = F.dz[k], icz = F.idz[k];
+      T FX[8], FY[8], FZ[8];
+      hex8_modal<T, HAS12>(X, Y, Z, make_coef(a, b, cz, ia, ib, icz, mt), FX, FY, FZ);
+      // (g, h) z back-transform: bottom share completes the face of plane k, top share carries to plane k+1
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        G[0][l] = topc[0][l] + (FX[l] - FX[l + 4]); topc[0][l] = FX[l] + FX[l + 4];
+        G[1][l] = topc[1][l] + (FY[l] - FY[l + 4]); topc[1][l] = FY[l] + FY[l + 4];
+        G[2][l] = topc[2][l] + (FZ[l] - FZ[l + 4]); topc[2][l] = FZ[l] + FZ[l + 4];
+      }
     } else {
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int l = 0; l < 8; ++l) f[c][l] = T(0);
+        for (int l = 0; l < 4; ++l) { G[c][l] = topc[c][l]; topc[c][l] = T(0); }
     }
-    T own[2][3];
+    // (i) y back-transform of the face of plane k: lower share stays, upper share goes to the row above
+    T hi[3][2];
 #pragma unroll
-    for (int zl = 0; zl < 2; ++zl) {
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        T left_own = __shfl_up_sync(0xffffffffu, f[c][1 + 4 * zl], 1);
-        T left_row = __shfl_up_sync(0xffffffffu, f[c][3 + 4 * zl], 1);
-        own[zl][c] = f[c][4 * zl] + (tx ? left_own : T(0));
-        rowp[ty][tx][3 * zl + c] = f[c][2 + 4 * zl] + (tx ? left_row : T(0));
+      for (int ax = 0; ax < 2; ++ax) {
+        plo[c][ax] = G[c][ax] - G[c][ax + 2];
+        hi[c][ax] = G[c][ax] + G[c][ax + 2];
       }
-    }
-    __syncthreads();
-    if (ty >= 1) {
+    put6(sB[slot(k)][ty][tx], hi);
+    // (j) advance
 #pragma unroll
-      for (int zl = 0; zl < 2; ++zl)
+    for (int c = 0; c < 3; ++c) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) own[zl][c] += rowp[ty - 1][tx][3 * zl + c];
-    }
-    if (k >= K0 && owner) {
-      T* dst = y + 3 * ((int64_t)ci + (int64_t)F.nxn * (cj + (int64_t)F.nyn * k));
-#pragma unroll
-      for (int c = 0; c < 3; ++c) dst[c] = acc[c] + own[0][c];
+      for (int l = 0; l < 4; ++l) Fk[c][l] = Fk1[c][l];
+      vn[c] = vp[c]; vp[c] = vq[c];
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[c] = own[1][c];
+    for (int q = 0; q < W; ++q) mc[q] = mn[q];
+  }
+  __syncthreads();
+  {
+    T up[3][2] = {};
+    if (ty >= 1) get6(sB[slot(K1 - 1)][ty - 1][tx], up);
+    T out[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T m = plo[c][0] + up[c][0], d = plo[c][1] + up[c][1];
+      const T left = __shfl_up_sync(0xffffffffu, m + d, 1);
+      out[c] = (m - d) + (tx ? left : T(0));
+    }
+    if (owner && K1 - 1 >= K0) {
+      T* dst = y + 3 * (nbase + plane * (K1 - 1));
+      dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2];
+    }
   }
 }
 
@@ -323,18 +428,38 @@ template void launch_dense_from_fine<MAT_ISO_SRI>(const FineView<double>&, const
 template void launch_dense_from_fine<MAT_ISO_FULL>(const FineView<double>&, const int*, double*, int, cudaStream_t);
 template void launch_dense_from_fine<MAT_ORTHO>(const FineView<double>&, const int*, double*, int, cudaStream_t);
 
+template <typename T, int MODE, int TY>
+void launch_struct(dim3 grid, size_t smem, const FineView<T>& F, const T* u, T* y, const int* skip, int zc,
+                   cudaStream_t s) {
+  static bool configured = false;   // one attribute call per instantiation (idempotent if repeated)
+  if (!configured) {
+    cudaFuncSetAttribute(k_fine_struct<T, MODE, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = true;
+  }
+  k_fine_struct<T, MODE, TY><<<grid, dim3(32, TY), smem, s>>>(F, u, y, skip, zc); note_launch();
+}
+
 template <typename T, int MODE>
-void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, int zchunk, cudaStream_t s) {
-  dim3 block(TX, TY);
-  dim3 grid(div_up(F.nxn, TX - 1), div_up(F.nyn, TY - 1), div_up(F.nzn, zchunk));
-  k_fine_struct<T, MODE><<<grid, block, 0, s>>>(F, u, y, skip, zchunk); note_launch();
+void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, KuConfig cfg, cudaStream_t s) {
+  const int ty = cfg.ty == 8 ? 8 : (cfg.ty == 12 ? 12 : 16);
+  const int zc = std::max(1, cfg.zchunk);
+  dim3 grid(div_up(F.nxn, 30), div_up(F.nyn, ty - 2), div_up(F.nzn, zc));
+  const size_t smem = sizeof(T) * (size_t)ty * 32 * 24;
+  if (ty == 8) {
+    launch_struct<T, MODE, 8>(grid, smem, F, u, y, skip, zc, s);
+  } else if (ty == 12) {
+    launch_struct<T, MODE, 12>(grid, smem, F, u, y, skip, zc, s);
+  } else {
+    launch_struct<T, MODE, 16>(grid, smem, F, u, y, skip, zc, s);
+  }
   if (F.ntotal > F.nnode) {
     int64_t n = 3 * (F.ntotal - F.nnode);
     k_zero_tail<T><<<div_up(n, kThreads), kThreads, 0, s>>>(y, 3 * F.nnode, 3 * F.ntotal, skip); note_launch();
   }
   int b_irr = div_up(F.nirr, kThreads), b_pen = div_up(F.npen, kThreads), b_row = div_up(F.nrow, kThreads);
-  if (b_irr + b_pen + b_row > 0)
+  if (b_irr + b_pen + b_row > 0) {
     k_fine_sparse<T, MODE><<<b_irr + b_pen + b_row, kThreads, 0, s>>>(F, u, y, skip, b_irr, b_pen); note_launch();
+  }
 }
 
 template <int MODE>
@@ -344,7 +469,7 @@ void launch_fine_diag(const FineView<double>& F, double* D, cudaStream_t s) {
   if (n > 0) k_fine_diag_sparse<MODE><<<div_up(n, kThreads), kThreads, 0, s>>>(F, D); note_launch();
 }
 
-#define INST(T, M) template void launch_fine_apply<T, M>(const FineView<T>&, const T*, T*, const int*, int, cudaStream_t);
+#define INST(T, M) template void launch_fine_apply<T, M>(const FineView<T>&, const T*, T*, const int*, KuConfig, cudaStream_t);
 INST(float, MAT_ISO_SRI) INST(float, MAT_ISO_FULL) INST(float, MAT_ORTHO)
 INST(double, MAT_ISO_SRI) INST(double, MAT_ISO_FULL) INST(double, MAT_ORTHO)
 #undef INST

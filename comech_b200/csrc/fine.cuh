@@ -26,8 +26,14 @@ struct FineView {
   int nrow; const int* row_dof; const int* row_ptr; const int* col; const T* val;
 };
 
+// launch shape of the structured K.u kernel: warps per CTA (8, 12 or 16) and node planes per CTA
+struct KuConfig {
+  int ty = 16;
+  int zchunk = 16;
+};
+
 template <typename T, int MODE>
-void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, int zchunk, cudaStream_t s);
+void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, KuConfig cfg, cudaStream_t s);
 
 // 3x3 diagonal blocks of the level-0 operator at every node (full layout), row-major [n][9].
 template <int MODE>

@@ -1,6 +1,8 @@
 // Additive rigid-body-mode correction z += Z pinv(Z^T K Z) Z^T r (fe/gmg.py:127-135, rb/gpusolve.py:216-228).
 // Z has 6 columns per node group (3 translations, rotations about x, y, z with r = (X - mean X) / 20,
 // rb/splitfe.py:105-120); its entries are recomputed from the grid coordinates, never stored.
+#include <algorithm>
+
 #include "rigid.cuh"
 
 namespace feb {
@@ -26,22 +28,39 @@ __device__ __forceinline__ void mode_vec(int m, double rx, double ry, double rz,
   }
 }
 
-__global__ void k_centroids(RigidView Z, double* __restrict__ cen) {
-  const int g = blockIdx.x;
+// partial coordinate sums per group: grid (blocks per group, groups); part[g][blk][3]
+__global__ void __launch_bounds__(kThreads) k_centroid_partial(RigidView Z, double* __restrict__ part) {
+  const int g = blockIdx.y;
   double sx = 0, sy = 0, sz = 0;
-  for (int e = Z.off[g] + threadIdx.x; e < Z.off[g + 1]; e += blockDim.x) {
+  for (int e = Z.off[g] + blockIdx.x * kThreads + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * kThreads) {
     double x, y, z;
     node_xyz(Z, Z.nodes[e], x, y, z);
     sx += x; sy += y; sz += z;
   }
-  sx = block_sum(sx);
-  __syncthreads();
-  sy = block_sum(sy);
-  __syncthreads();
-  sz = block_sum(sz);
-  if (threadIdx.x == 0) {
-    double n = double(Z.off[g + 1] - Z.off[g]);
-    cen[3 * g] = sx / n; cen[3 * g + 1] = sy / n; cen[3 * g + 2] = sz / n;
+  double v[3] = {sx, sy, sz};
+  for (int c = 0; c < 3; ++c) {
+    double t = block_sum(v[c]);
+    if (threadIdx.x == 0) part[((size_t)g * gridDim.x + blockIdx.x) * 3 + c] = t;
+    __syncthreads();
+  }
+}
+
+__global__ void k_centroid_finish(RigidView Z, int nblk, const double* __restrict__ part, double* __restrict__ cen) {
+  int t = threadIdx.x;
+  if (t >= 3 * Z.ngroups) return;
+  int g = t / 3, c = t % 3;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[((size_t)g * nblk + b) * 3 + c];
+  cen[t] = s / double(Z.off[g + 1] - Z.off[g]);
+}
+
+__global__ void k_rigid_rho(RigidView Z, double* __restrict__ rho) {
+  const int g = blockIdx.y;
+  const double cx = Z.cen[3 * g], cy = Z.cen[3 * g + 1], cz = Z.cen[3 * g + 2];
+  for (int e = Z.off[g] + blockIdx.x * blockDim.x + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * blockDim.x) {
+    double x, y, z;
+    node_xyz(Z, Z.nodes[e], x, y, z);
+    rho[3 * e] = (x - cx) / 20.0; rho[3 * e + 1] = (y - cy) / 20.0; rho[3 * e + 2] = (z - cz) / 20.0;
   }
 }
 
@@ -52,12 +71,9 @@ k_ztr_partial(RigidView Z, const T* __restrict__ r, double* __restrict__ part, c
   if (skip && *skip) return;
   const int g = blockIdx.y;
   double s[6] = {0, 0, 0, 0, 0, 0};
-  const double cx = Z.cen[3 * g], cy = Z.cen[3 * g + 1], cz = Z.cen[3 * g + 2];
   for (int e = Z.off[g] + blockIdx.x * kThreads + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * kThreads) {
-    int64_t n = Z.nodes[e];
-    double x, y, z;
-    node_xyz(Z, n, x, y, z);
-    double rx = (x - cx) / 20.0, ry = (y - cy) / 20.0, rz = (z - cz) / 20.0;
+    const int64_t n = Z.nodes[e];
+    const double rx = Z.rho[3 * e], ry = Z.rho[3 * e + 1], rz = Z.rho[3 * e + 2];
     double r0 = double(r[3 * n]), r1 = double(r[3 * n + 1]), r2 = double(r[3 * n + 2]);
     s[0] += r0; s[1] += r1; s[2] += r2;
     s[3] += -rz * r1 + ry * r2;
@@ -97,13 +113,10 @@ __global__ void k_z_scatter(RigidView Z, const double* __restrict__ coef, T* __r
                             const int* __restrict__ skip) {
   if (skip && *skip) return;
   const int g = blockIdx.y;
-  const double cx = Z.cen[3 * g], cy = Z.cen[3 * g + 1], cz = Z.cen[3 * g + 2];
   const double* c = coef + 6 * g;
   for (int e = Z.off[g] + blockIdx.x * blockDim.x + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * blockDim.x) {
-    int64_t n = Z.nodes[e];
-    double x, y, zz;
-    node_xyz(Z, n, x, y, zz);
-    double rx = (x - cx) / 20.0, ry = (y - cy) / 20.0, rz = (zz - cz) / 20.0;
+    const int64_t n = Z.nodes[e];
+    const double rx = Z.rho[3 * e], ry = Z.rho[3 * e + 1], rz = Z.rho[3 * e + 2];
     double v0 = c[0] + c[4] * rz - c[5] * ry;
     double v1 = c[1] - c[3] * rz + c[5] * rx;
     double v2 = c[2] + c[3] * ry - c[4] * rx;
@@ -116,13 +129,10 @@ __global__ void k_z_scatter(RigidView Z, const double* __restrict__ coef, T* __r
 // column `col` of Z as a full-layout vector (zeroed beforehand)
 __global__ void k_z_column(RigidView Z, int col, double* __restrict__ v) {
   const int g = col / 6, m = col % 6;
-  const double cx = Z.cen[3 * g], cy = Z.cen[3 * g + 1], cz = Z.cen[3 * g + 2];
   for (int e = Z.off[g] + blockIdx.x * blockDim.x + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * blockDim.x) {
-    int64_t n = Z.nodes[e];
-    double x, y, z;
-    node_xyz(Z, n, x, y, z);
+    const int64_t n = Z.nodes[e];
     double w[3];
-    mode_vec(m, (x - cx) / 20.0, (y - cy) / 20.0, (z - cz) / 20.0, w);
+    mode_vec(m, Z.rho[3 * e], Z.rho[3 * e + 1], Z.rho[3 * e + 2], w);
     v[3 * n] += w[0]; v[3 * n + 1] += w[1]; v[3 * n + 2] += w[2];
   }
 }
@@ -131,8 +141,11 @@ __global__ void k_z_column(RigidView Z, int col, double* __restrict__ v) {
 
 int rigid_blocks(const RigidView& Z) { (void)Z; return 2 * kSmCount / 4; }
 
-void launch_centroids(const RigidView& Z, double* cen, cudaStream_t s) {
-  k_centroids<<<Z.ngroups, kThreads, 0, s>>>(Z, cen); note_launch();
+void launch_centroids(const RigidView& Z, double* cen, double* part, cudaStream_t s) {
+  int nb = rigid_blocks(Z);
+  dim3 g(nb, Z.ngroups);
+  k_centroid_partial<<<g, kThreads, 0, s>>>(Z, part); note_launch();
+  k_centroid_finish<<<1, std::max(32, ((3 * Z.ngroups + 31) / 32) * 32), 0, s>>>(Z, nb, part, cen); note_launch();
 }
 
 template <typename T>
@@ -143,6 +156,11 @@ void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, doub
   k_ztr_partial<T><<<g, kThreads, 0, s>>>(Z, r, part, skip); note_launch();
   k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, Einv, zr, coef, skip); note_launch();
   if (Einv) k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip); note_launch();
+}
+
+void launch_rigid_rho(const RigidView& Z, double* rho, cudaStream_t s) {
+  dim3 g(rigid_blocks(Z), Z.ngroups);
+  k_rigid_rho<<<g, kThreads, 0, s>>>(Z, rho); note_launch();
 }
 
 void launch_ztr(const RigidView& Z, const double* r, double* part, double* zr, cudaStream_t s) {

@@ -13,10 +13,15 @@ struct RigidView {
   int64_t nnode;             // grid nodes
   const int* orig_copy;      // grid node of every copy
   const double* xe; const double* ye; const double* ze;   // node coordinates per axis
+  const double* rho;         // [3 * nodes] (X - centroid) / 20 of every group node, set by launch_rigid_rho
 };
 
+// rho of every group node from the centroids (after launch_centroids)
+void launch_rigid_rho(const RigidView& Z, double* rho, cudaStream_t s);
+
 int rigid_blocks(const RigidView& Z);
-void launch_centroids(const RigidView& Z, double* cen, cudaStream_t s);
+// part: rigid_blocks * ngroups * 6 doubles (scratch)
+void launch_centroids(const RigidView& Z, double* cen, double* part, cudaStream_t s);
 // z += Z Einv Z^T r   (part: rigid_blocks * ngroups * 6 doubles; zr, coef: 6 ngroups)
 template <typename T>
 void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, double* zr, double* coef,

@@ -13,6 +13,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -328,17 +330,44 @@ struct Level {
   int64_t ndof = 0;                       // 3 x used / kept nodes
   std::vector<double> coord[3];
   uint8_t* used = nullptr;
-  double* A64 = nullptr;                  // stencil (levels >= 1)
-  float* A32 = nullptr;
-  Csr sparse;                             // entries the stencil does not hold (levels >= 1)
+  double* A64 = nullptr;                  // full stencil [243][n] (levels >= 1, set-up only)
+  double* S64 = nullptr;                  // symmetric half storage [126][n] (levels >= 1)
+  float* S32 = nullptr;
+  int* node_ptr = nullptr;                // per-node CSR of the entries the stencil cannot hold
+  int8_t* ent_r = nullptr;
+  int* ent_col = nullptr;
+  double* ent_v64 = nullptr;
+  float* ent_v32 = nullptr;
   Entries nonlocal;                       // host copy of `sparse` (projected to the next level)
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
   AxisHost ax[3];                         // transfer to the next level
   TransferDev P{};
-  double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr, *t64 = nullptr;
-  float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr, *t32 = nullptr;
+  double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr, *t64 = nullptr, *e64 = nullptr;
+  float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr, *t32 = nullptr, *e32 = nullptr;
 };
+
+int upload_node_csr(Pool& pool, const Entries& E, int64_t nnode, Level& V) {
+  if (E.size() == 0) return FEB_OK;
+  std::vector<int> ptr(nnode + 1, 0), col(E.size());
+  std::vector<int8_t> rr(E.size());
+  std::vector<double> v(E.size());
+  std::vector<float> vf(E.size());
+  for (size_t e = 0; e < E.size(); ++e) ptr[E.r[e] / 3 + 1]++;
+  for (int64_t i = 0; i < nnode; ++i) ptr[i + 1] += ptr[i];
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (size_t e = 0; e < E.size(); ++e) {      // E is sorted by row dof, so each node's entries stay in order
+    int64_t node = E.r[e] / 3;
+    int at = fill[node]++;
+    rr[at] = (int8_t)(E.r[e] % 3); col[at] = (int)E.c[e]; v[at] = E.v[e]; vf[at] = (float)E.v[e];
+  }
+  FEB_TRY(pool.upload(&V.node_ptr, ptr.data(), ptr.size()));
+  FEB_TRY(pool.upload(&V.ent_r, rr.data(), rr.size()));
+  FEB_TRY(pool.upload(&V.ent_col, col.data(), col.size()));
+  FEB_TRY(pool.upload(&V.ent_v64, v.data(), v.size()));
+  FEB_TRY(pool.upload(&V.ent_v32, vf.data(), vf.size()));
+  return FEB_OK;
+}
 
 }  // namespace
 }  // namespace feb
@@ -414,6 +443,14 @@ struct FebHandle {
   cudaGraphExec_t g_outer = nullptr, g_inner = nullptr;
   int g_outer_nodes = 0, g_inner_nodes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  KuConfig ku32{}, ku64{};   // launch shapes of the fine K.u (autotuned per grid shape)
+  static constexpr int kStages = 10;
+  cudaEvent_t stage_ev[kStages + 1] = {};
+  int stage_n = 0;
+  double stage_ms[kStages] = {};
+  void stage_mark() {   // event after each set-up stage (device time between consecutive marks)
+    if (stage_n <= kStages) cudaEventRecord(stage_ev[stage_n++], s);
+  }
   double t_setup_ms = 0.0;
   int launches = 0;
 
@@ -426,6 +463,7 @@ struct FebHandle {
     pool.release();
     cudaStreamSynchronize(s);
     if (ev_sync) cudaEventDestroy(ev_sync);
+    for (auto& e : stage_ev) if (e) cudaEventDestroy(e);
     cudaStreamDestroy(s);
   }
 
@@ -437,21 +475,28 @@ struct FebHandle {
   void apply(int l, const T* u, T* y, const int* skip) {
     if (l == 0) {
       const FineView<T>& F = fine<T>();
-      const int zc = 16;
+      const KuConfig cfg = std::is_same<T, double>::value ? ku64 : ku32;
       switch (mode) {
-        case MAT_ISO_SRI: launch_fine_apply<T, MAT_ISO_SRI>(F, u, y, skip, zc, s); break;
-        case MAT_ISO_FULL: launch_fine_apply<T, MAT_ISO_FULL>(F, u, y, skip, zc, s); break;
-        default: launch_fine_apply<T, MAT_ORTHO>(F, u, y, skip, zc, s); break;
+        case MAT_ISO_SRI: launch_fine_apply<T, MAT_ISO_SRI>(F, u, y, skip, cfg, s); break;
+        case MAT_ISO_FULL: launch_fine_apply<T, MAT_ISO_FULL>(F, u, y, skip, cfg, s); break;
+        default: launch_fine_apply<T, MAT_ORTHO>(F, u, y, skip, cfg, s); break;
       }
     } else {
-      Level& V = L[l];
-      StencilView<T> S{V.nx, V.ny, V.nz, V.nnode, stencil<T>(V), V.sparse.nrow, V.sparse.row_dof, V.sparse.row_ptr,
-                       V.sparse.col, sval<T>(V)};
-      launch_stencil_apply<T>(S, u, y, skip, s);
+      launch_sym<T>(symview<T>(L[l]), EPI_APPLY, u, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0, skip, s);
     }
   }
-  template <typename T> static const T* stencil(const Level& V);
-  template <typename T> static const T* sval(const Level& V);
+  template <typename T>
+  static SymView<T> symview(const Level& V) {
+    SymView<T> S;
+    S.nx = V.nx; S.ny = V.ny; S.nz = V.nz; S.n = V.nnode;
+    S.S = symS<T>(V);
+    S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
+    S.Dinv = dinv<T>(V);
+    return S;
+  }
+  template <typename T> static const T* symS(const Level& V);
+  template <typename T> static const T* entv(const Level& V);
+  template <typename T> static T* ve(Level& V);
   template <typename T> static const T* dinv(const Level& V);
   template <typename T> static T* vb(Level& V);
   template <typename T> static T* vx(Level& V);
@@ -462,6 +507,23 @@ struct FebHandle {
   // ---------------------------------------------------------------------------------------------- V-cycle
   template <typename T>
   void smooth(int l, const T* b, T* x, bool zero_start, const int* skip) {
+    if (l > 0) {   // stencil level: residual and Chebyshev steps fused with the stencil product
+      Level& V = L[l];
+      const SymView<T> SV = symview<T>(V);
+      T *r = vr<T>(V), *d = vd<T>(V), *e = ve<T>(V);
+      const T* D = dinv<T>(V);
+      if (zero_start) {
+        launch_cheb_first<T>(b, r, d, x, D, lp + l, V.ntotal, skip, s);
+      } else {
+        launch_sym<T>(SV, EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s);
+        launch_cheb_from_r<T>(r, d, x, D, lp + l, V.ntotal, skip, s);
+      }
+      for (int k = 0; k + 1 < opt.cheb_degree; ++k) {
+        launch_sym<T>(SV, EPI_CHEB, d, nullptr, nullptr, r, e, x, lp + l, k, skip, s);
+        std::swap(d, e);
+      }
+      return;
+    }
     Level& V = L[l];
     const int64_t nn = V.ntotal;
     T *r = vr<T>(V), *d = vd<T>(V), *t = vt<T>(V);
@@ -489,8 +551,12 @@ struct FebHandle {
     Level& C = L[l + 1];
     smooth<T>(l, b, x, true, skip);
     T *t = vt<T>(V), *r = vr<T>(V);
-    apply<T>(l, x, t, skip);
-    launch_residual<T>(b, t, r, 3 * V.ntotal, skip, s);
+    if (l > 0) {
+      launch_sym<T>(symview<T>(V), EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s);
+    } else {
+      apply<T>(l, x, t, skip);
+      launch_residual<T>(b, t, r, 3 * V.ntotal, skip, s);
+    }
     launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s);
     vcycle<T>(l + 1, vb<T>(C), vx<T>(C), skip);
     launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), x, skip, s);
@@ -531,18 +597,42 @@ struct FebHandle {
     launch_finalize(FIN_CONV, partials, S, nullptr, 0, skip, s);
   }
 
+  // one CG iteration captured as a graph; with use_graphs == 2 the iteration is the body of a device-side
+  // while loop (conditional graph node): the whole CG then runs as one graph launch
   int capture(CgState* S, bool inner, cudaGraphExec_t* exec, int* nodes) {
     if (*exec) return FEB_OK;
-    cudaGraph_t g;
     const long long before = g_launches.load();
-    FEB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
-    else cg_body<double>(S, x, r, z, p, q);
-    FEB_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraph_t g = nullptr;
+    if (opt.use_graphs >= 2) {
+      FEB_CUDA(cudaGraphCreate(&g, 0));
+      cudaGraphConditionalHandle cond;
+      FEB_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      FEB_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      FEB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
+      else cg_body<double>(S, x, r, z, p, q);
+      launch_set_condition(cond, S, s);
+      FEB_CUDA(cudaStreamEndCapture(s, &body));
+      size_t nn = 0;
+      FEB_CUDA(cudaGraphGetNodes(body, nullptr, &nn));
+      *nodes = (int)nn;
+    } else {
+      FEB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      if (inner) cg_body<float>(S, xf, rf, zf, pf, qf);
+      else cg_body<double>(S, x, r, z, p, q);
+      FEB_CUDA(cudaStreamEndCapture(s, &g));
+      size_t nn = 0;
+      FEB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+      *nodes = (int)nn;
+    }
     g_launches.store(before);   // captured kernels are counted when the graph runs
-    size_t nn = 0;
-    FEB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
-    *nodes = (int)nn;
     FEB_CUDA(cudaGraphInstantiate(exec, g, 0));
     FEB_CUDA(cudaGraphDestroy(g));
     return FEB_OK;
@@ -553,6 +643,16 @@ struct FebHandle {
     cudaGraphExec_t* ex = inner ? &g_inner : &g_outer;
     int* nn = inner ? &g_inner_nodes : &g_outer_nodes;
     if (opt.use_graphs) FEB_TRY(capture(S, inner, ex, nn));
+    if (opt.use_graphs >= 2) {   // device-side loop: one launch, one synchronisation
+      FEB_CUDA(cudaGraphLaunch(*ex, s));
+      FEB_CUDA(cudaMemcpyAsync(st_h, S, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+      FEB_CUDA(cudaStreamSynchronize(s));
+      const int iters = st_h->it > 0 ? st_h->it : 1;
+      launches += iters * (*nn);
+      note_launch(iters * (*nn));
+      out = *st_h;
+      return FEB_OK;
+    }
     const int every = std::max(1, opt.check_every);
     for (int guard = 0; guard < 1000000; ++guard) {
       FEB_CUDA(cudaMemcpyAsync(st_h, S, sizeof(CgState), cudaMemcpyDeviceToHost, s));
@@ -610,10 +710,6 @@ struct FebHandle {
 
 template <> const FineView<double>& FebHandle::fine<double>() const { return F64; }
 template <> const FineView<float>& FebHandle::fine<float>() const { return F32; }
-template <> const double* FebHandle::stencil<double>(const Level& V) { return V.A64; }
-template <> const float* FebHandle::stencil<float>(const Level& V) { return V.A32; }
-template <> const double* FebHandle::sval<double>(const Level& V) { return V.sparse.v64; }
-template <> const float* FebHandle::sval<float>(const Level& V) { return V.sparse.v32; }
 template <> const double* FebHandle::dinv<double>(const Level& V) { return V.Dinv64; }
 template <> const float* FebHandle::dinv<float>(const Level& V) { return V.Dinv32; }
 template <> double* FebHandle::vb<double>(Level& V) { return V.b64; }
@@ -626,6 +722,12 @@ template <> double* FebHandle::vd<double>(Level& V) { return V.d64; }
 template <> float* FebHandle::vd<float>(Level& V) { return V.d32; }
 template <> double* FebHandle::vt<double>(Level& V) { return V.t64; }
 template <> float* FebHandle::vt<float>(Level& V) { return V.t32; }
+template <> double* FebHandle::ve<double>(Level& V) { return V.e64; }
+template <> float* FebHandle::ve<float>(Level& V) { return V.e32; }
+template <> const double* FebHandle::symS<double>(const Level& V) { return V.S64; }
+template <> const float* FebHandle::symS<float>(const Level& V) { return V.S32; }
+template <> const double* FebHandle::entv<double>(const Level& V) { return V.ent_v64; }
+template <> const float* FebHandle::entv<float>(const Level& V) { return V.ent_v32; }
 
 
 namespace feb {
@@ -656,11 +758,11 @@ int level_vectors(Pool& pool, Level& V, bool f64, bool f32) {
   size_t n = 3 * (size_t)V.ntotal;
   if (f64) {
     FEB_TRY(pool.zeros(&V.b64, n)); FEB_TRY(pool.zeros(&V.x64, n)); FEB_TRY(pool.zeros(&V.r64, n));
-    FEB_TRY(pool.zeros(&V.d64, n)); FEB_TRY(pool.zeros(&V.t64, n));
+    FEB_TRY(pool.zeros(&V.d64, n)); FEB_TRY(pool.zeros(&V.t64, n)); FEB_TRY(pool.zeros(&V.e64, n));
   }
   if (f32) {
     FEB_TRY(pool.zeros(&V.b32, n)); FEB_TRY(pool.zeros(&V.x32, n)); FEB_TRY(pool.zeros(&V.r32, n));
-    FEB_TRY(pool.zeros(&V.d32, n)); FEB_TRY(pool.zeros(&V.t32, n));
+    FEB_TRY(pool.zeros(&V.d32, n)); FEB_TRY(pool.zeros(&V.t32, n)); FEB_TRY(pool.zeros(&V.e32, n));
   }
   return FEB_OK;
 }
@@ -700,6 +802,72 @@ int power_iteration(FebHandle* h, int l) {
     launch_scale(V.d64, V.x64, h->lp + l, n, h->s);
   }
   FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ autotuner
+// Launch shape of the fine K.u (warps per CTA x node planes per CTA), picked by timing every candidate
+// on this operator and cached per (grid, material model, split copies) for the process lifetime.
+struct TuneKey {
+  int nx, ny, nz, mode, copies;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nx, ny, nz, mode, copies) < std::tie(o.nx, o.ny, o.nz, o.mode, o.copies);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<KuConfig, KuConfig>> g_tune_cache;
+
+template <typename T>
+int tune_one(FebHandle* h, KuConfig* best, T* u, T* y) {
+  const int tys[3] = {8, 12, 16};
+  const int zcs[6] = {6, 8, 12, 16, 24, 32};
+  float best_ms = 1e30f;
+  for (int ty : tys)
+    for (int zc : zcs) {
+      KuConfig c{ty, zc};
+      KuConfig& slot = std::is_same<T, double>::value ? h->ku64 : h->ku32;
+      slot = c;
+      for (int w = 0; w < 2; ++w) h->apply<T>(0, u, y, nullptr);
+      FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+      for (int r = 0; r < 3; ++r) h->apply<T>(0, u, y, nullptr);
+      FEB_CUDA(cudaEventRecord(h->ev1, h->s));
+      FEB_CUDA(cudaEventSynchronize(h->ev1));
+      float ms = 0.f;
+      FEB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+      if (ms < best_ms) { best_ms = ms; *best = c; }
+    }
+  return FEB_OK;
+}
+
+int autotune_ku(FebHandle* h) {
+  TuneKey key{h->nx, h->ny, h->nz, h->mode, h->ntotal > h->nnode ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      h->ku32 = it->second.first;
+      h->ku64 = it->second.second;
+      return FEB_OK;
+    }
+  }
+  const char* env = std::getenv("FEB_KU_CONFIG");     // "ty,zchunk" pins the shape (tests, profiling)
+  if (env && *env) {
+    int ty = 16, zc = 16;
+    if (std::sscanf(env, "%d,%d", &ty, &zc) == 2) { h->ku32 = h->ku64 = KuConfig{ty, zc}; return FEB_OK; }
+  }
+  const size_t n = 3 * (size_t)h->ntotal;
+  double *u64 = nullptr, *y64 = nullptr;
+  FEB_TRY(h->pool.zeros(&u64, n));
+  FEB_TRY(h->pool.alloc(&y64, n));
+  KuConfig b32{}, b64{};
+  FEB_TRY(tune_one<float>(h, &b32, (float*)u64, (float*)y64));
+  FEB_TRY(tune_one<double>(h, &b64, u64, y64));
+  h->pool.free(u64);
+  h->pool.free(y64);
+  h->ku32 = b32;
+  h->ku64 = b64;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_cache[key] = {b32, b64};
   return FEB_OK;
 }
 
@@ -783,6 +951,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     FEB_CUDA(cudaStreamSynchronize(s));
     H.orig_copy_h.assign(oc.begin(), oc.end());
   }
+  H.stage_mark();   // 1: cells, irregular list, copies
   std::vector<uint8_t> used_h(H.ntotal);
   FEB_CUDA(cudaMemcpyAsync(used_h.data(), V.used, H.ntotal, cudaMemcpyDeviceToHost, s));
   FEB_CUDA(cudaStreamSynchronize(s));
@@ -851,6 +1020,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   F.nrow = G.nrow = c0.nrow; F.row_dof = G.row_dof = c0.row_dof; F.row_ptr = G.row_ptr = c0.row_ptr;
   F.col = G.col = c0.col; F.val = c0.v64; G.val = c0.v32;
   // used nodes, diagonal blocks
+  H.stage_mark();   // 2: penalties and extra entries (host sort / classification, uploads)
   FEB_TRY(count_mask(h, V.used, H.ntotal, &H.ndof));
   H.ndof *= 3;
   V.ndof = H.ndof;
@@ -866,6 +1036,9 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   launch_block_inverse(D, H.ntotal, V.Dinv64, V.Dinv32, s);
   FEB_CUDA(cudaGetLastError());
   H.pool.free(D);
+  H.stage_mark();   // 3: used nodes, level-0 diagonal blocks
+  FEB_TRY(autotune_ku(h));
+  H.stage_mark();   // 4: K.u autotuning (first handle of a grid shape only)
   return FEB_OK;
 }
 
@@ -963,10 +1136,12 @@ int build_hierarchy(FebHandle* h) {
     }
     FEB_CUDA(cudaGetLastError());
     C.nonlocal = project(F.nonlocal, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
-    FEB_TRY(upload_csr(H.pool, C.nonlocal, C.sparse));
+    FEB_TRY(upload_node_csr(H.pool, C.nonlocal, C.nnode, C));
+    FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)C.ntotal));
+    launch_stencil_to_sym<double>(C.A64, C.ntotal, C.S64, H.s);
     if (f32) {
-      FEB_TRY(H.pool.alloc(&C.A32, 243 * (size_t)C.ntotal));
-      launch_convert<double, float>(C.A64, C.A32, 243 * (int64_t)C.ntotal, nullptr, H.s);
+      FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)C.ntotal));
+      launch_stencil_to_sym<float>(C.A64, C.ntotal, C.S32, H.s);
     }
     l += 1;
     bool last = (C.ndof <= H.opt.min_dofs) || (l == maxl - 1);
@@ -995,13 +1170,21 @@ int build_hierarchy(FebHandle* h) {
       H.pool.free(D);
     }
   }
+  H.stage_mark();   // 5: transfers, Galerkin products, coarse diagonal blocks
   // work vectors and smoother parameters
   for (int k = 0; k <= H.coarsest; ++k) {
     Level& V = H.L[k];
     FEB_TRY(level_vectors<double>(H.pool, V, true, f32));
   }
   for (int k = 0; k < H.coarsest; ++k) FEB_TRY(power_iteration(h, k));
+  H.stage_mark();   // 6: work vectors, power iterations
   FEB_TRY(build_dense(h));
+  H.stage_mark();   // 7: dense coarsest level and its inverse
+  for (int k = 1; k <= H.coarsest; ++k) {      // the full stencils only feed the Galerkin products
+    H.pool.free(H.L[k].A64);
+    H.L[k].A64 = nullptr;
+    if (f32) { H.pool.free(H.L[k].S64); H.L[k].S64 = nullptr; }
+  }
   return FEB_OK;
 }
 
@@ -1030,7 +1213,7 @@ void feb_default_options(FebOptions* o) {
   o->check_every = 1;
   o->inner_tol = 1e-3;
   o->inner_maxiter = 200;
-  o->use_graphs = 1;
+  o->use_graphs = 2;
   o->seed = 0;
 }
 
@@ -1042,6 +1225,15 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   *out = nullptr;
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) { set_last_error("feb_create: empty grid"); return FEB_ERR_ARG; }
   if (op->mat_mode < 0 || op->mat_mode > 2) { set_last_error("feb_create: bad mat_mode"); return FEB_ERR_ARG; }
+  {
+    // keep freed pool memory mapped for the next handle (set-up allocates and frees GBs per solve)
+    int dev = 0;
+    cudaMemPool_t mp;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   FebHandle* h = new FebHandle((cudaStream_t)stream);
   if (opt) h->opt = *opt; else feb_default_options(&h->opt);
   if (h->opt.cheb_degree < 1 || h->opt.cheb_degree > 9) { delete h; set_last_error("cheb_degree must be 1..9"); return FEB_ERR_ARG; }
@@ -1055,8 +1247,10 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   if (h->ntotal < h->nnode || h->ntotal > INT32_MAX / 3) { delete h; set_last_error("feb_create: bad nnode_total"); return FEB_ERR_ARG; }
   cudaEventCreate(&h->ev0);
   cudaEventCreate(&h->ev1);
+  for (auto& e : h->stage_ev) cudaEventCreate(&e);
   if (h->sync_in() != FEB_OK) { delete h; return FEB_ERR_CUDA; }
   cudaEventRecord(h->ev0, h->s);
+  h->stage_mark();   // 0: start
   int st = FEB_OK;
   do {
     h->L.reserve(kMaxLevels);
@@ -1095,6 +1289,11 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->t_setup_ms = ms;
+    for (int i = 0; i + 1 < h->stage_n; ++i) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, h->stage_ev[i], h->stage_ev[i + 1]);
+      h->stage_ms[i] = t;
+    }
   }
   if (st != FEB_OK) {
     delete h;
@@ -1145,9 +1344,13 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   Z.ngroups = G; Z.off = doff; Z.nodes = dnodes; Z.cen = cen;
   Z.nxn = H.nx + 1; Z.nyn = H.ny + 1; Z.nnode = H.nnode; Z.orig_copy = H.orig_copy;
   Z.xe = H.xe_d; Z.ye = H.ye_d; Z.ze = H.ze_d;
-  launch_centroids(Z, cen, H.s);
   const int nc = 6 * G;
   FEB_TRY(H.pool.alloc(&H.zpart, (size_t)rigid_blocks(Z) * G * 6));
+  launch_centroids(Z, cen, H.zpart, H.s);
+  double* rho = nullptr;
+  FEB_TRY(H.pool.alloc(&rho, 3 * kept.size()));
+  Z.rho = rho;
+  launch_rigid_rho(Z, rho, H.s);
   FEB_TRY(H.pool.alloc(&H.zr, nc));
   FEB_TRY(H.pool.alloc(&H.zcoef, nc));
   // Ec = Z^T K Z column by column (FP64 matrix-free K)
@@ -1270,6 +1473,9 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
     inf.lmax[l] = l < H.coarsest ? lp[l].lmax : 0.0;
   }
   inf.kernel_launches = H.launches;
+  for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
+  inf.ku_shape[0] = H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
+  inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
   if (info) *info = inf;
   FEB_TRY(H.sync_out());
   if (st != FEB_OK) {

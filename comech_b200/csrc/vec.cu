@@ -10,10 +10,17 @@ __global__ void __launch_bounds__(kThreads)
 k_dot_partial(const Ta* __restrict__ a, const Tb* __restrict__ b, int64_t n, double* __restrict__ partials,
               const int* __restrict__ skip) {
   if (skip && *skip) return;
-  double s = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
-    s += double(a[i]) * double(b[i]);
-  s = block_sum(s);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {     // four independent loads in flight per thread
+    s0 += double(a[i]) * double(b[i]);
+    s1 += double(a[i + stride]) * double(b[i + stride]);
+    s2 += double(a[i + 2 * stride]) * double(b[i + 2 * stride]);
+    s3 += double(a[i + 3 * stride]) * double(b[i + 3 * stride]);
+  }
+  for (; i < n; i += stride) s0 += double(a[i]) * double(b[i]);
+  double s = block_sum((s0 + s1) + (s2 + s3));
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
@@ -98,14 +105,25 @@ k_update_xr(const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
             const CgState* __restrict__ st, int64_t n, double* __restrict__ partials, const int* __restrict__ skip) {
   if (skip && *skip) return;
   const T alpha = T(st->alpha);
-  double s = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+  double s0 = 0.0, s1 = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  for (; i + stride < n; i += 2 * stride) {
+    const T p0 = p[i], p1 = p[i + stride], q0 = q[i], q1 = q[i + stride];
+    const T x0 = x[i], x1 = x[i + stride], ra = r[i], rb = r[i + stride];
+    x[i] = x0 + alpha * p0; x[i + stride] = x1 + alpha * p1;
+    const T r0 = ra - alpha * q0, r1 = rb - alpha * q1;
+    r[i] = r0; r[i + stride] = r1;
+    s0 += double(r0) * double(r0);
+    s1 += double(r1) * double(r1);
+  }
+  for (; i < n; i += stride) {
     x[i] += alpha * p[i];
     T ri = r[i] - alpha * q[i];
     r[i] = ri;
-    s += double(ri) * double(ri);
+    s0 += double(ri) * double(ri);
   }
-  s = block_sum(s);
+  double s = block_sum(s0 + s1);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
@@ -163,6 +181,20 @@ __global__ void k_cheb_step(const T* __restrict__ Ad, T* __restrict__ r, T* __re
   T d0 = a1 * d[3 * i] + a2 * z0, d1 = a1 * d[3 * i + 1] + a2 * z1, d2 = a1 * d[3 * i + 2] + a2 * z2;
   d[3 * i] = d0; d[3 * i + 1] = d1; d[3 * i + 2] = d2;
   x[3 * i] += d0; x[3 * i + 1] += d1; x[3 * i + 2] += d2;
+}
+
+template <typename T>
+__global__ void k_cheb_from_r(const T* __restrict__ r, T* __restrict__ d, T* __restrict__ x, const T* __restrict__ D,
+                              const LevelParams* __restrict__ lp, int64_t nn, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const T c = T(lp->c_init);
+  T z0, z1, z2;
+  bj(D, nn, i, r[3 * i], r[3 * i + 1], r[3 * i + 2], z0, z1, z2);
+  z0 *= c; z1 *= c; z2 *= c;
+  d[3 * i] = z0; d[3 * i + 1] = z1; d[3 * i + 2] = z2;
+  x[3 * i] += z0; x[3 * i + 1] += z1; x[3 * i + 2] += z2;
 }
 
 template <typename T>
@@ -248,9 +280,17 @@ __global__ void k_mask_vector(double* __restrict__ v, const uint8_t* __restrict_
   if (!used[i / 3]) v[i] = fill;
 }
 
+__global__ void k_set_condition(cudaGraphConditionalHandle h, const CgState* __restrict__ st) {
+  cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
 inline int grid_for(int64_t n) { return int(std::min<int64_t>((n + kThreads - 1) / kThreads, 8 * kSmCount)); }
 
 }  // namespace
+
+void launch_set_condition(cudaGraphConditionalHandle h, const CgState* st, cudaStream_t s) {
+  k_set_condition<<<1, 1, 0, s>>>(h, st); note_launch();
+}
 
 template <typename Ta, typename Tb>
 void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s) {
@@ -289,6 +329,12 @@ template <typename T>
 void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int k, int64_t nn,
                       const int* skip, cudaStream_t s) {
   k_cheb_step<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(Ad, r, d, x, Dinv, lp, k, nn, skip); note_launch();
+}
+
+template <typename T>
+void launch_cheb_from_r(const T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn, const int* skip,
+                        cudaStream_t s) {
+  k_cheb_from_r<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(r, d, x, Dinv, lp, nn, skip); note_launch();
 }
 
 template <typename T>
@@ -343,6 +389,8 @@ void launch_mask_vector(double* v, const uint8_t* used, int64_t nn, double fill,
   template void launch_cheb_step<T>(const T*, T*, T*, T*, const T*, const LevelParams*, int, int64_t,           \
                                     const int*, cudaStream_t);                                                 \
   template void launch_residual<T>(const T*, const T*, T*, int64_t, const int*, cudaStream_t);                 \
+  template void launch_cheb_from_r<T>(const T*, T*, T*, const T*, const LevelParams*, int64_t, const int*,      \
+                                      cudaStream_t);                                                           \
   template void launch_axpy_dev<T>(const T*, T*, int64_t, const int*, cudaStream_t);
 INST_T(float)
 INST_T(double)

@@ -5,7 +5,7 @@
 
 namespace feb {
 
-constexpr int kRedBlocks = 2 * kSmCount;   // partial sums per reduction
+constexpr int kRedBlocks = 4 * kSmCount;   // partial sums per reduction
 
 // CG state (one per solve); SciPy cg semantics (stop when ||r|| < tol ||b|| before an iteration).
 struct CgState {
@@ -21,6 +21,9 @@ struct LevelParams {
   double c_init;             // Chebyshev: 1 / theta
   double a1[8], a2[8];       // Chebyshev step k: d = a1[k] d + a2[k] M r
 };
+
+// sets the while-loop condition of a conditional graph node: continue while the CG is not done
+void launch_set_condition(cudaGraphConditionalHandle h, const CgState* st, cudaStream_t s);
 
 template <typename Ta, typename Tb>
 void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s);
@@ -46,6 +49,10 @@ void launch_cheb_init(const T* b, const T* Ax, T* r, T* d, T* x, const T* Dinv, 
 template <typename T>
 void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int k, int64_t nn,
                       const int* skip, cudaStream_t s);
+// d = (1/theta) Dinv r, x += d  (Chebyshev start from a given residual)
+template <typename T>
+void launch_cheb_from_r(const T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn, const int* skip,
+                        cudaStream_t s);
 template <typename T>
 void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s);
 

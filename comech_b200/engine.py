@@ -188,7 +188,8 @@ def _info_dict(info, t0, extra=None):
              t_gpu=round(info.t_solve_ms / 1e3, 4), coarse="dense-inverse", coarse_n=int(info.coarse_n),
              level_dofs=[int(info.level_dofs[i]) for i in range(int(info.levels))],
              lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
-             kernel_launches=int(info.kernel_launches), device=f"cuda:{_torch().cuda.current_device()}",
+             kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape),
+             t_stage_ms=[round(float(v), 3) for v in info.t_stage_ms], device=f"cuda:{_torch().cuda.current_device()}",
              t_wall=round(time.perf_counter() - t0, 4))
     if extra:
         d.update(extra)

@@ -83,7 +83,8 @@ typedef struct FebOptions {
   int32_t check_every;           /* host polls convergence every k iterations (>= 1) */
   double inner_tol;              /* REFINE: relative residual reduction of each FP32 sweep */
   int32_t inner_maxiter;         /* REFINE: CG iterations per sweep */
-  int32_t use_graphs;            /* capture the CG iteration in a CUDA graph */
+  int32_t use_graphs;            /* 0 direct launches; 1 one graph per CG iteration, host polls convergence;
+                                    2 the CG loop is a device-side while loop (conditional graph node) */
   uint64_t seed;                 /* power-iteration start vectors */
 } FebOptions;
 
@@ -100,6 +101,9 @@ typedef struct FebInfo {
   double lmax[8];
   int32_t coarse_n;              /* dofs of the dense coarsest level */
   int32_t kernel_launches;       /* kernels launched by feb_solve */
+  int32_t ku_shape[4];           /* autotuned fine K.u launch shape: FP32 (warps, planes), FP64 (warps, planes) */
+  double t_stage_ms[8];          /* feb_create stages: cells, penalties/extra, diagonal blocks, K.u tuning,
+                                    Galerkin hierarchy, power iterations, dense coarse level, (spare) */
 } FebInfo;
 
 /* Default options (tol 1e-6, maxiter 800 as rb/splitfe.py:123; GMG parameters of fe/gmg.py:80). */
