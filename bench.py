@@ -90,6 +90,26 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def rank_seed(rank):
+    """Seed of the instance a rank solves (independent instances, weak scaling)."""
+    return int(rank)
+
+
+def rank_instances(rank, world, n):
+    """Round-robin split of n independent instances over the ranks."""
+    return list(range(rank, n, world))
+
+
+def reduce_max(t, dist, device="cuda"):
+    """Max over ranks of a per-rank duration (identity without a process group)."""
+    if dist is None:
+        return float(t)
+    import torch
+    v = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return float(v.item())
+
+
 def make_problem(seed, dims=WORKLOAD):
     from comech_b200 import synth
     return synth.hindfoot_problem(dims["nx"], dims["ny"], dims["nz"], h=dims["h"], seed=seed)
@@ -168,7 +188,7 @@ def run_ours(args, rank, world, dist):
     from comech_b200 import engine, _lib
     lib = _lib.load()
     dev = torch.cuda.current_device()
-    P = make_problem(seed=rank)
+    P = make_problem(seed=rank_seed(rank))
     d = device_inputs(P)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
     prec = args.precision
@@ -194,11 +214,7 @@ def run_ours(args, rank, world, dist):
             dist.barrier()
         torch.cuda.synchronize()
     launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
-    t_total = sum(step_ms) / 1e3
-    if dist:
-        t = torch.tensor([t_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
+    t_total = reduce_max(sum(step_ms) / 1e3, dist)
     value = t_total / (args.steps * world)
     mixed_info = info
     U_mixed = U.cpu().numpy()
@@ -257,12 +273,7 @@ def run_ours(args, rank, world, dist):
     h2d = (2 * ncell * 8 + ncell + ncell * 64 + ntotal * 8 + 8 * sum(len(x) for x in P["node_groups"])
            + P["loads"][0][0].size * 32 + nact * 8 + P["fixed"][0].size * 32 + P["extra"].node_coo()[4].size * 24)
     d2h = ntotal * 24 + nact * 13 * 8
-    e2e_val = max(e2e_s)
-    if dist:
-        t = torch.tensor([e2e_val], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = float(t.item())
-    e2e_val /= world
+    e2e_val = reduce_max(max(e2e_s), dist) / world
     # ---------------------------------------------------------------- roofline of the K.u operator
     pk, pk_kind = peaks()
     pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"], pen_node=d["pen_node"],

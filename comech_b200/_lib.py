@@ -29,7 +29,7 @@ class FebOperator(C.Structure):
     _fields_ = [("mat_mode", C.c_int32), ("mat", C.c_void_p), ("active", C.c_void_p), ("cn", C.c_void_p),
                 ("nnode_total", C.c_int64), ("orig", C.c_void_p), ("npen", C.c_int64), ("pen_node", C.c_void_p),
                 ("pen_k", C.c_void_p), ("nextra", C.c_int64), ("extra_row", C.c_void_p), ("extra_col", C.c_void_p),
-                ("extra_val", C.c_void_p)]
+                ("extra_val", C.c_void_p), ("nmark", C.c_int64), ("mark_used", C.c_void_p)]
 
 
 class FebOptions(C.Structure):

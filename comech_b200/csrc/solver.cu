@@ -955,6 +955,15 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   std::vector<uint8_t> used_h(H.ntotal);
   FEB_CUDA(cudaMemcpyAsync(used_h.data(), V.used, H.ntotal, cudaMemcpyDeviceToHost, s));
   FEB_CUDA(cudaStreamSynchronize(s));
+  if (op->nmark > 0) {     // nodes of a matrix-only operator
+    for (int64_t e2 = 0; e2 < op->nmark; ++e2) {
+      int64_t node = op->mark_used[e2];
+      if (node < 0 || node >= H.ntotal) { set_last_error("mark_used node %lld out of range", (long long)node); return FEB_ERR_ARG; }
+      used_h[node] = 1;
+    }
+    FEB_CUDA(cudaMemcpyAsync(V.used, used_h.data(), H.ntotal, cudaMemcpyHostToDevice, s));
+    FEB_CUDA(cudaStreamSynchronize(s));
+  }
   // penalties (entries on unused nodes are dropped, fe/solver.py:213-215)
   std::vector<int> pn;
   std::vector<double> pk;

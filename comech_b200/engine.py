@@ -77,7 +77,7 @@ class Problem:
     """A level-0 operator on the device with its multigrid hierarchy (one FebHandle)."""
 
     def __init__(self, g, mat_mode, mat, active, cn=None, orig=None, pen_node=None, pen_k=None, extra_coo=None,
-                 precision="fp64", tol=1e-6, maxiter=800, options=None):
+                 precision="fp64", tol=1e-6, maxiter=800, options=None, mark_used=None):
         _lib.load()
         torch = _torch()
         self.g = g
@@ -99,11 +99,12 @@ class Problem:
             er = ec = np.zeros(0, np.int64); ev = np.zeros(0)
         else:
             er, ec, ev = (np.ascontiguousarray(a, dtype=t) for a, t in zip(extra_coo, (np.int64, np.int64, np.float64)))
+        mu = np.ascontiguousarray(mark_used if mark_used is not None else np.zeros(0), dtype=np.int64)
         op = _lib.FebOperator(mat_mode, self.mat.data_ptr(), self.active.data_ptr(),
                               self.cn.data_ptr() if self.cn is not None else None, self.ntotal,
                               self.orig.data_ptr() if self.orig is not None else None, len(pen_node),
                               pen_node.ctypes.data, pen_k.ctypes.data, len(ev), er.ctypes.data, ec.ctypes.data,
-                              ev.ctypes.data)
+                              ev.ctypes.data, len(mu), mu.ctypes.data)
         self.opt = _options(precision, tol, maxiter, options)
         h = C.c_void_p()
         _lib.check(_lib.load().feb_create(C.byref(self.grid), C.byref(op), C.byref(self.opt), _stream(), C.byref(h)))
@@ -380,3 +381,67 @@ def element_forces_cn(g, lam, mu, U, cells, cn, aniso=None):
     _lib.check(_lib.load().feb_element_forces(C.byref(gs), _ptr(mat), _ptr(Ud), n, _ptr(cd), _ptr(cnd), _ptr(out),
                                               _stream()))
     return out.view(n, 8, 3).cpu().numpy()
+
+
+def _rigid_groups_from_Z(Z, n):
+    """Node groups of a Z built like fe/solver.py:177-199 (6 columns per group: 3 unit translations, then 3
+    rotations); returns the compact node indices of every group, or raises if Z has another structure."""
+    import scipy.sparse as sp
+    Zc = sp.csc_matrix(Z)
+    if Zc.shape[1] % 6:
+        raise NotImplementedError("Z must hold 6 rigid-body columns per node group")
+    groups = []
+    for g in range(Zc.shape[1] // 6):
+        col = Zc[:, 6 * g].tocoo()
+        dofs = col.row[col.data != 0]
+        if len(dofs) == 0 or np.any(dofs % 3) or not np.allclose(col.data[col.data != 0], 1.0):
+            raise NotImplementedError("Z columns are not translations of node groups")
+        groups.append(dofs // 3)
+    return groups
+
+
+def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, A_op=None, Z=None, *, precision="fp64",
+            options=None):
+    """GMG-preconditioned CG for an assembled matrix on compact dofs (fe/gmg.py:120-137, the plugin point
+    that rb/rbfe.py:21-27 swaps).  Compatibility path: the fine level applies A as a sparse matrix on the
+    device and the coarse levels are its Galerkin products on the structured grid; node ``i`` of A sits at
+    grid node ``used_nodes[i]`` (split copies share their grid node, rb/splitfe.py:153).  Z, when given,
+    must be the per-group rigid-body modes of fe/solver.py:177-199.  Returns (x, info)."""
+    import scipy.sparse as sp
+    from .grid import Grid
+    if A_op is not None:
+        raise NotImplementedError("A_op is not supported by the device solver")
+    t0 = time.perf_counter()
+    xe, ye, ze = grid_edges
+    g = Grid(xe, ye, ze)
+    used_nodes = np.asarray(used_nodes, np.int64)
+    n_c = len(used_nodes)
+    # full layout: the first compact node at a grid position takes the grid id, later ones become copies
+    order = np.argsort(used_nodes, kind="stable")
+    first = np.ones(n_c, bool)
+    first[order[1:]] = used_nodes[order[1:]] != used_nodes[order[:-1]]
+    node_of = np.empty(n_c, np.int64)
+    node_of[first] = used_nodes[first]
+    dup = np.flatnonzero(~first)
+    node_of[dup] = g.nnode + np.arange(len(dup))
+    orig = np.concatenate([np.arange(g.nnode), used_nodes[dup]])
+    M = sp.coo_matrix(A)
+    coo = (3 * node_of[M.row // 3] + M.row % 3, 3 * node_of[M.col // 3] + M.col % 3, M.data)
+    ncell = g.nx * g.ny * g.nz
+    # no cells: the whole operator is the sparse part; the used nodes are the ones A is given on
+    P = Problem(g, _lib.MAT_ISO_SRI, np.zeros(2 * ncell), np.zeros(ncell, bool), cn=None, orig=orig, extra_coo=coo,
+                precision=precision, tol=tol, maxiter=maxiter, options=options, mark_used=node_of)
+    try:
+        if Z is not None:
+            P.set_rigid_groups([node_of[gr] for gr in _rigid_groups_from_Z(Z, n_c)])
+        bf = np.zeros((len(orig), 3)); bf[node_of] = np.asarray(b, np.float64).reshape(-1, 3)
+        f = _dev(bf.ravel(), np.float64)
+        x0d = None
+        if x0 is not None:
+            xf = np.zeros((len(orig), 3)); xf[node_of] = np.asarray(x0, np.float64).reshape(-1, 3)
+            x0d = _dev(xf.ravel(), np.float64)
+        x, info = P.solve(f, x0d)
+        xh = x.view(-1, 3).cpu().numpy()[node_of].ravel()
+        return xh, _info_dict(info, t0)
+    finally:
+        P.close()

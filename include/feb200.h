@@ -71,6 +71,8 @@ typedef struct FebOperator {
   const int64_t* extra_row;      /* [host] */
   const int64_t* extra_col;      /* [host] */
   const double* extra_val;       /* [host] */
+  int64_t nmark;                 /* nodes used although no active cell references them (an operator given only */
+  const int64_t* mark_used;      /* [host] as a matrix, fe/gmg.py:120 pcg_gmg); may be 0 / NULL              */
 } FebOperator;
 
 typedef struct FebOptions {

@@ -213,3 +213,45 @@ def test_operator_symmetry_and_rigid_nullspace():
             w *= used[:, None]
             Kw = Pr.apply(torch.from_numpy(w.ravel()).cuda()).cpu().numpy()
             assert np.linalg.norm(Kw) <= 1e-10 * np.linalg.norm(Ku) * np.linalg.norm(w) / np.linalg.norm(u)
+
+
+def test_pcg_gmg_on_assembled_matrix(golden):
+    """The CSR-accepting plugin point (fe/gmg.py:120 pcg_gmg) on the reference-assembled split-node matrix
+    with rigid-body modes, against the reference solution."""
+    from oracle import fe_oracle as O
+    z, g = _hindfoot(golden)
+    og = O.OGrid(z["xe"], z["ye"], z["ze"])
+    cells = np.flatnonzero(z["active"])
+    K, nmap, nused = O.assemble(og, z["lam"], z["mu"], cells, z["cn"], O.kl_sri(og))
+    n = K.shape[0]
+    kd = np.zeros(n)
+    for c in range(3):
+        np.add.at(kd, 3 * nmap[z["fixed_nodes"]] + c, z["fixed_area"] * 1e6)
+    K = K + O.sp.diags(kd) + _springs(z)(nmap, n)
+    f = np.zeros(n)
+    for c in range(3):
+        np.add.at(f, 3 * nmap[z["load_nodes"]] + c, z["load_area"] * z["load_t"][c])
+    Zm = O.rigid_modes(og.node_xyz[z["orig"]], nmap, n, _groups(z))
+    x, info = engine.pcg_gmg(K, f, z["orig"][nused], (g.xe, g.ye, g.ze), tol=1e-10, maxiter=800, Z=Zm)
+    assert info["flag"] == 0
+    assert rel(x, z["U"][nused].ravel()) < 1e-7
+
+
+def test_plugin_swaps_reference_style_modules(golden):
+    """plugin.install replaces module attributes the way rb/rbfe.py:21-27 does; the swapped solve_cn is the
+    device solver and uninstall restores the originals."""
+    import types
+    from comech_b200 import plugin
+    z, g = _hindfoot(golden)
+    mod = types.ModuleType("splitfe_like")
+    sentinel = lambda *a, **k: None
+    mod.solve_cn = mod.cell_stress_cn = mod.element_forces_cn = sentinel
+    plugin.install(splitfe=mod, precision="mixed")
+    assert mod._solve_cn_cpu is sentinel and mod.solve_cn is not sentinel
+    U, info, R = mod.solve_cn(g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"],
+                              (z["fixed_nodes"], z["fixed_area"]), [(z["load_nodes"], z["load_area"], z["load_t"])],
+                              _springs(z), _groups(z), tol=1e-8)
+    ok = ~np.isnan(z["U"])
+    assert info["flag"] == 0 and rel(U[ok], z["U"][ok]) < 1e-6
+    plugin.uninstall(splitfe=mod)
+    assert mod.solve_cn is sentinel and not hasattr(mod, "_solve_cn_cpu")
