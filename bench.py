@@ -33,6 +33,7 @@ WORKLOAD = dict(nx=160, ny=112, nz=96, h=0.5)
 SAMPLE_BIG = dict(nx=64, ny=45, nz=38, h=1.25)     # CPU sample (~25 s of oracle work on 1 core)
 SAMPLE_SMALL = dict(nx=40, ny=28, nz=24, h=2.0)    # CPU sample for long reference runs (~5 s)
 TOL = 1e-8
+SETUP_STAGES = ("cells", "penalties_extra", "diag_blocks", "ku_tuning", "hierarchy", "power_iterations", "dense_coarse")
 
 
 def peaks():
@@ -179,6 +180,20 @@ def device_solve(P, d, precision, x0=None):
         pr.close()
 
 
+KU_PROFILE = os.path.join(HERE, "profiles", "k_fine_struct_fp32_hindfoot_160x112x96.md")
+
+
+def ku_traffic():
+    """DRAM bytes (read + write) of one FP32 K.u launch from the committed ncu summary, or None."""
+    import re
+    try:
+        with open(KU_PROFILE) as f:
+            m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", f.read(), re.M)
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def flush_l2(buf):
     buf.add_(1.0)
 
@@ -298,14 +313,7 @@ def run_ours(args, rank, world, dist):
             roof[name] = dict(ms=ms.value, bytes=alg, gbs=alg / (ms.value * 1e-3) / 1e9)
     finally:
         pr.close()
-    traffic = None
-    tfile = os.path.join(HERE, "profiles", "ku_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            with open(tfile) as f:
-                traffic = json.load(f).get("fp32_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = ku_traffic()
     r32 = roof["fp32"]
     roofline = {"bound": "hbm", "achieved": round(r32["gbs"], 1), "peak": pk, "unit": "GB/s",
                 "frac": round(r32["gbs"] / pk, 4), "traffic": traffic, "kernel": "K.u FP32 (k_fine_struct + sparse pass)",
@@ -335,7 +343,8 @@ def run_ours(args, rank, world, dist):
                     "relres": info64.relres},
         speedup_vs_plain_fp64=round(min(fp64_ms) / 1e3 / value, 3) if world == 1 else None,
         parity_vs_fp64={"disp_rel_l2": disp_rel, "vm_rel_l2": vm_rel},
-        stage_ms={"setup": round(mixed_info.t_setup_ms, 3), "solve": round(mixed_info.t_solve_ms, 3)},
+        stage_ms={"setup": round(mixed_info.t_setup_ms, 3), "solve": round(mixed_info.t_solve_ms, 3),
+                  "setup_stages": dict(zip(SETUP_STAGES, (round(float(v), 3) for v in mixed_info.t_stage_ms)))},
         e2e={"value": round(e2e_val, 5), "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
              "d2h_bytes_per_step": int(d2h), "iters": int(infe["iters"]), "relres": infe["relres"],
              "t_host": infe["t_host"]},

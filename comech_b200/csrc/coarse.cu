@@ -420,54 +420,58 @@ __global__ void k_stencil_to_sym(const double* __restrict__ A, int64_t n, T* __r
     for (int t = 0; t < 9; ++t) S[(size_t)((o - 13) * 9 + t) * n + i] = T(A[(size_t)(o * 9 + t) * n + i]);
 }
 
-// One thread per node on a (x-blocks, y, z) grid: no integer division.  Rows that also hold entries
-// the stencil cannot (projected springs) are summed cooperatively by the whole warp.
+// Stencil product of a symmetric half-stored level with a fused epilogue.
+//
+// A CTA of 32 x 4 threads takes 32 consecutive nodes of one x-row.  The 14 stored block slots
+// q = 0..13 (self and the 13 forward offsets o = 13 + q) are split over the 4 warps, q = w, w+4, w+8,
+// w+12: every warp reads, for its 32 nodes, the forward block of slot q at the node and the backward
+// block (the transpose of the forward block stored at the neighbour n - off).  Out-of-range neighbours are
+// clamped to the node itself and their u zeroed, so the loads carry no branches and a warp keeps all of
+// its slots' loads in flight together.  Partial sums meet in shared memory; warps 0..2 then each finish
+// one component of the 32 nodes.  Entries the stencil cannot hold (per-node CSR) are summed by the warps
+// cooperatively: warp w takes the nodes of its 32 with entries whose lane is w mod 4.
 template <typename T, int EPI>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
       T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
       const int* __restrict__ skip) {
   if (skip && *skip) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  const bool valid = i < L.nx;
-  const int64_t n = i + (int64_t)L.nx * (j + (int64_t)L.ny * k);
+  __shared__ T red[4][3][32];
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int i = blockIdx.x * 32 + lane, j = blockIdx.y, k = blockIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const bool valid = i < nx;
+  const int ic = valid ? i : nx - 1;
+  const int n = ic + nx * (j + ny * k);
   const int64_t N = L.n;
   T a0 = 0, a1 = 0, a2 = 0;
-  const T* S = L.S;
-  if (valid) {
-    {
-      const T u0 = u[3 * n], u1 = u[3 * n + 1], u2 = u[3 * n + 2];
-      a0 += S[n] * u0 + S[N + n] * u1 + S[2 * N + n] * u2;
-      a1 += S[3 * N + n] * u0 + S[4 * N + n] * u1 + S[5 * N + n] * u2;
-      a2 += S[6 * N + n] * u0 + S[7 * N + n] * u1 + S[8 * N + n] * u2;
-    }
 #pragma unroll
-    for (int q = 1; q < 14; ++q) {
-      const int o = 13 + q;
-      const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
-      const int64_t off = dx + (int64_t)L.nx * (dy + (int64_t)L.ny * dz);
-      const T* B = S + (size_t)(q * 9) * N;
-      if (i + dx >= 0 && i + dx < L.nx && j + dy >= 0 && j + dy < L.ny && k + dz < L.nz) {
-        const int64_t m = n + off;
-        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-        a0 += B[n] * u0 + B[N + n] * u1 + B[2 * N + n] * u2;
-        a1 += B[3 * N + n] * u0 + B[4 * N + n] * u1 + B[5 * N + n] * u2;
-        a2 += B[6 * N + n] * u0 + B[7 * N + n] * u1 + B[8 * N + n] * u2;
-      }
-      if (i - dx >= 0 && i - dx < L.nx && j - dy >= 0 && j - dy < L.ny && k - dz >= 0) {
-        const int64_t m = n - off;
-        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-        a0 += B[m] * u0 + B[3 * N + m] * u1 + B[6 * N + m] * u2;
-        a1 += B[N + m] * u0 + B[4 * N + m] * u1 + B[7 * N + m] * u2;
-        a2 += B[2 * N + m] * u0 + B[5 * N + m] * u1 + B[8 * N + m] * u2;
-      }
-    }
+  for (int t = 0; t < 4; ++t) {
+    const int q = w + 4 * t;
+    if (q > 13) break;                                     // warp-uniform (t == 3, w >= 2)
+    const int o = 13 + q;
+    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+    const int off = dx + nx * (dy + ny * dz);
+    const T* B = L.S + (size_t)(q * 9) * N;
+    const bool vf = ic + dx >= 0 && ic + dx < nx && j + dy >= 0 && j + dy < ny && k + dz < nz;
+    const bool vb = q > 0 && ic - dx >= 0 && ic - dx < nx && j - dy >= 0 && j - dy < ny && k - dz >= 0;
+    const int mf = vf ? n + off : n, mb = vb ? n - off : n;
+    T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
+    T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
+    const T f0 = B[n], f1 = B[N + n], f2 = B[2 * N + n], f3 = B[3 * N + n], f4 = B[4 * N + n],
+            f5 = B[5 * N + n], f6 = B[6 * N + n], f7 = B[7 * N + n], f8 = B[8 * N + n];
+    const T g0 = B[mb], g1 = B[N + mb], g2 = B[2 * N + mb], g3 = B[3 * N + mb], g4 = B[4 * N + mb],
+            g5 = B[5 * N + mb], g6 = B[6 * N + mb], g7 = B[7 * N + mb], g8 = B[8 * N + mb];
+    if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
+    if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
+    a0 += f0 * uf0 + f1 * uf1 + f2 * uf2 + g0 * ub0 + g3 * ub1 + g6 * ub2;
+    a1 += f3 * uf0 + f4 * uf1 + f5 * uf2 + g1 * ub0 + g4 * ub1 + g7 * ub2;
+    a2 += f6 * uf0 + f7 * uf1 + f8 * uf2 + g2 * ub0 + g5 * ub1 + g8 * ub2;
   }
   if (L.node_ptr) {
-    const int lane = threadIdx.x & 31;
     int beg = 0, end = 0;
     if (valid) { beg = L.node_ptr[n]; end = L.node_ptr[n + 1]; }
-    unsigned todo = __ballot_sync(0xffffffffu, end > beg);
+    unsigned todo = __ballot_sync(0xffffffffu, end > beg) & (0x11111111u << w);
     while (todo) {
       const int src = __ffs(todo) - 1;
       todo &= todo - 1;
@@ -484,22 +488,36 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       if (lane == src) { a0 += s0; a1 += s1; a2 += s2; }
     }
   }
-  if (!valid) return;
+  red[w][0][lane] = a0; red[w][1][lane] = a1; red[w][2][lane] = a2;
+  // epilogue operands that do not depend on the product, read before the barrier (r is rewritten after it)
+  const int c = w;
+  T rold0 = 0, rold1 = 0, rold2 = 0, bc = 0, uc = 0, xc = 0, D0 = 0, D1 = 0, D2 = 0;
+  if (c < 3 && valid) {
+    if constexpr (EPI == EPI_RESID) bc = b[3 * n + c];
+    if constexpr (EPI == EPI_CHEB) {
+      rold0 = r[3 * n]; rold1 = r[3 * n + 1]; rold2 = r[3 * n + 2];
+      uc = u[3 * n + c]; xc = x[3 * n + c];
+      D0 = L.Dinv[(3 * c) * N + n]; D1 = L.Dinv[(3 * c + 1) * N + n]; D2 = L.Dinv[(3 * c + 2) * N + n];
+    }
+  }
+  __syncthreads();
+  if (c >= 3 || !valid) return;
   if constexpr (EPI == EPI_APPLY) {
-    y[3 * n] = a0; y[3 * n + 1] = a1; y[3 * n + 2] = a2;
+    y[3 * n + c] = red[0][c][lane] + red[1][c][lane] + red[2][c][lane] + red[3][c][lane];
   } else if constexpr (EPI == EPI_RESID) {
-    r[3 * n] = b[3 * n] - a0; r[3 * n + 1] = b[3 * n + 1] - a1; r[3 * n + 2] = b[3 * n + 2] - a2;
+    r[3 * n + c] = bc - (red[0][c][lane] + red[1][c][lane] + red[2][c][lane] + red[3][c][lane]);
   } else {
+    const T A0 = red[0][0][lane] + red[1][0][lane] + red[2][0][lane] + red[3][0][lane];
+    const T A1 = red[0][1][lane] + red[1][1][lane] + red[2][1][lane] + red[3][1][lane];
+    const T A2 = red[0][2][lane] + red[1][2][lane] + red[2][2][lane] + red[3][2][lane];
+    const T r0 = rold0 - A0, r1 = rold1 - A1, r2 = rold2 - A2;
+    const T rc = c == 0 ? r0 : (c == 1 ? r1 : r2);
     const T c1 = T(lp->a1[kstep]), c2 = T(lp->a2[kstep]);
-    const T r0 = r[3 * n] - a0, r1 = r[3 * n + 1] - a1, r2 = r[3 * n + 2] - a2;
-    r[3 * n] = r0; r[3 * n + 1] = r1; r[3 * n + 2] = r2;
-    const T* D = L.Dinv;
-    const T z0 = D[n] * r0 + D[N + n] * r1 + D[2 * N + n] * r2;
-    const T z1 = D[3 * N + n] * r0 + D[4 * N + n] * r1 + D[5 * N + n] * r2;
-    const T z2 = D[6 * N + n] * r0 + D[7 * N + n] * r1 + D[8 * N + n] * r2;
-    const T e0 = c1 * u[3 * n] + c2 * z0, e1 = c1 * u[3 * n + 1] + c2 * z1, e2 = c1 * u[3 * n + 2] + c2 * z2;
-    d_out[3 * n] = e0; d_out[3 * n + 1] = e1; d_out[3 * n + 2] = e2;
-    x[3 * n] += e0; x[3 * n + 1] += e1; x[3 * n + 2] += e2;
+    const T z = D0 * r0 + D1 * r1 + D2 * r2;
+    const T e = c1 * uc + c2 * z;
+    r[3 * n + c] = rc;
+    d_out[3 * n + c] = e;
+    x[3 * n + c] = xc + e;
   }
 }
 
@@ -508,13 +526,13 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
 template <typename T>
 void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
                 const LevelParams* lp, int k, const int* skip, cudaStream_t s) {
-  const dim3 g(div_up(L.nx, 128), L.ny, L.nz);
+  const dim3 g(div_up(L.nx, 32), L.ny, L.nz), blk(32, 4);
   if (epi == EPI_APPLY) {
-    k_sym<T, EPI_APPLY><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+    k_sym<T, EPI_APPLY><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
   } else if (epi == EPI_RESID) {
-    k_sym<T, EPI_RESID><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+    k_sym<T, EPI_RESID><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
   } else {
-    k_sym<T, EPI_CHEB><<<g, 128, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+    k_sym<T, EPI_CHEB><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
   }
 }
 

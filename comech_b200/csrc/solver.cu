@@ -180,6 +180,145 @@ Entries project(const Entries& E, const AxisHost (&ax)[3], const std::vector<int
   return out;
 }
 
+// Rank-1 terms lam_t v_t v_t^T of the extra matrix.  Non-local spring couplings (a ligament between two
+// bones, a penalty over a face) are low-rank by construction, rb/replica3.py:68-86 and
+// fe/solver.py:224-232 add k w w^T; carried as terms, a level's couplings are projected to the next level
+// as vectors (P^T v, at most 8x the entries) instead of as outer products (64x the entries).
+struct Terms {
+  std::vector<double> lam;
+  std::vector<int64_t> ptr{0};   // entries of term t: ptr[t] .. ptr[t+1]
+  std::vector<int64_t> dof;      // level dofs, 3 node + comp
+  std::vector<double> val;
+  size_t size() const { return lam.size(); }
+};
+
+// Symmetric m x m matrix (row-major, modified) -> terms by LDL^T with diagonal pivoting.  Succeeds when
+// the remainder after at most max_rank pivots vanishes (|entries| <= 1e-12 of the largest), which holds for
+// sums of a few positive semidefinite springs; returns false otherwise (the caller keeps the entries).
+// dofs maps the m local indices to level dofs.
+bool factor_terms(std::vector<double>& A, int m, const std::vector<int64_t>& dofs, int max_rank, Terms& out) {
+  double scale = 0.0;
+  for (double a : A) scale = std::max(scale, std::fabs(a));
+  if (scale == 0.0) return true;
+  const double tol = 1e-12 * scale;
+  std::vector<char> done(m, 0);
+  Terms T;
+  for (int step = 0; step < m; ++step) {
+    int p = -1;
+    double best = tol;
+    for (int i = 0; i < m; ++i)
+      if (!done[i] && std::fabs(A[(size_t)i * m + i]) > best) { best = std::fabs(A[(size_t)i * m + i]); p = i; }
+    if (p < 0) break;
+    if ((int)T.size() == max_rank) return false;
+    const double d = A[(size_t)p * m + p];
+    std::vector<double> l(m);
+    for (int i = 0; i < m; ++i) l[i] = A[(size_t)i * m + p] / d;
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) A[(size_t)i * m + j] -= d * l[i] * l[j];
+    done[p] = 1;
+    T.lam.push_back(d);
+    for (int i = 0; i < m; ++i)
+      if (l[i] != 0.0) { T.dof.push_back(dofs[i]); T.val.push_back(l[i]); }
+    T.ptr.push_back((int64_t)T.dof.size());
+  }
+  for (double a : A)
+    if (std::fabs(a) > tol) return false;
+  for (size_t t = 0; t < T.size(); ++t) {
+    out.lam.push_back(T.lam[t]);
+    for (int64_t e = T.ptr[t]; e < T.ptr[t + 1]; ++e) { out.dof.push_back(T.dof[e]); out.val.push_back(T.val[e]); }
+    out.ptr.push_back((int64_t)out.dof.size());
+  }
+  return true;
+}
+
+// P^T v of every term (same node positions and supports as project())
+Terms project_terms(const Terms& T, const AxisHost (&ax)[3], const std::vector<int64_t>& pos_of_node_copy,
+                    int64_t fnnode, int fnx, int fny) {
+  Terms out;
+  const int64_t cnx = ax[0].nc, cny = ax[1].nc;
+  auto position = [&](int64_t node) { return node < fnnode ? node : pos_of_node_copy[node - fnnode]; };
+  std::vector<std::pair<int64_t, double>> acc;
+  for (size_t t = 0; t < T.size(); ++t) {
+    acc.clear();
+    for (int64_t e = T.ptr[t]; e < T.ptr[t + 1]; ++e) {
+      const int64_t p = position(T.dof[e] / 3);
+      const int comp = int(T.dof[e] % 3);
+      const int ip[3] = {int(p % fnx), int((p / fnx) % fny), int(p / ((int64_t)fnx * fny))};
+      int J[3][2], n[3];
+      double w[3][2];
+      for (int d = 0; d < 3; ++d) n[d] = supp(ax[d], ip[d], J[d], w[d]);
+      for (int a = 0; a < n[0]; ++a) for (int b = 0; b < n[1]; ++b) for (int c = 0; c < n[2]; ++c)
+        acc.emplace_back(3 * (J[0][a] + cnx * (J[1][b] + cny * J[2][c])) + comp, w[0][a] * w[1][b] * w[2][c] * T.val[e]);
+    }
+    std::sort(acc.begin(), acc.end(), [](const std::pair<int64_t, double>& x, const std::pair<int64_t, double>& y) {
+      return x.first < y.first;
+    });
+    for (size_t i = 0; i < acc.size();) {
+      size_t j = i;
+      double v = 0.0;
+      for (; j < acc.size() && acc[j].first == acc[i].first; ++j) v += acc[j].second;
+      if (v != 0.0) { out.dof.push_back(acc[i].first); out.val.push_back(v); }
+      i = j;
+    }
+    out.lam.push_back(T.lam[t]);
+    out.ptr.push_back((int64_t)out.dof.size());
+  }
+  return out;
+}
+
+// entries lam v v^T of every term appended to E (duplicates are summed by the consumers)
+void expand_terms(const Terms& T, Entries& E) {
+  for (size_t t = 0; t < T.size(); ++t)
+    for (int64_t a = T.ptr[t]; a < T.ptr[t + 1]; ++a)
+      for (int64_t b = T.ptr[t]; b < T.ptr[t + 1]; ++b) {
+        E.r.push_back(T.dof[a]); E.c.push_back(T.dof[b]); E.v.push_back(T.lam[t] * T.val[a] * T.val[b]);
+      }
+}
+
+// Connected components (over dofs) of the non-local entries; each component of at most kTermDofs dofs
+// whose entries (every entry with both dofs in it, local ones included) factor into at most kTermRank
+// rank-1 terms is moved to `terms`.  Returns the flags of the entries that the terms now represent.
+constexpr int kTermDofs = 1024;
+constexpr int kTermRank = 48;
+std::vector<char> factor_nonlocal(const Entries& ex, const std::vector<char>& is_local, Terms& terms) {
+  std::vector<char> taken(ex.size(), 0);
+  std::unordered_map<int64_t, int64_t> parent;
+  auto find = [&](int64_t x) {
+    while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+    return x;
+  };
+  for (size_t e = 0; e < ex.size(); ++e) {
+    if (is_local[e]) continue;
+    for (int64_t d : {ex.r[e], ex.c[e]})
+      if (!parent.count(d)) parent[d] = d;
+    int64_t a = find(ex.r[e]), b = find(ex.c[e]);
+    if (a != b) parent[std::max(a, b)] = std::min(a, b);
+  }
+  if (parent.empty()) return taken;
+  std::map<int64_t, std::vector<int64_t>> members;   // root -> dofs, ordered for determinism
+  for (auto& kv : parent) members[find(kv.first)].push_back(kv.first);
+  std::map<int64_t, std::vector<size_t>> ents;
+  for (size_t e = 0; e < ex.size(); ++e) {
+    auto ia = parent.find(ex.r[e]), ib = parent.find(ex.c[e]);
+    if (ia == parent.end() || ib == parent.end()) continue;
+    int64_t ra = find(ex.r[e]), rb = find(ex.c[e]);
+    if (ra == rb) ents[ra].push_back(e);
+  }
+  for (auto& kv : members) {
+    std::vector<int64_t>& dofs = kv.second;
+    std::sort(dofs.begin(), dofs.end());
+    const int m = (int)dofs.size();
+    if (m > kTermDofs) continue;
+    std::vector<double> A((size_t)m * m, 0.0);
+    auto li = [&](int64_t d) { return int(std::lower_bound(dofs.begin(), dofs.end(), d) - dofs.begin()); };
+    const std::vector<size_t>& es = ents[kv.first];
+    for (size_t e : es) A[(size_t)li(ex.r[e]) * m + li(ex.c[e])] += ex.v[e];
+    if (factor_terms(A, m, dofs, kTermRank, terms))
+      for (size_t e : es) taken[e] = 1;
+  }
+  return taken;
+}
+
 // symmetric pseudo-inverse by cyclic Jacobi (numpy.linalg.pinv semantics: cutoff 1e-15 * max |eig|)
 std::vector<double> sym_pinv(const std::vector<double>& A0, int n) {
   std::vector<double> A(A0), V(n * n, 0.0);
@@ -338,7 +477,9 @@ struct Level {
   int* ent_col = nullptr;
   double* ent_v64 = nullptr;
   float* ent_v32 = nullptr;
-  Entries nonlocal;                       // host copy of `sparse` (projected to the next level)
+  Entries nonlocal;                       // non-local entries kept as entries (projected entry by entry)
+  Terms terms;                            // non-local couplings as rank-1 terms (projected as vectors)
+  Entries sparse;                         // this level's entries outside the stencil: nonlocal + expanded terms
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
   AxisHost ax[3];                         // transfer to the next level
@@ -356,7 +497,7 @@ int upload_node_csr(Pool& pool, const Entries& E, int64_t nnode, Level& V) {
   for (size_t e = 0; e < E.size(); ++e) ptr[E.r[e] / 3 + 1]++;
   for (int64_t i = 0; i < nnode; ++i) ptr[i + 1] += ptr[i];
   std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-  for (size_t e = 0; e < E.size(); ++e) {      // E is sorted by row dof, so each node's entries stay in order
+  for (size_t e = 0; e < E.size(); ++e) {      // a node keeps its entries in input order; duplicates add up
     int64_t node = E.r[e] / 3;
     int at = fill[node]++;
     rr[at] = (int8_t)(E.r[e] % 3); col[at] = (int)E.c[e]; v[at] = E.v[e]; vf[at] = (float)E.v[e];
@@ -1000,11 +1141,16 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   Entries loc;
   const int gx = H.nx + 1, gy = H.ny + 1;
   auto pos = [&](int64_t node) { return node < H.nnode ? node : H.orig_copy_h[node - H.nnode]; };
+  std::vector<char> is_local(ex.size());
   for (size_t e2 = 0; e2 < ex.size(); ++e2) {
     int64_t a = pos(ex.r[e2] / 3), b = pos(ex.c[e2] / 3);
     int da = int(a % gx) - int(b % gx), db = int((a / gx) % gy) - int((b / gx) % gy), dc = int(a / ((int64_t)gx * gy)) - int(b / ((int64_t)gx * gy));
-    bool local = std::abs(da) <= 1 && std::abs(db) <= 1 && std::abs(dc) <= 1;
-    Entries& dst = local ? loc : V.nonlocal;
+    is_local[e2] = std::abs(da) <= 1 && std::abs(db) <= 1 && std::abs(dc) <= 1;
+  }
+  std::vector<char> taken = factor_nonlocal(ex, is_local, V.terms);
+  for (size_t e2 = 0; e2 < ex.size(); ++e2) {
+    if (taken[e2]) continue;
+    Entries& dst = is_local[e2] ? loc : V.nonlocal;
     dst.r.push_back(ex.r[e2]); dst.c.push_back(ex.c[e2]); dst.v.push_back(ex.v[e2]);
   }
   H.nlocal = (int)loc.size();
@@ -1076,13 +1222,13 @@ int build_dense(FebHandle* h) {
     }
   } else {
     launch_dense_from_stencil(V.A64, V.nx, V.ny, V.nz, H.cmap, H.Minv, H.nd, H.s);
-    if (V.nonlocal.size()) {
-      std::vector<int> rr(V.nonlocal.r.begin(), V.nonlocal.r.end()), cc(V.nonlocal.c.begin(), V.nonlocal.c.end());
+    if (V.sparse.size()) {
+      std::vector<int> rr(V.sparse.r.begin(), V.sparse.r.end()), cc(V.sparse.c.begin(), V.sparse.c.end());
       int *dr, *dc;
       double* dv;
       FEB_TRY(H.pool.upload(&dr, rr.data(), rr.size()));
       FEB_TRY(H.pool.upload(&dc, cc.data(), cc.size()));
-      FEB_TRY(H.pool.upload(&dv, V.nonlocal.v.data(), V.nonlocal.v.size()));
+      FEB_TRY(H.pool.upload(&dv, V.sparse.v.data(), V.sparse.v.size()));
       launch_dense_add_entries((int)rr.size(), dr, dc, dv, H.cmap, H.Minv, H.nd, H.s);
     }
   }
@@ -1145,7 +1291,10 @@ int build_hierarchy(FebHandle* h) {
     }
     FEB_CUDA(cudaGetLastError());
     C.nonlocal = project(F.nonlocal, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
-    FEB_TRY(upload_node_csr(H.pool, C.nonlocal, C.nnode, C));
+    C.terms = project_terms(F.terms, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
+    C.sparse = C.nonlocal;
+    expand_terms(C.terms, C.sparse);
+    FEB_TRY(upload_node_csr(H.pool, C.sparse, C.nnode, C));
     FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)C.ntotal));
     launch_stencil_to_sym<double>(C.A64, C.ntotal, C.S64, H.s);
     if (f32) {
@@ -1160,9 +1309,9 @@ int build_hierarchy(FebHandle* h) {
       launch_stencil_diag(C.A64, C.ntotal, D, H.s);
       std::vector<int> dr, dc;
       std::vector<double> dv;
-      for (size_t e = 0; e < C.nonlocal.size(); ++e)
-        if (C.nonlocal.r[e] / 3 == C.nonlocal.c[e] / 3) {
-          dr.push_back((int)C.nonlocal.r[e]); dc.push_back((int)C.nonlocal.c[e]); dv.push_back(C.nonlocal.v[e]);
+      for (size_t e = 0; e < C.sparse.size(); ++e)
+        if (C.sparse.r[e] / 3 == C.sparse.c[e] / 3) {
+          dr.push_back((int)C.sparse.r[e]); dc.push_back((int)C.sparse.c[e]); dv.push_back(C.sparse.v[e]);
         }
       if (!dr.empty()) {
         int *ddr, *ddc;
