@@ -324,49 +324,50 @@ __global__ void k_galerkin_local(TransferDev P, int fnx, int fny, int64_t fnnode
   }
 }
 
-// A_c[J][o] = sum_{i in fan(J)} sum_{i' in fan(J+o), |i'-i| <= 1} P[i,J] A_f[i][i'-i] P[i',J+o]
-__global__ void k_galerkin_stencil(TransferDev P, const double* __restrict__ Af, int fnx, int fny, int fnz,
-                                   double* __restrict__ Ac, int cnx, int cny, int cnz) {
-  const int o = threadIdx.x;
-  const int64_t nc = (int64_t)cnx * cny * cnz, nf = (int64_t)fnx * fny * fnz;
-  const int64_t J = blockIdx.x * (int64_t)blockDim.y + threadIdx.y;
-  if (J >= nc) return;
-  const int jc[3] = {int(J % cnx), int((J / cnx) % cny), int(J / ((int64_t)cnx * cny))};
+// One axis of the Galerkin product P^T A P of a 27-point 3x3-block stencil.  P = Px (x) Py (x) Pz (x) I3 is
+// separable, so the product is three passes, each coarsening one axis d: the output grid is the input grid
+// with axis d coarsened and the stencil stays 27-point (coarse nodes J, J' couple only through fine nodes
+// at most one apart).  Thread per output node (x fastest, coalesced), block row per offset.
+__global__ void __launch_bounds__(128)
+k_galerkin_axis(AxisDev ax, int d, const double* __restrict__ Ain, int inx, int iny, int inz,
+                double* __restrict__ Aout, int onx, int ony, int onz) {
+  const int o = blockIdx.y;
+  const int64_t no = (int64_t)onx * ony * onz, ni = (int64_t)inx * iny * inz;
+  const int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (J >= no) return;
+  const int jc[3] = {int(J % onx), int((J / onx) % ony), int(J / ((int64_t)onx * ony))};
   const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
-  const int nn[3] = {cnx, cny, cnz};
-  // per axis: pairs (i, i'-i, weight)
-  int pi[3][9], pd[3][9], np[3];
-  double pw[3][9];
+  const int on[3] = {onx, ony, onz};
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   bool ok = true;
-  for (int d = 0; d < 3; ++d) {
-    np[d] = 0;
-    int K = jc[d] + od[d];
-    if (K < 0 || K >= nn[d]) { ok = false; break; }
-    int I[3]; double w[3];
-    int nI = axis_fan(P.ax[d], jc[d], I, w);
-    for (int t = 0; t < nI; ++t)
+  for (int e = 0; e < 3; ++e) {
+    const int K = jc[e] + od[e];
+    if (K < 0 || K >= on[e]) ok = false;
+  }
+  if (ok) {
+    int I[3];
+    double w[3];
+    const int nI = axis_fan(ax, jc[d], I, w);
+    const int K = jc[d] + od[d];
+    for (int a = 0; a < nI; ++a)
       for (int dd = -1; dd <= 1; ++dd) {
-        int i2 = I[t] + dd;
-        if (i2 < 0 || i2 >= P.ax[d].nf) continue;
-        double w2 = axis_w(P.ax[d], i2, K);
+        const int i2 = I[a] + dd;
+        if (i2 < 0 || i2 >= ax.nf) continue;
+        const double w2 = axis_w(ax, i2, K);
         if (w2 == 0.0) continue;
-        pi[d][np[d]] = I[t]; pd[d][np[d]] = dd; pw[d][np[d]] = w[t] * w2; ++np[d];
+        int p[3] = {jc[0], jc[1], jc[2]}, q[3] = {od[0], od[1], od[2]};
+        p[d] = I[a];
+        q[d] = dd;
+        const int64_t f = p[0] + (int64_t)inx * (p[1] + (int64_t)iny * p[2]);
+        const int oi = (q[0] + 1) + 3 * (q[1] + 1) + 9 * (q[2] + 1);
+        const double ww = w[a] * w2;
+        const double* src = Ain + (size_t)(oi * 9) * ni + f;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) acc[t] += ww * src[(size_t)t * ni];
       }
   }
-  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (ok) {
-    for (int c = 0; c < np[2]; ++c)
-      for (int b = 0; b < np[1]; ++b)
-        for (int a = 0; a < np[0]; ++a) {
-          int64_t f = pi[0][a] + (int64_t)fnx * (pi[1][b] + (int64_t)fny * pi[2][c]);
-          int of = (pd[0][a] + 1) + 3 * (pd[1][b] + 1) + 9 * (pd[2][c] + 1);
-          double w = pw[0][a] * pw[1][b] * pw[2][c];
-          const double* src = Af + (size_t)(of * 9) * nf + f;
 #pragma unroll
-          for (int t = 0; t < 9; ++t) acc[t] += w * src[(size_t)t * nf];
-        }
-  }
-  for (int t = 0; t < 9; ++t) Ac[(size_t)(o * 9 + t) * nc + J] = acc[t];
+  for (int t = 0; t < 9; ++t) Aout[(size_t)(o * 9 + t) * no + J] = acc[t];
 }
 
 __global__ void k_stencil_diag(const double* __restrict__ A, int64_t n, double* __restrict__ D) {
@@ -488,6 +489,25 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       if (lane == src) { a0 += s0; a1 += s1; a2 += s2; }
     }
   }
+  if (L.tn_ptr && valid) {      // rank-1 terms: lane-parallel dot and axpy, the node's pairs split over the warps
+    const int pe = L.tn_ptr[n + 1];
+    for (int p = L.tn_ptr[n] + w; p < pe; p += 4) {
+      const int t = L.tn_term[p], eb = L.t_ptr[t], ee = L.t_ptr[t + 1];
+      T d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+      int e = eb;
+      for (; e + 3 < ee; e += 4) {
+        d0 += L.t_val[e] * u[L.t_dof[e]];
+        d1 += L.t_val[e + 1] * u[L.t_dof[e + 1]];
+        d2 += L.t_val[e + 2] * u[L.t_dof[e + 2]];
+        d3 += L.t_val[e + 3] * u[L.t_dof[e + 3]];
+      }
+      for (; e < ee; ++e) d0 += L.t_val[e] * u[L.t_dof[e]];
+      const T dot = L.t_lam[t] * ((d0 + d1) + (d2 + d3));
+      a0 += dot * L.tn_coef[3 * p];
+      a1 += dot * L.tn_coef[3 * p + 1];
+      a2 += dot * L.tn_coef[3 * p + 2];
+    }
+  }
   red[w][0][lane] = a0; red[w][1][lane] = a1; red[w][2][lane] = a2;
   // epilogue operands that do not depend on the product, read before the barrier (r is rewritten after it)
   const int c = w;
@@ -545,6 +565,13 @@ template void launch_sym<float>(const SymView<float>&, int, const float*, float*
                                 float*, const LevelParams*, int, const int*, cudaStream_t);
 template void launch_sym<double>(const SymView<double>&, int, const double*, double*, const double*, double*,
                                  double*, double*, const LevelParams*, int, const int*, cudaStream_t);
+void launch_galerkin_axis(const AxisDev& ax, int d, const double* Ain, int inx, int iny, int inz, double* Aout,
+                          int onx, int ony, int onz, cudaStream_t s) {
+  const int64_t no = (int64_t)onx * ony * onz;
+  k_galerkin_axis<<<dim3(div_up(no, 128), 27), 128, 0, s>>>(ax, d, Ain, inx, iny, inz, Aout, onx, ony, onz);
+  note_launch();
+}
+
 template void launch_stencil_to_sym<float>(const double*, int64_t, float*, cudaStream_t);
 template void launch_stencil_to_sym<double>(const double*, int64_t, double*, cudaStream_t);
 
@@ -616,13 +643,6 @@ void launch_galerkin_local(const TransferDev& P, int fnx, int fny, int64_t fnnod
   k_galerkin_local<<<div_up(nent, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, orig_copy, nent, rdof, cdof, val,
                                                                 A1, cnx, cny, cn); note_launch();
   (void)cnz;
-}
-
-void launch_galerkin_stencil(const TransferDev& P, const double* Af, int fnx, int fny, int fnz, double* Ac, int cnx,
-                             int cny, int cnz, cudaStream_t s) {
-  int64_t n = (int64_t)cnx * cny * cnz;
-  dim3 blk(27, 8);
-  k_galerkin_stencil<<<div_up(n, 8), blk, 0, s>>>(P, Af, fnx, fny, fnz, Ac, cnx, cny, cnz); note_launch();
 }
 
 void launch_stencil_diag(const double* A, int64_t n, double* D, cudaStream_t s) {

@@ -47,6 +47,16 @@ struct SymView {
   const int* ent_col;
   const T* ent_v;
   const T* Dinv;           // block-Jacobi inverse, SoA [9][n]
+  // rank-1 terms lam_t v_t v_t^T (non-local springs projected to this level): entries t_ptr[t] .. t_ptr[t+1]
+  // of v_t as (dof, value); per node, the (term, 3 components of v_t at the node) pairs of the terms that
+  // touch it: tn_ptr[n] .. tn_ptr[n+1]
+  const int* tn_ptr;       // nullptr when the level has no terms
+  const int* tn_term;
+  const T* tn_coef;
+  const int* t_ptr;
+  const int* t_dof;
+  const T* t_val;
+  const T* t_lam;
 };
 
 // Fused level kernels: EPI_APPLY y = A u; EPI_RESID r = b - A u; EPI_CHEB Chebyshev step with ping-pong
@@ -75,6 +85,11 @@ void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
                         cudaStream_t s);
 
+// One axis pass of the separable Galerkin product P^T A P of a [243][n] stencil: axis d of the input grid
+// (inx, iny, inz) coarsened by ax to the output grid (onx, ony, onz).
+void launch_galerkin_axis(const AxisDev& ax, int d, const double* Ain, int inx, int iny, int inz, double* Aout,
+                          int onx, int ony, int onz, cudaStream_t s);
+
 // kept[J] = some used fine node interpolates from coarse node J (fe/gmg.py:95)
 void launch_kept_mask(const TransferDev& P, const uint8_t* used_f, uint8_t* kept_c, cudaStream_t s);
 
@@ -90,10 +105,6 @@ void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnn
 void launch_galerkin_local(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int nent,
                            const int* rdof, const int* cdof, const double* val, double* A1, int cnx, int cny, int cnz,
                            int64_t cn, cudaStream_t s);
-
-// Stencil Galerkin: A_c = P^T A_f P for structured levels.
-void launch_galerkin_stencil(const TransferDev& P, const double* Af, int fnx, int fny, int fnz, double* Ac, int cnx,
-                             int cny, int cnz, cudaStream_t s);
 
 // Diagonal 3x3 blocks of a stencil into D[n][9].
 void launch_stencil_diag(const double* A, int64_t n, double* D, cudaStream_t s);

@@ -199,6 +199,25 @@ void launch_dense_from_stencil(const double* A, int nx, int ny, int nz, const in
   k_dense_from_stencil<<<div_up(n, 8), blk, 0, s>>>(A, nx, ny, nz, cmap, M, nd); note_launch();
 }
 
+// M += lam_t v_t v_t^T of every term (one block per term; entries on dropped nodes are skipped)
+__global__ void k_dense_add_terms(const int* __restrict__ t_ptr, const int* __restrict__ t_dof,
+                                  const double* __restrict__ t_val, const double* __restrict__ t_lam,
+                                  const int* __restrict__ cmap, double* __restrict__ M, int nd) {
+  const int t = blockIdx.x, eb = t_ptr[t], ne = t_ptr[t + 1] - eb;
+  const double lam = t_lam[t];
+  for (int q = threadIdx.x; q < ne * ne; q += blockDim.x) {
+    const int a = eb + q / ne, b = eb + q % ne;
+    const int ca = cmap[t_dof[a] / 3], cb = cmap[t_dof[b] / 3];
+    if (ca < 0 || cb < 0) continue;
+    atomicAdd(M + (size_t)(3 * ca + t_dof[a] % 3) * nd + 3 * cb + t_dof[b] % 3, lam * t_val[a] * t_val[b]);
+  }
+}
+
+void launch_dense_add_terms(int nterms, const int* t_ptr, const int* t_dof, const double* t_val, const double* t_lam,
+                            const int* cmap, double* M, int nd, cudaStream_t s) {
+  if (nterms > 0) k_dense_add_terms<<<nterms, kThreads, 0, s>>>(t_ptr, t_dof, t_val, t_lam, cmap, M, nd); note_launch();
+}
+
 void launch_dense_add_entries(int nent, const int* rdof, const int* cdof, const double* val, const int* cmap,
                               double* M, int nd, cudaStream_t s) {
   if (nent > 0) k_dense_add_entries<<<div_up(nent, kThreads), kThreads, 0, s>>>(nent, rdof, cdof, val, cmap, M, nd); note_launch();

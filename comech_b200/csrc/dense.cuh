@@ -7,6 +7,8 @@ namespace feb {
 
 void launch_dense_from_stencil(const double* A, int nx, int ny, int nz, const int* cmap, double* M, int nd,
                                cudaStream_t s);
+void launch_dense_add_terms(int nterms, const int* t_ptr, const int* t_dof, const double* t_val, const double* t_lam,
+                            const int* cmap, double* M, int nd, cudaStream_t s);
 void launch_dense_add_entries(int nent, const int* rdof, const int* cdof, const double* val, const int* cmap,
                               double* M, int nd, cudaStream_t s);
 // In-place M <- M^-1 (symmetrised first); scratch: dense_scratch_doubles(nd); *status = FEB_ERR_COARSE on a

@@ -445,7 +445,15 @@ void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, 
   const int zc = std::max(1, cfg.zchunk);
   dim3 grid(div_up(F.nxn, 30), div_up(F.nyn, ty - 2), div_up(F.nzn, zc));
   const size_t smem = sizeof(T) * (size_t)ty * 32 * 24;
-  if (ty == 8) {
+  bool tc_done = false;
+  if constexpr (std::is_same<T, float>::value && MODE != MAT_ORTHO) {
+    if (cfg.tc) {
+      launch_fine_struct_tc<MODE>(F, u, y, skip, zc, s);
+      tc_done = true;
+    }
+  }
+  if (tc_done) {
+  } else if (ty == 8) {
     launch_struct<T, MODE, 8>(grid, smem, F, u, y, skip, zc, s);
   } else if (ty == 12) {
     launch_struct<T, MODE, 12>(grid, smem, F, u, y, skip, zc, s);

@@ -24,16 +24,32 @@ struct FineView {
   int npen; const int* pen_node; const T* pen_k;
   // sparse extra matrix, CSR over the dofs that have entries
   int nrow; const int* row_dof; const int* row_ptr; const int* col; const T* val;
+  // tensor-core path (FP32, equal cubic cells): B operand table, h/72 and the lambda factor (h/16 one-point,
+  // h/72 integrated), word set to 1 when a bounded wait gave up
+  const void* tc_b = nullptr;
+  float tc_hmu = 0.f, tc_hlam = 0.f;
+  int* tc_status = nullptr;
 };
 
 // launch shape of the structured K.u kernel: warps per CTA (8, 12 or 16) and node planes per CTA
 struct KuConfig {
   int ty = 16;
   int zchunk = 16;
+  int tc = 0;              // 1: tensor-core kernel (zchunk planes per CTA; ty unused)
 };
 
 template <typename T, int MODE>
 void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, KuConfig cfg, cudaStream_t s);
+
+// Tensor-core K.u of the regular cells (MODE ISO_SRI or ISO_FULL, equal cubic cells, FP32): operand columns
+// N of the B table (2 faces x 2 node rows x N rows x 8 BF16), kernel attributes (once per process), launch.
+template <int MODE> int tc_columns();
+template <int MODE> cudaError_t prepare_fine_tc();
+template <int MODE>
+void launch_fine_struct_tc(const FineView<float>& F, const float* u, float* y, const int* skip, int zchunk,
+                           cudaStream_t s);
+// K_lambda and K_mu of the unit cube, out[2][24][24] (dof 3 l + c), with the model's integration rule
+template <int MODE> void launch_unit_element(double* out, cudaStream_t s);
 
 // 3x3 diagonal blocks of the level-0 operator at every node (full layout), row-major [n][9].
 template <int MODE>

@@ -8,14 +8,15 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
-#include <unordered_map>
 #include <vector>
 
 #include "coarse.cuh"
@@ -28,6 +29,31 @@ namespace feb {
 
 static thread_local char g_err[512] = "";
 static std::atomic<long long> g_launches{0};
+
+// Set-up profiling (FEB_PROFILE_SETUP=1): wall time of each set-up segment, device work included (the
+// stream is synchronised at every mark), printed to stderr when feb_create returns.
+struct SetupProfile {
+  bool on = false;
+  std::vector<std::pair<std::string, double>> marks;
+  std::chrono::steady_clock::time_point t0;
+  void start(bool enable) {
+    on = enable;
+    marks.clear();
+    t0 = std::chrono::steady_clock::now();
+  }
+  void mark(const char* what, cudaStream_t s) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    auto t = std::chrono::steady_clock::now();
+    marks.emplace_back(what, std::chrono::duration<double, std::milli>(t - t0).count());
+    t0 = t;
+  }
+  void print() const {
+    if (!on) return;
+    for (const auto& m : marks) std::fprintf(stderr, "feb setup %-28s %8.3f ms\n", m.first.c_str(), m.second);
+  }
+};
+thread_local SetupProfile g_prof;
 
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
@@ -131,14 +157,40 @@ struct Entries {
   size_t size() const { return v.size(); }
 };
 
+// Sorts entries by (row, col) and sums duplicates: LSD radix sort of the packed key row << 32 | col
+// (dofs < 2^31, feb_create checks 3 nnode_total), 16-bit digits, digits that never vary skipped.
 void coo_merge(Entries& E) {
-  std::vector<size_t> idx(E.size());
-  for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
-  std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return E.r[a] != E.r[b] ? E.r[a] < E.r[b] : E.c[a] < E.c[b]; });
+  const size_t n = E.size();
+  if (n == 0) return;
+  std::vector<uint64_t> key(n), k2(n);
+  std::vector<uint32_t> idx(n), i2(n);
+  uint64_t any_or = 0, any_and = ~0ull;
+  for (size_t i = 0; i < n; ++i) {
+    key[i] = ((uint64_t)E.r[i] << 32) | (uint32_t)E.c[i];
+    idx[i] = (uint32_t)i;
+    any_or |= key[i];
+    any_and &= key[i];
+  }
+  std::vector<uint32_t> cnt(1 << 16);
+  for (int shift = 0; shift < 64; shift += 16) {
+    if ((((any_or ^ any_and) >> shift) & 0xFFFF) == 0) continue;     // digit constant over all keys
+    std::fill(cnt.begin(), cnt.end(), 0u);
+    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> shift) & 0xFFFF]++;
+    uint32_t sum = 0;
+    for (auto& c : cnt) { const uint32_t t = c; c = sum; sum += t; }
+    for (size_t i = 0; i < n; ++i) {
+      const uint32_t at = cnt[(key[i] >> shift) & 0xFFFF]++;
+      k2[at] = key[i];
+      i2[at] = idx[i];
+    }
+    key.swap(k2);
+    idx.swap(i2);
+  }
   Entries M;
-  for (size_t t = 0; t < idx.size(); ++t) {
-    size_t i = idx[t];
-    if (!M.v.empty() && M.r.back() == E.r[i] && M.c.back() == E.c[i]) M.v.back() += E.v[i];
+  M.r.reserve(n); M.c.reserve(n); M.v.reserve(n);
+  for (size_t t = 0; t < n; ++t) {
+    const size_t i = idx[t];
+    if (t > 0 && key[t] == key[t - 1]) M.v.back() += E.v[i];
     else { M.r.push_back(E.r[i]); M.c.push_back(E.c[i]); M.v.push_back(E.v[i]); }
   }
   E = std::move(M);
@@ -266,15 +318,6 @@ Terms project_terms(const Terms& T, const AxisHost (&ax)[3], const std::vector<i
   return out;
 }
 
-// entries lam v v^T of every term appended to E (duplicates are summed by the consumers)
-void expand_terms(const Terms& T, Entries& E) {
-  for (size_t t = 0; t < T.size(); ++t)
-    for (int64_t a = T.ptr[t]; a < T.ptr[t + 1]; ++a)
-      for (int64_t b = T.ptr[t]; b < T.ptr[t + 1]; ++b) {
-        E.r.push_back(T.dof[a]); E.c.push_back(T.dof[b]); E.v.push_back(T.lam[t] * T.val[a] * T.val[b]);
-      }
-}
-
 // Connected components (over dofs) of the non-local entries; each component of at most kTermDofs dofs
 // whose entries (every entry with both dofs in it, local ones included) factor into at most kTermRank
 // rank-1 terms is moved to `terms`.  Returns the flags of the entries that the terms now represent.
@@ -282,39 +325,52 @@ constexpr int kTermDofs = 1024;
 constexpr int kTermRank = 48;
 std::vector<char> factor_nonlocal(const Entries& ex, const std::vector<char>& is_local, Terms& terms) {
   std::vector<char> taken(ex.size(), 0);
-  std::unordered_map<int64_t, int64_t> parent;
-  auto find = [&](int64_t x) {
+  std::vector<int64_t> nd;                        // dofs of the non-local entries, sorted
+  for (size_t e = 0; e < ex.size(); ++e)
+    if (!is_local[e]) { nd.push_back(ex.r[e]); nd.push_back(ex.c[e]); }
+  if (nd.empty()) return taken;
+  std::sort(nd.begin(), nd.end());
+  nd.erase(std::unique(nd.begin(), nd.end()), nd.end());
+  auto index = [&](int64_t d) {
+    auto it = std::lower_bound(nd.begin(), nd.end(), d);
+    return (it != nd.end() && *it == d) ? int(it - nd.begin()) : -1;
+  };
+  std::vector<int> parent(nd.size());
+  for (size_t i = 0; i < nd.size(); ++i) parent[i] = (int)i;
+  auto find = [&](int x) {
     while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
     return x;
   };
   for (size_t e = 0; e < ex.size(); ++e) {
     if (is_local[e]) continue;
-    for (int64_t d : {ex.r[e], ex.c[e]})
-      if (!parent.count(d)) parent[d] = d;
-    int64_t a = find(ex.r[e]), b = find(ex.c[e]);
+    const int a = find(index(ex.r[e])), b = find(index(ex.c[e]));
     if (a != b) parent[std::max(a, b)] = std::min(a, b);
   }
-  if (parent.empty()) return taken;
-  std::map<int64_t, std::vector<int64_t>> members;   // root -> dofs, ordered for determinism
-  for (auto& kv : parent) members[find(kv.first)].push_back(kv.first);
-  std::map<int64_t, std::vector<size_t>> ents;
-  for (size_t e = 0; e < ex.size(); ++e) {
-    auto ia = parent.find(ex.r[e]), ib = parent.find(ex.c[e]);
-    if (ia == parent.end() || ib == parent.end()) continue;
-    int64_t ra = find(ex.r[e]), rb = find(ex.c[e]);
-    if (ra == rb) ents[ra].push_back(e);
+  // components in the order of their smallest dof; entries with both dofs in one component
+  std::vector<int> comp(nd.size(), -1), root_comp(nd.size(), -1);
+  std::vector<std::vector<int64_t>> dofs;
+  for (size_t i = 0; i < nd.size(); ++i) {
+    const int r = find((int)i);
+    if (root_comp[r] < 0) { root_comp[r] = (int)dofs.size(); dofs.emplace_back(); }
+    comp[i] = root_comp[r];
+    dofs[comp[i]].push_back(nd[i]);
   }
-  for (auto& kv : members) {
-    std::vector<int64_t>& dofs = kv.second;
-    std::sort(dofs.begin(), dofs.end());
-    const int m = (int)dofs.size();
+  std::vector<std::vector<size_t>> ents(dofs.size());
+  for (size_t e = 0; e < ex.size(); ++e) {
+    const int ia = index(ex.r[e]);
+    if (ia < 0) continue;
+    const int ib = index(ex.c[e]);
+    if (ib >= 0 && comp[ia] == comp[ib]) ents[comp[ia]].push_back(e);
+  }
+  for (size_t cpt = 0; cpt < dofs.size(); ++cpt) {
+    const std::vector<int64_t>& D = dofs[cpt];     // sorted (nd is sorted)
+    const int m = (int)D.size();
     if (m > kTermDofs) continue;
     std::vector<double> A((size_t)m * m, 0.0);
-    auto li = [&](int64_t d) { return int(std::lower_bound(dofs.begin(), dofs.end(), d) - dofs.begin()); };
-    const std::vector<size_t>& es = ents[kv.first];
-    for (size_t e : es) A[(size_t)li(ex.r[e]) * m + li(ex.c[e])] += ex.v[e];
-    if (factor_terms(A, m, dofs, kTermRank, terms))
-      for (size_t e : es) taken[e] = 1;
+    auto li = [&](int64_t d) { return int(std::lower_bound(D.begin(), D.end(), d) - D.begin()); };
+    for (size_t e : ents[cpt]) A[(size_t)li(ex.r[e]) * m + li(ex.c[e])] += ex.v[e];
+    if (factor_terms(A, m, D, kTermRank, terms))
+      for (size_t e : ents[cpt]) taken[e] = 1;
   }
   return taken;
 }
@@ -479,7 +535,11 @@ struct Level {
   float* ent_v32 = nullptr;
   Entries nonlocal;                       // non-local entries kept as entries (projected entry by entry)
   Terms terms;                            // non-local couplings as rank-1 terms (projected as vectors)
-  Entries sparse;                         // this level's entries outside the stencil: nonlocal + expanded terms
+  Entries sparse;                         // this level's entries outside the stencil (non-factored remainder)
+  int nterms = 0;                         // device copy of `terms` and its per-node pairs (levels >= 1)
+  int *t_ptr = nullptr, *t_dof = nullptr, *tn_ptr = nullptr, *tn_term = nullptr;
+  double *t_val64 = nullptr, *t_lam64 = nullptr, *tn_coef64 = nullptr;
+  float *t_val32 = nullptr, *t_lam32 = nullptr, *tn_coef32 = nullptr;
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
   AxisHost ax[3];                         // transfer to the next level
@@ -507,6 +567,48 @@ int upload_node_csr(Pool& pool, const Entries& E, int64_t nnode, Level& V) {
   FEB_TRY(pool.upload(&V.ent_col, col.data(), col.size()));
   FEB_TRY(pool.upload(&V.ent_v64, v.data(), v.size()));
   FEB_TRY(pool.upload(&V.ent_v32, vf.data(), vf.size()));
+  return FEB_OK;
+}
+
+// device copy of a level's terms: entries (dof, value) per term, and per node the (term, v_t at the node)
+// pairs of the terms touching it
+int upload_terms(Pool& pool, const Terms& T, int64_t nnode, Level& V) {
+  V.nterms = (int)T.size();
+  if (V.nterms == 0) return FEB_OK;
+  std::vector<int> tp(T.ptr.begin(), T.ptr.end()), td(T.dof.begin(), T.dof.end());
+  std::vector<float> tv32(T.val.begin(), T.val.end()), tl32(T.lam.begin(), T.lam.end());
+  // pairs: one per (term, node) with the node's three components
+  std::vector<int> cnt(nnode + 1, 0);
+  std::vector<std::pair<int64_t, int>> pairs;   // (node, term) in term order, one per distinct node
+  for (size_t t = 0; t < T.size(); ++t)
+    for (int64_t e = T.ptr[t]; e < T.ptr[t + 1]; ++e)
+      if (e == T.ptr[t] || T.dof[e] / 3 != T.dof[e - 1] / 3) pairs.emplace_back(T.dof[e] / 3, (int)t);
+  for (const auto& pr : pairs) cnt[pr.first + 1]++;
+  for (int64_t i = 0; i < nnode; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1), term(pairs.size());
+  std::vector<double> coef(3 * pairs.size(), 0.0);
+  size_t q = 0;
+  for (size_t t = 0; t < T.size(); ++t)
+    for (int64_t e = T.ptr[t]; e < T.ptr[t + 1]; ++e) {
+      const int64_t node = T.dof[e] / 3;
+      if (e == T.ptr[t] || node != T.dof[e - 1] / 3) {
+        const int at = fill[node]++;
+        term[at] = (int)t;
+        q = (size_t)at;
+      }
+      coef[3 * q + T.dof[e] % 3] = T.val[e];
+    }
+  std::vector<float> coef32(coef.begin(), coef.end());
+  FEB_TRY(pool.upload(&V.t_ptr, tp.data(), tp.size()));
+  FEB_TRY(pool.upload(&V.t_dof, td.data(), td.size()));
+  FEB_TRY(pool.upload(&V.t_val64, T.val.data(), T.val.size()));
+  FEB_TRY(pool.upload(&V.t_val32, tv32.data(), tv32.size()));
+  FEB_TRY(pool.upload(&V.t_lam64, T.lam.data(), T.lam.size()));
+  FEB_TRY(pool.upload(&V.t_lam32, tl32.data(), tl32.size()));
+  FEB_TRY(pool.upload(&V.tn_ptr, cnt.data(), cnt.size()));
+  FEB_TRY(pool.upload(&V.tn_term, term.data(), term.size()));
+  FEB_TRY(pool.upload(&V.tn_coef64, coef.data(), coef.size()));
+  FEB_TRY(pool.upload(&V.tn_coef32, coef32.data(), coef32.size()));
   return FEB_OK;
 }
 
@@ -550,6 +652,8 @@ struct FebHandle {
   int64_t nnode = 0, ntotal = 0, ndof = 0;
   FineView<double> F64{};
   FineView<float> F32{};
+  bool tc_ok = false;                     // FP32 K.u may run on the tensor cores (equal cubic cells, ISO model)
+  int* tc_status = nullptr;
   int* orig_copy = nullptr;
   std::vector<int64_t> orig_copy_h;
   double *xe_d = nullptr, *ye_d = nullptr, *ze_d = nullptr;
@@ -632,11 +736,16 @@ struct FebHandle {
     S.nx = V.nx; S.ny = V.ny; S.nz = V.nz; S.n = V.nnode;
     S.S = symS<T>(V);
     S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
+    S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
+    S.t_ptr = V.t_ptr; S.t_dof = V.t_dof; S.t_val = tval<T>(V); S.t_lam = tlam<T>(V);
     S.Dinv = dinv<T>(V);
     return S;
   }
   template <typename T> static const T* symS(const Level& V);
   template <typename T> static const T* entv(const Level& V);
+  template <typename T> static const T* tcoef(const Level& V);
+  template <typename T> static const T* tval(const Level& V);
+  template <typename T> static const T* tlam(const Level& V);
   template <typename T> static T* ve(Level& V);
   template <typename T> static const T* dinv(const Level& V);
   template <typename T> static T* vb(Level& V);
@@ -868,6 +977,12 @@ template <> float* FebHandle::ve<float>(Level& V) { return V.e32; }
 template <> const double* FebHandle::symS<double>(const Level& V) { return V.S64; }
 template <> const float* FebHandle::symS<float>(const Level& V) { return V.S32; }
 template <> const double* FebHandle::entv<double>(const Level& V) { return V.ent_v64; }
+template <> const double* FebHandle::tcoef<double>(const Level& V) { return V.tn_coef64; }
+template <> const float* FebHandle::tcoef<float>(const Level& V) { return V.tn_coef32; }
+template <> const double* FebHandle::tval<double>(const Level& V) { return V.t_val64; }
+template <> const float* FebHandle::tval<float>(const Level& V) { return V.t_val32; }
+template <> const double* FebHandle::tlam<double>(const Level& V) { return V.t_lam64; }
+template <> const float* FebHandle::tlam<float>(const Level& V) { return V.t_lam32; }
 template <> const float* FebHandle::entv<float>(const Level& V) { return V.ent_v32; }
 
 
@@ -950,22 +1065,35 @@ int power_iteration(FebHandle* h, int l) {
 // Launch shape of the fine K.u (warps per CTA x node planes per CTA), picked by timing every candidate
 // on this operator and cached per (grid, material model, split copies) for the process lifetime.
 struct TuneKey {
-  int nx, ny, nz, mode, copies;
+  int nx, ny, nz, mode, copies, tc;
   bool operator<(const TuneKey& o) const {
-    return std::tie(nx, ny, nz, mode, copies) < std::tie(o.nx, o.ny, o.nz, o.mode, o.copies);
+    return std::tie(nx, ny, nz, mode, copies, tc) < std::tie(o.nx, o.ny, o.nz, o.mode, o.copies, o.tc);
   }
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, std::pair<KuConfig, KuConfig>> g_tune_cache;
 
+// FEB_KU_TC: "0" keeps the FP32 K.u off the tensor cores, "1" puts it there without tuning (tests, profiling)
+int env_tc() {
+  const char* e = std::getenv("FEB_KU_TC");
+  return (e && *e) ? (e[0] == '1' ? 1 : 0) : -1;
+}
+
 template <typename T>
 int tune_one(FebHandle* h, KuConfig* best, T* u, T* y) {
-  const int tys[3] = {8, 12, 16};
-  const int zcs[6] = {6, 8, 12, 16, 24, 32};
+  std::vector<KuConfig> cand;
+  const bool tc = std::is_same<T, float>::value && h->tc_ok;
+  if (tc && env_tc() == 1) {
+    *best = KuConfig{16, 16, 1};
+    return FEB_OK;
+  }
+  for (int ty : {8, 12, 16})
+    for (int zc : {6, 8, 12, 16, 24, 32}) cand.push_back(KuConfig{ty, zc, 0});
+  if (tc)
+    for (int zc : {8, 12, 16, 24, 32}) cand.push_back(KuConfig{16, zc, 1});
   float best_ms = 1e30f;
-  for (int ty : tys)
-    for (int zc : zcs) {
-      KuConfig c{ty, zc};
+  {
+    for (const KuConfig& c : cand) {
       KuConfig& slot = std::is_same<T, double>::value ? h->ku64 : h->ku32;
       slot = c;
       for (int w = 0; w < 2; ++w) h->apply<T>(0, u, y, nullptr);
@@ -977,11 +1105,12 @@ int tune_one(FebHandle* h, KuConfig* best, T* u, T* y) {
       FEB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
       if (ms < best_ms) { best_ms = ms; *best = c; }
     }
+  }
   return FEB_OK;
 }
 
 int autotune_ku(FebHandle* h) {
-  TuneKey key{h->nx, h->ny, h->nz, h->mode, h->ntotal > h->nnode ? 1 : 0};
+  TuneKey key{h->nx, h->ny, h->nz, h->mode, h->ntotal > h->nnode ? 1 : 0, h->tc_ok ? 2 + env_tc() : 0};
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -994,7 +1123,11 @@ int autotune_ku(FebHandle* h) {
   const char* env = std::getenv("FEB_KU_CONFIG");     // "ty,zchunk" pins the shape (tests, profiling)
   if (env && *env) {
     int ty = 16, zc = 16;
-    if (std::sscanf(env, "%d,%d", &ty, &zc) == 2) { h->ku32 = h->ku64 = KuConfig{ty, zc}; return FEB_OK; }
+    if (std::sscanf(env, "%d,%d", &ty, &zc) == 2) {
+      h->ku32 = h->ku64 = KuConfig{ty, zc, 0};
+      if (h->tc_ok && env_tc() == 1) h->ku32 = KuConfig{16, zc, 1};
+      return FEB_OK;
+    }
   }
   const size_t n = 3 * (size_t)h->ntotal;
   double *u64 = nullptr, *y64 = nullptr;
@@ -1009,6 +1142,73 @@ int autotune_ku(FebHandle* h) {
   h->ku64 = b64;
   std::lock_guard<std::mutex> lock(g_tune_mu);
   g_tune_cache[key] = {b32, b64};
+  return FEB_OK;
+}
+
+// Tensor-core operand of the FP32 level-0 K.u: on equal cubic cells of edge h the ISO element matrices are
+// h K(1) with 72 K_mu(1), 72 K_lambda(1) integer and the one-point 16 K_lambda(1) = s s^T, s[3l+c] = +-1 by
+// bit c of l.  Read off the device element operator for the unit cube, checked to be those integers, laid
+// out as the kernel's B table: [face cz][node row b][output n][4a + c] in BF16 (exact).  Leaves tc_ok false
+// for other grids or models.
+int setup_tc(FebHandle* h) {
+  FebHandle& H = *h;
+  if ((H.mode != MAT_ISO_SRI && H.mode != MAT_ISO_FULL) || env_tc() == 0) return FEB_OK;
+  const double hc = H.xe[1] - H.xe[0];
+  auto uniform = [&](const std::vector<double>& e) {
+    for (size_t i = 0; i + 1 < e.size(); ++i)
+      if (std::fabs((e[i + 1] - e[i]) - hc) > 1e-12 * hc) return false;
+    return true;
+  };
+  if (!(hc > 0.0) || !uniform(H.xe) || !uniform(H.ye) || !uniform(H.ze)) return FEB_OK;
+  const bool sri = H.mode == MAT_ISO_SRI;
+  double* d = nullptr;
+  FEB_TRY(H.pool.alloc(&d, 1152));
+  if (sri) launch_unit_element<MAT_ISO_SRI>(d, H.s);
+  else launch_unit_element<MAT_ISO_FULL>(d, H.s);
+  std::vector<double> K(1152);
+  FEB_CUDA(cudaMemcpyAsync(K.data(), d, 1152 * sizeof(double), cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  H.pool.free(d);
+  const double* KL = K.data();
+  const double* KM = K.data() + 576;
+  int IM[24][24], IL[24][24], sg[24];
+  for (int r = 0; r < 24; ++r) sg[r] = (((r / 3) >> (r % 3)) & 1) ? 1 : -1;
+  for (int r = 0; r < 24; ++r)
+    for (int c = 0; c < 24; ++c) {
+      const double vm = 72.0 * KM[r * 24 + c], vl = 72.0 * KL[r * 24 + c];
+      IM[r][c] = (int)std::lround(vm);
+      IL[r][c] = (int)std::lround(vl);
+      if (std::fabs(vm - IM[r][c]) > 1e-9 || std::abs(IM[r][c]) > 256) return FEB_OK;
+      if (sri ? std::fabs(16.0 * KL[r * 24 + c] - sg[r] * sg[c]) > 1e-9
+              : (std::fabs(vl - IL[r][c]) > 1e-9 || std::abs(IL[r][c]) > 256))
+        return FEB_OK;
+    }
+  const int N = sri ? tc_columns<MAT_ISO_SRI>() : tc_columns<MAT_ISO_FULL>();
+  std::vector<uint16_t> tab((size_t)4 * N * 8, 0);
+  for (int cz = 0; cz < 2; ++cz)
+    for (int b = 0; b < 2; ++b)
+      for (int n = 0; n < N; ++n)
+        for (int a = 0; a < 2; ++a)
+          for (int c = 0; c < 3; ++c) {
+            const int kd = 3 * (a + 2 * b + 4 * cz) + c;
+            int v = 0;
+            if (n < 24) v = IM[n][kd];
+            else if (sri) v = (n == 24) ? sg[kd] : 0;
+            else v = IL[n - 24][kd];
+            const float fv = (float)v;
+            uint32_t bits;
+            std::memcpy(&bits, &fv, 4);
+            tab[((size_t)(cz * 2 + b) * N + n) * 8 + 4 * a + c] = (uint16_t)(bits >> 16);   // exact: |v| <= 256
+          }
+  uint16_t* dtab = nullptr;
+  FEB_TRY(H.pool.upload(&dtab, tab.data(), tab.size()));
+  FEB_TRY(H.pool.zeros(&H.tc_status, 1));
+  FEB_CUDA(sri ? prepare_fine_tc<MAT_ISO_SRI>() : prepare_fine_tc<MAT_ISO_FULL>());
+  H.F32.tc_b = dtab;
+  H.F32.tc_hmu = (float)(hc / 72.0);
+  H.F32.tc_hlam = (float)(sri ? hc / 16.0 : hc / 72.0);
+  H.F32.tc_status = H.tc_status;
+  H.tc_ok = true;
   return FEB_OK;
 }
 
@@ -1093,6 +1293,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     H.orig_copy_h.assign(oc.begin(), oc.end());
   }
   H.stage_mark();   // 1: cells, irregular list, copies
+  g_prof.mark("L0 cells/irregular/copies", s);
   std::vector<uint8_t> used_h(H.ntotal);
   FEB_CUDA(cudaMemcpyAsync(used_h.data(), V.used, H.ntotal, cudaMemcpyDeviceToHost, s));
   FEB_CUDA(cudaStreamSynchronize(s));
@@ -1105,6 +1306,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     FEB_CUDA(cudaMemcpyAsync(V.used, used_h.data(), H.ntotal, cudaMemcpyHostToDevice, s));
     FEB_CUDA(cudaStreamSynchronize(s));
   }
+  g_prof.mark("L0 used mask to host", s);
   // penalties (entries on unused nodes are dropped, fe/solver.py:213-215)
   std::vector<int> pn;
   std::vector<double> pk;
@@ -1126,6 +1328,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   // extra matrix: all entries applied on level 0; local ones folded into the level-1 stencil on the
   // device, non-local ones projected through the levels on the host
   Entries ex;
+  ex.r.reserve(op->nextra); ex.c.reserve(op->nextra); ex.v.reserve(op->nextra);
   for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
     int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
     if (rr < 0 || cc < 0 || rr >= 3 * H.ntotal || cc >= 3 * H.ntotal) {
@@ -1135,9 +1338,12 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     if (!used_h[rr / 3] || !used_h[cc / 3]) continue;
     ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
   }
+  g_prof.mark("L0 penalties + extra read", s);
   coo_merge(ex);
+  g_prof.mark("L0 extra merge", s);
   Csr c0;
   FEB_TRY(upload_csr(H.pool, ex, c0));
+  g_prof.mark("L0 extra CSR upload", s);
   Entries loc;
   const int gx = H.nx + 1, gy = H.ny + 1;
   auto pos = [&](int64_t node) { return node < H.nnode ? node : H.orig_copy_h[node - H.nnode]; };
@@ -1148,6 +1354,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     is_local[e2] = std::abs(da) <= 1 && std::abs(db) <= 1 && std::abs(dc) <= 1;
   }
   std::vector<char> taken = factor_nonlocal(ex, is_local, V.terms);
+  g_prof.mark("L0 extra classify + factor", s);
   for (size_t e2 = 0; e2 < ex.size(); ++e2) {
     if (taken[e2]) continue;
     Entries& dst = is_local[e2] ? loc : V.nonlocal;
@@ -1192,8 +1399,11 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   FEB_CUDA(cudaGetLastError());
   H.pool.free(D);
   H.stage_mark();   // 3: used nodes, level-0 diagonal blocks
+  g_prof.mark("L0 local upload, diag blocks", s);
+  FEB_TRY(setup_tc(h));
   FEB_TRY(autotune_ku(h));
   H.stage_mark();   // 4: K.u autotuning (first handle of a grid shape only)
+  g_prof.mark("L0 tensor-core operand, tuning", s);
   return FEB_OK;
 }
 
@@ -1231,6 +1441,7 @@ int build_dense(FebHandle* h) {
       FEB_TRY(H.pool.upload(&dv, V.sparse.v.data(), V.sparse.v.size()));
       launch_dense_add_entries((int)rr.size(), dr, dc, dv, H.cmap, H.Minv, H.nd, H.s);
     }
+    launch_dense_add_terms(V.nterms, V.t_ptr, V.t_dof, V.t_val64, V.t_lam64, H.cmap, H.Minv, H.nd, H.s);
   }
   double* scratch = nullptr;
   FEB_TRY(H.pool.alloc(&scratch, dense_scratch_doubles(H.nd)));
@@ -1260,6 +1471,7 @@ int build_hierarchy(FebHandle* h) {
     // transfer l -> l+1
     for (int d = 0; d < 3; ++d) V.ax[d] = make_axis(V.coord[d]);
     FEB_TRY(upload_transfer(H.pool, V));
+    g_prof.mark("Lk transfer", H.s);
     H.L.emplace_back();
     Level& C = H.L.back();
     Level& F = H.L[l];   // reference again after emplace_back
@@ -1271,6 +1483,7 @@ int build_hierarchy(FebHandle* h) {
     int64_t kept = 0;
     FEB_TRY(count_mask(h, C.used, C.ntotal, &kept));
     C.ndof = 3 * kept;
+    g_prof.mark("Lk kept mask + count", H.s);
     FEB_TRY(H.pool.zeros(&C.A64, 243 * (size_t)C.ntotal));
     if (l == 0) {
       double* KeC = nullptr;
@@ -1287,20 +1500,30 @@ int build_hierarchy(FebHandle* h) {
       launch_galerkin_local(F.P, F.nx, F.ny, F.nnode, H.orig_copy, H.nlocal, H.loc_r, H.loc_c, H.loc_v, C.A64, C.nx,
                             C.ny, C.nz, C.ntotal, H.s);
     } else {
-      launch_galerkin_stencil(F.P, F.A64, F.nx, F.ny, F.nz, C.A64, C.nx, C.ny, C.nz, H.s);
+      double *T1 = nullptr, *T2 = nullptr;    // x coarsened, then y; z lands in C.A64
+      FEB_TRY(H.pool.alloc(&T1, 243 * (size_t)C.nx * F.ny * F.nz));
+      FEB_TRY(H.pool.alloc(&T2, 243 * (size_t)C.nx * C.ny * F.nz));
+      launch_galerkin_axis(F.P.ax[0], 0, F.A64, F.nx, F.ny, F.nz, T1, C.nx, F.ny, F.nz, H.s);
+      launch_galerkin_axis(F.P.ax[1], 1, T1, C.nx, F.ny, F.nz, T2, C.nx, C.ny, F.nz, H.s);
+      launch_galerkin_axis(F.P.ax[2], 2, T2, C.nx, C.ny, F.nz, C.A64, C.nx, C.ny, C.nz, H.s);
+      H.pool.free(T1);
+      H.pool.free(T2);
     }
     FEB_CUDA(cudaGetLastError());
+    g_prof.mark("Lk Galerkin product", H.s);
     C.nonlocal = project(F.nonlocal, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
     C.terms = project_terms(F.terms, F.ax, H.orig_copy_h, F.nnode, F.nx, F.ny);
     C.sparse = C.nonlocal;
-    expand_terms(C.terms, C.sparse);
     FEB_TRY(upload_node_csr(H.pool, C.sparse, C.nnode, C));
+    FEB_TRY(upload_terms(H.pool, C.terms, C.nnode, C));
+    g_prof.mark("Lk sparse project + upload", H.s);
     FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)C.ntotal));
     launch_stencil_to_sym<double>(C.A64, C.ntotal, C.S64, H.s);
     if (f32) {
       FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)C.ntotal));
       launch_stencil_to_sym<float>(C.A64, C.ntotal, C.S32, H.s);
     }
+    g_prof.mark("Lk half stencils", H.s);
     l += 1;
     bool last = (C.ndof <= H.opt.min_dofs) || (l == maxl - 1);
     if (!last) {
@@ -1313,6 +1536,13 @@ int build_hierarchy(FebHandle* h) {
         if (C.sparse.r[e] / 3 == C.sparse.c[e] / 3) {
           dr.push_back((int)C.sparse.r[e]); dc.push_back((int)C.sparse.c[e]); dv.push_back(C.sparse.v[e]);
         }
+      for (size_t t = 0; t < C.terms.size(); ++t)      // lam v_n v_n^T: the terms' 3x3 diagonal blocks
+        for (int64_t a = C.terms.ptr[t]; a < C.terms.ptr[t + 1]; ++a)
+          for (int64_t b = C.terms.ptr[t]; b < C.terms.ptr[t + 1]; ++b)
+            if (C.terms.dof[a] / 3 == C.terms.dof[b] / 3) {
+              dr.push_back((int)C.terms.dof[a]); dc.push_back((int)C.terms.dof[b]);
+              dv.push_back(C.terms.lam[t] * C.terms.val[a] * C.terms.val[b]);
+            }
       if (!dr.empty()) {
         int *ddr, *ddc;
         double* ddv;
@@ -1326,6 +1556,7 @@ int build_hierarchy(FebHandle* h) {
       launch_block_inverse(D, C.ntotal, C.Dinv64, C.Dinv32, H.s);
       FEB_CUDA(cudaGetLastError());
       H.pool.free(D);
+      g_prof.mark("Lk block-Jacobi", H.s);
     }
   }
   H.stage_mark();   // 5: transfers, Galerkin products, coarse diagonal blocks
@@ -1334,15 +1565,28 @@ int build_hierarchy(FebHandle* h) {
     Level& V = H.L[k];
     FEB_TRY(level_vectors<double>(H.pool, V, true, f32));
   }
+  g_prof.mark("level work vectors", H.s);
   for (int k = 0; k < H.coarsest; ++k) FEB_TRY(power_iteration(h, k));
   H.stage_mark();   // 6: work vectors, power iterations
+  g_prof.mark("power iterations", H.s);
   FEB_TRY(build_dense(h));
   H.stage_mark();   // 7: dense coarsest level and its inverse
+  g_prof.mark("dense coarsest inverse", H.s);
   for (int k = 1; k <= H.coarsest; ++k) {      // the full stencils only feed the Galerkin products
     H.pool.free(H.L[k].A64);
     H.L[k].A64 = nullptr;
     if (f32) { H.pool.free(H.L[k].S64); H.L[k].S64 = nullptr; }
   }
+  return FEB_OK;
+}
+
+// a bounded wait inside the tensor-core K.u gave up (the kernel skipped its work and returned)
+int check_tc_status(FebHandle* h) {
+  if (!h->tc_status) return FEB_OK;
+  int st = 0;
+  FEB_CUDA(cudaMemcpyAsync(&st, h->tc_status, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+  FEB_CUDA(cudaStreamSynchronize(h->s));
+  if (st) { set_last_error("tensor-core K.u: an mbarrier wait timed out"); return FEB_ERR_TIMEOUT; }
   return FEB_OK;
 }
 
@@ -1409,6 +1653,7 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   if (h->sync_in() != FEB_OK) { delete h; return FEB_ERR_CUDA; }
   cudaEventRecord(h->ev0, h->s);
   h->stage_mark();   // 0: start
+  g_prof.start(env_flag("FEB_PROFILE_SETUP") != 0);
   int st = FEB_OK;
   do {
     h->L.reserve(kMaxLevels);
@@ -1457,6 +1702,8 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
     delete h;
     return st;
   }
+  g_prof.mark("work vectors", h->s);
+  g_prof.print();
   h->sync_out();
   *out = h;
   return FEB_OK;
@@ -1617,6 +1864,7 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   }
   FEB_CUDA(cudaEventRecord(H.ev1, H.s));
   FEB_CUDA(cudaEventSynchronize(H.ev1));
+  FEB_TRY(check_tc_status(h));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, H.ev0, H.ev1);
   inf.t_solve_ms = ms;
@@ -1632,7 +1880,7 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   }
   inf.kernel_launches = H.launches;
   for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
-  inf.ku_shape[0] = H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
+  inf.ku_shape[0] = H.ku32.tc ? 0 : H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
   inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
   if (info) *info = inf;
   FEB_TRY(H.sync_out());
@@ -1686,6 +1934,7 @@ int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int3
   float t = 0.f;
   FEB_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
   *ms = t / nrep;
+  FEB_TRY(check_tc_status(h));
   return h->sync_out();
 }
 

@@ -48,6 +48,19 @@ def _dev(a, dtype):
     return t.to("cuda", non_blocking=False)
 
 
+def _host(*ts):
+    """NumPy copies of device tensors through page-locked buffers (torch's caching host allocator reuses them
+    once the arrays are released), one stream synchronisation for all of them."""
+    torch = _torch()
+    outs = []
+    for t in ts:
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        outs.append(h)
+    torch.cuda.current_stream().synchronize()
+    return [h.numpy() for h in outs] if len(outs) > 1 else outs[0].numpy()
+
+
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
@@ -246,7 +259,7 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
         x, info = P.solve(f, x0d)
         stamps.append(("solve", time.perf_counter()))
         Ud = P.export(x)
-        U = Ud.view(ntotal, 3).cpu().numpy()
+        U = _host(Ud.view(ntotal, 3))
         stamps.append(("download", time.perf_counter()))
         R = np.zeros((ntotal, 3))
         np.add.at(R, fn, -(fa[:, None] * K_GROUND) * U[fn])
@@ -320,9 +333,9 @@ def solve(grid, lam, mu, active, springs, loads, method="cg", tol=1e-8, x0=None,
             x0 = full
         x0d = _dev(np.asarray(x0).ravel(), np.float64) if x0 is not None else None
         x, info = P.solve(f, x0d)
-        U = P.export(x).view(nnode, 3).cpu().numpy()
+        U = _host(P.export(x).view(nnode, 3))
         usedn = np.flatnonzero(used)
-        fh = f.view(nnode, 3).cpu().numpy()[usedn].ravel()
+        fh = _host(f.view(nnode, 3))[usedn].ravel()
         return U, _info_dict(info, t0, dict(K=None, f=fh, used=usedn))
     finally:
         P.close()
@@ -343,7 +356,7 @@ def _stress(g, mode, mat, U, cells, cn, nan_to_zero, to_host=True):
                                            int(nan_to_zero), _ptr(sig), _ptr(vm), _ptr(eps), _stream()))
     if not to_host:
         return sig.view(n, 6), vm, eps.view(n, 6)
-    return sig.view(n, 6).cpu().numpy(), vm.cpu().numpy(), eps.view(n, 6).cpu().numpy()
+    return tuple(_host(sig.view(n, 6), vm, eps.view(n, 6)))
 
 
 def cell_stress_cn(g, lam, mu, U, cells, cn, aniso=None, *, device=None):
@@ -380,7 +393,7 @@ def element_forces_cn(g, lam, mu, U, cells, cn, aniso=None):
     gs = _grid_struct(g)
     _lib.check(_lib.load().feb_element_forces(C.byref(gs), _ptr(mat), _ptr(Ud), n, _ptr(cd), _ptr(cnd), _ptr(out),
                                               _stream()))
-    return out.view(n, 8, 3).cpu().numpy()
+    return _host(out.view(n, 8, 3))
 
 
 def _rigid_groups_from_Z(Z, n):
@@ -441,7 +454,7 @@ def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, A_op=N
             xf = np.zeros((len(orig), 3)); xf[node_of] = np.asarray(x0, np.float64).reshape(-1, 3)
             x0d = _dev(xf.ravel(), np.float64)
         x, info = P.solve(f, x0d)
-        xh = x.view(-1, 3).cpu().numpy()[node_of].ravel()
+        xh = _host(x.view(-1, 3))[node_of].ravel()
         return xh, _info_dict(info, t0)
     finally:
         P.close()

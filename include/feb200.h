@@ -103,7 +103,8 @@ typedef struct FebInfo {
   double lmax[8];
   int32_t coarse_n;              /* dofs of the dense coarsest level */
   int32_t kernel_launches;       /* kernels launched by feb_solve */
-  int32_t ku_shape[4];           /* autotuned fine K.u launch shape: FP32 (warps, planes), FP64 (warps, planes) */
+  int32_t ku_shape[4];           /* autotuned fine K.u launch shape: FP32 (warps per CTA, 0 = tensor cores;
+                                    node planes per CTA), FP64 (warps, planes) */
   double t_stage_ms[8];          /* feb_create stages: cells, penalties/extra, diagonal blocks, K.u tuning,
                                     Galerkin hierarchy, power iterations, dense coarse level, (spare) */
 } FebInfo;

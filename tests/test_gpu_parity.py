@@ -84,13 +84,50 @@ def test_stress_and_element_forces_exact(golden):
     np.testing.assert_allclose(F, z["F"], rtol=0, atol=1e-10 * np.abs(z["F"]).max())
 
 
+@pytest.mark.parametrize("tc", ["0", "1"])
+@pytest.mark.parametrize("mode", ["sri", "full"])
+def test_fp32_operator_on_tensor_cores(golden, monkeypatch, tc, mode):
+    """FP32 K.u with the tensor-core kernel forced on (1) or kept off (0): within 2e-6 of the FP64 product
+    (the reference assembly's for the SRI split-node model; the integrated model on the block grid)."""
+    import torch
+    monkeypatch.setenv("FEB_KU_TC", tc)
+    if mode == "sri":
+        z, g = _hindfoot(golden)
+        args = (g, _lib.MAT_ISO_SRI, np.concatenate([z["lam"], z["mu"]]), z["active"])
+        kw = dict(cn=z["cn"], orig=z["orig"])
+    else:
+        z = golden("block_small")
+        g = Grid(z["xe"], z["ye"], z["ze"])
+        args = (g, _lib.MAT_ISO_FULL, np.concatenate([z["lam"], z["mu"]]), np.ones(g.ncell, bool))
+        kw = {}
+    rng = np.random.default_rng(7)
+    with engine.Problem(*args, options=dict(max_levels=0), **kw) as P:
+        m, _ = P.used_mask()
+        used = m.cpu().numpy().astype(bool)
+        for _ in range(3):
+            u = rng.standard_normal((P.ntotal, 3)) * used[:, None]
+            y64 = P.apply(torch.from_numpy(u.ravel()).cuda()).cpu().numpy()
+            y32 = P.apply(torch.from_numpy(u.ravel().astype(np.float32)).cuda()).cpu().numpy()
+            assert rel(y32, y64) < 2e-6
+            # a smooth field: the element forces cancel between neighbours
+            xyz = np.stack(np.meshgrid(g.xe, g.ye, g.ze, indexing="ij"), -1).transpose(2, 1, 0, 3).reshape(-1, 3)
+            us = np.zeros((P.ntotal, 3)); us[: len(xyz)] = np.sin(xyz / 7.0)
+            us *= used[:, None]
+            y64 = P.apply(torch.from_numpy(us.ravel()).cuda()).cpu().numpy()
+            y32 = P.apply(torch.from_numpy(us.ravel().astype(np.float32)).cuda()).cpu().numpy()
+            assert rel(y32, y64) < 2e-5
+
+
+@pytest.mark.parametrize("tc", ["0", "1"])
 @pytest.mark.parametrize("precision", ["mixed", "refine"])
-def test_reduced_precision_solve_cn(golden, precision):
+def test_reduced_precision_solve_cn(golden, monkeypatch, precision, tc):
+    monkeypatch.setenv("FEB_KU_TC", tc)
     z, g = _hindfoot(golden)
     U, info, R = engine.solve_cn(g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"],
                                  (z["fixed_nodes"], z["fixed_area"]),
                                  [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z),
                                  tol=1e-8, maxiter=800, precision=precision)
+    assert (info["ku_shape"][0] == 0) == (tc == "1")
     ok = ~np.isnan(z["U"])
     assert info["flag"] == 0 and info["relres"] < 1e-8
     assert rel(U[ok], z["U"][ok]) < 1e-6
