@@ -1590,6 +1590,32 @@ int check_tc_status(FebHandle* h) {
   return FEB_OK;
 }
 
+// The device's default stream-ordered pool serves every allocation of a handle.  Freed memory stays mapped
+// (release threshold at its maximum) for the next handle, and the pool is reserved up front in one block of
+// about twice the largest set-up seen (at least ~3 KB per node): growing it piece by piece during set-up
+// costs up to hundreds of milliseconds per new peak, in whichever stage happens to need the memory.
+void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
+  int dev = 0;
+  cudaMemPool_t mp;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&mp, dev) != cudaSuccess) return;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+  uint64_t have = 0, high = 0;
+  cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &have);
+  cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &high);
+  const uint64_t nodes = (uint64_t)std::max(nnode, nnode_total);
+  uint64_t want = std::max<uint64_t>(2 * high, nodes * 3072ull);
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) want = std::min<uint64_t>(want, have + free_b / 2);
+  if (have >= want) return;
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, want - have, caller) == cudaSuccess) {
+    cudaFreeAsync(p, caller);
+    cudaStreamSynchronize(caller);      // the block is free for the handle's own stream from here on
+  }
+  cudaGetLastError();                   // a failed reservation is not an error: set-up grows the pool as needed
+}
+
 int env_flag(const char* name) {
   const char* v = std::getenv(name);
   return v && *v && std::strcmp(v, "0") != 0;
@@ -1627,15 +1653,7 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   *out = nullptr;
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) { set_last_error("feb_create: empty grid"); return FEB_ERR_ARG; }
   if (op->mat_mode < 0 || op->mat_mode > 2) { set_last_error("feb_create: bad mat_mode"); return FEB_ERR_ARG; }
-  {
-    // keep freed pool memory mapped for the next handle (set-up allocates and frees GBs per solve)
-    int dev = 0;
-    cudaMemPool_t mp;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
-      uint64_t keep = UINT64_MAX;
-      cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-  }
+  reserve_pool((int64_t)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1), op->nnode_total, (cudaStream_t)stream);
   FebHandle* h = new FebHandle((cudaStream_t)stream);
   if (opt) h->opt = *opt; else feb_default_options(&h->opt);
   if (h->opt.cheb_degree < 1 || h->opt.cheb_degree > 9) { delete h; set_last_error("cheb_degree must be 1..9"); return FEB_ERR_ARG; }
