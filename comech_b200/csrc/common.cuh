@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/feb200.h"
 
@@ -33,6 +34,10 @@ void set_last_error(const char* fmt, ...);
 
 // host-side count of kernel launches issued by the library (feb_launch_count)
 void note_launch(int n = 1);
+
+// symmetric pseudo-inverse by cyclic Jacobi, numpy.linalg.pinv semantics (cutoff 1e-15 max |eigenvalue|);
+// A is n x n row-major (host)
+std::vector<double> sym_pinv(const std::vector<double>& A, int n);
 
 constexpr int kThreads = 256;
 constexpr int kSmCount = 148;

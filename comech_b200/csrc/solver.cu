@@ -375,6 +375,8 @@ std::vector<char> factor_nonlocal(const Entries& ex, const std::vector<char>& is
   return taken;
 }
 
+}  // namespace
+
 // symmetric pseudo-inverse by cyclic Jacobi (numpy.linalg.pinv semantics: cutoff 1e-15 * max |eig|)
 std::vector<double> sym_pinv(const std::vector<double>& A0, int n) {
   std::vector<double> A(A0), V(n * n, 0.0);
@@ -418,6 +420,8 @@ std::vector<double> sym_pinv(const std::vector<double>& A0, int n) {
   }
   return P;
 }
+
+namespace {
 
 // ------------------------------------------------------------------------------------------------ cell set-up
 template <int W>

@@ -33,7 +33,7 @@ def _torch():
     return torch
 
 
-_TDT = {np.float64: "float64", np.int64: "int64", np.uint8: "uint8", np.float32: "float32"}
+_TDT = {np.float64: "float64", np.int64: "int64", np.uint8: "uint8", np.float32: "float32", np.int32: "int32"}
 
 
 def _dev(a, dtype):

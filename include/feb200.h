@@ -168,6 +168,37 @@ FEB_API int feb_cell_stress_noalloc(const FebGrid* grid, int32_t mat_mode, const
 FEB_API int feb_element_forces(const FebGrid* grid, const double* mat, const double* U, int64_t ncells,
                        const int64_t* cells, const int64_t* cn, double* out, void* stream);
 
+/* Forces on a bone from its neighbourhood (rb/rbfe.py:194-213): the nodes of the active cells of part
+ * `target` are marked; every other active cell touching them contributes minus its nodal forces K_e u_e (SRI,
+ * as feb_element_forces) at the marked corners, summed per cell label.  part, lab: [dev] int32 per cell
+ * (cell-id order); lab in 0..nlab-1 (1 <= nlab <= 64, other values ignored); cn [dev] or NULL; out [dev]
+ * nlab x 3; present [dev] nlab flags (1 = some contributing cell has the label). */
+FEB_API int feb_region_forces(const FebGrid* grid, const double* mat, const double* U, const int64_t* cn,
+                              const uint8_t* active, const int32_t* part, const int32_t* lab, int32_t nlab,
+                              int32_t target, int64_t nnode_total, double* out, int32_t* present, void* stream);
+
+/* Rigid-body least-squares fit (rb/rbsim.py:99-107): U ~ t + w x (X - c), c the centroid of X.  X, U [dev] n x 3
+ * (U as given: the reference's callers pass nan_to_num(U)); fit [host] 9: t, w, c (minimum-norm solution,
+ * numpy.linalg.lstsq convention). */
+FEB_API int feb_rigid_fit(const double* X, const double* U, int64_t n, double* fit, void* stream);
+
+/* Displacement relative to a rigid fit (rb/rbsim.py:184): out = nan_to_num(U) - (t + w x (X - c)) at every node;
+ * fit [host] 9 as from feb_rigid_fit; U, out [dev] nnode_total x 3. */
+FEB_API int feb_relative_displacement(const FebGrid* grid, const int64_t* orig, int64_t nnode_total, const double* U,
+                                      const double* fit, double* out, void* stream);
+
+/* Fields on an analysis grid of mx x my x mz cells (cell id z fastest), sub^3 points per cell (rb/rbsim.py:110-138):
+ * per axis and point p the FE cell index i[p], the local coordinate t[p] in [0, 1] and the inside flag in[p]
+ * ([dev], m*sub entries); relative displacement (trilinear in the FE cell), von Mises VM [dev] float ncell and
+ * stress SIG [dev] float ncell x 6 averaged over the points in active FE cells.  Outputs [dev] float:
+ * vm mx*my*mz, u x3, frac (fraction of points in active cells), sig x6. */
+FEB_API int feb_sample_cells(const FebGrid* grid, int32_t mx, int32_t my, int32_t mz, int32_t sub, const int32_t* ix,
+                             const double* tx, const uint8_t* inx, const int32_t* iy, const double* ty,
+                             const uint8_t* iny, const int32_t* iz, const double* tz, const uint8_t* inz,
+                             const int64_t* cn, const uint8_t* active, const double* Urel, const float* VM,
+                             const float* SIG, float* vm_out, float* u_out, float* frac_out, float* sig_out,
+                             void* stream);
+
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
 

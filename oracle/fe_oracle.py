@@ -14,6 +14,8 @@ It is a NumPy/SciPy restatement, written for this project, of the reference algo
 * SRI lambda matrices, split assembly, solve_cn         -- rb/splitfe.py:58-158
 * element forces                                        -- rb/splitfe.py:178-193
 * geometric multigrid + PCG                             -- fe/gmg.py:7-137
+* forces between regions, rigid fit, relative displacement, resampling on an analysis grid
+                                                        -- rb/rbfe.py:194-219, rb/rbsim.py:99-161
 * CG stopping rule                                      -- SciPy 1.18.1 ``scipy.sparse.linalg.cg``
   (installed dependency of the reference, not vendored): ``||r|| < rtol*||b||`` tested before
   every iteration, ``info = maxiter`` when the loop is exhausted.
@@ -509,3 +511,105 @@ def element_forces(g, lam, mu, U, cells, cn):
         m = did == d
         out[m] = lam[cells[m], None] * (ue[m] @ KLs[d].T) + mu[cells[m], None] * (ue[m] @ g.KM[d].T)
     return out.reshape(len(cells), 8, 3)
+
+
+# ------------------------------------------------------------------------------------------ post-processing
+def region_forces(g, lam, mu, U, cn, active, part, lab, nlab, target):
+    """Forces on the nodes of the active cells of part ``target`` from every other active cell touching them,
+    summed per cell label (the sums of rb/rbfe.py:199-213).  Returns (nlab x 3, present flags)."""
+    cells = np.arange(g.ncell)
+    tgt = (part == target) & active
+    tn = np.zeros(len(U), bool)
+    tn[cn[cells[tgt]].ravel()] = True
+    oc = cells[active & ~tgt]
+    oc = oc[tn[cn[oc]].any(1)]
+    fsum = -(element_forces(g, lam, mu, U, oc, cn) * tn[cn[oc]][:, :, None]).sum(1)
+    out = np.zeros((nlab, 3))
+    present = np.zeros(nlab, bool)
+    for i in range(nlab):
+        m = lab[oc] == i
+        if m.any():
+            out[i] = fsum[m].sum(0)
+            present[i] = True
+    return out, present
+
+
+def rigid_fit(X, U):
+    """Least-squares rigid motion U ~ t + w x (X - c) (rb/rbsim.py:99-107); minimum-norm lstsq."""
+    c = X.mean(0)
+    r = X - c
+    A = np.zeros((3 * len(X), 6))
+    A[0::3, 0] = A[1::3, 1] = A[2::3, 2] = 1.0
+    A[0::3, 4], A[0::3, 5] = r[:, 2], -r[:, 1]
+    A[1::3, 3], A[1::3, 5] = -r[:, 2], r[:, 0]
+    A[2::3, 3], A[2::3, 4] = r[:, 1], -r[:, 0]
+    sol = np.linalg.lstsq(A, U.ravel(), rcond=None)[0]
+    return sol[:3], sol[3:], c
+
+
+def relative_displacement(xyz, U, t, w, c):
+    """nan_to_num(U) minus the rigid motion (rb/rbsim.py:184)."""
+    return np.nan_to_num(U) - (t[None, :] + np.cross(w[None, :], xyz - c[None, :]))
+
+
+def _axis_samples(fe_edges, ml_edges, sub):
+    """Per analysis-grid axis: the sub points per cell, the FE cell holding each, the local coordinate in it
+    and whether the point lies inside the FE grid (rb/rbsim.py:112-119)."""
+    oo = (np.arange(sub) + 0.5) / sub
+    X = (ml_edges[:-1, None] + np.diff(ml_edges)[:, None] * oo).ravel()
+    n = len(fe_edges) - 1
+    i = np.clip(np.searchsorted(fe_edges, X) - 1, 0, n - 1)
+    t = np.clip((X - fe_edges[i]) / np.diff(fe_edges)[i], 0, 1)
+    inside = (X >= fe_edges[0]) & (X <= fe_edges[-1])
+    return i, t, inside
+
+
+def sample_fe(g, cn, active, VM, SIG, Urel, ml_edges, sub=2):
+    """Mean von Mises, relative displacement and stress over the sub^3 points of every analysis cell that
+    fall in active FE cells, and the fraction of such points (rb/rbsim.py:110-138).  Returns
+    (vm, u, frac, sig), float32."""
+    (i, tx, ix), (j, ty, iy), (k, tz, iz) = (_axis_samples(e, m, sub) for e, m in zip((g.xe, g.ye, g.ze), ml_edges))
+    I, J, K = np.meshgrid(i, j, k, indexing="ij")
+    c = ((I * g.ny + J) * g.nz + K).ravel()
+    ok = (ix[:, None, None] & iy[None, :, None] & iz[None, None, :]).ravel() & active[c]
+    TX, TY, TZ = (a.ravel() for a in np.meshgrid(tx, ty, tz, indexing="ij"))
+    u = np.zeros((len(c), 3))
+    for l in range(8):
+        a, b, d = CORNERS[l]
+        w = np.where(a, TX, 1 - TX) * np.where(b, TY, 1 - TY) * np.where(d, TZ, 1 - TZ)
+        u += w[:, None] * np.nan_to_num(Urel[cn[c, l]])
+    vm = np.where(ok, VM[c], 0.0)
+    sg = np.where(ok[:, None], SIG[c], 0.0)
+    mx, my, mz = (len(m) - 1 for m in ml_edges)
+
+    def cellsum(a):
+        a = a.reshape(mx, sub, my, sub, mz, sub, *a.shape[1:]).transpose(0, 2, 4, 1, 3, 5, *range(6, a.ndim + 5))
+        return a.reshape(mx * my * mz, sub ** 3, *a.shape[6:]).sum(1)
+    okc = cellsum(ok.astype(np.float32))
+    den = np.maximum(okc, 1)
+    return ((cellsum(vm) / den).astype(np.float32), (cellsum(u * ok[:, None]) / den[:, None]).astype(np.float32),
+            okc / sub ** 3, (cellsum(sg) / den[:, None]).astype(np.float32))
+
+
+def sample_nodes(g, cn, active, Urel, ml_node_xyz):
+    """Relative displacement at analysis-grid nodes: trilinear in the FE cell that holds the node, or in the
+    nearest active FE cell (exact Euclidean feature transform over cell indices, clamped local coordinates)
+    for nodes in empty cells (rb/rbsim.py:141-161)."""
+    from scipy import ndimage
+    P = ml_node_xyz
+    i = np.clip(np.searchsorted(g.xe, P[:, 0]) - 1, 0, g.nx - 1)
+    j = np.clip(np.searchsorted(g.ye, P[:, 1]) - 1, 0, g.ny - 1)
+    k = np.clip(np.searchsorted(g.ze, P[:, 2]) - 1, 0, g.nz - 1)
+    _, ind = ndimage.distance_transform_edt(~active.reshape(g.nx, g.ny, g.nz), return_indices=True)
+    ci, cj, ck = ind[0, i, j, k], ind[1, i, j, k], ind[2, i, j, k]
+    c = (ci * g.ny + cj) * g.nz + ck
+    dx, dy, dz = np.diff(g.xe), np.diff(g.ye), np.diff(g.ze)
+    tx = np.clip((P[:, 0] - g.xe[ci]) / dx[ci], 0, 1)
+    ty = np.clip((P[:, 1] - g.ye[cj]) / dy[cj], 0, 1)
+    tz = np.clip((P[:, 2] - g.ze[ck]) / dz[ck], 0, 1)
+    u = np.zeros((len(P), 3))
+    for l in range(8):
+        a, b, d = CORNERS[l]
+        w = np.where(a, tx, 1 - tx) * np.where(b, ty, 1 - ty) * np.where(d, tz, 1 - tz)
+        u += w[:, None] * np.nan_to_num(Urel[cn[c, l]])
+    return u.astype(np.float32)

@@ -8,7 +8,10 @@ Every fixture stores its inputs as well as the reference's outputs, so the tests
 reference (nor the synthetic generator) at run time.  Reference functions used:
 fe/solver.py (element_matrices, element_basis, Grid, assemble, solve, cell_stress),
 fe/gmg.py (GMG, pcg_gmg), rb/splitfe.py (split_connectivity[_fast], KL_family, assemble_cn,
-solve_cn, cell_stress_cn, element_forces_cn), fe/test_patch.py (patch-test set-up).
+solve_cn, cell_stress_cn, element_forces_cn), fe/test_patch.py (patch-test set-up),
+rb/rbsim.py (rigid_fit, sample_fe, sample_nodes) and the region-force sums of rb/rbfe.py:194-213.
+
+    python tests/golden/make_golden.py [fixture ...]      # default: all fixtures
 """
 import os
 import sys
@@ -107,6 +110,62 @@ def hindfoot_solve():
          lmax=np.array([L.lmax for L in mg.levels]))
 
 
+def region_forces_ref(g, lam, mu, U, cn, active, part, lab, nlab, target):
+    """The force sums of rb/rbfe.py:199-213 (inline there) for one target part, per label."""
+    cells = np.arange(g.ncell)
+    tgt = (part == target) & active
+    tn = np.zeros(len(U), bool)
+    tn[cn[cells[tgt]].ravel()] = True
+    oc = cells[active & ~tgt]
+    oc = oc[tn[cn[oc]].any(1)]
+    fe = RSF.element_forces_cn(g, lam, mu, U, oc, cn)
+    fsum = -(fe * tn[cn[oc]][:, :, None]).sum(1)
+    out = np.zeros((nlab, 3))
+    present = np.zeros(nlab, bool)
+    for i in range(nlab):
+        m = lab[oc] == i
+        if m.any():
+            out[i] = fsum[m].sum(0)
+            present[i] = True
+    return out, present
+
+
+def post():
+    """Post-processing of the hindfoot_small solution: region forces on two bones, rigid fit of a bone and the
+    displacement relative to it, resampling on an analysis grid that sticks out of the FE grid."""
+    sys.path.insert(0, os.path.join(REF, "rb"))
+    import rbsim as RB                   # noqa: E402
+    P = synth.hindfoot_problem(24, 18, 16, h=3.0, seed=1)
+    g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    U, info, R = RSF.solve_cn(g, P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"],
+                              P["extra"], P["node_groups"], tol=1e-10, maxiter=800)
+    cells = np.flatnonzero(P["active"])
+    sig, vm, eps = RSF.cell_stress_cn(g, P["lam"], P["mu"], U, cells, P["cn"])
+    VM = np.zeros(g.ncell, np.float32); VM[cells] = vm
+    SIG = np.zeros((g.ncell, 6), np.float32); SIG[cells] = sig
+    rng = np.random.default_rng(21)
+    nlab = 7
+    lab = rng.integers(0, nlab, g.ncell).astype(np.int32)
+    part = P["part"].astype(np.int32)
+    out = dict(xe=g.xe, ye=g.ye, ze=g.ze, lam=P["lam"], mu=P["mu"], active=P["active"], cn=P["cn"], orig=P["orig"],
+               U=U, VM=VM, SIG=SIG, lab=lab, part=part, nlab=nlab)
+    for target in (1, 2):
+        F, pres = region_forces_ref(g, P["lam"], P["mu"], U, P["cn"], P["active"], part, lab, nlab, target)
+        out[f"F{target}"] = F
+        out[f"present{target}"] = pres
+    xyz = g.node_xyz[P["orig"]]
+    nodes = np.unique(P["cn"][cells[part[cells] == 1]].ravel())
+    t, w, c = RB.rigid_fit(xyz[nodes], np.nan_to_num(U[nodes]))
+    Urel = np.nan_to_num(U) - (t[None, :] + np.cross(w[None, :], xyz - c[None, :]))
+    out.update(fit_nodes=nodes, fit_t=t, fit_w=w, fit_c=c, Urel=Urel)
+    gm = RS.Grid(np.arange(-4.0, 80.0, 5.0), np.arange(-3.0, 60.0, 5.0), np.arange(2.0, 52.0, 5.0))
+    o = dict(g=g, cn=P["cn"], active=P["active"], VM=VM, SIG=SIG)
+    vm_c, u_c, frac = RB.sample_fe(o, gm, Urel, sub=2)
+    out.update(ml_xe=gm.xe, ml_ye=gm.ye, ml_ze=gm.ze, vm_c=vm_c, u_c=u_c, frac=frac, sig_c=RB.sample_fe.sig)
+    out["u_nodes"] = RB.sample_nodes(o, gm, Urel)
+    save("post", **out)
+
+
 def block_solves():
     P = synth.block_problem(12, 10, 8, h=1.0, seed=2)
     g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
@@ -147,8 +206,7 @@ def patch():
 
 
 if __name__ == "__main__":
-    elements()
-    split_cases()
-    hindfoot_solve()
-    block_solves()
-    patch()
+    fixtures = dict(elements=elements, split=split_cases, hindfoot=hindfoot_solve, block=block_solves, patch=patch,
+                    post=post)
+    for name in (sys.argv[1:] or list(fixtures)):
+        fixtures[name]()

@@ -76,3 +76,12 @@ def test_engine_without_gpu_fails_loudly():
     with pytest.raises(RuntimeError, match="CUDA"):
         engine.solve_cn(g, np.ones(8), np.ones(8), np.ones(8, bool), np.zeros((8, 8), np.int64), np.arange(27),
                         (np.zeros(0, np.int64), np.zeros(0)), [])
+
+
+def test_every_export_has_argtypes():
+    """Integer arguments past the sixth travel on the stack: without argtypes ctypes would pass a 32-bit int
+    into a 64-bit slot.  Every binding declares its argument types."""
+    lib = _lib.load()
+    for name in _lib.EXPORTS:
+        assert getattr(lib, name).argtypes is not None, name
+    assert len(lib.feb_sample_cells.argtypes) == 24

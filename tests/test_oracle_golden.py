@@ -143,3 +143,25 @@ def test_oracle_patch(golden):
     sig, vm, _ = O.cell_stress(g, lam, mu, U, np.arange(g.ncell))
     np.testing.assert_allclose(sig, z["sig"], rtol=0, atol=1e-9)
     assert abs(np.nanmin(U[:, 2]) + 10.0 / float(z["E"])) < 1e-8
+
+
+def test_oracle_post_processing(golden):
+    """Region forces, rigid fit, relative displacement and both resamplings of the oracle against the
+    reference's own outputs (rb/rbfe.py:194-213, rb/rbsim.py:99-161)."""
+    z = golden("post")
+    g = O.OGrid(z["xe"], z["ye"], z["ze"])
+    for t in (1, 2):
+        F, p = O.region_forces(g, z["lam"], z["mu"], z["U"], z["cn"], z["active"], z["part"], z["lab"], int(z["nlab"]), t)
+        np.testing.assert_allclose(F, z[f"F{t}"], rtol=0, atol=1e-12 * np.abs(z[f"F{t}"]).max())
+        assert (p == z[f"present{t}"]).all()
+    xyz = g.node_xyz[z["orig"]]
+    nodes = z["fit_nodes"]
+    t, w, c = O.rigid_fit(xyz[nodes], np.nan_to_num(z["U"][nodes]))
+    for a, key in ((t, "fit_t"), (w, "fit_w"), (c, "fit_c")):
+        np.testing.assert_allclose(a, z[key], rtol=1e-12, atol=1e-15)
+    np.testing.assert_array_equal(O.relative_displacement(xyz, z["U"], t, w, c), z["Urel"])
+    vm, u, fr, sg = O.sample_fe(g, z["cn"], z["active"], z["VM"], z["SIG"], z["Urel"], (z["ml_xe"], z["ml_ye"], z["ml_ze"]))
+    for a, key in ((vm, "vm_c"), (u, "u_c"), (fr, "frac"), (sg, "sig_c")):
+        np.testing.assert_array_equal(a, z[key])
+    gm = O.OGrid(z["ml_xe"], z["ml_ye"], z["ml_ze"])
+    np.testing.assert_array_equal(O.sample_nodes(g, z["cn"], z["active"], z["Urel"], gm.node_xyz), z["u_nodes"])
