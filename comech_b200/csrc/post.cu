@@ -208,6 +208,119 @@ __global__ void k_sample_cells(Geom G, int mx, int my, int mz, int sub, const in
   frac_out[e] = float((double)okc / ((double)sub * sub * sub));
 }
 
+// Exact Euclidean feature transform over cell indices (nearest active cell of every cell), separable in the
+// manner of Maurer, Qi and Raghavan (2003): one pass per axis in the order x, y, z.  Along each line the lower
+// envelope of the parabolas g_s + (p - s)^2 of the candidate sites s is built on a stack (a site is dropped when
+// the envelope test is positive), then every position takes the first site of minimal distance: ties go to the
+// lower index, as scipy.ndimage.distance_transform_edt resolves them.  One thread per line; the stack (site
+// position, partial distance and the site's feature coordinates) lives in global scratch, one slot per cell.
+//   pass 0 (x lines, fixed j k): FI = i of the nearest active cell on the line
+//   pass 1 (y lines, fixed i k): FI, FJ of the nearest active cell in the x-y plane, g = (FI - i)^2
+//   pass 2 (z lines, fixed i j): ft = cell id of the nearest active cell, g = (FI - i)^2 + (FJ - j)^2
+// "none" is -1 throughout (a grid without active cells gives ft = -1 everywhere).
+__global__ void k_ft_pass(int pass, int nx, int ny, int nz, const uint8_t* __restrict__ active,
+                          int32_t* __restrict__ FI, int32_t* __restrict__ FJ, int32_t* __restrict__ ft,
+                          int32_t* __restrict__ sp, int64_t* __restrict__ sg, int32_t* __restrict__ sa,
+                          int32_t* __restrict__ sb) {
+  const int64_t line = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int n = pass == 0 ? nx : (pass == 1 ? ny : nz);
+  const int64_t nlines = pass == 0 ? (int64_t)ny * nz : (pass == 1 ? (int64_t)nx * nz : (int64_t)nx * ny);
+  if (line >= nlines) return;
+  const int a = int(pass == 2 ? line / ny : line / nz);   // pass 0: j; pass 1: i; pass 2: i
+  const int b = int(pass == 2 ? line % ny : line % nz);   // pass 0: k; pass 1: k; pass 2: j
+  auto cell = [&](int p) -> int64_t {
+    if (pass == 0) return ((int64_t)p * ny + a) * nz + b;
+    if (pass == 1) return ((int64_t)a * ny + p) * nz + b;
+    return ((int64_t)a * ny + b) * nz + p;
+  };
+  int32_t* S = sp + line * n;
+  int64_t* G = sg + line * n;
+  int32_t* A = sa + line * n;
+  int32_t* B = sb + line * n;
+  int top = 0;
+  for (int p = 0; p < n; ++p) {
+    const int64_t c = cell(p);
+    int32_t fa = p, fb = 0;
+    int64_t gp = 0;
+    if (pass == 0) {
+      if (!active[c]) continue;
+    } else {
+      if (FI[c] < 0) continue;
+      fa = FI[c];
+      const int64_t di = fa - a;
+      gp = di * di;
+      if (pass == 2) {
+        fb = FJ[c];
+        const int64_t dj = fb - b;
+        gp += dj * dj;
+      }
+    }
+    while (top >= 2) {
+      const int64_t u = S[top - 2], v = S[top - 1], w = p;
+      const int64_t x = v - u, y = w - v, z = w - u;
+      if (z * G[top - 1] - y * G[top - 2] - x * gp - x * y * z > 0) --top;
+      else break;
+    }
+    S[top] = p; G[top] = gp; A[top] = fa; B[top] = fb;
+    ++top;
+  }
+  int l = 0;
+  for (int p = 0; p < n; ++p) {
+    const int64_t c = cell(p);
+    if (top == 0) {
+      if (pass == 0) FI[c] = -1;
+      else if (pass == 1) { FI[c] = -1; FJ[c] = -1; }
+      else ft[c] = -1;
+      continue;
+    }
+    while (l < top - 1) {
+      const int64_t d0 = G[l] + (int64_t)(S[l] - p) * (S[l] - p);
+      const int64_t d1 = G[l + 1] + (int64_t)(S[l + 1] - p) * (S[l + 1] - p);
+      if (d0 > d1) ++l;
+      else break;
+    }
+    if (pass == 0) FI[c] = S[l];
+    else if (pass == 1) { FI[c] = A[l]; FJ[c] = S[l]; }
+    else ft[c] = (int32_t)(((int64_t)A[l] * ny + B[l]) * nz + S[l]);
+  }
+}
+
+// Relative displacement at analysis-grid nodes (x fastest): the node's FE cell from per-axis indices, replaced
+// by its nearest active cell (ft); local coordinates clamped to [0, 1]; trilinear in that cell
+// (rb/rbsim.py:141-161).
+__global__ void k_sample_nodes(Geom G, int mx1, int my1, int mz1, const int32_t* __restrict__ ix,
+                               const double* __restrict__ px, const int32_t* __restrict__ iy,
+                               const double* __restrict__ py, const int32_t* __restrict__ iz,
+                               const double* __restrict__ pz, const int32_t* __restrict__ ft,
+                               const int64_t* __restrict__ cn, const double* __restrict__ Urel, float* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)mx1 * my1 * mz1) return;
+  const int a = int(e % mx1), b = int((e / mx1) % my1), c = int(e / ((int64_t)mx1 * my1));
+  const int64_t near = ft[((int64_t)ix[a] * G.ny + iy[b]) * G.nz + iz[c]];
+  if (near < 0) {
+    out[3 * e] = out[3 * e + 1] = out[3 * e + 2] = 0.f;
+    return;
+  }
+  int64_t nd[8];
+  int ci, cj, ck;
+  cell_of(G, near, cn, nd, ci, cj, ck);
+  const double tx = fmin(fmax((px[a] - G.xe[ci]) / (G.xe[ci + 1] - G.xe[ci]), 0.0), 1.0);
+  const double ty = fmin(fmax((py[b] - G.ye[cj]) / (G.ye[cj + 1] - G.ye[cj]), 0.0), 1.0);
+  const double tz = fmin(fmax((pz[c] - G.ze[ck]) / (G.ze[ck + 1] - G.ze[ck]), 0.0), 1.0);
+  double u[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    const double w = ((l & 1) ? tx : 1.0 - tx) * (((l >> 1) & 1) ? ty : 1.0 - ty) * (((l >> 2) & 1) ? tz : 1.0 - tz);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double v = Urel[3 * nd[l] + q];
+      u[q] += w * (isnan(v) ? 0.0 : v);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) out[3 * e + q] = float(u[q]);
+}
+
 struct DevGeom {
   Geom G{};
   double* buf = nullptr;
@@ -344,6 +457,51 @@ extern "C" int feb_sample_cells(const FebGrid* grid, int32_t mx, int32_t my, int
   const int64_t n = (int64_t)mx * my * mz;
   k_sample_cells<<<div_up(n, kThreads), kThreads, 0, s>>>(D.G, mx, my, mz, sub, ix, tx, inx, iy, ty, iny, iz, tz, inz,
                                                          cn, active, Urel, VM, SIG, vm_out, u_out, frac_out, sig_out);
+  note_launch();
+  FEB_CUDA(cudaGetLastError());
+  FEB_CUDA(cudaFreeAsync(D.buf, s));
+  return FEB_OK;
+}
+
+extern "C" int feb_nearest_active(const FebGrid* grid, const uint8_t* active, int32_t* ft, void* stream) {
+  if (!grid || !active || !ft || grid->nx < 1 || grid->ny < 1 || grid->nz < 1) {
+    set_last_error("feb_nearest_active: bad argument");
+    return FEB_ERR_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nx = grid->nx, ny = grid->ny, nz = grid->nz;
+  const int64_t ncell = (int64_t)nx * ny * nz;
+  int32_t *FI = nullptr, *FJ = nullptr, *sp = nullptr, *sa = nullptr, *sb = nullptr;
+  int64_t* sg = nullptr;
+  FEB_CUDA(cudaMallocAsync((void**)&FI, ncell * sizeof(int32_t), s));
+  FEB_CUDA(cudaMallocAsync((void**)&FJ, ncell * sizeof(int32_t), s));
+  FEB_CUDA(cudaMallocAsync((void**)&sp, ncell * sizeof(int32_t), s));
+  FEB_CUDA(cudaMallocAsync((void**)&sa, ncell * sizeof(int32_t), s));
+  FEB_CUDA(cudaMallocAsync((void**)&sb, ncell * sizeof(int32_t), s));
+  FEB_CUDA(cudaMallocAsync((void**)&sg, ncell * sizeof(int64_t), s));
+  const int64_t lines[3] = {(int64_t)ny * nz, (int64_t)nx * nz, (int64_t)nx * ny};
+  for (int pass = 0; pass < 3; ++pass) {
+    k_ft_pass<<<div_up(lines[pass], 128), 128, 0, s>>>(pass, nx, ny, nz, active, FI, FJ, ft, sp, sg, sa, sb);
+    note_launch();
+  }
+  FEB_CUDA(cudaGetLastError());
+  for (void* p : {(void*)FI, (void*)FJ, (void*)sp, (void*)sa, (void*)sb, (void*)sg}) FEB_CUDA(cudaFreeAsync(p, s));
+  return FEB_OK;
+}
+
+extern "C" int feb_sample_nodes(const FebGrid* grid, int32_t mx1, int32_t my1, int32_t mz1, const int32_t* ix,
+                                const double* px, const int32_t* iy, const double* py, const int32_t* iz,
+                                const double* pz, const int32_t* ft, const int64_t* cn, const double* Urel, float* out,
+                                void* stream) {
+  if (!grid || mx1 < 1 || my1 < 1 || mz1 < 1 || !ix || !px || !iy || !py || !iz || !pz || !ft || !Urel || !out) {
+    set_last_error("feb_sample_nodes: bad argument");
+    return FEB_ERR_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  DevGeom D;
+  FEB_TRY(make_dev_geom(grid, D, s));
+  const int64_t n = (int64_t)mx1 * my1 * mz1;
+  k_sample_nodes<<<div_up(n, kThreads), kThreads, 0, s>>>(D.G, mx1, my1, mz1, ix, px, iy, py, iz, pz, ft, cn, Urel, out);
   note_launch();
   FEB_CUDA(cudaGetLastError());
   FEB_CUDA(cudaFreeAsync(D.buf, s));

@@ -5,6 +5,8 @@
 * ``rigid_fit``                        -- rb/rbsim.py:99-107
 * ``relative_displacement``            -- the displacement relative to a rigid fit, rb/rbsim.py:183-186
 * ``sample_fe``                        -- rb/rbsim.py:110-138 (also sets ``sample_fe.sig`` like the reference)
+* ``sample_nodes`` / ``nearest_active`` -- rb/rbsim.py:141-161 (nearest active cell by an exact Euclidean
+                                        feature transform on the device)
 
 Inputs are NumPy arrays (or CUDA tensors); the work runs in libfeb200.so.  No CPU fallback.
 """
@@ -125,3 +127,36 @@ def sample_fe(o, grid_ml, Urel, sub=2):
     vm_h, u_h, frac_h, sig_h = _host(vm, u.view(ncm, 3), frac, sig.view(ncm, 6))
     sample_fe.sig = sig_h
     return vm_h, u_h, frac_h
+
+
+def nearest_active(g, active):
+    """Cell id of the nearest active cell of every cell (exact Euclidean feature transform over cell indices,
+    ties as scipy.ndimage.distance_transform_edt; -1 when no cell is active), as a device int32 tensor."""
+    torch = _torch()
+    act = _dev(np.asarray(active, bool).view(np.uint8).ravel(), np.uint8)
+    ft = torch.empty(g.nx * g.ny * g.nz, dtype=torch.int32, device="cuda")
+    gs = _grid_struct(g)
+    _lib.check(_lib.load().feb_nearest_active(C.byref(gs), _ptr(act), _ptr(ft), _stream()))
+    return ft
+
+
+def sample_nodes(o, grid_ml, Urel):
+    """Relative displacement at the nodes of the analysis grid: trilinear in the FE cell that holds the node,
+    or in the nearest active FE cell with clamped local coordinates (rb/rbsim.py:141-161).  float32, node order
+    x fastest."""
+    torch = _torch()
+    g = o["g"]
+    axes = []
+    for fe, ml, n in ((g.xe, grid_ml.xe, g.nx), (g.ye, grid_ml.ye, g.ny), (g.ze, grid_ml.ze, g.nz)):
+        P = np.asarray(ml, np.float64)
+        i = np.clip(np.searchsorted(np.asarray(fe, np.float64), P) - 1, 0, n - 1).astype(np.int32)
+        axes += [_dev(i, np.int32), _dev(P, np.float64)]
+    m1 = [len(e) for e in (grid_ml.xe, grid_ml.ye, grid_ml.ze)]
+    ft = nearest_active(g, o["active"])
+    cn = _dev(np.asarray(o["cn"], np.int64), np.int64) if o.get("cn") is not None else None
+    Ud = _dev(np.asarray(Urel, np.float64).reshape(-1), np.float64)
+    out = torch.empty(3 * m1[0] * m1[1] * m1[2], dtype=torch.float32, device="cuda")
+    gs = _grid_struct(g)
+    _lib.check(_lib.load().feb_sample_nodes(C.byref(gs), *m1, *[_ptr(a) for a in axes], _ptr(ft), _ptr(cn), _ptr(Ud),
+                                            _ptr(out), _stream()))
+    return _host(out.view(-1, 3))

@@ -199,6 +199,20 @@ FEB_API int feb_sample_cells(const FebGrid* grid, int32_t mx, int32_t my, int32_
                              const float* SIG, float* vm_out, float* u_out, float* frac_out, float* sig_out,
                              void* stream);
 
+/* Nearest active cell of every cell (exact Euclidean feature transform over cell indices; ties resolved as
+ * scipy.ndimage.distance_transform_edt resolves them: separable passes x, y, z, the lower index first).
+ * active [dev] ncell flags (cell id z fastest); ft [dev] int32 ncell: cell id of the nearest active cell, -1 when
+ * no cell is active. */
+FEB_API int feb_nearest_active(const FebGrid* grid, const uint8_t* active, int32_t* ft, void* stream);
+
+/* Relative displacement at the nodes of an analysis grid (rb/rbsim.py:141-161): node (a, b, c), x fastest, at
+ * (px[a], py[b], pz[c]) lies in FE cell (ix[a], iy[b], iz[c]); that cell is replaced by its nearest active cell
+ * ft[...] and Urel is interpolated trilinearly there with clamped local coordinates.  Per-axis arrays [dev]
+ * (mx1, my1, mz1 entries); out [dev] float mx1*my1*mz1 x 3. */
+FEB_API int feb_sample_nodes(const FebGrid* grid, int32_t mx1, int32_t my1, int32_t mz1, const int32_t* ix,
+                             const double* px, const int32_t* iy, const double* py, const int32_t* iz, const double* pz,
+                             const int32_t* ft, const int64_t* cn, const double* Urel, float* out, void* stream);
+
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
 

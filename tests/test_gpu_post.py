@@ -53,3 +53,32 @@ def test_sample_fe_matches_reference(golden):
     for a, key in ((vm, "vm_c"), (u, "u_c"), (post.sample_fe.sig, "sig_c")):
         assert a.dtype == np.float32
         np.testing.assert_allclose(a, z[key], rtol=0, atol=ulp * np.abs(z[key]).max())
+
+
+def test_nearest_active_matches_scipy_exactly():
+    """Integer work: the feature transform equals scipy.ndimage.distance_transform_edt's indices, ties
+    included, on random masks of assorted sizes and densities (and a grid without active cells)."""
+    from scipy import ndimage
+    rng = np.random.default_rng(3)
+    for trial in range(25):
+        shape = tuple(int(v) for v in rng.integers(2, 23, 3))
+        act = rng.random(shape) < rng.uniform(0.01, 0.5)
+        if trial == 0:
+            act[...] = False
+        g = Grid(np.arange(shape[0] + 1.0), np.arange(shape[1] + 1.0), np.arange(shape[2] + 1.0))
+        ft = post.nearest_active(g, act.ravel()).cpu().numpy()
+        if not act.any():
+            assert (ft == -1).all()
+            continue
+        _, ind = ndimage.distance_transform_edt(~act, return_indices=True)
+        ref = ((ind[0] * shape[1] + ind[1]) * shape[2] + ind[2]).ravel()
+        np.testing.assert_array_equal(ft, ref)
+
+
+def test_sample_nodes_matches_reference(golden):
+    z, g = _case(golden)
+    gm = Grid(z["ml_xe"], z["ml_ye"], z["ml_ze"])
+    o = dict(g=g, cn=z["cn"], active=z["active"])
+    u = post.sample_nodes(o, gm, z["Urel"])
+    assert u.dtype == np.float32 and u.shape == z["u_nodes"].shape
+    np.testing.assert_allclose(u, z["u_nodes"], rtol=0, atol=2 * np.finfo(np.float32).eps * np.abs(z["u_nodes"]).max())
