@@ -15,11 +15,14 @@ from . import engine
 _SWAPS = {
     "gmg": ("pcg_gmg",),
     "solver": ("solve", "cell_stress"),
-    "splitfe": ("solve_cn", "cell_stress_cn", "element_forces_cn"),
+    "splitfe": ("solve_cn", "cell_stress_cn", "element_forces_cn", "split_connectivity", "split_connectivity_fast"),
 }
 
 
 def _wrap(name, precision):
+    if name.startswith("split_connectivity"):
+        from .split import split_connectivity_device
+        return split_connectivity_device
     fn = getattr(engine, name)
     if precision is None or name not in ("pcg_gmg", "solve", "solve_cn"):
         return fn
@@ -33,13 +36,15 @@ def _wrap(name, precision):
 
 
 def install(gmg=None, solver=None, splitfe=None, precision=None):
-    """Replace the solve entry points of the given reference modules; ``precision`` ('fp64', 'mixed',
-    'refine') becomes the default of the replaced solves."""
+    """Replace the solve entry points of the given reference modules (those the module has); ``precision``
+    ('fp64', 'mixed', 'refine') becomes the default of the replaced solves."""
     mods = {"gmg": gmg, "solver": solver, "splitfe": splitfe}
     for key, mod in mods.items():
         if mod is None:
             continue
         for name in _SWAPS[key]:
+            if not hasattr(mod, name):           # an older module without this entry point
+                continue
             if not hasattr(mod, "_%s_cpu" % name):
                 setattr(mod, "_%s_cpu" % name, getattr(mod, name))
             setattr(mod, name, _wrap(name, precision))

@@ -60,3 +60,29 @@ def split_connectivity(g, active, part, bone_share):
     take = nid >= 0
     cn[cell[take], ll[take]] = nid[take]
     return cn, orig, int(split.sum())
+
+
+def split_connectivity_device(g, active, part, bone_share):
+    """The same connectivity computed on the device (libfeb200 ``feb_split_connectivity``): returns
+    (cn (ncell, 8) int64, orig (nnew,) int64, number of split grid nodes), equal bit for bit to
+    ``split_connectivity`` and to the reference's."""
+    import ctypes as C
+    from . import _lib
+    from .engine import _dev, _grid_struct, _host, _ptr, _stream, _torch
+    torch = _torch()
+    share = np.asarray(bone_share, np.float64)
+    nb = share.shape[1]
+    act = _dev(np.asarray(active, bool).view(np.uint8).ravel(), np.uint8)
+    pt = _dev(np.asarray(part).ravel(), np.int32)
+    sh = _dev(share.ravel(), np.float64)
+    gs = _grid_struct(g)
+    lib = _lib.load()
+    ntot, nspl = C.c_int64(), C.c_int64()
+    _lib.check(lib.feb_split_connectivity(C.byref(gs), _ptr(act), _ptr(pt), _ptr(sh), nb, None, None, 0, C.byref(ntot),
+                                          C.byref(nspl), _stream()))
+    cn = torch.empty(8 * g.ncell, dtype=torch.int64, device="cuda")
+    orig = torch.empty(ntot.value, dtype=torch.int64, device="cuda")
+    _lib.check(lib.feb_split_connectivity(C.byref(gs), _ptr(act), _ptr(pt), _ptr(sh), nb, _ptr(cn), _ptr(orig),
+                                          ntot.value, C.byref(ntot), C.byref(nspl), _stream()))
+    cn_h, orig_h = _host(cn.view(g.ncell, 8), orig)
+    return cn_h, orig_h, int(nspl.value)

@@ -213,6 +213,14 @@ FEB_API int feb_sample_nodes(const FebGrid* grid, int32_t mx1, int32_t my1, int3
                              const double* px, const int32_t* iy, const double* py, const int32_t* iz, const double* pz,
                              const int32_t* ft, const int64_t* cn, const double* Urel, float* out, void* stream);
 
+/* Split-node connectivity between bones (rb/splitfe.py:261-305 == :17-55), bit for bit.  active [dev] ncell
+ * flags, part [dev] int32 ncell (0 joint / soft, 1..nb-1 bone), share [dev] float64 ncell x nb (bone shares of
+ * the cells).  Call once with cn = orig = NULL for the sizes: *nnode_total (grid nodes + copies) and *nsplit
+ * (split grid nodes); then with cn [dev] ncell x 8 and orig [dev] of orig_cap >= *nnode_total entries. */
+FEB_API int feb_split_connectivity(const FebGrid* grid, const uint8_t* active, const int32_t* part, const double* share,
+                                   int32_t nb, int64_t* cn, int64_t* orig, int64_t orig_cap, int64_t* nnode_total,
+                                   int64_t* nsplit, void* stream);
+
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
 

@@ -292,3 +292,24 @@ def test_plugin_swaps_reference_style_modules(golden):
     assert info["flag"] == 0 and rel(U[ok], z["U"][ok]) < 1e-6
     plugin.uninstall(splitfe=mod)
     assert mod.solve_cn is sentinel and not hasattr(mod, "_solve_cn_cpu")
+    # a module with the split-connectivity entry points gets the device versions (bit-exact)
+    zs = golden("split")
+    mod.split_connectivity_fast = sentinel
+    plugin.install(splitfe=mod)
+    gs = Grid(zs["h_edges_x"], zs["h_edges_y"], zs["h_edges_z"])
+    cn, orig, ns = mod.split_connectivity_fast(gs, zs["h_active"], zs["h_part"], zs["h_share"])
+    assert (cn == zs["h_cn"]).all() and (orig == zs["h_orig"]).all() and ns == int(zs["h_nsplit"])
+    plugin.uninstall(splitfe=mod)
+    assert mod.split_connectivity_fast is sentinel
+
+
+@pytest.mark.parametrize("case", ["h", "r"])
+def test_split_connectivity_on_device_bit_exact(golden, case):
+    from comech_b200.split import split_connectivity_device
+    z = golden("split")
+    g = Grid(*[z[f"{case}_edges_{a}"] for a in "xyz"])
+    cn, orig, ns = split_connectivity_device(g, z[f"{case}_active"], z[f"{case}_part"], z[f"{case}_share"])
+    assert cn.dtype == np.int64 and orig.dtype == np.int64
+    assert (cn == z[f"{case}_cn"]).all()
+    assert (orig == z[f"{case}_orig"]).all()
+    assert ns == int(z[f"{case}_nsplit"])
