@@ -19,7 +19,8 @@ EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_sol
            "feb_export_solution", "feb_used_nodes", "feb_destroy", "feb_accumulate_nodal", "feb_cell_stress",
            "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_launch_count", "feb_last_error",
            "feb_region_forces", "feb_rigid_fit", "feb_relative_displacement", "feb_sample_cells",
-           "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity"]
+           "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
+           "feb_mix_materials"]
 
 
 class FebGrid(C.Structure):
@@ -89,6 +90,7 @@ def load():
     lib.feb_sample_nodes.argtypes = [C.POINTER(FebGrid)] + [C.c_int32] * 3 + [P] * 6 + [P] * 4 + [P]
     lib.feb_split_connectivity.argtypes = [C.POINTER(FebGrid), P, P, P, C.c_int32, P, P, C.c_int64,
                                            C.POINTER(C.c_int64), C.POINTER(C.c_int64), P]
+    lib.feb_mix_materials.argtypes = [C.c_int32] * 4 + [P, C.c_int32] + [P] * 11
     lib.feb_launch_count.argtypes = []
     lib.feb_launch_count.restype = C.c_int64
     lib.feb_last_error.argtypes = []

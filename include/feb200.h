@@ -221,6 +221,16 @@ FEB_API int feb_split_connectivity(const FebGrid* grid, const uint8_t* active, c
                                    int32_t nb, int64_t* cn, int64_t* orig, int64_t orig_cap, int64_t* nnode_total,
                                    int64_t* nsplit, void* stream);
 
+/* Material mixing of the engine's cells (rb/rbfe.py:75-134), bit for bit: L [dev] int32 ncell x ns3 sub-voxel body
+ * labels (cell id z fastest); body_class / body_group [dev] int8 per body id (nbody entries): class 0..9 (void
+ * cortical cancellous cartilage fascia soft plate fibrous fat gap) and bone group (0 none, 1..64); class_lam,
+ * class_mu, class_M [host] 10 per-class lambda, mu, lambda + 2 mu.  Outputs [dev]: F ncell x 10 class fractions,
+ * E, nu (float64), active and joint-cell flags (uint8). */
+FEB_API int feb_mix_materials(int32_t nx, int32_t ny, int32_t nz, int32_t ns3, const int32_t* L, int32_t nbody,
+                              const int8_t* body_class, const int8_t* body_group, const double* class_lam,
+                              const double* class_mu, const double* class_M, double* F, double* E, double* nu,
+                              uint8_t* active, uint8_t* ser, void* stream);
+
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
 

@@ -613,3 +613,76 @@ def sample_nodes(g, cn, active, Urel, ml_node_xyz):
         w = np.where(a, tx, 1 - tx) * np.where(b, ty, 1 - ty) * np.where(d, tz, 1 - tz)
         u += w[:, None] * np.nan_to_num(Urel[cn[c, l]])
     return u.astype(np.float32)
+
+
+# ------------------------------------------------------------------------------------------ material mixing
+MIX_CLASSES = ["void", "cortical", "cancellous", "cartilage", "fascia", "soft", "plate", "fibrous", "fat", "gap"]
+MIX_MAT = {"cortical": (7300.0, 0.3), "cancellous": (100.0, 0.3), "cartilage": (10.0, 0.4), "fascia": (350.0, 0.4),
+           "soft": (1.15, 0.49), "plate": (17000.0, 0.1), "fibrous": (60.0, 0.4), "fat": (1.15, 0.45),
+           "gap": (0.01, 0.3)}
+
+
+def mix_materials(cls, L, shape, groups, cart_E=10.0, nu_soft=0.49):
+    """Class fractions and constrained-modulus mixing of the engine (rb/rbfe.py:75-134).  cls: body -> class,
+    L: ncell x ns^3 body labels, groups: bone body -> group id.  Returns (E, nu, active, F, ser)."""
+    from scipy import ndimage
+    nb = max(max(cls), int(L.max()))
+    lut = np.zeros(nb + 1, np.int16)
+    for b, c in cls.items():
+        lut[b] = c
+    C = lut[L]
+    F = np.stack([(C == k).mean(1) for k in range(len(MIX_CLASSES))], 1).astype(np.float64)
+    mat = dict(MIX_MAT)
+    mat["cartilage"] = (cart_E, 0.4)
+    mat["soft"] = (1.15, nu_soft)
+    E_ = np.array([1.0] + [mat[c][0] for c in MIX_CLASSES[1:]])
+    nu_ = np.array([0.3] + [mat[c][1] for c in MIX_CLASSES[1:]])
+    lam_i = E_ * nu_ / ((1 + nu_) * (1 - 2 * nu_))
+    mu_i = E_ / (2 * (1 + nu_))
+    H, LAY, SOFTC, GAPC = [1, 2, 4], [3, 7], [5, 8], [9]
+    PH = H + LAY + SOFTC
+    occ = F[:, PH].sum(1)
+    hard, lay, fgap = F[:, H].sum(1), F[:, LAY].sum(1), F[:, GAPC].sum(1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lamV = (F[:, PH] * lam_i[PH]).sum(1) / occ
+        muV = (F[:, PH] * mu_i[PH]).sum(1) / occ
+        lam_h = (F[:, H] * lam_i[H]).sum(1) / hard
+        mu_h = (F[:, H] * mu_i[H]).sum(1) / hard
+        M_h, G_h = lam_h + 2 * mu_h, mu_h
+        hM = np.where(hard > 0, hard / M_h, 0.0)
+        hG = np.where(hard > 0, hard / G_h, 0.0)
+        Mi = lam_i + 2 * mu_i
+        gapM = (F[:, GAPC] / Mi[GAPC]).sum(1)
+        gapG = (F[:, GAPC] / mu_i[GAPC]).sum(1)
+        layM = (F[:, LAY] / Mi[LAY]).sum(1) + gapM
+        layG = (F[:, LAY] / mu_i[LAY]).sum(1) + gapG
+        fch = lay + hard + fgap
+        occ_g = occ + fgap
+        M_ch, G_ch = fch / (layM + hM), fch / (layG + hG)
+        lam_soft = (F[:, SOFTC] * lam_i[SOFTC]).sum(1)
+        mu_soft = (F[:, SOFTC] * mu_i[SOFTC]).sum(1)
+        lam_c = (fch * (M_ch - 2 * G_ch) + lam_soft) / occ_g
+        mu_c = (fch * G_ch + mu_soft) / occ_g
+        softM = (F[:, SOFTC] / Mi[SOFTC]).sum(1)
+        softG = (F[:, SOFTC] / mu_i[SOFTC]).sum(1)
+        M_s = occ_g / (softM + hM + gapM)
+        G_s = occ_g / (softG + hG + gapG)
+        lam_s, mu_s = M_s - 2 * G_s, G_s
+    lutg = np.zeros(nb + 1, np.int16)
+    for b, k in groups.items():
+        lutg[b] = k
+    Gb = lutg[L]
+    count = np.zeros(len(L), np.int16)
+    for k in np.unique(Gb[Gb > 0]):
+        count += ndimage.binary_dilation((Gb == k).any(1).reshape(shape), np.ones((3, 3, 3), bool)).ravel()
+    cart = lay > 0
+    ser = cart | (count >= 2)
+    lamX = np.where(cart, lam_c, np.where(ser, lam_s, lamV))
+    muX = np.where(cart, mu_c, np.where(ser, mu_s, muV))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        E = muX * (3 * lamX + 2 * muX) / (lamX + muX)
+        nu = lamX / (2 * (lamX + muX))
+    active = np.where(ser, occ > 0.15, occ >= 0.5)
+    E = np.where(active, E, 1.0)
+    nu = np.where(active, np.clip(nu, 0.0, 0.4995), 0.3)
+    return np.nan_to_num(E, nan=1.0), np.nan_to_num(nu, nan=0.3), active, F, ser

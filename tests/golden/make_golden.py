@@ -166,6 +166,48 @@ def post():
     save("post", **out)
 
 
+def materials_case():
+    """Material mixing of rb/rbfe.py:75-134 on a seeded sub-voxel label raster: bone bodies of the atlas
+    roles (cortical / cancellous), joint cartilages, coalition / fibrous / fat / fusion / gap bodies, soft
+    tissue and fascia, in blobs so that joint cells (two bone groups within one cell) occur."""
+    sys.path.insert(0, os.path.join(REF, "rb"))
+    import rbfe as RF                    # noqa: E402
+    import rbgeom as RG                  # noqa: E402
+    rng = np.random.default_rng(31)
+    nx, ny, nz, ns = 14, 11, 9, 3
+    bodies = [1, 53, 2, 52, 40, 45, 43, 49, 3, 54, 4, 13, 70, 71] + list(RG.CART.values()) + \
+        [RG.SOFT, RG.FASCIA, RG.COAL, RG.FIB, RG.INTERP, RG.FUSE, RG.GAP]
+    cls = {1: 1, 53: 2, 2: 1, 52: 2, 40: 1, 45: 2, 43: 1, 49: 2, 3: 1, 54: 2, 4: 1, 13: 2, 70: 1, 71: 2,
+           RG.SOFT: 5, RG.FASCIA: 4, RG.COAL: 1, RG.FIB: 7, RG.INTERP: 8, RG.FUSE: 1, RG.GAP: 9}
+    for c in RG.CART.values():
+        cls[c] = 3
+    # blobs on the sub-voxel grid, void elsewhere
+    sx, sy, sz = nx * ns, ny * ns, nz * ns
+    lab = np.zeros((sx, sy, sz), np.int64)
+    X, Y, Z = np.meshgrid(np.arange(sx), np.arange(sy), np.arange(sz), indexing="ij")
+    for _ in range(60):
+        b = bodies[rng.integers(len(bodies))]
+        c = rng.uniform(0, 1, 3) * (sx, sy, sz)
+        r = rng.uniform(2, 9)
+        lab[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 < r * r] = b
+    # cell sample order: cell id (z fastest), then the sub-voxels (z fastest)
+    L = lab.reshape(nx, ns, ny, ns, nz, ns).transpose(0, 2, 4, 1, 3, 5).reshape(nx * ny * nz, ns ** 3)
+    V = dict(cls={str(k): v for k, v in cls.items()}, L=L, xe=np.arange(nx + 1.0), ye=np.arange(ny + 1.0),
+             ze=np.arange(nz + 1.0))
+    out = dict(L=L, nx=nx, ny=ny, nz=nz, cls_body=np.array(sorted(cls)), cls_class=np.array([cls[b] for b in sorted(cls)]))
+    for name, kw in (("a", {}), ("b", dict(cart_E=3.0, nu_soft=0.45))):
+        E, nu, active, F, ser = RF.materials(V, RF.ROLES, **kw)
+        out.update({f"{name}_E": E, f"{name}_nu": nu, f"{name}_active": active, f"{name}_F": F, f"{name}_ser": ser})
+    out["b_cart_E"] = 3.0
+    out["b_nu_soft"] = 0.45
+    names = list(RF.ROLES["bones"])
+    out["role_names"] = np.array(names)
+    out["role_len"] = np.array([len(RF.ROLES["bones"][n]) for n in names])
+    out["role_bodies"] = np.concatenate([np.array(RF.ROLES["bones"][n]) for n in names])
+    out["role_bonded_extra"] = np.array(RF.ROLES["bonded_extra"])
+    save("materials", **out)
+
+
 def block_solves():
     P = synth.block_problem(12, 10, 8, h=1.0, seed=2)
     g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
@@ -207,6 +249,6 @@ def patch():
 
 if __name__ == "__main__":
     fixtures = dict(elements=elements, split=split_cases, hindfoot=hindfoot_solve, block=block_solves, patch=patch,
-                    post=post)
+                    post=post, materials=materials_case)
     for name in (sys.argv[1:] or list(fixtures)):
         fixtures[name]()

@@ -82,3 +82,21 @@ def test_sample_nodes_matches_reference(golden):
     u = post.sample_nodes(o, gm, z["Urel"])
     assert u.dtype == np.float32 and u.shape == z["u_nodes"].shape
     np.testing.assert_allclose(u, z["u_nodes"], rtol=0, atol=2 * np.finfo(np.float32).eps * np.abs(z["u_nodes"]).max())
+
+
+def test_material_mixing_on_device_bit_exact(golden):
+    """rb/rbfe.py:75-134 on the device: class fractions, joint cells, E, nu and active flags equal the
+    reference's bit for bit (two parameter sets)."""
+    from comech_b200.materials import materials
+    z = golden("materials")
+    names = [str(n) for n in z["role_names"]]
+    bodies = np.split(z["role_bodies"], np.cumsum(z["role_len"])[:-1])
+    roles = {"bones": {n: tuple(int(b) for b in bb) for n, bb in zip(names, bodies)},
+             "bonded_extra": [int(b) for b in z["role_bonded_extra"]]}
+    nx, ny, nz = int(z["nx"]), int(z["ny"]), int(z["nz"])
+    V = dict(cls={str(int(b)): int(c) for b, c in zip(z["cls_body"], z["cls_class"])}, L=z["L"],
+             xe=np.arange(nx + 1.0), ye=np.arange(ny + 1.0), ze=np.arange(nz + 1.0))
+    for name, kw in (("a", {}), ("b", dict(cart_E=float(z["b_cart_E"]), nu_soft=float(z["b_nu_soft"])))):
+        E, nu, active, F, ser = materials(V, roles, **kw)
+        for a, key in ((E, "E"), (nu, "nu"), (active, "active"), (F, "F"), (ser, "ser")):
+            np.testing.assert_array_equal(a, z[f"{name}_{key}"], err_msg=key)

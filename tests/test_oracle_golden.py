@@ -165,3 +165,23 @@ def test_oracle_post_processing(golden):
         np.testing.assert_array_equal(a, z[key])
     gm = O.OGrid(z["ml_xe"], z["ml_ye"], z["ml_ze"])
     np.testing.assert_array_equal(O.sample_nodes(g, z["cn"], z["active"], z["Urel"], gm.node_xyz), z["u_nodes"])
+
+
+def _roles(z):
+    names = [str(n) for n in z["role_names"]]
+    bodies = np.split(z["role_bodies"], np.cumsum(z["role_len"])[:-1])
+    return {"bones": {n: tuple(int(b) for b in bb) for n, bb in zip(names, bodies)},
+            "bonded_extra": [int(b) for b in z["role_bonded_extra"]]}
+
+
+def test_oracle_material_mixing(golden):
+    """Material mixing of the oracle equals the reference's rb/rbfe.py:75-134, bit for bit."""
+    from comech_b200.materials import bone_groups
+    z = golden("materials")
+    cls = {int(b): int(c) for b, c in zip(z["cls_body"], z["cls_class"])}
+    groups, _ = bone_groups(cls, _roles(z))
+    shape = (int(z["nx"]), int(z["ny"]), int(z["nz"]))
+    for name, kw in (("a", {}), ("b", dict(cart_E=float(z["b_cart_E"]), nu_soft=float(z["b_nu_soft"])))):
+        E, nu, active, F, ser = O.mix_materials(cls, z["L"], shape, groups, **kw)
+        for a, key in ((E, "E"), (nu, "nu"), (active, "active"), (F, "F"), (ser, "ser")):
+            np.testing.assert_array_equal(a, z[f"{name}_{key}"])
