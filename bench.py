@@ -385,6 +385,85 @@ def run_profile(args):
     return out
 
 
+def run_post(args):
+    """The rows around the solve on the workload: region forces, rigid fit, relative displacement, resampling on a
+    2-mm analysis grid, split connectivity and material mixing.  Device: the public calls from host arrays (inputs
+    uploaded and results downloaded inside the timed region), median of 5 after one warm-up; CPU: the oracle on
+    the same inputs, one run each."""
+    import torch
+    from comech_b200 import _lib, engine, materials as MX, post
+    from comech_b200.grid import Grid
+    from comech_b200.split import split_connectivity_device
+    from oracle import fe_oracle as O
+    P = make_problem(0)
+    g = P["grid"]
+    d = device_inputs(P)
+    U, _, _ = device_solve(P, d, "mixed")
+    sig, vm, _ = engine._stress(g, _lib.MAT_ISO_SRI, d["mat"], U, d["cells"], d["cn"], True, to_host=True)
+    Uh = U.view(-1, 3).cpu().numpy()
+    cells = np.flatnonzero(P["active"])
+    VM = np.zeros(g.ncell, np.float32); VM[cells] = vm
+    SIG = np.zeros((g.ncell, 6), np.float32); SIG[cells] = sig
+    rng = np.random.default_rng(5)
+    lab = rng.integers(0, 7, g.ncell).astype(np.int32)
+    part = P["part"].astype(np.int32)
+    og = O.OGrid(g.xe, g.ye, g.ze)
+    xyz = og.node_xyz[P["orig"]]
+    nodes = np.unique(P["cn"][cells[part[cells] == 1]].ravel())
+    gm = Grid(np.arange(g.xe[0] - 4.0, g.xe[-1] + 4.01, 2.0), np.arange(g.ye[0] - 4.0, g.ye[-1] + 4.01, 2.0),
+              np.arange(g.ze[0] - 4.0, g.ze[-1] + 4.01, 2.0))
+    ogm = O.OGrid(gm.xe, gm.ye, gm.ze)
+    t, w, c = O.rigid_fit(xyz[nodes], np.nan_to_num(Uh[nodes]))
+    Urel = O.relative_displacement(xyz, Uh, t, w, c)
+    o = dict(g=g, cn=P["cn"], active=P["active"], VM=VM, SIG=SIG)
+    # sub-voxel body labels (3^3 per cell): the cell's bone (cortical body of its part), soft tissue in joint
+    # cells, void outside; a fifth of the sub-voxels take the label of a neighbouring cell
+    body_of_part = np.array([63, 1, 2, 40, 43, 3, 4])
+    base = np.where(P["active"], body_of_part[np.clip(part, 0, 6)], 0)
+    nbr = np.clip(np.arange(g.ncell)[:, None] + rng.integers(-1, 2, (g.ncell, 27)), 0, g.ncell - 1)
+    L = np.where(rng.random((g.ncell, 27)) < 0.2, base[nbr], base[:, None]).astype(np.int32)
+    cls = {1: 1, 53: 2, 2: 1, 52: 2, 40: 1, 45: 2, 43: 1, 49: 2, 3: 1, 54: 2, 4: 1, 13: 2, 63: 5}
+    roles = {"bones": {"calcaneus": (1, 53), "talus": (2, 52), "fibula": (3, 54), "tibia": (4, 13),
+                       "navicular": (40, 45), "cuboid": (43, 49)}, "bonded_extra": [101, 104]}
+    V = dict(cls={str(k): v for k, v in cls.items()}, L=L, xe=g.xe, ye=g.ye, ze=g.ze)
+    groups, _ = MX.bone_groups(cls, roles)
+    steps = {
+        "region_forces_2_bones": (lambda: [post.region_forces_cn(g, P["lam"], P["mu"], Uh, P["cn"], P["active"], part,
+                                                                 lab, 7, k) for k in (1, 2)],
+                                  lambda: [O.region_forces(og, P["lam"], P["mu"], Uh, P["cn"], P["active"], part, lab,
+                                                           7, k) for k in (1, 2)]),
+        "rigid_fit": (lambda: post.rigid_fit(xyz[nodes], np.nan_to_num(Uh[nodes])),
+                      lambda: O.rigid_fit(xyz[nodes], np.nan_to_num(Uh[nodes]))),
+        "relative_displacement": (lambda: post.relative_displacement(g, P["orig"], Uh, t, w, c),
+                                  lambda: O.relative_displacement(xyz, Uh, t, w, c)),
+        "sample_fe": (lambda: post.sample_fe(o, gm, Urel),
+                      lambda: O.sample_fe(og, P["cn"], P["active"], VM, SIG, Urel, (gm.xe, gm.ye, gm.ze))),
+        "sample_nodes": (lambda: post.sample_nodes(o, gm, Urel),
+                         lambda: O.sample_nodes(og, P["cn"], P["active"], Urel, ogm.node_xyz)),
+        "split_connectivity": (lambda: split_connectivity_device(g, P["active"], part, P["bone_share"]),
+                               lambda: O.split_connectivity(og, P["active"], part, P["bone_share"])),
+        "material_mixing": (lambda: MX.materials(V, roles),
+                            lambda: O.mix_materials(cls, L, (g.nx, g.ny, g.nz), groups)),
+    }
+    gpu_ms, cpu_s = {}, {}
+    for name, (dev_fn, cpu_fn) in steps.items():
+        dev_fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            dev_fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        gpu_ms[name] = round(1e3 * statistics.median(ts), 3)
+        t0 = time.perf_counter()
+        cpu_fn()
+        cpu_s[name] = round(time.perf_counter() - t0, 3)
+    return {"mode": "post", "workload": f"hindfoot {g.nx}x{g.ny}x{g.nz}, analysis grid {gm.nx}x{gm.ny}x{gm.nz} (2 mm)",
+            "gpu_e2e_ms": gpu_ms, "cpu_oracle_s": cpu_s,
+            "speedup": {k: round(cpu_s[k] * 1e3 / max(gpu_ms[k], 1e-6), 1) for k in gpu_ms}}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -420,8 +499,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["full", "solve-once", "ku"], default="full",
-                    help="solve-once / ku: one device solve or a few K.u products of the workload (profiling)")
+    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "post"], default="full",
+                    help="solve-once / ku: one device solve or a few K.u products of the workload (profiling); "
+                         "post: the rows around the solve, device against the CPU oracle")
     ap.add_argument("--size", default=None, help="override the workload grid, e.g. 96x64x56x0.833 (profiling)")
     ap.add_argument("--inner-tol", type=float, default=None, help="refinement: FP32 sweep tolerance")
     ap.add_argument("--use-graphs", type=int, default=None, help="0 direct, 1 graph per iteration, 2 device loop")
@@ -450,6 +530,8 @@ def main():
             dist = tdist
         if args.mode == "full":
             out = run_ours(args, rank, world, dist)
+        elif args.mode == "post":
+            out = run_post(args)
         else:
             out = run_profile(args)
         if dist:
