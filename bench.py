@@ -150,6 +150,8 @@ def device_inputs(P):
     (ln, la, lt), = P["loads"]
     d["l_nodes"] = torch.from_numpy(np.asarray(ln, np.int64)).cuda()
     d["l_vals"] = torch.from_numpy(np.asarray(la, np.float64)[:, None] * lt[None, :]).cuda()
+    d["load_nodes_h"] = np.asarray(ln, np.int64)
+    d["load_z_h"] = np.asarray(la, np.float64) * float(lt[2])
     d["cells"] = torch.from_numpy(np.flatnonzero(P["active"]).astype(np.int64)).cuda()
     fn, fa = P["fixed"]
     d["pen_node"] = np.asarray(fn, np.int64)
@@ -162,8 +164,9 @@ def device_inputs(P):
 SOLVER_OPTIONS = {}
 
 
-def device_solve(P, d, precision, x0=None):
-    """One solve from device-resident inputs (same work as engine.solve_cn + cell_stress_cn)."""
+def device_solve(P, d, precision, x0=None, warm=None):
+    """One solve from device-resident inputs (same work as engine.solve_cn + cell_stress_cn); with ``warm`` (a
+    trained warmnet.WarmNet) the network's prediction is the initial guess, computed inside the step."""
     from comech_b200 import engine, _lib
     g = P["grid"]
     pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
@@ -172,6 +175,10 @@ def device_solve(P, d, precision, x0=None):
     try:
         pr.set_rigid_groups(d["g_nodes"], offsets=d["g_off"])
         f = pr.rhs([(d["l_nodes"], d["l_vals"])])
+        if warm is not None and x0 is None:
+            nc = g.nx * g.ny * g.nz
+            x0 = warm.predict_x0(g, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
+                                 d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
         x, info = pr.solve(f, x0)
         U = pr.export(x)
         sig, vm, eps = engine._stress(g, _lib.MAT_ISO_SRI, d["mat"], U, d["cells"], d["cn"], True, to_host=False)
@@ -207,8 +214,16 @@ def run_ours(args, rank, world, dist):
     d = device_inputs(P)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
     prec = args.precision
+    warm = None
+    if args.warm != "off":
+        from comech_b200 import warmnet
+        try:
+            warm = warmnet.default_net()
+        except RuntimeError:
+            if args.warm == "on":
+                raise
     for _ in range(args.warmup):
-        device_solve(P, d, prec)
+        device_solve(P, d, prec, warm=warm)
     torch.cuda.synchronize()
     # ---------------------------------------------------------------- timed: device-resident inputs
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -221,7 +236,7 @@ def run_ours(args, rank, world, dist):
         for _ in range(args.steps):
             flush_l2(flush)
             ev0.record()
-            U, vm, info = device_solve(P, d, prec)
+            U, vm, info = device_solve(P, d, prec, warm=warm)
             ev1.record()
             torch.cuda.synchronize()
             step_ms.append(ev0.elapsed_time(ev1))
@@ -233,6 +248,7 @@ def run_ours(args, rank, world, dist):
     value = t_total / (args.steps * world)
     mixed_info = info
     U_mixed = U.cpu().numpy()
+    g0 = P["grid"]
     # ---------------------------------------------------------------- plain FP64 GMG-PCG, same inputs
     device_solve(P, d, "fp64")
     torch.cuda.synchronize()
@@ -246,6 +262,31 @@ def run_ours(args, rank, world, dist):
         fp64_ms.append(ev0.elapsed_time(ev1))
     U64h = U64.cpu().numpy()
     ok = ~np.isnan(U64h)
+    # ---------------------------------------------------------------- the same precision from a zero start
+    zero = None
+    if warm is not None:
+        z_ms = []
+        for _ in range(max(1, min(args.steps, 3))):
+            flush_l2(flush)
+            ev0.record()
+            _, _, infz = device_solve(P, d, prec)
+            ev1.record()
+            torch.cuda.synchronize()
+            z_ms.append(ev0.elapsed_time(ev1))
+        nc = g0.nx * g0.ny * g0.nz
+        torch.cuda.synchronize()
+        ev0.record()
+        x0w = warm.predict_x0(g0, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
+                              d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
+        ev1.record()
+        torch.cuda.synchronize()
+        t_pred = ev0.elapsed_time(ev1)
+        xw = x0w.view(-1, 3).cpu().numpy()
+        Ur = U64h.reshape(-1, 3)
+        okn = ok.reshape(-1, 3).all(1)
+        zero = {"s_per_solve": round(min(z_ms) / 1e3, 5), "iters": int(infz.iters), "relres": infz.relres,
+                "prediction_ms": round(t_pred, 3), "x0_used": int(info.x0_used),
+                "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn]))}
     disp_rel = float(np.linalg.norm(U_mixed[ok] - U64h[ok]) / np.linalg.norm(U64h[ok]))
     vm_rel = float(torch.linalg.norm(vm - vm64).item() / torch.linalg.norm(vm64).item())
     # ---------------------------------------------------------------- e2e through the public API
@@ -265,7 +306,7 @@ def run_ours(args, rank, world, dist):
         t_a = time.perf_counter()
         U, inf, R = engine.solve_cn(g, pinned["lam"], pinned["mu"], pinned["active"], pinned["cn"], pinned["orig"],
                                     P["fixed"], P["loads"], P["extra"], P["node_groups"], tol=TOL, maxiter=800,
-                                    precision=prec, keep_device=True)
+                                    precision=prec, keep_device=True, warm_start=warm)
         t_b = time.perf_counter()
         sig, vmh, eps = engine.cell_stress_cn(g, pinned["lam"], pinned["mu"], U, cells_h, pinned["cn"],
                                               device=inf["device"])
@@ -335,13 +376,16 @@ def run_ours(args, rank, world, dist):
         dtype="f32 inner / f64 refinement" if prec == "refine" else ("f64" if prec == "fp64" else "f64 CG / f32 V-cycle"),
         data="synthetic (seeded hindfoot generator)",
         config={"workload": "hindfoot 160x112x96 h=0.5mm (C2 generator)", "ndof": int(mixed_info.ndof),
-                "precision": prec, "warm_start": "zero (learned warm start not used)", "tol": TOL,
+                "precision": prec,
+                "warm_start": ("learned (3D conv encoder-decoder trained on 96x64x48 C5 solves, prediction inside "
+                               "the step)" if warm is not None else "zero (no trained network found)"), "tol": TOL,
                 "iters": int(mixed_info.iters), "sweeps": int(mixed_info.sweeps), "relres": mixed_info.relres,
                 "levels": int(mixed_info.levels), "l2": "flushed (256 MB write) before every step",
                 "parallelism": f"independent solves x{world}"},
         plain_fp64={"s_per_solve": round(min(fp64_ms) / 1e3, 5), "iters": int(info64.iters),
                     "relres": info64.relres},
         speedup_vs_plain_fp64=round(min(fp64_ms) / 1e3 / value, 3) if world == 1 else None,
+        same_precision_zero_start=zero,
         parity_vs_fp64={"disp_rel_l2": disp_rel, "vm_rel_l2": vm_rel},
         stage_ms={"setup": round(mixed_info.t_setup_ms, 3), "solve": round(mixed_info.t_solve_ms, 3),
                   "setup_stages": dict(zip(SETUP_STAGES, (round(float(v), 3) for v in mixed_info.t_stage_ms)))},
@@ -505,6 +549,8 @@ def main():
     ap.add_argument("--size", default=None, help="override the workload grid, e.g. 96x64x56x0.833 (profiling)")
     ap.add_argument("--inner-tol", type=float, default=None, help="refinement: FP32 sweep tolerance")
     ap.add_argument("--use-graphs", type=int, default=None, help="0 direct, 1 graph per iteration, 2 device loop")
+    ap.add_argument("--warm", choices=["auto", "on", "off"], default="auto",
+                    help="learned warm start (auto: when the packaged network is present)")
     args = ap.parse_args()
     if args.inner_tol is not None:
         SOLVER_OPTIONS["inner_tol"] = args.inner_tol

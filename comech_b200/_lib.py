@@ -20,7 +20,10 @@ EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_sol
            "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_launch_count", "feb_last_error",
            "feb_region_forces", "feb_rigid_fit", "feb_relative_displacement", "feb_sample_cells",
            "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
-           "feb_mix_materials"]
+           "feb_mix_materials", "feb_net_conv", "feb_net_wgrad", "feb_net_colsum", "feb_net_weights", "feb_net_head",
+           "feb_net_adam", "feb_net_sumsq", "feb_net_inputs", "feb_net_targets", "feb_net_to_nodes"]
+
+GATHER_SHIFT, GATHER_DOWN, GATHER_ONE, GATHER_UP = 0, 1, 2, 3
 
 
 class FebGrid(C.Structure):
@@ -47,7 +50,26 @@ class FebInfo(C.Structure):
                 ("relres", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("ndof", C.c_int64), ("level_dofs", C.c_int64 * 8), ("lmax", C.c_double * 8),
                 ("coarse_n", C.c_int32), ("kernel_launches", C.c_int32), ("ku_shape", C.c_int32 * 4),
-                ("t_stage_ms", C.c_double * 8)]
+                ("t_stage_ms", C.c_double * 8), ("x0_used", C.c_int32), ("pad_", C.c_int32)]
+
+
+class FebNetGrid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32)]
+
+
+class FebConv(C.Structure):
+    _fields_ = [("gather", C.c_int32), ("scatter", C.c_int32), ("grid", FebNetGrid), ("fine", FebNetGrid),
+                ("in", C.c_void_p), ("in_ld", C.c_int32), ("in_c0", C.c_int32), ("kc", C.c_int32), ("n", C.c_int32),
+                ("wt", C.c_void_p), ("out", C.c_void_p), ("out_ld", C.c_int32), ("out_c0", C.c_int32),
+                ("scatter_c", C.c_int32), ("relu", C.c_int32), ("bias", C.c_void_p), ("mask", C.c_void_p),
+                ("mask_ld", C.c_int32), ("mask_c0", C.c_int32), ("accumulate", C.c_int32), ("pad_", C.c_int32),
+                ("status", C.c_void_p)]
+
+
+class FebWgrad(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("pad_", C.c_int32), ("grid", FebNetGrid), ("fine", FebNetGrid),
+                ("p", C.c_void_p), ("p_ld", C.c_int32), ("p_c0", C.c_int32), ("na", C.c_int32),
+                ("q_ld", C.c_int32), ("q_c0", C.c_int32), ("nb", C.c_int32), ("q", C.c_void_p), ("dw", C.c_void_p)]
 
 
 class FebError(RuntimeError):
@@ -91,6 +113,18 @@ def load():
     lib.feb_split_connectivity.argtypes = [C.POINTER(FebGrid), P, P, P, C.c_int32, P, P, C.c_int64,
                                            C.POINTER(C.c_int64), C.POINTER(C.c_int64), P]
     lib.feb_mix_materials.argtypes = [C.c_int32] * 4 + [P, C.c_int32] + [P] * 11
+    lib.feb_net_conv.argtypes = [C.POINTER(FebConv), P]
+    lib.feb_net_wgrad.argtypes = [C.POINTER(FebWgrad), P]
+    lib.feb_net_colsum.argtypes = [P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, P, P]
+    lib.feb_net_weights.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P]
+    lib.feb_net_head.argtypes = [P, C.c_int32, C.c_int64, P, P, P, P, P, C.c_float, P, P, C.c_int32, P, P, P]
+    lib.feb_net_adam.argtypes = [P, P, P, P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32,
+                                 C.c_float, P]
+    lib.feb_net_sumsq.argtypes = [P, C.c_int64, P, P]
+    lib.feb_net_inputs.argtypes = [FebNetGrid, P, C.POINTER(FebGrid), P, P, P, C.c_int64, P, C.c_int64, P, C.c_int64,
+                                   P, P, C.c_double, P, P, P]
+    lib.feb_net_targets.argtypes = [FebNetGrid, P, C.c_double, P, P, P]
+    lib.feb_net_to_nodes.argtypes = [FebNetGrid, P, P, C.c_double, C.POINTER(FebGrid), P, P, C.c_int64, P, P]
     lib.feb_launch_count.argtypes = []
     lib.feb_launch_count.restype = C.c_int64
     lib.feb_last_error.argtypes = []

@@ -25,10 +25,13 @@
 #include <cuda_bf16.h>
 
 #include "fine.cuh"
+#include "tcgen05.cuh"
 
 namespace feb {
 
 namespace {
+
+using namespace tc;
 
 constexpr int kRows = 8;                        // cell rows per CTA: 2 MMA groups of 4 rows x 32 cells
 constexpr int kGroups = kRows / 4;
@@ -41,72 +44,10 @@ constexpr int kRowBytes = 32 * 16;              // one node row of pair-words
 constexpr int kSliceBytes = kNodeRows * kRowBytes;
 constexpr int kPlaneBytes = kSlices * kSliceBytes;
 constexpr int kXchBytes = 2 * kRows * 6 * 32 * 4;   // y exchange, double-buffered by layer
-constexpr int kWaitPolls = 1 << 22;
 
 template <int MODE> struct TcCols { static constexpr int value = (MODE == MAT_ISO_SRI) ? 32 : 48; };
 
 constexpr size_t tc_smem_bytes(int ncol) { return (size_t)3 * kPlaneBytes + 64 * (size_t)ncol + kXchBytes + 32; }
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// tcgen05 shared-memory matrix descriptor: K-major, no swizzle (start, leading and stride byte offsets >> 4,
-// descriptor version 1 at bits 46-47)
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kWaitPolls; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.b32 %0, 1, 0, P;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&d)[32]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
-      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-#pragma unroll
-  for (int q = 0; q < 32; ++q) d[q] = __uint_as_float(r[q]);
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&d)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int q = 0; q < 16; ++q) d[q] = __uint_as_float(r[q]);
-}
-
-__device__ __forceinline__ void sync_for_tensor_core() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
 
 // three BF16 slices of a node's (c0, c1, c2): per slice two 32-bit words (c0 c1) and (c2, 0)
 __device__ __forceinline__ void split3(float a, float b, float c, uint32_t (&lo)[kSlices], uint32_t (&hi)[kSlices]) {

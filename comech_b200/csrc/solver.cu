@@ -1833,6 +1833,15 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   if (err) return err;
   const double fnorm = std::sqrt(fn2);
   const double thr2 = fn2 > 0 ? H.opt.tol * H.opt.tol * fn2 : 1.0;
+  // a start value is kept only if its residual is below ||f|| (else the solve starts from zero, as without one)
+  if (x0 && fn2 > 0.0) {
+    H.apply<double>(0, x0, H.q, nullptr);
+    launch_residual<double>(f, H.q, H.r, n, nullptr, H.s);
+    const double rr0 = H.read_dot(H.r, H.r, n, &err);
+    if (err) return err;
+    if (!(rr0 < fn2)) x0 = nullptr;
+  }
+  inf.x0_used = x0 ? 1 : 0;
   if (fn2 == 0.0) {
     FEB_CUDA(cudaMemsetAsync(xout, 0, n * sizeof(double), H.s));
     inf.flag = 0; inf.iters = 0; inf.relres = 0.0;

@@ -204,7 +204,7 @@ def _info_dict(info, t0, extra=None):
              lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
              kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape),
              t_stage_ms=[round(float(v), 3) for v in info.t_stage_ms], device=f"cuda:{_torch().cuda.current_device()}",
-             t_wall=round(time.perf_counter() - t0, 4))
+             x0_used=bool(info.x0_used), t_wall=round(time.perf_counter() - t0, 4))
     if extra:
         d.update(extra)
     return d
@@ -226,9 +226,11 @@ def _extra_entries(extra, used_nodes_fn, ntotal):
 
 
 def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups=None, tol=1e-6, maxiter=800,
-             aniso=None, *, precision="fp64", x0=None, options=None, keep_device=False):
+             aniso=None, *, precision="fp64", x0=None, options=None, keep_device=False, warm_start=None):
     """Split-node solve on the GPU (rb/splitfe.py:123-158): returns (U (nnew, 3) with NaN on unused nodes,
-    info, reactions R)."""
+    info, reactions R).  ``warm_start``: True (the packaged network) or a ``warmnet.WarmNet`` predicts the initial
+    guess when no ``x0`` is given; the solve falls back to a zero start if the guess's residual is not below
+    ||f|| (info["x0_used"])."""
     if aniso is not None:
         raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
     t0 = time.perf_counter()
@@ -255,7 +257,16 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
         P.set_rigid_groups(node_groups)
         stamps.append(("rigid", time.perf_counter()))
         f = P.rhs(loads)
-        x0d = _dev(np.nan_to_num(np.asarray(x0, np.float64)).ravel(), np.float64) if x0 is not None else None
+        if x0 is not None:
+            x0d = _dev(np.nan_to_num(np.asarray(x0, np.float64)).ravel(), np.float64)
+        elif warm_start is not None and warm_start is not False:
+            from . import warmnet
+            net = warmnet.default_net() if warm_start is True else warm_start
+            ln, lz = warmnet.load_z(loads)
+            x0d = net.predict_x0(g, lam, mu, active, orig, fn, ln, lz, ntotal, orig_dev=P.orig)
+            stamps.append(("warm_start", time.perf_counter()))
+        else:
+            x0d = None
         x, info = P.solve(f, x0d)
         stamps.append(("solve", time.perf_counter()))
         Ud = P.export(x)

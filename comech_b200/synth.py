@@ -134,10 +134,11 @@ def hindfoot_problem(nx=160, ny=112, nz=96, h=0.5, seed=0, action="none", n_liga
     """Synthetic hindfoot for ``solve_cn``; ``action`` in ACTIONS applies a seeded surgical edit:
     resection (bridge cells inactive), osteotomy (calcaneal fragment behind a plane shifted 3-8 mm along
     x), interposition (bridge E = 5 MPa), fusion (no split between talus and calcaneus: both become one
-    part), load (load x U(0.5, 2))."""
+    part), load (load x U(0.5, 2)).  ``h`` is the voxel edge (mm), or (hx, hy, hz) for box-shaped voxels."""
     rng = np.random.default_rng(seed)
-    g = Grid(uniform_edges(nx, h), uniform_edges(ny, h), uniform_edges(nz, h))
-    L, W, H = nx * h, ny * h, nz * h
+    hx, hy, hz = (float(h),) * 3 if np.isscalar(h) else (float(v) for v in h)
+    g = Grid(uniform_edges(nx, hx), uniform_edges(ny, hy), uniform_edges(nz, hz))
+    L, W, H = nx * hx, ny * hy, nz * hz
     bones = _bone_layout(rng, L, W, H)
     arng = np.random.default_rng(seed + 7919)
     shift = 0.0
@@ -165,7 +166,7 @@ def hindfoot_problem(nx=160, ny=112, nz=96, h=0.5, seed=0, action="none", n_liga
         lab[inside] = k; best[inside] = v[inside]
         depth = np.where(inside, (1.0 - v ** (1.0 / p)) * a.min(), depth)
     if shift:
-        gap = (X >= cut_x - 0.5 * h) & (X < cut_x + shift) & (lab == 2)
+        gap = (X >= cut_x - 0.5 * hx) & (X < cut_x + shift) & (lab == 2)
         lab[gap] = 0
     sub = lab.reshape(nx, ns, ny, ns, nz, ns).transpose(0, 2, 4, 1, 3, 5).reshape(nx, ny, nz, ns ** 3)
     share = np.stack([(sub == k).mean(-1) for k in range(len(bones) + 1)], -1).reshape(g.ncell, len(bones) + 1)
@@ -218,7 +219,7 @@ def hindfoot_problem(nx=160, ny=112, nz=96, h=0.5, seed=0, action="none", n_liga
     # plantar ground springs: z- faces of the active cells of the lowest layer, K_GROUND per interior node
     bottom = cells[(g.cK == 0) & active]
     fn, fa = face_node_areas(g, cn, bottom, "z-")
-    fa = fa * (K_GROUND / (1e6 * h * h))
+    fa = fa * (K_GROUND / (1e6 * hx * hy))
     # load on the talar dome: z+ faces of talus cells with no talus above, upper half of the talus
     tal = (part == 1) & active
     above = np.zeros(g.ncell, bool)

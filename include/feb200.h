@@ -107,6 +107,9 @@ typedef struct FebInfo {
                                     node planes per CTA), FP64 (warps, planes) */
   double t_stage_ms[8];          /* feb_create stages: cells, penalties/extra, diagonal blocks, K.u tuning,
                                     Galerkin hierarchy, power iterations, dense coarse level, (spare) */
+  int32_t x0_used;               /* 1: the solve started from the caller's x0; 0: from zero (no x0, or an x0 whose
+                                    residual ||f - K x0|| was not below ||f||: the fallback of a warm start) */
+  int32_t pad_;
 } FebInfo;
 
 /* Default options (tol 1e-6, maxiter 800 as rb/splitfe.py:123; GMG parameters of fe/gmg.py:80). */
@@ -230,6 +233,109 @@ FEB_API int feb_mix_materials(int32_t nx, int32_t ny, int32_t nz, int32_t ns3, c
                               const int8_t* body_class, const int8_t* body_group, const double* class_lam,
                               const double* class_mu, const double* class_M, double* F, double* E, double* nu,
                               uint8_t* active, uint8_t* ser, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------
+ * Learned warm start: a 3D convolutional encoder-decoder whose prediction is the PCG initial guess.  The
+ * reference has no counterpart (its PCG starts from x0 = 0 or a caller's x0, fe/gmg.py:120-137); these entry
+ * points are the network's layers, training steps and its coupling to the solve's inputs and outputs.
+ *
+ * Activations live on a padded voxel grid: a grid of nx x ny x nz cells has (nx+2)(ny+2)(nz+2) rows, row
+ * ((x+1)(ny+2) + (y+1))(nz+2) + (z+1) for cell (x, y, z) (z fastest, like the FE cell id), with a shell of
+ * zero rows around the cells.  A row holds `ld` BF16 channels (ld a multiple of 8); a tensor may be a channel
+ * range [c0, c0 + C) of a wider buffer (skip connections share one buffer).
+ * --------------------------------------------------------------------------------------------------------- */
+#define FEB_GATHER_SHIFT 0       /* 3x3x3 taps, stride 1: tap t = 9(dx+1) + 3(dy+1) + (dz+1)                  */
+#define FEB_GATHER_DOWN 1        /* 2x2x2 taps, stride 2: coarse row V reads fine cells 2V + (tx, ty, tz),
+                                    tap t = 4 tx + 2 ty + tz                                                  */
+#define FEB_GATHER_ONE 2         /* one tap: row r reads row r                                                */
+#define FEB_GATHER_UP 3          /* (weight gradient only) P rows at fine cells 2V + t, Q rows at coarse V   */
+
+typedef struct FebNetGrid {
+  int32_t nx, ny, nz;            /* cells per axis (rows: (nx+2)(ny+2)(nz+2)) */
+} FebNetGrid;
+
+/* One implicit-GEMM pass on the tensor cores: out[row][n] = sum over taps t and channels k of
+ * in[src(row, t)][in_c0 + k] * wt[t][n][k], then  + bias[n], ReLU, + existing out (accumulate), * (mask > 0).
+ * Rows run over `grid` (gather SHIFT / ONE: the input's own grid; DOWN: the coarse output grid reading the
+ * fine grid `fine`).  scatter = 1: the GEMM columns are 8 groups of scatter_c channels and the row of coarse
+ * cell V in group t is written to fine cell 2V + t of `fine` (a transposed 2x2x2 stride-2 convolution).
+ * Shell rows of the output are written as zeros (scatter: never written; callers zero them once).  kc (channels
+ * per tap) is a multiple of 32; n a multiple of 32; ld / c0 multiples of 8.  status [dev] is set to 1 if a
+ * bounded tensor-core wait ran out (the result is then invalid). */
+typedef struct FebConv {
+  int32_t gather, scatter;
+  FebNetGrid grid, fine;
+  const void* in;                /* [dev] bf16 */
+  int32_t in_ld, in_c0, kc, n;
+  const void* wt;                /* [dev] bf16 [taps][n][kc] */
+  void* out;                     /* [dev] bf16 */
+  int32_t out_ld, out_c0, scatter_c, relu;
+  const float* bias;             /* [dev] n (scatter: scatter_c) or NULL */
+  const void* mask;              /* [dev] bf16 or NULL */
+  int32_t mask_ld, mask_c0, accumulate, pad_;
+  int32_t* status;               /* [dev] or NULL */
+} FebConv;
+
+FEB_API int feb_net_conv(const FebConv* c, void* stream);
+
+/* Weight gradient: dw[t][a][b] += sum over rows r of P[rowP(r, t)][p_c0 + a] * Q[rowQ(r, t)][q_c0 + b], rows r over
+ * `grid`; mode SHIFT: rowP = r, rowQ = r + tap offset; DOWN: rowP = r (coarse), rowQ = fine cell 2V + t; UP:
+ * rowP = fine cell 2V + t, rowQ = r (coarse).  na, nb multiples of 32.  dw [dev] fp32, accumulated. */
+typedef struct FebWgrad {
+  int32_t mode, pad_;
+  FebNetGrid grid, fine;
+  const void* p;                 /* [dev] bf16 */
+  int32_t p_ld, p_c0, na;
+  int32_t q_ld, q_c0, nb;
+  const void* q;                 /* [dev] bf16 */
+  float* dw;                     /* [dev] [taps][na][nb] */
+} FebWgrad;
+
+FEB_API int feb_net_wgrad(const FebWgrad* w, void* stream);
+
+/* out[c] += sum over rows of g[r][c0 + c], c < nc (bias gradients; shell rows of g are zero). */
+FEB_API int feb_net_colsum(const void* g, int64_t rows, int32_t ld, int32_t c0, int32_t nc, float* out, void* stream);
+
+/* BF16 weight tables from FP32 master weights W [taps][co][ci]: fwd [taps][co][ci]; bwd (if not NULL)
+ * [taps][ci][co], tap order reversed when flip = 1 (the data gradient of a 3x3x3 convolution). */
+FEB_API int feb_net_weights(const float* W, int32_t taps, int32_t co, int32_t ci, void* fwd, void* bwd, int32_t flip,
+                            void* stream);
+
+/* Output head (1x1 convolution of 32 channels to 3) and, when target is not NULL, the weighted mean squared error
+ * with its gradients: pred[r][c] = b[c] + sum_k X[r][k] W[c][k] (pred may be NULL); loss += sum_r wgt[r] |pred -
+ * target|^2 * inv_n; dX[r][k] = (X[r][k] > 0) sum_c 2 inv_n wgt[r] (pred - target)[c] W[c][k]; dW, db
+ * accumulated.  All [dev]; X, dX bf16 with row stride x_ld / dx_ld. */
+FEB_API int feb_net_head(const void* X, int32_t x_ld, int64_t rows, const float* W, const float* b, float* pred,
+                         const float* target, const float* wgt, float inv_n, double* loss, void* dX, int32_t dx_ld,
+                         float* dW, float* db, void* stream);
+
+/* Adam step on n FP32 parameters (bias-corrected, step >= 1); the gradient is scaled by gscale first and
+ * zeroed afterwards.  sumsq (if not NULL) receives += sum of squared gradients before the step is taken. */
+FEB_API int feb_net_adam(float* w, float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                         float eps, int32_t step, float gscale, void* stream);
+FEB_API int feb_net_sumsq(const float* g, int64_t n, double* out, void* stream);
+
+/* Network input (32 BF16 channels per row, channels 0-5 used) on the network grid `net` of spacing hn [host 3],
+ * from the solve's inputs on the FE grid of uniform spacing h [host 3] covering the same box from the origin:
+ * 0 log10(E)/4 and 1 (nu - 0.3) * 4 of the FE cell at the network cell's centre (active cells), 2 active; 3
+ * split-node, 4 contact (ground spring) and 5 load marks of the FE grid nodes that fall in the cell (load: the z
+ * load of the nodes, times load_scale).  split / contact / load node lists hold grid node ids [dev]; mat =
+ * (lambda | mu) [dev] per FE cell; active [dev] uint8 per FE cell.  scratch [dev] 3 floats per network cell. */
+FEB_API int feb_net_inputs(FebNetGrid net, const double* hn, const FebGrid* fe, const double* h, const double* mat,
+                           const uint8_t* active, int64_t nsplit, const int64_t* split_nodes, int64_t ncontact,
+                           const int64_t* contact_nodes, int64_t nload, const int64_t* load_nodes,
+                           const double* load_z, double load_scale, float* scratch, void* out, void* stream);
+
+/* Training target on a network grid equal to the FE grid: target[row of cell (i,j,k)] = U[node (i,j,k)] / scale
+ * (fp32, 3 per row) and wgt = 1 where that node's displacement is finite, else 0 (shell rows 0).  U [dev] full
+ * layout fp64 (NaN on unused nodes), at least (nx+1)(ny+1)(nz+1) nodes. */
+FEB_API int feb_net_targets(FebNetGrid net, const double* U, double scale, float* target, float* wgt, void* stream);
+
+/* Initial guess from a prediction: x0[3n + c] = scale * trilinear interpolation of pred (values at the lower
+ * corner nodes of the network cells, spacing hn) at the position of FE node n (grid node orig[n], spacing h), for
+ * every node id n < nnode_total.  orig may be NULL (no copies). */
+FEB_API int feb_net_to_nodes(FebNetGrid net, const double* hn, const float* pred, double scale, const FebGrid* fe,
+                             const double* h, const int64_t* orig, int64_t nnode_total, double* x0, void* stream);
 
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);

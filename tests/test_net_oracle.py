@@ -1,0 +1,43 @@
+"""The CPU oracle of the warm-start network pinned by finite differences (no GPU): every parameter gradient of
+the chain-rule backward pass of oracle/net_oracle.py against central differences of the loss, on a tiny network."""
+import numpy as np
+
+from oracle import net_oracle as O
+
+
+def test_oracle_gradients_match_finite_differences():
+    c = (2, 3, 4, 5)
+    P = O.init_params(c, cin=3, cin_used=3, seed=1)
+    rng = np.random.default_rng(2)
+    P["head"] = (rng.normal(0, 0.5, (3, 2)), np.array([0.1, -0.2, 0.3]))
+    P = {k: (W, b + rng.normal(0, 0.1, b.shape)) for k, (W, b) in P.items()}
+    net = O.Net(P, c)
+    x = rng.normal(size=(8, 8, 8, 3))
+    T = rng.normal(size=(8, 8, 8, 3))
+    w = (rng.random((8, 8, 8)) < 0.7).astype(float)
+    loss, g = net.loss_and_grads(x, T, w)
+    assert np.isfinite(loss) and loss > 0
+    worst = 0.0
+    for name in [n for n, _, _, _ in O.layers(c, 3)] + ["head"]:
+        for which in (0, 1):
+            arr = P[name][which]
+            for _ in range(2):
+                idx = tuple(int(rng.integers(0, s)) for s in arr.shape)
+                num = net.numeric_grad(x, T, w, name, which, idx)
+                ana = g[name][which][idx]
+                worst = max(worst, abs(num - ana) / max(1e-8, abs(num) + abs(ana)))
+    assert worst < 1e-5
+
+
+def test_layers_are_adjoint():
+    """<conv(X), G> = <X, conv_back(G)> for the three layer kinds (the data gradients are the adjoints)."""
+    rng = np.random.default_rng(3)
+    for fwd, back, xs, taps in ((O.conv3, O.conv3_back, (4, 6, 2, 3), 27), (O.down, O.down_back, (4, 6, 2, 3), 8),
+                                (O.up, O.up_back, (2, 3, 1, 3), 8)):
+        X = rng.normal(size=xs)
+        W = rng.normal(size=(taps, 5, 3))
+        Y = fwd(X, W)
+        G = rng.normal(size=Y.shape)
+        dX, dW, _ = back(X, W, G)
+        assert abs((Y * G).sum() - (X * dX).sum()) < 1e-9 * abs((Y * G).sum())
+        assert abs((Y * G).sum() - (W * dW).sum()) < 1e-9 * abs((Y * G).sum())
