@@ -286,6 +286,7 @@ def run_ours(args, rank, world, dist):
         okn = ok.reshape(-1, 3).all(1)
         zero = {"s_per_solve": round(min(z_ms) / 1e3, 5), "iters": int(infz.iters), "relres": infz.relres,
                 "prediction_ms": round(t_pred, 3), "x0_used": int(info.x0_used),
+                "x0_scale": float(info.x0_scale),
                 "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn]))}
     disp_rel = float(np.linalg.norm(U_mixed[ok] - U64h[ok]) / np.linalg.norm(U64h[ok]))
     vm_rel = float(torch.linalg.norm(vm - vm64).item() / torch.linalg.norm(vm64).item())
@@ -404,11 +405,20 @@ def run_profile(args):
     P = make_problem(seed=0)
     d = device_inputs(P)
     if args.mode == "solve-once":
+        warm = None
+        if args.warm != "off":
+            from comech_b200 import warmnet
+            try:
+                warm = warmnet.default_net()
+            except RuntimeError:
+                if args.warm == "on":
+                    raise
         for _ in range(args.warmup):
-            device_solve(P, d, args.precision)
-        U, vm, info = device_solve(P, d, args.precision)
+            device_solve(P, d, args.precision, warm=warm)
+        U, vm, info = device_solve(P, d, args.precision, warm=warm)
         torch.cuda.synchronize()
-        return {"mode": "solve-once", "precision": args.precision, "options": SOLVER_OPTIONS, "iters": int(info.iters),
+        return {"mode": "solve-once", "precision": args.precision, "options": SOLVER_OPTIONS,
+                "warm_start": warm is not None, "x0_used": int(info.x0_used), "iters": int(info.iters),
                 "sweeps": int(info.sweeps), "relres": info.relres, "t_setup_ms": round(info.t_setup_ms, 2),
                 "t_solve_ms": round(info.t_solve_ms, 2), "ndof": int(info.ndof), "ku_shape": list(info.ku_shape),
                 "t_stage_ms": [round(float(v), 2) for v in info.t_stage_ms]}
@@ -426,6 +436,53 @@ def run_profile(args):
             out[name + "_ms"] = ms.value
     finally:
         pr.close()
+    return out
+
+
+BATCH_ACTIONS = ("resection", "osteotomy", "interposition", "fusion", "load")
+
+
+def batch_instance(seed):
+    """One batch instance: a grid drawn from the seed between 64x48x40 and 128x96x80 cells over an 80-mm-long box,
+    one surgical action (runs in a worker process; no CUDA)."""
+    from comech_b200 import synth
+    rng = np.random.default_rng(10_000 + seed)
+    f = rng.uniform(0.0, 1.0)
+    nx, ny, nz = (int(round(a + f * (b - a))) for a, b in ((64, 128), (48, 96), (40, 80)))
+    P = synth.hindfoot_problem(nx, ny, nz, h=80.0 / nx, seed=seed, action=BATCH_ACTIONS[seed % 5])
+    for k in ("bone_share", "E", "nu", "part", "bridge", "contact"):
+        P.pop(k, None)
+    return P
+
+
+def run_batch(args):
+    """64 independent instances of uneven size and seeded action, solved on one GPU one at a time and with 8 / 16
+    solves in flight (comech_b200.batch).  Times are wall-clock around the whole batch through the public API
+    (host inputs, uploads, solves, downloads), after one warm-up pass."""
+    import multiprocessing as mp
+    n = args.batch_n
+    with mp.get_context("spawn").Pool(max(1, min(16, (os.cpu_count() or 2) - 1))) as pool:
+        items = pool.map(batch_instance, range(n))
+    import torch
+    from comech_b200 import batch
+    batch.solve_batch(items[:4], precision=args.precision, tol=TOL, concurrency=4)      # warm-up
+    out = {"mode": "batch", "instances": n, "precision": args.precision, "tol": TOL,
+           "dims": sorted({(P["grid"].nx, P["grid"].ny, P["grid"].nz) for P in items})[:: max(1, n // 8)],
+           "actions": list(BATCH_ACTIONS)}
+    runs = {}
+    for conc in (1, 8, 16):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = batch.solve_batch(items, precision=args.precision, tol=TOL, concurrency=conc)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        runs[conc] = dict(seconds=round(dt, 3), solves_per_s=round(n / dt, 2),
+                          iters_median=float(np.median([r[1]["iters"] for r in res])),
+                          relres_max=float(max(r[1]["relres"] for r in res)),
+                          flags=sorted({int(r[1]["flag"]) for r in res}))
+    out["ndof_total"] = int(sum(r[1]["ndof"] for r in res))
+    out["runs"] = {str(k): v for k, v in runs.items()}
+    out["speedup_16_vs_1"] = round(runs[1]["seconds"] / runs[16]["seconds"], 2)
     return out
 
 
@@ -543,9 +600,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "post"], default="full",
+    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "post", "batch"], default="full",
                     help="solve-once / ku: one device solve or a few K.u products of the workload (profiling); "
-                         "post: the rows around the solve, device against the CPU oracle")
+                         "post: the rows around the solve, device against the CPU oracle; batch: 64 uneven "
+                         "instances with seeded actions, one at a time and 8 / 16 in flight")
+    ap.add_argument("--batch-n", type=int, default=64)
     ap.add_argument("--size", default=None, help="override the workload grid, e.g. 96x64x56x0.833 (profiling)")
     ap.add_argument("--inner-tol", type=float, default=None, help="refinement: FP32 sweep tolerance")
     ap.add_argument("--use-graphs", type=int, default=None, help="0 direct, 1 graph per iteration, 2 device loop")
@@ -564,6 +623,8 @@ def main():
     dist = None
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.mode == "batch":
+        out = run_batch(args)                     # the instance pool starts before the first CUDA call
     else:
         import torch
         local = int(os.environ.get("LOCAL_RANK", "0"))

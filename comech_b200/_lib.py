@@ -42,7 +42,7 @@ class FebOptions(C.Structure):
     _fields_ = [("precision", C.c_int32), ("maxiter", C.c_int32), ("tol", C.c_double), ("min_dofs", C.c_int32),
                 ("max_levels", C.c_int32), ("cheb_degree", C.c_int32), ("check_every", C.c_int32),
                 ("inner_tol", C.c_double), ("inner_maxiter", C.c_int32), ("use_graphs", C.c_int32),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("x0_mode", C.c_int32), ("pad_", C.c_int32)]
 
 
 class FebInfo(C.Structure):
@@ -50,7 +50,7 @@ class FebInfo(C.Structure):
                 ("relres", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("ndof", C.c_int64), ("level_dofs", C.c_int64 * 8), ("lmax", C.c_double * 8),
                 ("coarse_n", C.c_int32), ("kernel_launches", C.c_int32), ("ku_shape", C.c_int32 * 4),
-                ("t_stage_ms", C.c_double * 8), ("x0_used", C.c_int32), ("pad_", C.c_int32)]
+                ("t_stage_ms", C.c_double * 8), ("x0_used", C.c_int32), ("x0_scale", C.c_float)]
 
 
 class FebNetGrid(C.Structure):

@@ -481,6 +481,12 @@ __global__ void k_orig_copy(const int64_t* __restrict__ orig, int64_t nnode, int
   out[e] = int(orig[nnode + e]);
 }
 
+// x += a y (y may alias x: x *= 1 + a)
+__global__ void k_axpy_inplace(double* __restrict__ x, const double* y, int64_t n, double a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += a * y[i];
+}
+
 __global__ void k_masked_copy(const double* __restrict__ src, const uint8_t* __restrict__ used, int64_t n,
                               double* __restrict__ dst) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1647,6 +1653,7 @@ void feb_default_options(FebOptions* o) {
   o->inner_maxiter = 200;
   o->use_graphs = 2;
   o->seed = 0;
+  o->x0_mode = 2;
 }
 
 int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt, void* stream, FebHandle** out) {
@@ -1833,13 +1840,32 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   if (err) return err;
   const double fnorm = std::sqrt(fn2);
   const double thr2 = fn2 > 0 ? H.opt.tol * H.opt.tol * fn2 : 1.0;
-  // a start value is kept only if its residual is below ||f|| (else the solve starts from zero, as without one)
-  if (x0 && fn2 > 0.0) {
-    H.apply<double>(0, x0, H.q, nullptr);
-    launch_residual<double>(f, H.q, H.r, n, nullptr, H.s);
-    const double rr0 = H.read_dot(H.r, H.r, n, &err);
+  // Start value.  x0_mode 2 (default): s = x0 + M (f - K x0), one application of the preconditioner, which
+  // removes the start's rough (high-frequency) error; modes 1-2 then use a s with a = s.f / s.K s, the multiple of s
+  // closest to the solution in the energy norm (||x* - a s||_K^2 = ||x*||_K^2 - (s.f)^2 / s.K s, never above the
+  // zero start's error); when s.f <= 0 the solve starts from zero.  Mode 0 uses x0 as given.
+  inf.x0_scale = 0.f;
+  if (x0 && fn2 > 0.0 && H.opt.x0_mode >= 1) {
+    if (H.opt.x0_mode >= 2) {
+      H.apply<double>(0, H.z, H.q, nullptr);
+      launch_residual<double>(f, H.q, H.r, n, nullptr, H.s);
+      H.precondition<double>(H.r, H.p, nullptr);
+      k_axpy_inplace<<<div_up(n, kThreads), kThreads, 0, H.s>>>(H.z, H.p, n, 1.0); note_launch();
+    }
+    H.apply<double>(0, H.z, H.q, nullptr);
+    const double sf = H.read_dot(H.z, f, n, &err);
     if (err) return err;
-    if (!(rr0 < fn2)) x0 = nullptr;
+    const double sks = H.read_dot(H.z, H.q, n, &err);
+    if (err) return err;
+    if (sf > 0.0 && sks > 0.0 && std::isfinite(sf) && std::isfinite(sks)) {
+      const double a = sf / sks;
+      k_axpy_inplace<<<div_up(n, kThreads), kThreads, 0, H.s>>>(H.z, H.z, n, a - 1.0); note_launch();
+      inf.x0_scale = (float)a;
+    } else {
+      x0 = nullptr;
+    }
+  } else if (x0) {
+    inf.x0_scale = 1.f;
   }
   inf.x0_used = x0 ? 1 : 0;
   if (fn2 == 0.0) {

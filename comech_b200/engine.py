@@ -204,7 +204,7 @@ def _info_dict(info, t0, extra=None):
              lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
              kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape),
              t_stage_ms=[round(float(v), 3) for v in info.t_stage_ms], device=f"cuda:{_torch().cuda.current_device()}",
-             x0_used=bool(info.x0_used), t_wall=round(time.perf_counter() - t0, 4))
+             x0_used=bool(info.x0_used), x0_scale=float(info.x0_scale), t_wall=round(time.perf_counter() - t0, 4))
     if extra:
         d.update(extra)
     return d

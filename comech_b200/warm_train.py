@@ -11,8 +11,9 @@ GMG-PCG) and turns inputs and solution into the network's input and target, kept
 Training: Adam on the weighted mean squared error of the displacement (in units of ``u_unit``, scaled by the
 total load), gradients accumulated over ``--batch`` instances, cosine learning-rate decay, all passes in
 libfeb200.so.  Evaluation on the held-out instances: mixed-precision PCG iterations and time to rel-res 1e-8
-from zero and from the network's prediction (with the zero-start fallback of ``feb_solve``), the prediction's
-relative error, and the fallback rate.
+from zero and from the network's prediction (as given, and as ``feb_solve`` prepares it by default: one
+preconditioner application, then its energy-optimal multiple, or a zero start when that multiple is not positive),
+the prediction's relative error, and the fallback rate.
 """
 import argparse
 import json
@@ -41,7 +42,7 @@ def make_instance(seed):
     return int(seed), P
 
 
-def device_problem(P, precision):
+def device_problem(P, precision, options=None):
     """engine.Problem of an instance, with its rigid groups and right-hand side."""
     import torch
     from comech_b200 import engine, _lib
@@ -52,7 +53,7 @@ def device_problem(P, precision):
     mat = torch.from_numpy(np.concatenate([P["lam"], P["mu"]])).cuda()
     pr = engine.Problem(P["grid"], _lib.MAT_ISO_SRI, mat, P["active"], cn=P["cn"].astype(np.int64), orig=P["orig"],
                         pen_node=np.asarray(fn, np.int64), pen_k=pen_k, extra_coo=(3 * nr + cr, 3 * nc + cc, v),
-                        precision=precision, tol=TOL, maxiter=800)
+                        precision=precision, tol=TOL, maxiter=800, options=options)
     pr.set_rigid_groups(P["node_groups"])
     f = pr.rhs(P["loads"])
     return pr, f
@@ -63,14 +64,75 @@ def load_parts(P):
     return np.asarray(ln, np.int64), np.asarray(la, np.float64) * float(lt[2])
 
 
-def solve(P, precision, x0=None):
-    pr, f = device_problem(P, precision)
+def solve(P, precision, x0=None, options=None):
+    pr, f = device_problem(P, precision, options)
     try:
         x, info = pr.solve(f, x0)
         U = pr.export(x)
         return U, info
     finally:
         pr.close()
+
+
+X0_MODES = {"as_given": 0, "smoothed": 2}
+
+
+def evaluate(net, items):
+    """Held-out instances: the FP64 solution, then mixed-precision PCG iterations / time to rel-res 1e-8 from zero and
+    from the network's prediction, used as given (x0_mode 0) and smoothed by one preconditioner application and
+    scaled to its energy-optimal multiple (x0_mode 2, the default)."""
+    import torch
+    ev = []
+    for seed, P in items:
+        ln, lz = load_parts(P)
+        nt = len(P["orig"])
+        U64, _ = solve(P, "fp64")
+        Ur = U64.view(-1, 3).cpu().numpy()
+        used = np.isfinite(Ur).all(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, i0 = solve(P, "mixed")
+        torch.cuda.synchronize()
+        rec = dict(seed=int(seed), action=ACTIONS[int(seed) % len(ACTIONS)], iters_zero=int(i0.iters),
+                   t_zero_s=time.perf_counter() - t0, solve_zero_ms=float(i0.t_solve_ms))
+        for variant, mode in X0_MODES.items():
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            x0 = net.predict_x0(P["grid"], P["lam"], P["mu"], P["active"], P["orig"], P["fixed"][0], ln, lz, nt)
+            torch.cuda.synchronize()
+            tp = time.perf_counter() - t0
+            _, i1 = solve(P, "mixed", x0, options=dict(x0_mode=mode))
+            torch.cuda.synchronize()
+            pr = x0.view(-1, 3).cpu().numpy()
+            rec[variant] = dict(iters=int(i1.iters), x0_used=int(i1.x0_used), x0_scale=float(i1.x0_scale),
+                                t_s=time.perf_counter() - t0, t_predict_s=tp, solve_ms=float(i1.t_solve_ms),
+                                pred_rel_l2=float(np.linalg.norm(pr[used] - Ur[used]) / np.linalg.norm(Ur[used])),
+                                relres=float(i1.relres), flag=int(i1.flag))
+        ev.append(rec)
+    return ev
+
+
+def summarize(ev):
+    if not ev:
+        return {}
+    med = lambda xs: float(np.median(xs))
+    zero = [e["iters_zero"] for e in ev]
+    out = dict(held_iters_zero_median=med(zero), held_t_zero_median_s=med([e["t_zero_s"] for e in ev]),
+               held_solve_zero_ms_median=med([e["solve_zero_ms"] for e in ev]))
+    for v in X0_MODES:
+        out[v] = dict(iters_median=med([e[v]["iters"] for e in ev]),
+                      iters_ratio=float(np.mean([e[v]["iters"] for e in ev]) / np.mean(zero)),
+                      fallback_rate=float(np.mean([1 - e[v]["x0_used"] for e in ev])),
+                      pred_rel_l2_median=med([e[v]["pred_rel_l2"] for e in ev]),
+                      x0_scale_median=med([e[v]["x0_scale"] for e in ev]),
+                      t_median_s=med([e[v]["t_s"] for e in ev]), t_predict_median_s=med([e[v]["t_predict_s"] for e in ev]),
+                      solve_ms_median=med([e[v]["solve_ms"] for e in ev]),
+                      relres_max=float(max(e[v]["relres"] for e in ev)),
+                      flags=sorted({e[v]["flag"] for e in ev}),
+                      per_action={a: [round(float(np.mean([e["iters_zero"] for e in ev if e["action"] == a] or [0])), 2),
+                                      round(float(np.mean([e[v]["iters"] for e in ev if e["action"] == a] or [0])), 2)]
+                                  for a in ACTIONS})
+    return out
 
 
 def cosine(step, total, lr0, lr1):
@@ -89,12 +151,24 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
     ap.add_argument("--time-budget", type=float, default=0.0, help="stop training after this many seconds (0: none)")
+    ap.add_argument("--eval-only", default=None, help="evaluate these weights on --held instances (no training)")
     args = ap.parse_args(argv)
     nw = args.workers or max(1, min(32, (os.cpu_count() or 2) - 2))
     ctx = mp.get_context("spawn")
     pool = ctx.Pool(nw)                         # before the first CUDA call
     import torch
     from comech_b200 import warmnet
+    if args.eval_only:
+        seeds = list(range(args.seed0 + args.train, args.seed0 + args.train + args.held))
+        items = pool.map(make_instance, seeds, chunksize=2)
+        pool.close()
+        ev = evaluate(warmnet.WarmNet.load(args.eval_only), items)
+        summary = dict(weights=args.eval_only, held=len(ev), **summarize(ev))
+        print(json.dumps(summary), flush=True)
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(dict(summary=summary, held=ev), f, indent=1)
+        return summary
     t_start = time.perf_counter()
     N, Nh = args.train, args.held
     seeds = list(range(args.seed0, args.seed0 + N + Nh))
@@ -168,55 +242,17 @@ def main(argv=None):
     t_step = t_train / max(step, 1) / args.batch
 
     # ---------------------------------------------------------------------------------------------- evaluation
-    ev = []
-    for j, P in held.items():
-        ln, lz = load_parts(P)
-        nt = len(P["orig"])
-        U64, _ = solve(P, "fp64")
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        _, i0 = solve(P, "mixed")
-        torch.cuda.synchronize()
-        tz = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        x0 = net.predict_x0(P["grid"], P["lam"], P["mu"], P["active"], P["orig"], P["fixed"][0], ln, lz, nt)
-        torch.cuda.synchronize()
-        tp = time.perf_counter() - t0
-        _, i1 = solve(P, "mixed", x0)
-        torch.cuda.synchronize()
-        tw = time.perf_counter() - t0
-        Ur = U64.view(-1, 3).cpu().numpy()
-        used = np.isfinite(Ur).all(1)
-        pr = x0.view(-1, 3).cpu().numpy()
-        err = float(np.linalg.norm(pr[used] - Ur[used]) / np.linalg.norm(Ur[used]))
-        ev.append(dict(seed=seeds[j], action=ACTIONS[seeds[j] % len(ACTIONS)], iters_zero=int(i0.iters),
-                       iters_warm=int(i1.iters), x0_used=int(i1.x0_used), t_zero_s=tz, t_warm_s=tw, t_predict_s=tp,
-                       solve_zero_ms=float(i0.t_solve_ms), solve_warm_ms=float(i1.t_solve_ms), pred_rel_l2=err,
-                       relres_warm=float(i1.relres)))
-    it0 = np.array([e["iters_zero"] for e in ev]) if ev else np.zeros(1)
-    it1 = np.array([e["iters_warm"] for e in ev]) if ev else np.zeros(1)
+    ev = evaluate(net, [(seeds[j], P) for j, P in held.items()])
     summary = dict(
         grid=GRID, box_mm=BOX, train=N, held=Nh, epochs_run=len(hist), batch=args.batch, params=net.nparam,
         u_unit=u_unit, t_data_s=round(t_data, 1), t_solve_fp64_s=round(t_solve, 1),
         fp64_iters_median=float(np.median(iters_fp64)) if iters_fp64 else None,
         t_train_s=round(t_train, 1), t_per_sample_step_ms=round(1e3 * t_step, 3), stopped_early=stopped_early,
-        history=hist,
-        held_iters_zero_median=float(np.median(it0)), held_iters_warm_median=float(np.median(it1)),
-        held_iters_ratio=float(np.mean(it1) / max(np.mean(it0), 1)),
-        held_fallback_rate=float(np.mean([1 - e["x0_used"] for e in ev])) if ev else None,
-        held_pred_rel_l2_median=float(np.median([e["pred_rel_l2"] for e in ev])) if ev else None,
-        held_t_zero_median_s=float(np.median([e["t_zero_s"] for e in ev])) if ev else None,
-        held_t_warm_median_s=float(np.median([e["t_warm_s"] for e in ev])) if ev else None,
-        held_t_predict_median_s=float(np.median([e["t_predict_s"] for e in ev])) if ev else None,
-        held_relres_warm_max=float(max(e["relres_warm"] for e in ev)) if ev else None,
-        per_action={a: dict(n=len([e for e in ev if e["action"] == a]),
-                            iters_zero=float(np.mean([e["iters_zero"] for e in ev if e["action"] == a] or [0])),
-                            iters_warm=float(np.mean([e["iters_warm"] for e in ev if e["action"] == a] or [0])))
-                    for a in ACTIONS})
-    print(json.dumps({k: v for k, v in summary.items() if k != "history"}), flush=True)
+        history=hist, **summarize(ev))
     if args.out:
         os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
         net.save(args.out, train=N, epochs=len(hist), box=np.array(BOX))
+    print(json.dumps({k: v for k, v in summary.items() if k != "history"}), flush=True)
     if args.report:
         with open(args.report, "w") as f:
             json.dump(dict(summary=summary, held=ev), f, indent=1)

@@ -88,6 +88,9 @@ typedef struct FebOptions {
   int32_t use_graphs;            /* 0 direct launches; 1 one graph per CG iteration, host polls convergence;
                                     2 the CG loop is a device-side while loop (conditional graph node) */
   uint64_t seed;                 /* power-iteration start vectors */
+  int32_t x0_mode;               /* start value x0: 0 as given; 1 its energy-optimal multiple; 2 (default) x0 + M (f -
+                                    K x0) (one preconditioner application), then its energy-optimal multiple */
+  int32_t pad_;
 } FebOptions;
 
 typedef struct FebInfo {
@@ -107,9 +110,9 @@ typedef struct FebInfo {
                                     node planes per CTA), FP64 (warps, planes) */
   double t_stage_ms[8];          /* feb_create stages: cells, penalties/extra, diagonal blocks, K.u tuning,
                                     Galerkin hierarchy, power iterations, dense coarse level, (spare) */
-  int32_t x0_used;               /* 1: the solve started from the caller's x0; 0: from zero (no x0, or an x0 whose
-                                    residual ||f - K x0|| was not below ||f||: the fallback of a warm start) */
-  int32_t pad_;
+  int32_t x0_used;               /* 1: the solve started from the caller's x0 (as FebOptions.x0_mode prepares it); 0:
+                                    from zero (no x0, or a start s with s.f <= 0: the fallback of a warm start) */
+  float x0_scale;                /* the energy-optimal multiple a = s.f / s.K s applied to the start (1 in mode 0) */
 } FebInfo;
 
 /* Default options (tol 1e-6, maxiter 800 as rb/splitfe.py:123; GMG parameters of fe/gmg.py:80). */
