@@ -376,7 +376,8 @@ def run_ours(args, rank, world, dist):
         ms_per_step=round(1e3 * t_total / args.steps, 3), higher_is_better=False, scaling="weak", vs_baseline=None,
         dtype="f32 inner / f64 refinement" if prec == "refine" else ("f64" if prec == "fp64" else "f64 CG / f32 V-cycle"),
         data="synthetic (seeded hindfoot generator)",
-        config={"workload": "hindfoot 160x112x96 h=0.5mm (C2 generator)", "ndof": int(mixed_info.ndof),
+        config={"workload": (f"hindfoot {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} h={WORKLOAD['h']}mm "
+                             f"(C2 generator)"), "ndof": int(mixed_info.ndof),
                 "precision": prec,
                 "warm_start": ("learned (3D conv encoder-decoder trained on 96x64x48 C5 solves, prediction inside "
                                "the step)" if warm is not None else "zero (no trained network found)"), "tol": TOL,
@@ -585,7 +586,8 @@ def run_reference(args, rank, world):
     return dict(metric=METRIC, value=round(value, 3), unit="s/solve", n_gpus=world, steps=args.steps,
                 warmup=args.warmup, ms_per_step=round(1e3 * sum(secs) / len(secs), 1), higher_is_better=False,
                 scaling="weak", vs_baseline=None, dtype="f64", data="synthetic (seeded hindfoot generator)",
-                config={"workload": "hindfoot 160x112x96 h=0.5mm (C2 generator)", "tol": TOL,
+                config={"workload": (f"hindfoot {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} h={WORKLOAD['h']}mm "
+                             f"(C2 generator)"), "tol": TOL,
                         "parallelism": "CPU, 1 process"},
                 impl="reference",
                 cpu_baseline={"value": round(value, 3), "unit": "s/solve", "cores": 1, "kind": "port", "sample": desc},
