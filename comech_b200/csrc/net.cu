@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(128) k_head(const bf16* __restrict__ X, int x_
                                               float* __restrict__ pred, const float* __restrict__ target,
                                               const float* __restrict__ wgt, float inv_n, double* __restrict__ loss,
                                               bf16* __restrict__ dX, int dx_ld, float* __restrict__ dW,
-                                              float* __restrict__ db) {
+                                              float* __restrict__ db, const float* __restrict__ dpred_in) {
   __shared__ float sW[3 * kHeadC + 3];
   __shared__ float sdW[3 * kHeadC + 3];
   for (int e = threadIdx.x; e < 3 * kHeadC + 3; e += blockDim.x) {
@@ -458,16 +458,21 @@ __global__ void __launch_bounds__(128) k_head(const bf16* __restrict__ X, int x_
 #pragma unroll
     for (int c = 0; c < 3; ++c) pred[3 * r + c] = o[c];
   }
-  if (!target) return;
+  if (!target && !dpred_in) return;
   float d[3] = {0.f, 0.f, 0.f};
   double l = 0.0;
   if (live) {
-    const float w = wgt[r];
+    if (dpred_in) {                       // a given gradient of the output (the caller's loss)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float e = w > 0.f ? o[c] - target[3 * r + c] : 0.f;
-      l += (double)(w * e * e) * inv_n;
-      d[c] = 2.f * inv_n * w * e;
+      for (int c = 0; c < 3; ++c) d[c] = dpred_in[3 * r + c];
+    } else {
+      const float w = wgt[r];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float e = w > 0.f ? o[c] - target[3 * r + c] : 0.f;
+        l += (double)(w * e * e) * inv_n;
+        d[c] = 2.f * inv_n * w * e;
+      }
     }
     float dx[kHeadC];
 #pragma unroll
@@ -492,12 +497,64 @@ __global__ void __launch_bounds__(128) k_head(const bf16* __restrict__ X, int x_
     if (lane == 0) atomicAdd(&sdW[3 * kHeadC + c], s);
   }
   l = warp_sum(l);
-  if (lane == 0 && l != 0.0) atomicAdd(loss, l);
+  if (lane == 0 && l != 0.0 && loss) atomicAdd(loss, l);
   __syncthreads();
   for (int e = threadIdx.x; e < 3 * kHeadC + 3; e += blockDim.x) {
     if (e < 3 * kHeadC) atomicAdd(dW + e, sdW[e]);
     else atomicAdd(db + e - 3 * kHeadC, sdW[e]);
   }
+}
+
+// Loss of a prediction on a network grid: weighted squared error (mse_scale) plus the stiffness-weighted squared
+// error of its differences along the grid edges (h1_scale): the edge from node (x,y,z) to its +1 neighbour along
+// an axis carries the weight E / e_ref of the cell at (x,y,z) (E from the input channel 0 = log10 E / 4; zero for
+// inactive cells), so the second term follows the strain energy of the error the way the solve weighs it.  pred
+// NULL: the target's own norms (loss only).  Adds the gradient to dpred (if not NULL) and the loss to *loss.
+__global__ void k_loss(FebNetGrid net, const bf16* __restrict__ xin, const float* __restrict__ pred,
+                       const float* __restrict__ T, const float* __restrict__ wgt, float e_ref_inv, float mse_scale,
+                       float h1_scale, double* __restrict__ loss, float* __restrict__ dpred) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double l = 0.0;
+  int x, y, z;
+  if (r < grid_rows(net) && row_cell(net, r, x, y, z) && wgt[r] > 0.f) {
+    float e0[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e0[c] = (pred ? pred[3 * r + c] : 0.f) - T[3 * r + c];
+    if (mse_scale != 0.f) {
+      l += (double)mse_scale * (e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
+      if (dpred) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(dpred + 3 * r + c, 2.f * mse_scale * e0[c]);
+      }
+    }
+    const bf16* xr = xin + r * 32;
+    const float w = __bfloat162float(xr[2]) > 0.f ? exp10f(4.f * __bfloat162float(xr[0])) * e_ref_inv : 0.f;
+    if (h1_scale != 0.f && w > 0.f) {
+      const int n3[3] = {net.nx, net.ny, net.nz};
+      const int c3[3] = {x, y, z};
+      const int64_t off[3] = {(int64_t)(net.ny + 2) * (net.nz + 2), net.nz + 2, 1};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (c3[a] + 1 >= n3[a]) continue;
+        const int64_t r2 = r + off[a];
+        if (!(wgt[r2] > 0.f)) continue;
+        float dd[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dd[c] = ((pred ? pred[3 * r2 + c] : 0.f) - T[3 * r2 + c]) - e0[c];
+        l += (double)(h1_scale * w) * (dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+        if (dpred) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float g = 2.f * h1_scale * w * dd[c];
+            atomicAdd(dpred + 3 * r2 + c, g);
+            atomicAdd(dpred + 3 * r + c, -g);
+          }
+        }
+      }
+    }
+  }
+  l = block_sum(l);
+  if (threadIdx.x == 0 && l != 0.0) atomicAdd(loss, l);
 }
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
@@ -794,7 +851,7 @@ extern "C" int feb_net_head(const void* X, int32_t x_ld, int64_t rows, const flo
   }
   k_head<<<div_up(rows, 128), 128, 0, (cudaStream_t)stream>>>(reinterpret_cast<const bf16*>(X), x_ld, rows, W, b, pred,
                                                               target, wgt, inv_n, loss, reinterpret_cast<bf16*>(dX),
-                                                              dx_ld, dW, db);
+                                                              dx_ld, dW, db, nullptr);
   note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
@@ -870,6 +927,36 @@ extern "C" int feb_net_to_nodes(FebNetGrid net, const double* hn, const float* p
   }
   k_net_to_nodes<<<div_up(nnode_total, kThreads), kThreads, 0, (cudaStream_t)stream>>>(net, A, pred, scale, orig,
                                                                                        nnode_total, x0);
+  note_launch();
+  FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+extern "C" int feb_net_head_grad(const void* X, int32_t x_ld, int64_t rows, const float* W, const float* dpred,
+                                 void* dX, int32_t dx_ld, float* dW, float* db, void* stream) {
+  if (!X || !W || !dpred || !dX || !dW || !db || rows < 1 || x_ld < kHeadC || x_ld % 8 || dx_ld < kHeadC || dx_ld % 8) {
+    set_last_error("feb_net_head_grad: bad argument");
+    return FEB_ERR_ARG;
+  }
+  // the bias only enters the recomputed output, which this pass does not use
+  k_head<<<div_up(rows, 128), 128, 0, (cudaStream_t)stream>>>(reinterpret_cast<const bf16*>(X), x_ld, rows, W, W,
+                                                              nullptr, nullptr, nullptr, 0.f, nullptr,
+                                                              reinterpret_cast<bf16*>(dX), dx_ld, dW, db, dpred);
+  note_launch();
+  FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+extern "C" int feb_net_loss(FebNetGrid net, const void* xin, const float* pred, const float* target, const float* wgt,
+                            float e_ref_inv, float mse_scale, float h1_scale, double* loss, float* dpred, void* stream) {
+  if (!grid_ok(net) || !xin || !target || !wgt || !loss || !(e_ref_inv > 0.f)) {
+    set_last_error("feb_net_loss: bad argument");
+    return FEB_ERR_ARG;
+  }
+  const int64_t rows = grid_rows(net);
+  k_loss<<<div_up(rows, kThreads), kThreads, 0, (cudaStream_t)stream>>>(net, reinterpret_cast<const bf16*>(xin), pred,
+                                                                        target, wgt, e_ref_inv, mse_scale, h1_scale,
+                                                                        loss, dpred);
   note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;

@@ -8,9 +8,10 @@ interposition, fusion, load scaling; ``synth.hindfoot_problem``).  The host core
 process pool started before the first CUDA call); the GPU solves each in FP64 to rel-res 1e-8 (the plain
 GMG-PCG) and turns inputs and solution into the network's input and target, kept on the device for training.
 
-Training: Adam on the weighted mean squared error of the displacement (in units of ``u_unit``, scaled by the
-total load), gradients accumulated over ``--batch`` instances, cosine learning-rate decay, all passes in
-libfeb200.so.  Evaluation on the held-out instances: mixed-precision PCG iterations and time to rel-res 1e-8
+Training: Adam on the relative squared error of the displacement (in units of ``u_unit``, scaled by the total
+load; weight ``--mse``) plus the relative stiffness-weighted squared error of its differences along the grid edges
+(weight ``--h1``; ``feb_net_loss``), the part of the error that the solve's energy norm weighs; gradients
+accumulated over ``--batch`` instances, cosine learning-rate decay, all passes in libfeb200.so.  Evaluation on the held-out instances: mixed-precision PCG iterations and time to rel-res 1e-8
 from zero and from the network's prediction (as given, and as ``feb_solve`` prepares it by default: one
 preconditioner application, then its energy-optimal multiple, or a zero start when that multiple is not positive),
 the prediction's relative error, and the fallback rate.
@@ -151,6 +152,8 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
     ap.add_argument("--time-budget", type=float, default=0.0, help="stop training after this many seconds (0: none)")
+    ap.add_argument("--h1", type=float, default=1.0, help="weight of the stiffness-weighted edge term (0: plain MSE)")
+    ap.add_argument("--mse", type=float, default=0.2, help="weight of the squared error when --h1 > 0")
     ap.add_argument("--eval-only", default=None, help="evaluate these weights on --held instances (no training)")
     args = ap.parse_args(argv)
     nw = args.workers or max(1, min(32, (os.cpu_count() or 2) - 2))
@@ -177,6 +180,7 @@ def main(argv=None):
     T = torch.zeros(N + Nh, rows, 3, dtype=torch.float32, device="cuda")
     Wt = torch.zeros(N + Nh, rows, dtype=torch.float32, device="cuda")
     inv_n = np.zeros(N + Nh)
+    inv_h1 = np.zeros(N + Nh)
     loadf = np.zeros(N + Nh)
     held = {}
     net = warmnet.WarmNet(seed=0, grid=GRID)
@@ -199,6 +203,7 @@ def main(argv=None):
         T[i].copy_(Ti)
         Wt[i].copy_(wi)
         inv_n[i] = 1.0 / max(float(wi.sum().item()), 1.0)
+        inv_h1[i] = 1.0 / max(warmnet.h1_norm(X[i], GRID, T[i], Wt[i]), 1e-30)
         if i >= N:
             held[i] = P
     pool.close()
@@ -206,6 +211,10 @@ def main(argv=None):
     t_data = time.perf_counter() - t_start
 
     # ---------------------------------------------------------------------------------------------- training
+    def loss_scales(j, nb):
+        # relative squared error (weight args.mse) + relative stiffness-weighted edge error, averaged over the batch
+        return None if args.h1 <= 0 else (args.mse * inv_n[j] / nb, args.h1 * inv_h1[j] / nb)
+
     rng = np.random.default_rng(0)
     steps_per_epoch = N // args.batch
     total = steps_per_epoch * args.epochs
@@ -220,7 +229,7 @@ def main(argv=None):
         for s in range(steps_per_epoch):
             for j in perm[s * args.batch:(s + 1) * args.batch]:
                 net.forward(X[j], GRID)
-                net.backward(X[j], GRID, T[j], Wt[j], inv_n[j] / args.batch)
+                net.backward(X[j], GRID, T[j], Wt[j], inv_n[j] / args.batch, h1=loss_scales(j, args.batch))
             net.adam(cosine(step, total, args.lr, args.lr * 0.02), clip=10.0)
             step += 1
         train_loss = float(B["loss"].item()) / steps_per_epoch
@@ -228,7 +237,7 @@ def main(argv=None):
         B["loss"].zero_()
         for j in range(N, N + Nh):
             net.forward(X[j], GRID)
-            net.backward(X[j], GRID, T[j], Wt[j], inv_n[j])
+            net.backward(X[j], GRID, T[j], Wt[j], inv_n[j], h1=loss_scales(j, 1))
         net.grad.zero_()
         val_loss = float(B["loss"].item()) / max(Nh, 1)
         hist.append(dict(epoch=ep, train_loss=train_loss, val_loss=val_loss, t=round(time.perf_counter() - t1, 1)))

@@ -33,6 +33,7 @@ WIDTHS = (32, 64, 128, 256)
 CIN = 32
 TAPS = {"conv3": 27, "down": 8, "up": 8}
 REF_LOAD = 450.0
+E_REF_INV = 1e-4          # 1 / E of cortical bone (MPa): stiffness weights of the edge term of the training loss
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warm_hindfoot_96x64x48.npz")
 
 
@@ -170,7 +171,7 @@ class WarmNet:
         B = dict(G=G, R=R,
                  a0=z(0, c0), cat0=z(0, 2 * c0), D1=z(1, c1), cat1=z(1, 2 * c1), D2=z(2, c2), cat2=z(2, 2 * c2),
                  D3=z(3, c3), B3=z(3, c3), F2=z(2, c2), F1=z(1, c1), F0a=z(0, c0), F0b=z(0, c0),
-                 pred=z(0, 3, torch.float32),
+                 pred=z(0, 3, torch.float32), dpred=z(0, 3, torch.float32),
                  gA0=z(0, c0), gB0=z(0, c0), gcat0=z(0, 2 * c0), gcat1=z(1, 2 * c1), gcat2=z(2, 2 * c2),
                  gA1=z(1, c1), gB1=z(1, c1), gA2=z(2, c2), gB2=z(2, c2), gA3=z(3, c3), gB3=z(3, c3),
                  loss=torch.zeros(1, dtype=torch.float64, device="cuda"))
@@ -240,9 +241,11 @@ class WarmNet:
                                             _stream()))
         return B["pred"]
 
-    def backward(self, x, dims, target, wgt, inv_n):
+    def backward(self, x, dims, target, wgt, inv_n, h1=None):
         """Loss (device scalar, accumulated in the buffers' `loss`) and parameter gradients (accumulated in
-        `grad`) of the weighted mean squared error of the last forward pass."""
+        `grad`) of the last forward pass: the weighted mean squared error (scaled by inv_n), or with ``h1`` =
+        (mse_scale, h1_scale) that error times mse_scale plus the stiffness-weighted squared error of the
+        prediction's differences along the grid edges times h1_scale (``feb_net_loss``)."""
         B = self.buffers(dims)
         G = B["G"]
         c0, c1, c2, c3 = self.c
@@ -250,9 +253,16 @@ class WarmNet:
         U = _lib.GATHER_UP
         k = self.bwd
         lib, s = _lib.load(), _stream()
-        _lib.check(lib.feb_net_head(_ptr(B["F0b"]), c0, B["R"][0], _ptr(self.W("head")), _ptr(self.b("head")), None,
-                                    _ptr(target), _ptr(wgt), C.c_float(inv_n), _ptr(B["loss"]), _ptr(B["gA0"]), c0,
-                                    _ptr(self.gW("head")), _ptr(self.gb("head")), s))
+        if h1 is None:
+            _lib.check(lib.feb_net_head(_ptr(B["F0b"]), c0, B["R"][0], _ptr(self.W("head")), _ptr(self.b("head")),
+                                        None, _ptr(target), _ptr(wgt), C.c_float(inv_n), _ptr(B["loss"]),
+                                        _ptr(B["gA0"]), c0, _ptr(self.gW("head")), _ptr(self.gb("head")), s))
+        else:
+            B["dpred"].zero_()
+            _lib.check(lib.feb_net_loss(_lib.FebNetGrid(*dims), _ptr(x), _ptr(B["pred"]), _ptr(target), _ptr(wgt),
+                                        E_REF_INV, float(h1[0]), float(h1[1]), _ptr(B["loss"]), _ptr(B["dpred"]), s))
+            _lib.check(lib.feb_net_head_grad(_ptr(B["F0b"]), c0, B["R"][0], _ptr(self.W("head")), _ptr(B["dpred"]),
+                                             _ptr(B["gA0"]), c0, _ptr(self.gW("head")), _ptr(self.gb("head")), s))
 
         def conv_back(name, G_, Pbuf, p_c0, na, Qbuf, q_c0, nb):
             self._wgrad(S, G_, None, Pbuf, p_c0, na, Qbuf, q_c0, nb, self.gW(name))
@@ -401,6 +411,15 @@ def load_z(loads):
     if not ln:
         return np.zeros(0, np.int64), np.zeros(0)
     return np.concatenate(ln), np.concatenate(lz)
+
+
+def h1_norm(x, net_dims, target, wgt):
+    """The stiffness-weighted edge-difference norm of a target (the normaliser of that loss term); a host float."""
+    torch = _torch()
+    acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().feb_net_loss(_lib.FebNetGrid(*net_dims), _ptr(x), None, _ptr(target), _ptr(wgt), E_REF_INV,
+                                        0.0, 1.0, _ptr(acc), None, _stream()))
+    return float(acc.item())
 
 
 def load_targets(net_dims, U, scale):

@@ -312,6 +312,20 @@ FEB_API int feb_net_head(const void* X, int32_t x_ld, int64_t rows, const float*
                          const float* target, const float* wgt, float inv_n, double* loss, void* dX, int32_t dx_ld,
                          float* dW, float* db, void* stream);
 
+/* Backward pass of the head for a given gradient dpred [dev] (fp32, 3 per row) of its output: dX[r][k] = (X[r][k] >
+ * 0) sum_c dpred[r][c] W[c][k]; dW, db accumulated. */
+FEB_API int feb_net_head_grad(const void* X, int32_t x_ld, int64_t rows, const float* W, const float* dpred, void* dX,
+                              int32_t dx_ld, float* dW, float* db, void* stream);
+
+/* Training loss of a prediction pred [dev] (fp32, 3 per row; NULL: zero) against target / wgt on the network grid:
+ * mse_scale sum_r wgt |e|^2 plus h1_scale sum over grid edges (node r to its +1 neighbour along x, y, z, both with
+ * wgt > 0) of (E / e_ref) |e(r2) - e(r)|^2, e = pred - target, E the Young's modulus of the cell at r read from the
+ * network input xin (channel 0 = log10 E / 4, channel 2 = active; 0 for inactive cells).  The second term weighs the
+ * error's differences by stiffness, as the strain energy of the error does.  loss [dev] += the sum; dpred [dev] (if
+ * not NULL) += its gradient. */
+FEB_API int feb_net_loss(FebNetGrid net, const void* xin, const float* pred, const float* target, const float* wgt,
+                         float e_ref_inv, float mse_scale, float h1_scale, double* loss, float* dpred, void* stream);
+
 /* Adam step on n FP32 parameters (bias-corrected, step >= 1); the gradient is scaled by gscale first and
  * zeroed afterwards.  sumsq (if not NULL) receives += sum of squared gradients before the step is taken. */
 FEB_API int feb_net_adam(float* w, float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,

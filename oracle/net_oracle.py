@@ -230,3 +230,29 @@ def init_params(c, cin=32, cin_used=6, seed=0):
         P[name] = (W, np.zeros(co))
     P["head"] = (rng.normal(0.0, 1e-2, (3, c[0])), np.zeros(3))
     return P
+
+
+def edge_loss(xin, pred, target, wgt, e_ref_inv, mse_scale, h1_scale):
+    """Training loss of the warm start with its stiffness-weighted edge term, and its gradient in the prediction.
+
+    mse_scale sum_v wgt |e|^2 + h1_scale sum over edges (v, v + unit step along x, y or z; both with wgt > 0) of
+    w(v) |e(v + step) - e(v)|^2, e = pred - target, w(v) = 10^(4 xin[v][0]) e_ref_inv for active cells
+    (xin[v][2] > 0), else 0.  Arrays over the cells [nx, ny, nz, ...].  Returns (loss, dpred)."""
+    e = np.where((wgt > 0)[..., None], pred - target, 0.0)
+    valid = wgt > 0
+    loss = mse_scale * float((e * e).sum())
+    g = 2.0 * mse_scale * e
+    w = np.where(xin[..., 2] > 0, 10.0 ** (4.0 * xin[..., 0]) * e_ref_inv, 0.0) * valid
+    for a in range(3):
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[a] = slice(0, -1)
+        hi[a] = slice(1, None)
+        lo, hi = tuple(lo), tuple(hi)
+        m = w[lo] * valid[hi]
+        d = (pred[hi] - target[hi]) - (pred[lo] - target[lo])
+        loss += h1_scale * float((m[..., None] * d * d).sum())
+        gd = 2.0 * h1_scale * m[..., None] * d
+        g[hi] += gd
+        g[lo] -= gd
+    return loss, g
