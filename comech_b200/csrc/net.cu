@@ -26,14 +26,22 @@ namespace {
 using bf16 = __nv_bfloat16;
 
 constexpr int kConvThreads = 128;
-constexpr int kStages = 4;
-constexpr int kKS = 32;                          // channels per K step (two K16 MMAs)
-constexpr int kABytes = 128 * kKS * 2;           // A slot: 128 rows x 32 BF16
-constexpr int kAHalf = 128 * 16;                 // bytes between 8-channel core-matrix columns of A
+constexpr int kKS = 32;                          // channels per K step slice (two K16 MMAs per tap)
 
-template <int NT> struct ConvSmem {
-  static constexpr int kB = NT * kKS * 2;
-  static constexpr int kStage = kABytes + kB;
+// Shared-memory ring of the convolution.  A 3x3x3 (SHIFT) step covers the three z taps of one (x, y) offset: the
+// rows they read are one window of 130 rows (stored as 136) shifted by one row per tap, so one A tile serves three
+// MMA groups through descriptors 16 bytes apart, and B holds the three taps' weights.  Other gathers: 128 rows,
+// one tap per step.
+template <int NT, int GATHER> struct ConvSmem {
+  static constexpr bool kZ3 = GATHER == FEB_GATHER_SHIFT;
+  static constexpr int kARows = kZ3 ? 136 : 128;
+  static constexpr int kAHalf = kARows * 16;     // bytes between 8-channel core-matrix columns of A
+  static constexpr int kA = kARows * kKS * 2;
+  static constexpr int kTaps = kZ3 ? 3 : 1;      // taps per step
+  static constexpr int kBTap = NT * kKS * 2;
+  static constexpr int kB = kTaps * kBTap;
+  static constexpr int kStage = kA + kB;
+  static constexpr int kStages = (kZ3 && NT == 128) ? 3 : 4;
   static constexpr size_t kTotal = (size_t)kStages * kStage + 8 * kStages + 16;
 };
 
@@ -70,38 +78,46 @@ __device__ __forceinline__ int64_t fine_off(const FebNetGrid& f, int tap) {
   return ((int64_t)(tap >> 2) * (f.ny + 2) + ((tap >> 1) & 1)) * (f.nz + 2) + (tap & 1);
 }
 
-// one K step (tap, channel slice) of A (gathered rows) and B (weights) into a ring slot
+// one K step of A (gathered rows) and B (weights) into a ring slot.  SHIFT: step = ((x, y) offset p, channel slice),
+// A row i = input row m0 - 1 + i + offset(p), B = the weights of taps 3p, 3p+1, 3p+2 (dz = -1, 0, +1).  DOWN / ONE:
+// step = (tap, channel slice), A row i = the tap's source row of output row m0 + i.
 template <int NT, int GATHER>
 __device__ __forceinline__ void conv_load(const FebConv& P, int step, int kcs, uint32_t sA, int64_t m0, int64_t M,
                                           int64_t Pin, const int64_t (&fbase)[4], int n0, int tid) {
-  const int tap = step / kcs, c0 = (step - tap * kcs) * kKS;
-  const int ch = tid & 3;
+  using S = ConvSmem<NT, GATHER>;
+  const int grp = step / kcs, c0 = (step - grp * kcs) * kKS;
   const bf16* in = reinterpret_cast<const bf16*>(P.in);
-  int64_t off = 0;
-  if (GATHER == FEB_GATHER_SHIFT) off = shift_off(P.grid, tap);
-  if (GATHER == FEB_GATHER_DOWN) off = fine_off(P.fine, tap);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int row = (tid >> 2) + 32 * i;
-    const int64_t m = m0 + row;
-    int64_t src = -1;
-    if (GATHER == FEB_GATHER_SHIFT) {
-      src = m + off;
-      if (m >= M || src < 0 || src >= Pin) src = -1;
-    } else if (GATHER == FEB_GATHER_DOWN) {
-      src = fbase[i] >= 0 ? fbase[i] + off : -1;
-    } else {
-      src = m < M ? m : -1;
+  if (GATHER == FEB_GATHER_SHIFT) {
+    const int dx = grp / 3 - 1, dy = grp % 3 - 1;
+    const int64_t off = ((int64_t)dx * (P.grid.ny + 2) + dy) * (P.grid.nz + 2);
+    for (int e = tid; e < S::kARows * 4; e += kConvThreads) {
+      const int row = e >> 2, ch = e & 3;
+      int64_t src = m0 - 1 + row + off;
+      if (row >= 130 || src < 0 || src >= Pin) src = -1;
+      const bf16* g = src >= 0 ? in + src * P.in_ld + P.in_c0 + c0 + ch * 8 : in;
+      cp16(sA + ch * S::kAHalf + row * 16, g, src >= 0 ? 16 : 0);
     }
-    const bf16* g = src >= 0 ? in + src * P.in_ld + P.in_c0 + c0 + ch * 8 : in;
-    cp16(sA + ch * kAHalf + row * 16, g, src >= 0 ? 16 : 0);
+  } else {
+    const int ch = tid & 3;
+    const int64_t off = GATHER == FEB_GATHER_DOWN ? fine_off(P.fine, grp) : 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = (tid >> 2) + 32 * i;
+      const int64_t m = m0 + row;
+      int64_t src;
+      if (GATHER == FEB_GATHER_DOWN) src = fbase[i] >= 0 ? fbase[i] + off : -1;
+      else src = m < M ? m : -1;
+      const bf16* g = src >= 0 ? in + src * P.in_ld + P.in_c0 + c0 + ch * 8 : in;
+      cp16(sA + ch * S::kAHalf + row * 16, g, src >= 0 ? 16 : 0);
+    }
   }
   const bf16* wt = reinterpret_cast<const bf16*>(P.wt);
-  const uint32_t sB = sA + kABytes;
+  const uint32_t sB = sA + S::kA;
+  const int tap0 = GATHER == FEB_GATHER_SHIFT ? 3 * grp : grp;
 #pragma unroll
-  for (int i = 0; i < NT / 32; ++i) {
-    const int e = tid + kConvThreads * i, n = e >> 2, c = e & 3;
-    cp16(sB + c * (NT * 16) + n * 16, wt + ((int64_t)tap * P.n + n0 + n) * P.kc + c0 + c * 8, 16);
+  for (int i = 0; i < S::kTaps * NT / 32; ++i) {
+    const int e = tid + kConvThreads * i, t = e / (4 * NT), rem = e - t * 4 * NT, n = rem >> 2, c = rem & 3;
+    cp16(sB + t * S::kBTap + c * (NT * 16) + n * 16, wt + ((int64_t)(tap0 + t) * P.n + n0 + n) * P.kc + c0 + c * 8, 16);
   }
 }
 
@@ -129,7 +145,8 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
 template <int NT, int GATHER, int SCATTER>
 __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t M, int64_t Pin) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  using S = ConvSmem<NT>;
+  using S = ConvSmem<NT, GATHER>;
+  constexpr int kStages = S::kStages;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kStages * S::kStage);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kStages);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -154,8 +171,8 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
     }
   }
   const int kcs = P.kc / kKS;
-  const int ntap = GATHER == FEB_GATHER_SHIFT ? 27 : (GATHER == FEB_GATHER_DOWN ? 8 : 1);
-  const int nk = ntap * kcs;
+  const int ngroups = GATHER == FEB_GATHER_SHIFT ? 9 : (GATHER == FEB_GATHER_DOWN ? 8 : 1);
+  const int nk = ngroups * kcs;
   const uint32_t base = tc::smem_addr(smem);
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
@@ -173,11 +190,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
     if (!ok) break;
     const int slot = it % kStages;
     if (tid == 0) {
-      const uint32_t a = base + slot * S::kStage, b = a + kABytes;
+      const uint32_t a = base + slot * S::kStage, b = a + S::kA;
 #pragma unroll
-      for (int s = 0; s < 2; ++s)
-        tc::mma_bf16(tmem, tc::smem_desc(a + 2 * s * kAHalf, kAHalf, 128), tc::smem_desc(b + 2 * s * NT * 16, NT * 16, 128),
-                     idesc, (it | s) != 0);
+      for (int t = 0; t < S::kTaps; ++t)
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+          tc::mma_bf16(tmem, tc::smem_desc(a + t * 16 + 2 * s * S::kAHalf, S::kAHalf, 128),
+                       tc::smem_desc(b + t * S::kBTap + 2 * s * NT * 16, NT * 16, 128), idesc, (it | t | s) != 0);
       tc::commit(mbar + slot);
     }
     const int nxt = it + kStages - 1;
@@ -705,11 +724,11 @@ int launch_conv(const FebConv& c, int64_t M, int64_t Pin, cudaStream_t s) {
   static bool prepared = false;
   if (!prepared) {
     FEB_CUDA(cudaFuncSetAttribute(k_conv<NT, GATHER, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)ConvSmem<NT>::kTotal));
+                                  (int)ConvSmem<NT, GATHER>::kTotal));
     prepared = true;
   }
   const dim3 grid(div_up(M, 128), c.n / NT);
-  k_conv<NT, GATHER, SCATTER><<<grid, kConvThreads, ConvSmem<NT>::kTotal, s>>>(c, M, Pin);
+  k_conv<NT, GATHER, SCATTER><<<grid, kConvThreads, ConvSmem<NT, GATHER>::kTotal, s>>>(c, M, Pin);
   note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
