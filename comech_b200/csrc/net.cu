@@ -1,8 +1,8 @@
 // Learned warm start: the layers of a 3D convolutional encoder-decoder, its training steps, and its coupling to
 // the solve (network input from the solve's inputs, targets from solutions, the initial guess from a prediction).
 //
-// Convolutions are implicit GEMMs on the 5th-generation tensor cores.  A CTA of 128 threads owns 128 rows (voxels
-// of the padded grid) x NT output channels; its FP32 accumulator lives in NT columns of tensor memory.  The K loop
+// Convolutions are implicit GEMMs on the 5th-generation tensor cores.  A CTA of 128 threads owns 128 rows (256 for
+// 3x3x3 convolutions; voxels of the padded grid) x NT output channels; its FP32 accumulators live in tensor memory.  The K loop
 // runs over (tap, 32-channel slice): each step stages 128 gathered input rows x 32 channels (cp.async, zero fill for
 // rows outside the grid) and NT weight rows x 32 channels in a 4-slot shared-memory ring, in the K-major
 // unswizzled core-matrix layout, and one thread issues two M128 x NT x K16 BF16 MMAs and commits them to the slot's
@@ -28,13 +28,15 @@ using bf16 = __nv_bfloat16;
 constexpr int kConvThreads = 128;
 constexpr int kKS = 32;                          // channels per K step slice (two K16 MMAs per tap)
 
-// Shared-memory ring of the convolution.  A 3x3x3 (SHIFT) step covers the three z taps of one (x, y) offset: the
-// rows they read are one window of 130 rows (stored as 136) shifted by one row per tap, so one A tile serves three
-// MMA groups through descriptors 16 bytes apart, and B holds the three taps' weights.  Other gathers: 128 rows,
-// one tap per step.
+// Shared-memory ring of the convolution.  A 3x3x3 (SHIFT) CTA owns 256 output rows (two M128 accumulators) and a
+// step covers the three z taps of one (x, y) offset: the rows they read are one window of 258 rows (stored as 264)
+// shifted by one row per tap, so one A tile serves the three taps and both halves through descriptors 16 bytes
+// apart (12 MMAs per step), and B holds the three taps' weights.  Other gathers: 128 rows, one tap per step.
 template <int NT, int GATHER> struct ConvSmem {
   static constexpr bool kZ3 = GATHER == FEB_GATHER_SHIFT;
-  static constexpr int kARows = kZ3 ? 136 : 128;
+  static constexpr int kM = kZ3 ? 256 : 128;     // output rows per CTA (kM / 128 accumulators of NT columns)
+  static constexpr int kHalves = kM / 128;
+  static constexpr int kARows = kZ3 ? kM + 8 : 128;
   static constexpr int kAHalf = kARows * 16;     // bytes between 8-channel core-matrix columns of A
   static constexpr int kA = kARows * kKS * 2;
   static constexpr int kTaps = kZ3 ? 3 : 1;      // taps per step
@@ -93,7 +95,7 @@ __device__ __forceinline__ void conv_load(const FebConv& P, int step, int kcs, u
     for (int e = tid; e < S::kARows * 4; e += kConvThreads) {
       const int row = e >> 2, ch = e & 3;
       int64_t src = m0 - 1 + row + off;
-      if (row >= 130 || src < 0 || src >= Pin) src = -1;
+      if (row >= S::kM + 2 || src < 0 || src >= Pin) src = -1;
       const bf16* g = src >= 0 ? in + src * P.in_ld + P.in_c0 + c0 + ch * 8 : in;
       cp16(sA + ch * S::kAHalf + row * 16, g, src >= 0 ? 16 : 0);
     }
@@ -150,15 +152,16 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kStages * S::kStage);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kStages);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t m0 = (int64_t)blockIdx.x * 128;
+  const int64_t m0 = (int64_t)blockIdx.x * S::kM;
   const int n0 = blockIdx.y * NT;
+  constexpr uint32_t kCols = NT * S::kHalves;
 
   if (tid == 0) {
 #pragma unroll
     for (int s = 0; s < kStages; ++s) tc::mbar_init(mbar + s, 1);
     tc::mbar_fence_init();
   }
-  if (warp == 0) tc::tmem_alloc(tslot, NT);
+  if (warp == 0) tc::tmem_alloc(tslot, kCols);
 
   // DOWN gather: the fine row of cell 2V of this thread's four A rows (-1 for shell / out-of-range rows)
   int64_t fbase[4] = {-1, -1, -1, -1};
@@ -192,11 +195,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
     if (tid == 0) {
       const uint32_t a = base + slot * S::kStage, b = a + S::kA;
 #pragma unroll
-      for (int t = 0; t < S::kTaps; ++t)
+      for (int h = 0; h < S::kHalves; ++h)
 #pragma unroll
-        for (int s = 0; s < 2; ++s)
-          tc::mma_bf16(tmem, tc::smem_desc(a + t * 16 + 2 * s * S::kAHalf, S::kAHalf, 128),
-                       tc::smem_desc(b + t * S::kBTap + 2 * s * NT * 16, NT * 16, 128), idesc, (it | t | s) != 0);
+        for (int t = 0; t < S::kTaps; ++t)
+#pragma unroll
+          for (int s = 0; s < 2; ++s)
+            tc::mma_bf16(tmem + (uint32_t)(h * NT), tc::smem_desc(a + (h * 128 + t) * 16 + 2 * s * S::kAHalf, S::kAHalf, 128),
+                         tc::smem_desc(b + t * S::kBTap + 2 * s * NT * 16, NT * 16, 128), idesc, (it | t | s) != 0);
       tc::commit(mbar + slot);
     }
     const int nxt = it + kStages - 1;
@@ -212,15 +217,17 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
   ok = __syncthreads_and(ok ? 1 : 0) != 0;
 
   if (ok) {
-    const int64_t m = m0 + 32 * warp + lane;
+   bf16* out = reinterpret_cast<bf16*>(P.out);
+   const bf16* mask = reinterpret_cast<const bf16*>(P.mask);
+#pragma unroll 1
+   for (int h = 0; h < S::kHalves; ++h) {
+    const int64_t m = m0 + h * 128 + 32 * warp + lane;
     int x = 0, y = 0, z = 0;
     const bool inside = m < M && row_cell(P.grid, m, x, y, z);
-    bf16* out = reinterpret_cast<bf16*>(P.out);
-    const bf16* mask = reinterpret_cast<const bf16*>(P.mask);
 #pragma unroll 1
     for (int cc = 0; cc < NT; cc += 32) {
       float v[32];
-      tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cc, v);
+      tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(h * NT + cc), v);
       tc::wait_ld();
       const int n = n0 + cc;
       int64_t orow;
@@ -272,13 +279,14 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const FebConv P, int64_t 
 #pragma unroll
       for (int q = 0; q < 4; ++q) dst[q] = pack8(v + 8 * q);
     }
+   }
   } else if (tid == 0 && P.status) {
     atomicExch(P.status, 1);
   }
   cp_wait<0>();
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) tc::tmem_free(tmem, NT);
+  if (warp == 0) tc::tmem_free(tmem, kCols);
 }
 
 // ------------------------------------------------------------------------------------------ weight gradient
@@ -727,7 +735,7 @@ int launch_conv(const FebConv& c, int64_t M, int64_t Pin, cudaStream_t s) {
                                   (int)ConvSmem<NT, GATHER>::kTotal));
     prepared = true;
   }
-  const dim3 grid(div_up(M, 128), c.n / NT);
+  const dim3 grid(div_up(M, ConvSmem<NT, GATHER>::kM), c.n / NT);
   k_conv<NT, GATHER, SCATTER><<<grid, kConvThreads, ConvSmem<NT, GATHER>::kTotal, s>>>(c, M, Pin);
   note_launch();
   FEB_CUDA(cudaGetLastError());
