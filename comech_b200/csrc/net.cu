@@ -43,7 +43,7 @@ template <int NT, int GATHER> struct ConvSmem {
   static constexpr int kBTap = NT * kKS * 2;
   static constexpr int kB = kTaps * kBTap;
   static constexpr int kStage = kA + kB;
-  static constexpr int kStages = (kZ3 && NT == 128) ? 3 : 4;
+  static constexpr int kStages = kZ3 ? 3 : 4;    // 3x3x3: 3 slots keep 3 CTAs per SM at N = 32
   static constexpr size_t kTotal = (size_t)kStages * kStage + 8 * kStages + 16;
 };
 
