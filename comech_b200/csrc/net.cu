@@ -1,14 +1,15 @@
 // Learned warm start: the layers of a 3D convolutional encoder-decoder, its training steps, and its coupling to
 // the solve (network input from the solve's inputs, targets from solutions, the initial guess from a prediction).
 //
-// Convolutions are implicit GEMMs on the 5th-generation tensor cores.  A CTA of 128 threads owns 128 rows (256 for
-// 3x3x3 convolutions; voxels of the padded grid) x NT output channels; its FP32 accumulators live in tensor memory.  The K loop
-// runs over (tap, 32-channel slice): each step stages 128 gathered input rows x 32 channels (cp.async, zero fill for
-// rows outside the grid) and NT weight rows x 32 channels in a 4-slot shared-memory ring, in the K-major
-// unswizzled core-matrix layout, and one thread issues two M128 x NT x K16 BF16 MMAs and commits them to the slot's
-// mbarrier; the slot is refilled once those MMAs have completed, so loads run three steps ahead of the tensor core.
-// The epilogue reads the accumulator back (tcgen05.ld), adds the bias, applies ReLU / the ReLU-gradient mask /
-// accumulation, and stores BF16 rows (direct, or scattered to the 8 fine cells of a transposed stride-2 conv).
+// Convolutions are implicit GEMMs on the 5th-generation tensor cores.  A CTA of 128 threads owns 128 output rows
+// (256 for 3x3x3 convolutions, in two accumulators; rows are voxels of the padded grid) x NT output channels, its
+// FP32 accumulators in tensor memory.  The K loop runs over (tap group, 32-channel slice): each step stages the
+// gathered input rows x 32 channels (cp.async, zero fill for rows outside the grid) and the weight rows in a 3- or
+// 4-slot shared-memory ring, in the K-major unswizzled core-matrix layout, and one thread issues the step's
+// M128 x NT x K16 BF16 MMAs (2 per tap and accumulator) and commits them to the slot's mbarrier; the slot is
+// refilled once those MMAs have completed, so loads run ahead of the tensor core.  The epilogue reads the
+// accumulators back (tcgen05.ld), adds the bias, applies ReLU / the ReLU-gradient mask / accumulation, and stores
+// BF16 rows (direct, or scattered to the 8 fine cells of a transposed stride-2 conv).
 //
 // Weight gradients (a reduction over voxels) use warp-level mma.sync with transposing ldmatrix loads of the
 // row-major activation tiles, split over row chunks with FP32 atomics into the gradient.
