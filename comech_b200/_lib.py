@@ -22,7 +22,7 @@ EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_sol
            "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
            "feb_mix_materials", "feb_net_conv", "feb_net_wgrad", "feb_net_colsum", "feb_net_weights", "feb_net_head",
            "feb_net_adam", "feb_net_sumsq", "feb_net_inputs", "feb_net_targets", "feb_net_to_nodes",
-           "feb_net_head_grad", "feb_net_loss"]
+           "feb_net_head_grad", "feb_net_loss", "feb_net_energy_loss"]
 
 GATHER_SHIFT, GATHER_DOWN, GATHER_ONE, GATHER_UP = 0, 1, 2, 3
 
@@ -128,6 +128,7 @@ def load():
     lib.feb_net_to_nodes.argtypes = [FebNetGrid, P, P, C.c_double, C.POINTER(FebGrid), P, P, C.c_int64, P, P]
     lib.feb_net_head_grad.argtypes = [P, C.c_int32, C.c_int64, P, P, P, C.c_int32, P, P, P]
     lib.feb_net_loss.argtypes = [FebNetGrid, P, P, P, P, C.c_float, C.c_float, C.c_float, P, P, P]
+    lib.feb_net_energy_loss.argtypes = [FebNetGrid, P, P, P, P, P, C.c_float, P, P, P]
     lib.feb_launch_count.argtypes = []
     lib.feb_launch_count.restype = C.c_int64
     lib.feb_last_error.argtypes = []

@@ -18,6 +18,7 @@
 #include <cfloat>
 
 #include "common.cuh"
+#include "element.cuh"
 #include "tcgen05.cuh"
 
 namespace feb {
@@ -585,6 +586,53 @@ __global__ void k_loss(FebNetGrid net, const bf16* __restrict__ xin, const float
   if (threadIdx.x == 0 && l != 0.0) atomicAdd(loss, l);
 }
 
+// Strain energy of a prediction's error on a network grid equal to the FE grid: for every cell whose 8 corner nodes
+// are network nodes (x < nx-1, y < ny-1, z < nz-1) and have targets, with the cell active, e^T K_e e with e = pred -
+// target at the corners and K_e the solve's hex8 element (lambda at the centre, mu 2x2x2) of the cell's Lame
+// constants, read from the network input (channel 0 = log10 E / 4, channel 1 = (nu - 0.3) * 4, channel 2 = active).
+// loss += scale * sum; dpred[corner] += 2 scale K_e e.  pred NULL: the target's own energy.
+__global__ void k_energy_loss(FebNetGrid net, float hx, float hy, float hz, const bf16* __restrict__ xin,
+                              const float* __restrict__ pred, const float* __restrict__ T, const float* __restrict__ wgt,
+                              float scale, double* __restrict__ loss, float* __restrict__ dpred) {
+  const int64_t ncell = (int64_t)(net.nx - 1) * (net.ny - 1) * (net.nz - 1);
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if (c < ncell) {
+    const int z = int(c % (net.nz - 1)), y = int((c / (net.nz - 1)) % (net.ny - 1)),
+              x = int(c / ((int64_t)(net.nz - 1) * (net.ny - 1)));
+    const bf16* xr = xin + prow(net, x, y, z) * 32;
+    bool ok = __bfloat162float(xr[2]) > 0.f;
+    int64_t rows[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      rows[k] = prow(net, x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
+      ok = ok && wgt[rows[k]] > 0.f;
+    }
+    if (ok) {
+      float u[3][8], f[3][8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) u[q][k] = (pred ? pred[3 * rows[k] + q] : 0.f) - T[3 * rows[k] + q];
+      const float E = exp10f(4.f * __bfloat162float(xr[0])), nu = 0.25f * __bfloat162float(xr[1]) + 0.3f;
+      const float m[2] = {E * nu / ((1.f + nu) * (1.f - 2.f * nu)), E / (2.f * (1.f + nu))};
+      const Material<float> mat = make_material<float, MAT_ISO_SRI>(m);
+      hex8_apply<float>(u, hx, hy, hz, 1.f / hx, 1.f / hy, 1.f / hz, mat, f);
+      float s = 0.f;
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          s += u[q][k] * f[q][k];
+          if (dpred) atomicAdd(dpred + 3 * rows[k] + q, 2.f * scale * f[q][k]);
+        }
+      l = (double)scale * s;
+    }
+  }
+  l = block_sum(l);
+  if (threadIdx.x == 0 && l != 0.0) atomicAdd(loss, l);
+}
+
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                        int64_t n, float lr_t, float b1, float b2, float eps, float gscale) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -985,6 +1033,22 @@ extern "C" int feb_net_loss(FebNetGrid net, const void* xin, const float* pred, 
   k_loss<<<div_up(rows, kThreads), kThreads, 0, (cudaStream_t)stream>>>(net, reinterpret_cast<const bf16*>(xin), pred,
                                                                         target, wgt, e_ref_inv, mse_scale, h1_scale,
                                                                         loss, dpred);
+  note_launch();
+  FEB_CUDA(cudaGetLastError());
+  return FEB_OK;
+}
+
+extern "C" int feb_net_energy_loss(FebNetGrid net, const double* h, const void* xin, const float* pred, const float* target,
+                                   const float* wgt, float scale, double* loss, float* dpred, void* stream) {
+  if (!grid_ok(net) || net.nx < 2 || net.ny < 2 || net.nz < 2 || !h || !(h[0] > 0) || !(h[1] > 0) || !(h[2] > 0) ||
+      !xin || !target || !wgt || !loss) {
+    set_last_error("feb_net_energy_loss: bad argument");
+    return FEB_ERR_ARG;
+  }
+  const int64_t ncell = (int64_t)(net.nx - 1) * (net.ny - 1) * (net.nz - 1);
+  k_energy_loss<<<div_up(ncell, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      net, (float)h[0], (float)h[1], (float)h[2], reinterpret_cast<const bf16*>(xin), pred, target, wgt, scale, loss,
+      dpred);
   note_launch();
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;

@@ -153,7 +153,8 @@ def main(argv=None):
     ap.add_argument("--report", default=None)
     ap.add_argument("--time-budget", type=float, default=0.0, help="stop training after this many seconds (0: none)")
     ap.add_argument("--h1", type=float, default=1.0, help="weight of the stiffness-weighted edge term (0: plain MSE)")
-    ap.add_argument("--mse", type=float, default=0.2, help="weight of the squared error when --h1 > 0")
+    ap.add_argument("--mse", type=float, default=0.2, help="weight of the squared error when --h1 or --energy > 0")
+    ap.add_argument("--energy", type=float, default=0.0, help="weight of the error's strain energy (feb_net_energy_loss)")
     ap.add_argument("--eval-only", default=None, help="evaluate these weights on --held instances (no training)")
     args = ap.parse_args(argv)
     nw = args.workers or max(1, min(32, (os.cpu_count() or 2) - 2))
@@ -181,6 +182,7 @@ def main(argv=None):
     Wt = torch.zeros(N + Nh, rows, dtype=torch.float32, device="cuda")
     inv_n = np.zeros(N + Nh)
     inv_h1 = np.zeros(N + Nh)
+    inv_en = np.zeros(N + Nh)
     loadf = np.zeros(N + Nh)
     held = {}
     net = warmnet.WarmNet(seed=0, grid=GRID)
@@ -204,6 +206,7 @@ def main(argv=None):
         Wt[i].copy_(wi)
         inv_n[i] = 1.0 / max(float(wi.sum().item()), 1.0)
         inv_h1[i] = 1.0 / max(warmnet.h1_norm(X[i], GRID, T[i], Wt[i]), 1e-30)
+        inv_en[i] = 1.0 / max(warmnet.energy_norm(X[i], GRID, H, T[i], Wt[i]), 1e-30)
         if i >= N:
             held[i] = P
     pool.close()
@@ -212,8 +215,14 @@ def main(argv=None):
 
     # ---------------------------------------------------------------------------------------------- training
     def loss_scales(j, nb):
-        # relative squared error (weight args.mse) + relative stiffness-weighted edge error, averaged over the batch
-        return None if args.h1 <= 0 else (args.mse * inv_n[j] / nb, args.h1 * inv_h1[j] / nb)
+        # relative squared error (weight args.mse) + relative stiffness-weighted edge error (args.h1), averaged over
+        # the batch; the relative strain energy of the error (args.energy) is passed separately
+        if args.h1 <= 0 and args.energy <= 0:
+            return None
+        return (args.mse * inv_n[j] / nb, args.h1 * inv_h1[j] / nb)
+
+    def energy_scale(j, nb):
+        return None if args.energy <= 0 else (args.energy * inv_en[j] / nb, H)
 
     rng = np.random.default_rng(0)
     steps_per_epoch = N // args.batch
@@ -229,7 +238,8 @@ def main(argv=None):
         for s in range(steps_per_epoch):
             for j in perm[s * args.batch:(s + 1) * args.batch]:
                 net.forward(X[j], GRID)
-                net.backward(X[j], GRID, T[j], Wt[j], inv_n[j] / args.batch, h1=loss_scales(j, args.batch))
+                net.backward(X[j], GRID, T[j], Wt[j], inv_n[j] / args.batch, h1=loss_scales(j, args.batch),
+                             energy=energy_scale(j, args.batch))
             net.adam(cosine(step, total, args.lr, args.lr * 0.02), clip=10.0)
             step += 1
         train_loss = float(B["loss"].item()) / steps_per_epoch
@@ -237,7 +247,7 @@ def main(argv=None):
         B["loss"].zero_()
         for j in range(N, N + Nh):
             net.forward(X[j], GRID)
-            net.backward(X[j], GRID, T[j], Wt[j], inv_n[j], h1=loss_scales(j, 1))
+            net.backward(X[j], GRID, T[j], Wt[j], inv_n[j], h1=loss_scales(j, 1), energy=energy_scale(j, 1))
         net.grad.zero_()
         val_loss = float(B["loss"].item()) / max(Nh, 1)
         hist.append(dict(epoch=ep, train_loss=train_loss, val_loss=val_loss, t=round(time.perf_counter() - t1, 1)))

@@ -241,11 +241,12 @@ class WarmNet:
                                             _stream()))
         return B["pred"]
 
-    def backward(self, x, dims, target, wgt, inv_n, h1=None):
+    def backward(self, x, dims, target, wgt, inv_n, h1=None, energy=None):
         """Loss (device scalar, accumulated in the buffers' `loss`) and parameter gradients (accumulated in
         `grad`) of the last forward pass: the weighted mean squared error (scaled by inv_n), or with ``h1`` =
         (mse_scale, h1_scale) that error times mse_scale plus the stiffness-weighted squared error of the
-        prediction's differences along the grid edges times h1_scale (``feb_net_loss``)."""
+        prediction's differences along the grid edges times h1_scale (``feb_net_loss``); ``energy`` = (scale,
+        spacing (3,)) adds scale times the strain energy of the prediction's error (``feb_net_energy_loss``)."""
         B = self.buffers(dims)
         G = B["G"]
         c0, c1, c2, c3 = self.c
@@ -253,6 +254,8 @@ class WarmNet:
         U = _lib.GATHER_UP
         k = self.bwd
         lib, s = _lib.load(), _stream()
+        if h1 is None and energy is not None:
+            h1 = (0.0, 0.0)
         if h1 is None:
             _lib.check(lib.feb_net_head(_ptr(B["F0b"]), c0, B["R"][0], _ptr(self.W("head")), _ptr(self.b("head")),
                                         None, _ptr(target), _ptr(wgt), C.c_float(inv_n), _ptr(B["loss"]),
@@ -261,6 +264,11 @@ class WarmNet:
             B["dpred"].zero_()
             _lib.check(lib.feb_net_loss(_lib.FebNetGrid(*dims), _ptr(x), _ptr(B["pred"]), _ptr(target), _ptr(wgt),
                                         E_REF_INV, float(h1[0]), float(h1[1]), _ptr(B["loss"]), _ptr(B["dpred"]), s))
+            if energy is not None:
+                hsp = np.ascontiguousarray(energy[1], np.float64)
+                _lib.check(lib.feb_net_energy_loss(_lib.FebNetGrid(*dims), hsp.ctypes.data_as(C.c_void_p), _ptr(x),
+                                                   _ptr(B["pred"]), _ptr(target), _ptr(wgt), float(energy[0]),
+                                                   _ptr(B["loss"]), _ptr(B["dpred"]), s))
             _lib.check(lib.feb_net_head_grad(_ptr(B["F0b"]), c0, B["R"][0], _ptr(self.W("head")), _ptr(B["dpred"]),
                                              _ptr(B["gA0"]), c0, _ptr(self.gW("head")), _ptr(self.gb("head")), s))
 
@@ -419,6 +427,16 @@ def h1_norm(x, net_dims, target, wgt):
     acc = torch.zeros(1, dtype=torch.float64, device="cuda")
     _lib.check(_lib.load().feb_net_loss(_lib.FebNetGrid(*net_dims), _ptr(x), None, _ptr(target), _ptr(wgt), E_REF_INV,
                                         0.0, 1.0, _ptr(acc), None, _stream()))
+    return float(acc.item())
+
+
+def energy_norm(x, net_dims, spacing, target, wgt):
+    """The strain energy of a target field on the network grid (the normaliser of the energy loss); a host float."""
+    torch = _torch()
+    acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+    hsp = np.ascontiguousarray(spacing, np.float64)
+    _lib.check(_lib.load().feb_net_energy_loss(_lib.FebNetGrid(*net_dims), hsp.ctypes.data_as(C.c_void_p), _ptr(x), None,
+                                               _ptr(target), _ptr(wgt), 1.0, _ptr(acc), None, _stream()))
     return float(acc.item())
 
 

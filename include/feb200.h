@@ -326,6 +326,14 @@ FEB_API int feb_net_head_grad(const void* X, int32_t x_ld, int64_t rows, const f
 FEB_API int feb_net_loss(FebNetGrid net, const void* xin, const float* pred, const float* target, const float* wgt,
                          float e_ref_inv, float mse_scale, float h1_scale, double* loss, float* dpred, void* stream);
 
+/* Training loss: strain energy of a prediction's error on a network grid equal to the FE grid (spacing h [host 3]):
+ * scale * sum over active cells whose 8 corners have targets of e^T K_e e, e = pred - target at the corners, K_e the
+ * hex8 element of the solve (lambda at the centre, mu 2x2x2) with the Lame constants of the cell read from the network
+ * input xin (channel 0 = log10 E / 4, channel 1 = (nu - 0.3) * 4, channel 2 = active).  pred [dev] NULL: the target's
+ * energy.  loss [dev] += the sum; dpred [dev] (if not NULL) += its gradient 2 scale K_e e. */
+FEB_API int feb_net_energy_loss(FebNetGrid net, const double* h, const void* xin, const float* pred, const float* target,
+                                const float* wgt, float scale, double* loss, float* dpred, void* stream);
+
 /* Adam step on n FP32 parameters (bias-corrected, step >= 1); the gradient is scaled by gscale first and
  * zeroed afterwards.  sumsq (if not NULL) receives += sum of squared gradients before the step is taken. */
 FEB_API int feb_net_adam(float* w, float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,

@@ -256,3 +256,35 @@ def edge_loss(xin, pred, target, wgt, e_ref_inv, mse_scale, h1_scale):
         g[hi] += gd
         g[lo] -= gd
     return loss, g
+
+
+def energy_loss(xin, pred, target, wgt, h, scale):
+    """Strain energy of the prediction's error, and its gradient: scale * sum over cells (x < nx-1, y < ny-1,
+    z < nz-1) that are active (xin[..., 2] > 0) and whose 8 corner nodes have wgt > 0 of e_c^T K_e e_c, e = pred -
+    target at the corners (corner l at offset (l & 1, (l >> 1) & 1, l >> 2), dof 3 l + c), K_e = lambda K_lambda(one
+    point) + mu K_mu(2x2x2) of a cell of edges h (the hex8 matrices of oracle/fe_oracle.py), E = 10^(4 xin[0]),
+    nu = xin[1] / 4 + 0.3.  Arrays over the network nodes [nx, ny, nz, ...].  Returns (loss, dpred)."""
+    from oracle import fe_oracle as F
+    KL, KM, Bc = F.hex8_matrices(h)
+    KLs = np.prod(h) * (Bc.T @ F.D_LAMBDA @ Bc)
+    nx, ny, nz = wgt.shape
+    e = pred - target
+    g = np.zeros_like(pred)
+    loss = 0.0
+    for x in range(nx - 1):
+        for y in range(ny - 1):
+            for z in range(nz - 1):
+                if xin[x, y, z, 2] <= 0:
+                    continue
+                corners = [(x + (l & 1), y + ((l >> 1) & 1), z + (l >> 2)) for l in range(8)]
+                if not all(wgt[c] > 0 for c in corners):
+                    continue
+                E = 10.0 ** (4.0 * xin[x, y, z, 0])
+                nu = xin[x, y, z, 1] / 4.0 + 0.3
+                lam, mu = E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+                ue = np.concatenate([e[c] for c in corners])
+                f = (lam * KLs + mu * KM) @ ue
+                loss += scale * float(ue @ f)
+                for l, c in enumerate(corners):
+                    g[c] += 2.0 * scale * f[3 * l:3 * l + 3]
+    return loss, g

@@ -421,3 +421,29 @@ def test_edge_loss_and_head_gradient():
     assert rel(host(dW).reshape(3, 32), np.einsum("xyzc,xyzk->ck", g, X)) < 1e-5
     assert rel(host(db), g.sum((0, 1, 2))) < 1e-5
     assert rel(from_rows(host(dX), dims), (g @ Wh) * (X > 0)) < 1e-2
+
+
+def test_energy_loss_matches_oracle():
+    """feb_net_energy_loss (the strain energy of the prediction's error with the solve's hex8 element) against the
+    oracle, value and gradient, on a box-cell grid with mixed materials, inactive cells and nodes without targets."""
+    import torch
+    rng = np.random.default_rng(9)
+    dims = (5, 4, 6)
+    h = np.array([0.8, 0.9, 1.1])
+    x = np.zeros(dims + (32,))
+    x[..., 0] = bf16(np.log10(rng.choice([1.15, 10.0, 500.0, 1e4], dims)) / 4)
+    x[..., 1] = bf16((rng.choice([0.3, 0.4, 0.45], dims) - 0.3) * 4)
+    x[..., 2] = (rng.random(dims) < 0.85).astype(float)
+    pred = rng.normal(size=dims + (3,)).astype(np.float32)
+    T = rng.normal(size=dims + (3,)).astype(np.float32)
+    w = (rng.random(dims) < 0.95).astype(float)
+    ref, gref = O.energy_loss(x, pred.astype(np.float64), T.astype(np.float64), w, h, 1e-3)
+    f32 = lambda a: torch.as_tensor(np.asarray(a, np.float32)).cuda().contiguous()
+    xd, pd, Td, wd = dev_rows(x), f32(to_rows(pred)), f32(to_rows(T)), f32(to_rows(w[..., None])[:, 0])
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    dp = torch.zeros_like(pd)
+    _lib.check(_lib.load().feb_net_energy_loss(_lib.FebNetGrid(*dims), h.ctypes.data_as(C.c_void_p), _ptr(xd), _ptr(pd),
+                                               _ptr(Td), _ptr(wd), 1e-3, _ptr(loss), _ptr(dp), _stream()))
+    assert ref > 0
+    assert abs(float(loss.item()) - ref) < 1e-4 * ref
+    assert rel(from_rows(host(dp), dims), gref) < 1e-4

@@ -41,3 +41,31 @@ def test_layers_are_adjoint():
         dX, dW, _ = back(X, W, G)
         assert abs((Y * G).sum() - (X * dX).sum()) < 1e-9 * abs((Y * G).sum())
         assert abs((Y * G).sum() - (W * dW).sum()) < 1e-9 * abs((Y * G).sum())
+
+
+def test_energy_loss_gradient_and_positivity():
+    """The oracle's strain-energy loss is non-negative, zero for a rigid-body error, and its gradient matches central
+    differences."""
+    rng = np.random.default_rng(4)
+    dims = (4, 3, 3)
+    h = np.array([1.0, 0.8, 1.2])
+    x = np.zeros(dims + (32,))
+    x[..., 0] = np.log10(rng.choice([1.0, 500.0, 1e4], dims)) / 4
+    x[..., 1] = (rng.choice([0.3, 0.45], dims) - 0.3) * 4
+    x[..., 2] = 1.0
+    w = np.ones(dims)
+    T = rng.normal(size=dims + (3,))
+    pred = T + rng.normal(size=dims + (3,)) * 0.1
+    loss, g = O.energy_loss(x, pred, T, w, h, 1.0)
+    assert loss > 0
+    # a rigid translation and an infinitesimal rotation carry no strain energy
+    X = np.stack(np.meshgrid(*(np.arange(n) * hh for n, hh in zip(dims, h)), indexing="ij"), -1)
+    rigid = np.array([0.3, -0.2, 0.5]) + np.cross(np.array([0.01, 0.02, -0.03]), X)
+    assert O.energy_loss(x, T + rigid, T, w, h, 1.0)[0] < 1e-12 * loss
+    for _ in range(4):
+        idx = tuple(int(rng.integers(0, s)) for s in pred.shape)
+        eps = 1e-6
+        p1 = pred.copy(); p1[idx] += eps
+        p2 = pred.copy(); p2[idx] -= eps
+        num = (O.energy_loss(x, p1, T, w, h, 1.0)[0] - O.energy_loss(x, p2, T, w, h, 1.0)[0]) / (2 * eps)
+        assert abs(num - g[idx]) < 1e-5 * max(1.0, abs(num))
