@@ -15,8 +15,8 @@ metric's problem size by the dof ratio.  Under torchrun every rank solves its ow
 (independent units, weak scaling); rank 0 prints one JSON line.
 
 When the packaged warm-start network is present, the same solve started from its prediction (the metric's
-learned + mixed configuration) is timed beside the headline in ``learned_warm_start``; it does not lower the
-iteration count, so the headline ``value`` is the mixed solve from a zero start.  ``--mode batch`` times 64
+learned + mixed configuration) is timed beside the headline in ``learned_warm_start``; it changes the iteration
+count by a few percent at most, so the headline ``value`` is the mixed solve from a zero start.  ``--mode batch`` times 64
 independent instances of uneven size, one at a time and with 8 / 16 solves in flight.
 """
 import argparse
@@ -389,7 +389,7 @@ def run_ours(args, rank, world, dist):
                              f"(C2 generator)"), "ndof": int(mixed_info.ndof),
                 "precision": prec,
                 "warm_start": ("zero; the learned start (the metric's learned+mixed) is measured beside in "
-                               "learned_warm_start and gives no iteration gain" if warm is not None
+                               "learned_warm_start (a few percent of the iterations at most)" if warm is not None
                                else "zero (no trained network found)"), "tol": TOL,
                 "iters": int(mixed_info.iters), "sweeps": int(mixed_info.sweeps), "relres": mixed_info.relres,
                 "levels": int(mixed_info.levels), "l2": "flushed (256 MB write) before every step",

@@ -356,18 +356,18 @@ def test_inputs_and_targets_of_a_hindfoot():
 
 
 def test_packaged_network_on_held_out_instances():
-    """The network shipped in comech_b200/weights (trained on seeds 1000-2999 of the 96x64x48 generator with the
-    stiffness-weighted edge loss) on three instances it never saw (an osteotomy, an interposition, a fusion).
+    """The network shipped in comech_b200/weights (trained on seeds 1000-2999 of the 96x64x48 generator against the
+    strain energy of its error plus 0.2 x the relative squared error) on three instances it never saw (an
+    osteotomy, an interposition, a fusion).
 
     Bars, from the 200-instance held-out study of comech_b200.warm_train:
-    - its prediction is within 70 % relative L2 of the FP64 solution (median 20 %; osteotomies, whose fragment
-      position the network must infer, reach 60 %);
+    - its prediction is within 90 % relative L2 of the FP64 solution (median 57 %, at most 73 %: the energy term
+      leaves rigid motions to the squared-error term, and the solve's springs and rigid-mode correction to CG);
     - the mixed-precision solve started from it (smoothed once by the preconditioner, scaled to its
       energy-optimal multiple) converges to rel-res 1e-8;
-    - it takes at most 8 more iterations than the zero start (per instance -8 to +6, mean -0.7).
+    - it takes at most 8 more iterations than the zero start (per instance -6 to +5, mean -1.7).
 
-    So the learned start is close to the solution and safe, and its gain over the zero start is about one
-    iteration in 64."""
+    So the learned start is safe, and its gain over the zero start is about 2 iterations in 63."""
     import os
     from comech_b200 import warm_train as W
     assert os.path.exists(warmnet.WEIGHTS), "packaged network missing"
@@ -383,7 +383,7 @@ def test_packaged_network_on_held_out_instances():
         Ur = host(U64).reshape(-1, 3)
         ok = np.isfinite(Ur).all(1)
         pr = host(x0).reshape(-1, 3)
-        assert np.linalg.norm(pr[ok] - Ur[ok]) < 0.7 * np.linalg.norm(Ur[ok])
+        assert np.linalg.norm(pr[ok] - Ur[ok]) < 0.9 * np.linalg.norm(Ur[ok])
         assert i0.flag == 0 and i1.flag == 0 and i1.relres < 1e-8
         assert i1.x0_used == 1 and i1.x0_scale > 0
         assert i1.iters <= i0.iters + 8, (seed, i0.iters, i1.iters)
