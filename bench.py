@@ -270,33 +270,37 @@ def run_ours(args, rank, world, dist):
     # ---------------------------------------------------------------- the learned start, measured beside
     learned = None
     if warm is not None:
-        device_solve(P, d, prec, warm=warm)
-        torch.cuda.synchronize()
-        w_ms = []
-        for _ in range(max(1, min(args.steps, 3))):
-            flush_l2(flush)
+        try:
+            device_solve(P, d, prec, warm=warm)
+            torch.cuda.synchronize()
+            w_ms = []
+            for _ in range(max(1, min(args.steps, 3))):
+                flush_l2(flush)
+                ev0.record()
+                _, _, infw = device_solve(P, d, prec, warm=warm)
+                ev1.record()
+                torch.cuda.synchronize()
+                w_ms.append(ev0.elapsed_time(ev1))
+            nc = g0.nx * g0.ny * g0.nz
+            torch.cuda.synchronize()
             ev0.record()
-            _, _, infw = device_solve(P, d, prec, warm=warm)
+            x0w = warm.predict_x0(g0, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
+                                  d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
             ev1.record()
             torch.cuda.synchronize()
-            w_ms.append(ev0.elapsed_time(ev1))
-        nc = g0.nx * g0.ny * g0.nz
-        torch.cuda.synchronize()
-        ev0.record()
-        x0w = warm.predict_x0(g0, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
-                              d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
-        ev1.record()
-        torch.cuda.synchronize()
-        t_pred = ev0.elapsed_time(ev1)
-        xw = x0w.view(-1, 3).cpu().numpy()
-        Ur = U64h.reshape(-1, 3)
-        okn = ok.reshape(-1, 3).all(1)
-        learned = {"s_per_solve": round(min(w_ms) / 1e3, 5), "steps_ms": [round(t, 2) for t in w_ms],
-                   "iters": int(infw.iters), "relres": infw.relres, "prediction_ms": round(t_pred, 3),
-                   "x0_used": int(infw.x0_used), "x0_scale": float(infw.x0_scale),
-                   "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn])),
-                   "network": "3D conv encoder-decoder, 4.26M parameters, trained on 2000 FP64 solves of the "
-                              "96x64x48 generator; start = x0 + M(f - K x0), scaled to its energy-optimal multiple"}
+            t_pred = ev0.elapsed_time(ev1)
+            xw = x0w.view(-1, 3).cpu().numpy()
+            Ur = U64h.reshape(-1, 3)
+            okn = ok.reshape(-1, 3).all(1)
+            learned = {"s_per_solve": round(min(w_ms) / 1e3, 5), "steps_ms": [round(t, 2) for t in w_ms],
+                       "iters": int(infw.iters), "relres": infw.relres, "prediction_ms": round(t_pred, 3),
+                       "x0_used": int(infw.x0_used), "x0_scale": float(infw.x0_scale),
+                       "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn])),
+                       "network": "3D conv encoder-decoder, 4.26M parameters, trained on 2000 FP64 solves of the "
+                                  "96x64x48 generator; start = x0 + M(f - K x0), scaled to its energy-optimal multiple"}
+        except _lib.FebError as e:     # a network pass whose tensor-core wait ran out
+            learned = {"error": str(e)}
+
     disp_rel = float(np.linalg.norm(U_mixed[ok] - U64h[ok]) / np.linalg.norm(U64h[ok]))
     vm_rel = float(torch.linalg.norm(vm - vm64).item() / torch.linalg.norm(vm64).item())
     # ---------------------------------------------------------------- e2e through the public API

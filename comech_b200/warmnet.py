@@ -378,7 +378,9 @@ class WarmNet:
         """Initial guess (full layout, FP64, device) for the solve of these inputs (orig: host node map; orig_dev:
         the same map already on the device, if any)."""
         x, meta = self.inputs(g, lam, mu, active, orig, fixed_nodes, load_nodes, load_z)
+        self.status.zero_()
         pred = self.forward(x, meta["dims"])
+        self.check_status()                  # a network pass whose tensor-core wait ran out gives no start value
         scale = self.u_unit * meta["total_load"] / REF_LOAD
         x0 = self.torch.empty(3 * nnode_total, dtype=self.torch.float64, device="cuda")
         nnode = (g.nx + 1) * (g.ny + 1) * (g.nz + 1)
