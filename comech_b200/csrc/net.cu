@@ -778,12 +778,9 @@ __global__ void k_net_to_nodes(FebNetGrid net, Axes A, const float* __restrict__
 
 template <int NT, int GATHER, int SCATTER>
 int launch_conv(const FebConv& c, int64_t M, int64_t Pin, cudaStream_t s) {
-  static bool prepared = false;
-  if (!prepared) {
-    FEB_CUDA(cudaFuncSetAttribute(k_conv<NT, GATHER, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)ConvSmem<NT, GATHER>::kTotal));
-    prepared = true;
-  }
+  // set on every launch (microseconds): the attribute belongs to the current device, and a process may use several
+  FEB_CUDA(cudaFuncSetAttribute(k_conv<NT, GATHER, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ConvSmem<NT, GATHER>::kTotal));
   const dim3 grid(div_up(M, ConvSmem<NT, GATHER>::kM), c.n / NT);
   k_conv<NT, GATHER, SCATTER><<<grid, kConvThreads, ConvSmem<NT, GATHER>::kTotal, s>>>(c, M, Pin);
   note_launch();

@@ -69,3 +69,15 @@ def test_energy_loss_gradient_and_positivity():
         p2 = pred.copy(); p2[idx] -= eps
         num = (O.energy_loss(x, p1, T, w, h, 1.0)[0] - O.energy_loss(x, p2, T, w, h, 1.0)[0]) / (2 * eps)
         assert abs(num - g[idx]) < 1e-5 * max(1.0, abs(num))
+
+
+def test_product_and_oracle_describe_the_same_network():
+    """The device network (comech_b200.warmnet) and its oracle list the same layers, kinds and widths in the same
+    order, and the same parameter count (checked without a GPU)."""
+    from comech_b200 import warmnet
+    assert warmnet.layer_table() == O.layers(warmnet.WIDTHS, warmnet.CIN)
+    n = sum(O.TAPS_OF[k] * ci * co + co for _, k, ci, co in O.layers(warmnet.WIDTHS, warmnet.CIN))
+    n += 3 * warmnet.WIDTHS[0] + 3
+    import numpy as np
+    z = np.load(warmnet.WEIGHTS)
+    assert z["theta"].size == n and tuple(z["widths"]) == warmnet.WIDTHS
