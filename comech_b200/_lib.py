@@ -51,7 +51,8 @@ class FebInfo(C.Structure):
                 ("relres", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("ndof", C.c_int64), ("level_dofs", C.c_int64 * 8), ("lmax", C.c_double * 8),
                 ("coarse_n", C.c_int32), ("kernel_launches", C.c_int32), ("ku_shape", C.c_int32 * 4),
-                ("t_stage_ms", C.c_double * 8), ("x0_used", C.c_int32), ("x0_scale", C.c_float)]
+                ("t_stage_ms", C.c_double * 8), ("x0_used", C.c_int32), ("x0_scale", C.c_float),
+                ("ku_kind", C.c_int32)]
 
 
 class FebNetGrid(C.Structure):

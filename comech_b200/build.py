@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfeb200.so")
-SOURCES = ["fine.cu", "fine_tc.cu", "coarse.cu", "vec.cu", "dense.cu", "rigid.cu", "stress.cu", "post.cu", "split.cu", "materials.cu", "net.cu", "solver.cu"]
+SOURCES = ["fine.cu", "fine_pair.cu", "fine_tc.cu", "coarse.cu", "vec.cu", "dense.cu", "rigid.cu", "stress.cu", "post.cu", "split.cu", "materials.cu", "net.cu", "solver.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

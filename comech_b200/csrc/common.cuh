@@ -35,6 +35,10 @@ void set_last_error(const char* fmt, ...);
 // host-side count of kernel launches issued by the library (feb_launch_count)
 void note_launch(int n = 1);
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device (the attribute is per
+// device; set once per device and kernel, thread-safe); returns a status.
+int set_dyn_smem(const void* kernel, int bytes);
+
 // symmetric pseudo-inverse by cyclic Jacobi, numpy.linalg.pinv semantics (cutoff 1e-15 max |eigenvalue|);
 // A is n x n row-major (host)
 std::vector<double> sym_pinv(const std::vector<double>& A, int n);

@@ -428,15 +428,21 @@ template void launch_dense_from_fine<MAT_ISO_SRI>(const FineView<double>&, const
 template void launch_dense_from_fine<MAT_ISO_FULL>(const FineView<double>&, const int*, double*, int, cudaStream_t);
 template void launch_dense_from_fine<MAT_ORTHO>(const FineView<double>&, const int*, double*, int, cudaStream_t);
 
+// A failed attribute call leaves its message in the last error and the launch then fails; the caller's
+// next status check reports it.
 template <typename T, int MODE, int TY>
 void launch_struct(dim3 grid, size_t smem, const FineView<T>& F, const T* u, T* y, const int* skip, int zc,
                    cudaStream_t s) {
-  static bool configured = false;   // one attribute call per instantiation (idempotent if repeated)
-  if (!configured) {
-    cudaFuncSetAttribute(k_fine_struct<T, MODE, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
+  if (set_dyn_smem((const void*)k_fine_struct<T, MODE, TY>, (int)smem) != FEB_OK) return;
   k_fine_struct<T, MODE, TY><<<grid, dim3(32, TY), smem, s>>>(F, u, y, skip, zc); note_launch();
+}
+
+template <typename T, int MODE>
+void launch_fine_sparse_into(const FineView<T>& F, const T* u, T* acc, const int* skip, cudaStream_t s) {
+  int b_irr = div_up(F.nirr, kThreads), b_pen = div_up(F.npen, kThreads), b_row = div_up(F.nrow, kThreads);
+  if (b_irr + b_pen + b_row > 0) {
+    k_fine_sparse<T, MODE><<<b_irr + b_pen + b_row, kThreads, 0, s>>>(F, u, acc, skip, b_irr, b_pen); note_launch();
+  }
 }
 
 template <typename T, int MODE>
@@ -477,7 +483,8 @@ void launch_fine_diag(const FineView<double>& F, double* D, cudaStream_t s) {
   if (n > 0) k_fine_diag_sparse<MODE><<<div_up(n, kThreads), kThreads, 0, s>>>(F, D); note_launch();
 }
 
-#define INST(T, M) template void launch_fine_apply<T, M>(const FineView<T>&, const T*, T*, const int*, KuConfig, cudaStream_t);
+#define INST(T, M) template void launch_fine_apply<T, M>(const FineView<T>&, const T*, T*, const int*, KuConfig, cudaStream_t); \
+  template void launch_fine_sparse_into<T, M>(const FineView<T>&, const T*, T*, const int*, cudaStream_t);
 INST(float, MAT_ISO_SRI) INST(float, MAT_ISO_FULL) INST(float, MAT_ORTHO)
 INST(double, MAT_ISO_SRI) INST(double, MAT_ISO_FULL) INST(double, MAT_ORTHO)
 #undef INST

@@ -41,6 +41,76 @@ struct KuConfig {
 template <typename T, int MODE>
 void launch_fine_apply(const FineView<T>& F, const T* u, T* y, const int* skip, KuConfig cfg, cudaStream_t s);
 
+// Sparse part of the level-0 operator only (irregular cells, penalties, extra entries), added with atomics
+// into acc (3 per node).
+template <typename T, int MODE>
+void launch_fine_sparse_into(const FineView<T>& F, const T* u, T* acc, const int* skip, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------------ paired K.u
+// Operator of the paired-row kernel (fine_pair.cu): regular cells by 7-bit material ids, the sparse part
+// through the accumulator tsp (zero between products), the smoother update fused in the epilogue.
+constexpr int kMaxMatIds = 128;   // ids 1..127; 0 = no regular cell
+
+template <typename T>
+struct PairView {
+  int nx, ny, nz;            // cells
+  int nxn, nyn, nzn;         // grid nodes per axis
+  int mp;                    // row pairs per (x, z) column: nyn / 2 + 1 (rows 2m-1, 2m)
+  int64_t nnode, ntotal;     // grid nodes; grid nodes + split copies
+  const uint16_t* cellpair;  // [nzn][mp][nxn]: per row byte bits 0-6 material id, bit 7 node is special
+  const double* mtab;        // [kMaxMatIds][W] material values of the ids (FP64)
+  int nmat;                  // ids in use are < nmat
+  bool cube;                 // equal cubic cells of edge h, SRI model: reduced modal core
+  double h;
+  const T* dx; const T* dy; const T* dz;      // cell widths per axis (general core)
+  const T* idx; const T* idy; const T* idz;
+  T* tsp;                    // sparse-part accumulator, 3 per node (ntotal), zero between products
+  const T* dinv6;            // symmetric block-Jacobi inverse [6][ntotal]: 00 11 22 01 02 12
+};
+
+struct LevelParams;
+// Smoother epilogue of one product t = K u (u the direction d of the step):
+//   r = r_in - t            -> r_out (if given)
+//   d' = a1 u + a2 Dinv r   -> d_out (if given);  x_out = x_in + d' (x_in may be null: zero)
+// with (a1, a2) = (0, c_init) for k < 0 and (a1[k], a2[k]) of the level's Chebyshev parameters otherwise.
+// With neither d_out nor x_out the step is the residual update r_out = r_in - K u.
+template <typename T>
+struct SmoothArgs {
+  const T* r_in = nullptr;
+  T* r_out = nullptr;
+  const T* x_in = nullptr;
+  T* x_out = nullptr;
+  T* d_out = nullptr;
+  const LevelParams* lp = nullptr;
+  int k = -1;
+};
+
+struct PairConfig {
+  int wy = 16;       // warps per CTA (2 node rows each); 16 only on the cubic SRI path in FP32
+  int zchunk = 16;   // node planes per CTA
+};
+
+// y = K u (S null) or the smoother step S; returns a status
+template <typename T, int MODE>
+int launch_fine_pair(const PairView<T>& F, const FineView<T>& G, const T* u, T* y, const SmoothArgs<T>* S,
+                     const int* skip, PairConfig cfg, cudaStream_t s);
+// sets the shared-memory limits of every paired-kernel variant of this model on the current device (call
+// before any stream capture)
+int prepare_fine_pair(int mode, bool cube);
+template <int W>
+void launch_mat_ids(const double* mat_s, int64_t ncell, unsigned long long* keys, double* vals, uint8_t* ids,
+                    int* status, cudaStream_t s);
+void launch_flag_nodes(const int* pen_node, int npen, const int* irr_nodes, int nirr, const int* row_dof, int nrow,
+                       int64_t nnode, uint8_t* flag, cudaStream_t s);
+template <int W>
+void launch_pack_pairs(int nx, int ny, int nz, int mp, const uint8_t* ids, const uint8_t* flag, const double* mat_s,
+                       const double* vals, uint16_t* cellpair, int* status, cudaStream_t s);
+template <typename T>
+void launch_dinv6(const double* D9, int64_t n, T* out, cudaStream_t s);
+template <typename T>
+void launch_cheb_first6(const T* b, const T* D6, const LevelParams* lp, T* d, T* x, int64_t n, const int* skip,
+                        cudaStream_t s);
+
 // Tensor-core K.u of the regular cells (MODE ISO_SRI or ISO_FULL, equal cubic cells, FP32): operand columns
 // N of the B table (2 faces x 2 node rows x N rows x 8 BF16), kernel attributes (once per process), launch.
 template <int MODE> int tc_columns();

@@ -57,6 +57,19 @@ thread_local SetupProfile g_prof;
 
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+int set_dyn_smem(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;   // (kernel, device) -> bytes set
+  int dev = 0;
+  FEB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find({kernel, dev});
+  if (it != done.end() && it->second >= bytes) return FEB_OK;
+  FEB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done[{kernel, dev}] = bytes;
+  return FEB_OK;
+}
+
 void set_last_error(const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -481,8 +494,8 @@ __global__ void k_orig_copy(const int64_t* __restrict__ orig, int64_t nnode, int
   out[e] = int(orig[nnode + e]);
 }
 
-// x += a y (y may alias x: x *= 1 + a)
-__global__ void k_axpy_inplace(double* __restrict__ x, const double* y, int64_t n, double a) {
+// x += a y (y may alias x: x *= 1 + a; no restrict qualifiers for that reason)
+__global__ void k_axpy_inplace(double* x, const double* y, int64_t n, double a) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) x[i] += a * y[i];
 }
@@ -629,6 +642,37 @@ using namespace feb;
 
 // own non-blocking stream (stream capture is impossible on the legacy default stream); ordered with the
 // caller's stream by events at every entry point
+// Pinned host slots for the CG state read-backs.  Page-locking host memory can take tens of milliseconds
+// when the system is busy, so the slots come from blocks that are allocated once and reused by every handle
+// of the process (a handle takes a slot at creation and returns it when destroyed).
+namespace feb {
+class PinnedSlots {
+ public:
+  CgState* take() {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (free_.empty()) {
+      CgState* blk = nullptr;
+      if (cudaMallocHost(&blk, kBlock * sizeof(CgState)) != cudaSuccess) return nullptr;
+      for (int i = kBlock - 1; i >= 0; --i) free_.push_back(blk + i);
+    }
+    CgState* p = free_.back();
+    free_.pop_back();
+    return p;
+  }
+  void give(CgState* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu_);
+    free_.push_back(p);
+  }
+
+ private:
+  static constexpr int kBlock = 64;
+  std::mutex mu_;
+  std::vector<CgState*> free_;   // blocks stay allocated until the process exits
+};
+static PinnedSlots g_pinned;
+}  // namespace feb
+
 static cudaStream_t make_stream() {
   cudaStream_t st = nullptr;
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -699,6 +743,13 @@ struct FebHandle {
   int g_outer_nodes = 0, g_inner_nodes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   KuConfig ku32{}, ku64{};   // launch shapes of the fine K.u (autotuned per grid shape)
+  // paired-row level-0 kernels (fine_pair.cu): used when every regular cell's material fits the id table
+  bool pair_ok = false;
+  PairView<float> P32{};
+  PairView<double> P64{};
+  PairConfig pc32{}, pc64{};
+  float* D6_32 = nullptr;    // level-0 symmetric block-Jacobi inverse [6][ntotal]
+  double* D6_64 = nullptr;
   static constexpr int kStages = 10;
   cudaEvent_t stage_ev[kStages + 1] = {};
   int stage_n = 0;
@@ -712,7 +763,7 @@ struct FebHandle {
   ~FebHandle() {
     if (g_outer) cudaGraphExecDestroy(g_outer);
     if (g_inner) cudaGraphExecDestroy(g_inner);
-    if (st_h) cudaFreeHost(st_h);
+    g_pinned.give(st_h);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     pool.release();
@@ -726,8 +777,28 @@ struct FebHandle {
   template <typename T>
   const FineView<T>& fine() const;
 
+  template <typename T> const PairView<T>& pview() const;
+  template <typename T> const T* dinv6() const;
+  template <typename T>
+  PairConfig pcfg() const { return std::is_same<T, double>::value ? pc64 : pc32; }
+  // the paired kernel serves precision T (FEB_KU_TC=1 keeps FP32 products on the tensor-core kernel)
+  template <typename T>
+  bool pair_on() const { return pair_ok && (std::is_same<T, double>::value || !(tc_ok && ku32.tc)); }
+  template <typename T>
+  void pair_run(const T* u, T* y, const SmoothArgs<T>* S, const int* skip) {
+    switch (mode) {
+      case MAT_ISO_SRI: launch_fine_pair<T, MAT_ISO_SRI>(pview<T>(), fine<T>(), u, y, S, skip, pcfg<T>(), s); break;
+      case MAT_ISO_FULL: launch_fine_pair<T, MAT_ISO_FULL>(pview<T>(), fine<T>(), u, y, S, skip, pcfg<T>(), s); break;
+      default: launch_fine_pair<T, MAT_ORTHO>(pview<T>(), fine<T>(), u, y, S, skip, pcfg<T>(), s); break;
+    }
+  }
+
   template <typename T>
   void apply(int l, const T* u, T* y, const int* skip) {
+    if (l == 0 && pair_on<T>()) {
+      pair_run<T>(u, y, nullptr, skip);
+      return;
+    }
     if (l == 0) {
       const FineView<T>& F = fine<T>();
       const KuConfig cfg = std::is_same<T, double>::value ? ku64 : ku32;
@@ -800,8 +871,53 @@ struct FebHandle {
     }
   }
 
+  // Level-0 V-cycle leg with the smoother fused into the paired K.u (same arithmetic as smooth() +
+  // residual + transfers): pre-smoothing from zero keeps x = d0 + d1 + ... and the residual of the smoothed
+  // iterate is r - K d_last; post-smoothing starts from xs and writes the result into x.
+  template <typename T>
+  void vcycle0_pair(const T* b, T* x, const int* skip) {
+    Level& V = L[0];
+    Level& C = L[1];
+    T *r = vr<T>(V), *d = vd<T>(V), *e = ve<T>(V), *xs = vt<T>(V);
+    const int deg = std::max(1, opt.cheb_degree);
+    launch_cheb_first6<T>(b, dinv6<T>(), lp, d, deg == 1 ? xs : nullptr, ntotal, skip, s);
+    for (int k = 1; k < deg; ++k) {
+      SmoothArgs<T> A;
+      A.r_in = (k == 1) ? b : r; A.r_out = r; A.x_in = (k == 1) ? d : xs; A.x_out = xs; A.d_out = e; A.lp = lp;
+      A.k = k - 1;
+      pair_run<T>(d, nullptr, &A, skip);
+      std::swap(d, e);
+    }
+    {
+      SmoothArgs<T> A;
+      A.r_in = (deg == 1) ? b : r; A.r_out = r;
+      pair_run<T>(d, nullptr, &A, skip);
+    }
+    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s);
+    vcycle<T>(1, vb<T>(C), vx<T>(C), skip);
+    launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), xs, skip, s);
+    {
+      SmoothArgs<T> A;
+      A.r_in = b; A.r_out = deg > 1 ? r : nullptr; A.x_in = xs; A.x_out = x; A.d_out = deg > 1 ? d : nullptr;
+      A.lp = lp; A.k = -1;
+      pair_run<T>(xs, nullptr, &A, skip);
+    }
+    for (int k = 1; k < deg; ++k) {
+      const bool last = (k == deg - 1);
+      SmoothArgs<T> A;
+      A.r_in = r; A.r_out = last ? nullptr : r; A.x_in = x; A.x_out = x; A.d_out = last ? nullptr : e; A.lp = lp;
+      A.k = k - 1;
+      pair_run<T>(d, nullptr, &A, skip);
+      std::swap(d, e);
+    }
+  }
+
   template <typename T>
   void vcycle(int l, const T* b, T* x, const int* skip) {
+    if (l == 0 && coarsest > 0 && pair_on<T>()) {
+      vcycle0_pair<T>(b, x, skip);
+      return;
+    }
     if (l == coarsest) {
       Level& V = L[l];
       launch_dense_solve<T>(Minv, nd, klist, cmap, V.ntotal, b, x, bd, xd, skip, s);
@@ -968,6 +1084,10 @@ struct FebHandle {
   }
 };
 
+template <> const PairView<double>& FebHandle::pview<double>() const { return P64; }
+template <> const PairView<float>& FebHandle::pview<float>() const { return P32; }
+template <> const double* FebHandle::dinv6<double>() const { return D6_64; }
+template <> const float* FebHandle::dinv6<float>() const { return D6_32; }
 template <> const FineView<double>& FebHandle::fine<double>() const { return F64; }
 template <> const FineView<float>& FebHandle::fine<float>() const { return F32; }
 template <> const double* FebHandle::dinv<double>(const Level& V) { return V.Dinv64; }
@@ -1075,18 +1195,34 @@ int power_iteration(FebHandle* h, int l) {
 // Launch shape of the fine K.u (warps per CTA x node planes per CTA), picked by timing every candidate
 // on this operator and cached per (grid, material model, split copies) for the process lifetime.
 struct TuneKey {
-  int nx, ny, nz, mode, copies, tc;
+  int nx, ny, nz, mode, copies, tc, pair;
   bool operator<(const TuneKey& o) const {
-    return std::tie(nx, ny, nz, mode, copies, tc) < std::tie(o.nx, o.ny, o.nz, o.mode, o.copies, o.tc);
+    return std::tie(nx, ny, nz, mode, copies, tc, pair) < std::tie(o.nx, o.ny, o.nz, o.mode, o.copies, o.tc, o.pair);
   }
 };
+struct Tuned {
+  KuConfig k32, k64;
+  PairConfig p32, p64;
+};
 std::mutex g_tune_mu;
-std::map<TuneKey, std::pair<KuConfig, KuConfig>> g_tune_cache;
+std::map<TuneKey, Tuned> g_tune_cache;
 
 // FEB_KU_TC: "0" keeps the FP32 K.u off the tensor cores, "1" puts it there without tuning (tests, profiling)
 int env_tc() {
   const char* e = std::getenv("FEB_KU_TC");
   return (e && *e) ? (e[0] == '1' ? 1 : 0) : -1;
+}
+
+// average time of 3 products after 2 warm-up products (ms)
+template <typename T>
+int time_apply(FebHandle* h, T* u, T* y, float* ms) {
+  for (int w = 0; w < 2; ++w) h->apply<T>(0, u, y, nullptr);
+  FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+  for (int r = 0; r < 3; ++r) h->apply<T>(0, u, y, nullptr);
+  FEB_CUDA(cudaEventRecord(h->ev1, h->s));
+  FEB_CUDA(cudaEventSynchronize(h->ev1));
+  FEB_CUDA(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  return FEB_OK;
 }
 
 template <typename T>
@@ -1102,56 +1238,93 @@ int tune_one(FebHandle* h, KuConfig* best, T* u, T* y) {
   if (tc)
     for (int zc : {8, 12, 16, 24, 32}) cand.push_back(KuConfig{16, zc, 1});
   float best_ms = 1e30f;
-  {
-    for (const KuConfig& c : cand) {
-      KuConfig& slot = std::is_same<T, double>::value ? h->ku64 : h->ku32;
-      slot = c;
-      for (int w = 0; w < 2; ++w) h->apply<T>(0, u, y, nullptr);
-      FEB_CUDA(cudaEventRecord(h->ev0, h->s));
-      for (int r = 0; r < 3; ++r) h->apply<T>(0, u, y, nullptr);
-      FEB_CUDA(cudaEventRecord(h->ev1, h->s));
-      FEB_CUDA(cudaEventSynchronize(h->ev1));
-      float ms = 0.f;
-      FEB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-      if (ms < best_ms) { best_ms = ms; *best = c; }
-    }
+  for (const KuConfig& c : cand) {
+    KuConfig& slot = std::is_same<T, double>::value ? h->ku64 : h->ku32;
+    slot = c;
+    float ms = 0.f;
+    FEB_TRY(time_apply<T>(h, u, y, &ms));
+    if (ms < best_ms) { best_ms = ms; *best = c; }
   }
   return FEB_OK;
 }
 
+// launch shape of the paired kernel: warps per CTA x node planes per CTA
+template <typename T>
+int tune_pair(FebHandle* h, PairConfig* best, T* u, T* y) {
+  std::vector<PairConfig> cand;
+  const bool wide = std::is_same<T, float>::value && h->P32.cube;
+  for (int wy : {8, 16}) {
+    if (wy == 16 && !wide) continue;
+    for (int zc : {8, 12, 16, 24, 32, 48}) cand.push_back(PairConfig{wy, zc});
+  }
+  float best_ms = 1e30f;
+  PairConfig& slot = std::is_same<T, double>::value ? h->pc64 : h->pc32;
+  for (const PairConfig& c : cand) {
+    slot = c;
+    float ms = 0.f;
+    FEB_TRY(time_apply<T>(h, u, y, &ms));
+    if (ms < best_ms) { best_ms = ms; *best = c; }
+  }
+  slot = *best;
+  return FEB_OK;
+}
+
 int autotune_ku(FebHandle* h) {
-  TuneKey key{h->nx, h->ny, h->nz, h->mode, h->ntotal > h->nnode ? 1 : 0, h->tc_ok ? 2 + env_tc() : 0};
+  TuneKey key{h->nx, h->ny, h->nz, h->mode, h->ntotal > h->nnode ? 1 : 0, h->tc_ok ? 2 + env_tc() : 0,
+              h->pair_ok ? (h->P32.cube ? 2 : 1) : 0};
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      h->ku32 = it->second.first;
-      h->ku64 = it->second.second;
+      h->ku32 = it->second.k32;
+      h->ku64 = it->second.k64;
+      h->pc32 = it->second.p32;
+      h->pc64 = it->second.p64;
       return FEB_OK;
     }
   }
-  const char* env = std::getenv("FEB_KU_CONFIG");     // "ty,zchunk" pins the shape (tests, profiling)
+  const char* env = std::getenv("FEB_KU_CONFIG");     // "ty,zchunk" pins the per-cell kernel's shape
+  const char* penv = std::getenv("FEB_PAIR_CONFIG");  // "wy,zchunk" pins the paired kernel's shape
+  bool pinned = false, ppinned = false;
   if (env && *env) {
     int ty = 16, zc = 16;
     if (std::sscanf(env, "%d,%d", &ty, &zc) == 2) {
       h->ku32 = h->ku64 = KuConfig{ty, zc, 0};
-      if (h->tc_ok && env_tc() == 1) h->ku32 = KuConfig{16, zc, 1};
-      return FEB_OK;
+      pinned = true;
     }
   }
+  if (h->tc_ok && env_tc() == 1) h->ku32 = KuConfig{16, 16, 1};
+  if (penv && *penv) {
+    int wy = 8, zc = 16;
+    if (std::sscanf(penv, "%d,%d", &wy, &zc) == 2) {
+      h->pc32 = PairConfig{(wy == 16 && h->P32.cube) ? 16 : 8, zc};
+      h->pc64 = PairConfig{8, zc};
+      ppinned = true;
+    }
+  }
+  const bool need_cell = !h->pair_ok && !pinned, need_pair = h->pair_ok && !ppinned;
+  if (!need_cell && !need_pair) return FEB_OK;
   const size_t n = 3 * (size_t)h->ntotal;
   double *u64 = nullptr, *y64 = nullptr;
   FEB_TRY(h->pool.zeros(&u64, n));
   FEB_TRY(h->pool.alloc(&y64, n));
-  KuConfig b32{}, b64{};
-  FEB_TRY(tune_one<float>(h, &b32, (float*)u64, (float*)y64));
-  FEB_TRY(tune_one<double>(h, &b64, u64, y64));
+  Tuned t{h->ku32, h->ku64, h->pc32, h->pc64};
+  if (need_cell) {
+    FEB_TRY(tune_one<float>(h, &t.k32, (float*)u64, (float*)y64));
+    FEB_TRY(tune_one<double>(h, &t.k64, u64, y64));
+  }
+  if (need_pair) {
+    FEB_TRY(tune_pair<float>(h, &t.p32, (float*)u64, (float*)y64));
+    FEB_TRY(tune_pair<double>(h, &t.p64, u64, y64));
+  }
   h->pool.free(u64);
   h->pool.free(y64);
-  h->ku32 = b32;
-  h->ku64 = b64;
+  h->ku32 = t.k32;
+  h->ku64 = t.k64;
+  h->pc32 = t.p32;
+  h->pc64 = t.p64;
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  g_tune_cache[key] = {b32, b64};
+  g_tune_cache[key] = t;
   return FEB_OK;
 }
 
@@ -1160,6 +1333,80 @@ int autotune_ku(FebHandle* h) {
 // bit c of l.  Read off the device element operator for the unit cube, checked to be those integers, laid
 // out as the kernel's B table: [face cz][node row b][output n][4a + c] in BF16 (exact).  Leaves tc_ok false
 // for other grids or models.
+// Paired-row level-0 operator (fine_pair.cu): material ids of the regular cells (FEB_KU_PAIR=0 keeps the
+// per-cell kernels), flags of the grid nodes that receive sparse contributions, the cell-pair words, the
+// sparse accumulators and the symmetric level-0 block-Jacobi inverse.  Leaves pair_ok false when more than
+// kMaxMatIds - 1 distinct materials occur (or on a hash collision).
+template <int W>
+int setup_pair(FebHandle* h, const double* mat_s64) {
+  FebHandle& H = *h;
+  const char* env = std::getenv("FEB_KU_PAIR");
+  if (env && env[0] == '0') return FEB_OK;
+  const int64_t ncell = (int64_t)H.nx * H.ny * H.nz;
+  const int nxn = H.nx + 1, nyn = H.ny + 1, nzn = H.nz + 1;
+  const int mp = nyn / 2 + 1;
+  unsigned long long* keys = nullptr;
+  double* vals = nullptr;
+  uint8_t *ids = nullptr, *flag = nullptr;
+  int* status = nullptr;
+  uint16_t* cellpair = nullptr;
+  FEB_TRY(H.pool.zeros(&keys, kMaxMatIds));
+  FEB_TRY(H.pool.zeros(&vals, (size_t)W * kMaxMatIds));
+  FEB_TRY(H.pool.alloc(&ids, ncell));
+  FEB_TRY(H.pool.zeros(&flag, H.nnode));
+  FEB_TRY(H.pool.zeros(&status, 1));
+  FEB_TRY(H.pool.alloc(&cellpair, (size_t)nxn * mp * nzn));
+  launch_mat_ids<W>(mat_s64, ncell, keys, vals, ids, status, H.s);
+  launch_flag_nodes(H.F64.pen_node, H.F64.npen, H.F64.irr_nodes, H.F64.nirr, H.F64.row_dof, H.F64.nrow, H.nnode, flag,
+                    H.s);
+  launch_pack_pairs<W>(H.nx, H.ny, H.nz, mp, ids, flag, mat_s64, vals, cellpair, status, H.s);
+  FEB_CUDA(cudaGetLastError());
+  int st = 0;
+  FEB_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  H.pool.free(ids);
+  H.pool.free(flag);
+  H.pool.free(keys);
+  H.pool.free(status);
+  if (st != 0) {
+    H.pool.free(cellpair);
+    H.pool.free(vals);
+    return FEB_OK;
+  }
+  const size_t n3 = 3 * (size_t)H.ntotal;
+  float* tsp32 = nullptr;
+  double* tsp64 = nullptr;
+  FEB_TRY(H.pool.zeros(&tsp32, n3));
+  FEB_TRY(H.pool.zeros(&tsp64, n3));
+  FEB_TRY(H.pool.alloc(&H.D6_32, 6 * (size_t)H.ntotal));
+  FEB_TRY(H.pool.alloc(&H.D6_64, 6 * (size_t)H.ntotal));
+  launch_dinv6<float>(H.L[0].Dinv64, H.ntotal, H.D6_32, H.s);
+  launch_dinv6<double>(H.L[0].Dinv64, H.ntotal, H.D6_64, H.s);
+  FEB_CUDA(cudaGetLastError());
+  const double hc = H.xe[1] - H.xe[0];
+  auto uniform = [&](const std::vector<double>& e) {
+    for (size_t i = 0; i + 1 < e.size(); ++i)
+      if (std::fabs((e[i + 1] - e[i]) - hc) > 1e-12 * hc) return false;
+    return true;
+  };
+  const bool cube = H.mode == MAT_ISO_SRI && hc > 0.0 && uniform(H.xe) && uniform(H.ye) && uniform(H.ze);
+  auto fill = [&](auto& P, const auto& F, auto* tsp, const auto* d6) {
+    P.nx = H.nx; P.ny = H.ny; P.nz = H.nz; P.nxn = nxn; P.nyn = nyn; P.nzn = nzn; P.mp = mp;
+    P.nnode = H.nnode; P.ntotal = H.ntotal;
+    P.cellpair = cellpair; P.mtab = vals; P.nmat = kMaxMatIds;
+    P.cube = cube; P.h = hc;
+    P.dx = F.dx; P.dy = F.dy; P.dz = F.dz; P.idx = F.idx; P.idy = F.idy; P.idz = F.idz;
+    P.tsp = tsp; P.dinv6 = d6;
+  };
+  fill(H.P32, H.F32, tsp32, H.D6_32);
+  fill(H.P64, H.F64, tsp64, H.D6_64);
+  FEB_TRY(prepare_fine_pair(H.mode, cube));
+  H.pc32 = PairConfig{cube ? 16 : 8, 16};
+  H.pc64 = PairConfig{8, 16};
+  H.pair_ok = true;
+  return FEB_OK;
+}
+
 int setup_tc(FebHandle* h) {
   FebHandle& H = *h;
   if ((H.mode != MAT_ISO_SRI && H.mode != MAT_ISO_FULL) || env_tc() == 0) return FEB_OK;
@@ -1408,8 +1655,9 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   launch_block_inverse(D, H.ntotal, V.Dinv64, V.Dinv32, s);
   FEB_CUDA(cudaGetLastError());
   H.pool.free(D);
-  H.stage_mark();   // 3: used nodes, level-0 diagonal blocks
-  g_prof.mark("L0 local upload, diag blocks", s);
+  FEB_TRY(setup_pair<W>(h, mat_s64));
+  H.stage_mark();   // 3: used nodes, level-0 diagonal blocks, paired-row operator
+  g_prof.mark("L0 local upload, diag blocks, pair operator", s);
   FEB_TRY(setup_tc(h));
   FEB_TRY(autotune_ku(h));
   H.stage_mark();   // 4: K.u autotuning (first handle of a grid shape only)
@@ -1693,7 +1941,7 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
     if ((st = h->pool.alloc(&h->partials, kRedBlocks)) != FEB_OK) break;
     if ((st = h->pool.zeros(&h->sc, 4)) != FEB_OK) break;
     if ((st = h->pool.zeros(&h->status, 1)) != FEB_OK) break;
-    if (cudaMallocHost(&h->st_h, sizeof(CgState)) != cudaSuccess) { st = FEB_ERR_CUDA; set_last_error("cudaMallocHost"); break; }
+    if (!(h->st_h = g_pinned.take())) { st = FEB_ERR_CUDA; set_last_error("cudaMallocHost"); break; }
     st = (h->mode == MAT_ORTHO) ? setup_level0<6>(h, op) : setup_level0<2>(h, op);
     if (st != FEB_OK) break;
     st = build_hierarchy(h);
@@ -1939,6 +2187,11 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
   inf.ku_shape[0] = H.ku32.tc ? 0 : H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
   inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
+  inf.ku_kind = (H.tc_ok && H.ku32.tc) ? 2 : (H.pair_ok ? 1 : 0);
+  if (H.pair_ok) {
+    if (!(H.tc_ok && H.ku32.tc)) { inf.ku_shape[0] = H.pc32.wy; inf.ku_shape[1] = H.pc32.zchunk; }
+    inf.ku_shape[2] = H.pc64.wy; inf.ku_shape[3] = H.pc64.zchunk;
+  }
   if (info) *info = inf;
   FEB_TRY(H.sync_out());
   if (st != FEB_OK) {

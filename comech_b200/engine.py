@@ -202,7 +202,7 @@ def _info_dict(info, t0, extra=None):
              t_gpu=round(info.t_solve_ms / 1e3, 4), coarse="dense-inverse", coarse_n=int(info.coarse_n),
              level_dofs=[int(info.level_dofs[i]) for i in range(int(info.levels))],
              lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
-             kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape),
+             kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape), ku_kind=int(info.ku_kind),
              t_stage_ms=[round(float(v), 3) for v in info.t_stage_ms], device=f"cuda:{_torch().cuda.current_device()}",
              x0_used=bool(info.x0_used), x0_scale=float(info.x0_scale), t_wall=round(time.perf_counter() - t0, 4))
     if extra:

@@ -113,6 +113,9 @@ typedef struct FebInfo {
   int32_t x0_used;               /* 1: the solve started from the caller's x0 (as FebOptions.x0_mode prepares it); 0:
                                     from zero (no x0, or a start s with s.f <= 0: the fallback of a warm start) */
   float x0_scale;                /* the energy-optimal multiple a = s.f / s.K s applied to the start (1 in mode 0) */
+  int32_t ku_kind;               /* level-0 K.u kernel of FP32 products: 0 per-cell kernel, 1 paired-row kernel
+                                    (ku_shape then holds warps per CTA and node planes of that kernel), 2 tensor
+                                    cores; FP64 products use the paired-row kernel whenever it is set up */
 } FebInfo;
 
 /* Default options (tol 1e-6, maxiter 800 as rb/splitfe.py:123; GMG parameters of fe/gmg.py:80). */

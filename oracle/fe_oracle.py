@@ -23,6 +23,8 @@ It is a NumPy/SciPy restatement, written for this project, of the reference algo
 Parity of this restatement is pinned against golden vectors produced by running the reference
 itself (``tests/golden/make_golden.py``, committed fixtures in ``tests/golden/``).
 """
+import time
+
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
@@ -394,6 +396,7 @@ def pcg(A, b, precond, tol, maxiter, x0=None):
 
 def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, Z=None):
     """GMG-preconditioned CG with an optional additive correction Z pinv(Z^T A Z) Z^T (fe/gmg.py:120-137)."""
+    t0 = time.perf_counter()
     mg = Multigrid(A, used_nodes, *grid_edges)
     prec = mg.vcycle
     if Z is not None and Z.shape[1] > 0:
@@ -401,8 +404,36 @@ def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, Z=None
         Ec = Zd.T @ (A @ Zd)
         Einv = np.linalg.pinv(0.5 * (Ec + Ec.T))
         prec = lambda r: mg.vcycle(r) + Zd @ (Einv @ (Zd.T @ r))
+    t1 = time.perf_counter()
     x, flag, iters = pcg(A, b, prec, tol, maxiter, x0)
-    return x, dict(iters=iters, flag=flag, levels=len(mg.levels))
+    t2 = time.perf_counter()
+    return x, dict(iters=iters, flag=flag, levels=len(mg.levels), t_setup=t1 - t0, t_pcg=t2 - t1)
+
+
+def spring_matrix_cn(xyz, springs, bone_nodes):
+    """Ligament hook for solve_cn's ``extra`` (rb/replica3.py:68-86): spring s pulls along d = (b - a)/|b - a|;
+    each end is the mean over the used nodes of its bone within max(4 mm, distance of the 8th-nearest), so
+    w = +d/n_A on the A-end nodes and -d/n_B on the B-end nodes, and K += k w w^T."""
+    def build(nmap, n):
+        rows, cols, vals = [], [], []
+        for s in springs:
+            a, b = np.asarray(s["a"], float), np.asarray(s["b"], float)
+            d = (b - a) / np.linalg.norm(b - a)
+            w = np.zeros(n)
+            for pt, sign, key in ((a, 1.0, "A"), (b, -1.0, "B")):
+                cand = np.asarray(bone_nodes[s[key]])
+                cand = cand[nmap[cand] >= 0]
+                dist = np.linalg.norm(xyz[cand] - pt, axis=1)
+                radius = max(4.0, np.sort(dist)[min(7, len(dist) - 1)])
+                ln = nmap[cand[dist <= radius]]
+                for c in range(3):
+                    np.add.at(w, 3 * ln + c, sign * d[c] / len(ln))
+            nz = np.flatnonzero(w)
+            rows.append(np.repeat(nz, len(nz)))
+            cols.append(np.tile(nz, len(nz)))
+            vals.append(s["k"] * np.outer(w[nz], w[nz]).ravel())
+        return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    return build
 
 
 # ----------------------------------------------------------------------------------------- solves
@@ -410,6 +441,7 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
     """Split-node solve (rb/splitfe.py:123-158): ground penalty k = 1e6 per unit area on all three
     components of the fixed nodes, nodal loads area * t, K += diag(kd) + extra(nmap, n), per-bone rigid
     modes, GMG-PCG.  Returns U (nnew, 3) with NaN on unused nodes, info, reactions R."""
+    t0 = time.perf_counter()
     cells = np.flatnonzero(active)
     K, nmap, nused = assemble(g, lam, mu, cells, cn, kl_sri(g))
     n = K.shape[0]
@@ -424,7 +456,9 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
     if extra is not None:
         K = K + extra(nmap, n)
     Z = rigid_modes(g.node_xyz[orig], nmap, n, node_groups) if node_groups else None
+    t_asm = time.perf_counter() - t0
     u, info = pcg_gmg(K, f, orig[nused], (g.xe, g.ye, g.ze), tol=tol, Z=Z, maxiter=maxiter)
+    info["t_assemble"] = t_asm
     U = np.full((len(orig), 3), np.nan)
     U[nused] = u.reshape(-1, 3)
     R = np.zeros((len(orig), 3))

@@ -1,8 +1,8 @@
 """Generate the golden fixtures of tests/golden/ by running the reference CoMech code itself.
 
-Run in a container where the reference is mounted (default /root/reference, override with COMECH_REF):
+Run where the reference checkout is readable, naming its root in COMECH_REF:
 
-    python tests/golden/make_golden.py
+    COMECH_REF=<path to the CoMech checkout> python tests/golden/make_golden.py
 
 Every fixture stores its inputs as well as the reference's outputs, so the tests never need the
 reference (nor the synthetic generator) at run time.  Reference functions used:
@@ -11,7 +11,7 @@ fe/gmg.py (GMG, pcg_gmg), rb/splitfe.py (split_connectivity[_fast], KL_family, a
 solve_cn, cell_stress_cn, element_forces_cn), fe/test_patch.py (patch-test set-up),
 rb/rbsim.py (rigid_fit, sample_fe, sample_nodes) and the region-force sums of rb/rbfe.py:194-213.
 
-    python tests/golden/make_golden.py [fixture ...]      # default: all fixtures
+    COMECH_REF=... python tests/golden/make_golden.py [fixture ...]      # default: all fixtures
 """
 import os
 import sys
@@ -19,7 +19,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("COMECH_REF", "/root/reference")
+REF = os.environ.get("COMECH_REF")
+if not REF:
+    sys.exit("make_golden.py: set COMECH_REF to the root of the reference CoMech checkout")
 sys.path.insert(0, REPO)
 sys.path.insert(1, REF)
 sys.path.insert(2, os.path.join(REF, "rb"))
@@ -247,8 +249,83 @@ def patch():
     save("patch", xe=g.xe, ye=g.ye, ze=g.ze, E=E, nu=nu, U=U, sig=sig, vm=vm)
 
 
+# seeded surgical actions of the batch configuration on a mid-size hindfoot (80 x 55 x 47.5 mm at 2.5 mm)
+ACTION_CASE = dict(nx=32, ny=22, nz=19, h=2.5, seed=4)
+
+
+def input_digest(P):
+    """Sums of the generator's output that the tests recompute to detect a changed generator."""
+    return np.array([P["lam"].sum(), P["mu"].sum(), P["active"].sum(), P["cn"].sum(), len(P["orig"]),
+                     P["fixed"][1].sum(), P["loads"][0][1].sum(), P["extra"].node_coo()[4].sum()], float)
+
+
+def actions():
+    """solve_cn of the reference on the instance of each action (rb/splitfe.py:123-158), with stress."""
+    out = {}
+    for act in ("resection", "osteotomy", "interposition", "fusion", "load"):
+        P = synth.hindfoot_problem(ACTION_CASE["nx"], ACTION_CASE["ny"], ACTION_CASE["nz"], h=ACTION_CASE["h"],
+                                   seed=ACTION_CASE["seed"], action=act)
+        g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+        U, info, R = RSF.solve_cn(g, P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"],
+                                  P["extra"], P["node_groups"], tol=1e-10, maxiter=800)
+        cells = np.flatnonzero(P["active"])
+        sig, vm, eps = RSF.cell_stress_cn(g, P["lam"], P["mu"], U, cells, P["cn"])
+        out.update({f"{act}_digest": input_digest(P), f"{act}_U": U, f"{act}_R": R, f"{act}_vm": vm,
+                    f"{act}_iters": info["iters"], f"{act}_ndof": info["ndof"]})
+    save("actions", case=np.array([ACTION_CASE[k] for k in ("nx", "ny", "nz", "h", "seed")], float), **out)
+
+
+def spring_hook():
+    """The reference's ligament hook (rb/replica3.py:68-86): ends averaged over the bone nodes within
+    max(4 mm, the 8th-nearest distance), K += k w w^T per spring, used through solve_cn's extra argument the way
+    the engine builds it (rb/rbfe.py:167-179: end bone = the bone nearest to the end point)."""
+    import replica3 as R3
+    from scipy.spatial import cKDTree
+    P = synth.hindfoot_problem(24, 18, 16, h=3.0, seed=3)
+    g = RS.Grid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
+    cn, orig, active, part = P["cn"], P["orig"], P["active"], P["part"]
+    cells = np.flatnonzero(active)
+    xyz = g.node_xyz[orig]
+    names = {1: "talus", 2: "calcaneus", 3: "navicular"}
+    allc = np.arange(g.ncell)
+    bone_nodes = {nm: np.unique(cn[allc[(part == k) & active]].ravel()) for k, nm in names.items()}
+    rng = np.random.default_rng(17)
+    springs = []
+    for (ka, kb) in ((1, 2), (1, 3), (2, 3), (1, 2), (2, 3), (1, 3)):
+        na, nb = bone_nodes[names[ka]], bone_nodes[names[kb]]
+        a = xyz[na[rng.integers(len(na))]] + rng.uniform(-1.0, 1.0, 3)
+        b = xyz[nb[rng.integers(len(nb))]] + rng.uniform(-1.0, 1.0, 3)
+        springs.append(dict(a=a.tolist(), b=b.tolist(), k=float(rng.uniform(50.0, 200.0))))
+    trees = {nm: cKDTree(xyz[nd]) for nm, nd in bone_nodes.items() if len(nd)}
+    for s_ in springs:
+        for key, pt in (("A", s_["a"]), ("B", s_["b"])):
+            s_[key] = min(trees, key=lambda nm: trees[nm].query(pt)[0])
+    hook = R3.spring_matrix_cn(xyz, springs, bone_nodes)
+    U, info, R = RSF.solve_cn(g, P["lam"], P["mu"], active, cn, orig, P["fixed"], P["loads"], hook, P["node_groups"],
+                              tol=1e-10, maxiter=800)
+    # the hook's matrix on full-layout dofs (3 node + component), for a hook-shaped callable in the tests
+    nused = np.unique(cn[cells])
+    nmap = -np.ones(len(orig), np.int64)
+    nmap[nused] = np.arange(len(nused))
+    M = hook(nmap, 3 * len(nused)).tocoo()
+    rows = 3 * nused[M.row // 3] + M.row % 3
+    cols = 3 * nused[M.col // 3] + M.col % 3
+    (ln, la, lt), = P["loads"]
+    groups = np.concatenate(P["node_groups"]); glen = np.array([len(x) for x in P["node_groups"]])
+    bn = np.concatenate([bone_nodes[names[k]] for k in (1, 2, 3)])
+    blen = np.array([len(bone_nodes[names[k]]) for k in (1, 2, 3)])
+    save("spring_hook", xe=g.xe, ye=g.ye, ze=g.ze, lam=P["lam"], mu=P["mu"], active=active, cn=cn, orig=orig,
+         fixed_nodes=P["fixed"][0], fixed_area=P["fixed"][1], load_nodes=ln, load_area=la, load_t=lt, groups=groups,
+         group_len=glen, bone_nodes=bn, bone_len=blen,
+         spring_a=np.array([s_["a"] for s_ in springs]), spring_b=np.array([s_["b"] for s_ in springs]),
+         spring_k=np.array([s_["k"] for s_ in springs]),
+         spring_ends=np.array([[list(names.values()).index(s_["A"]), list(names.values()).index(s_["B"])]
+                               for s_ in springs]),
+         hook_rows=rows, hook_cols=cols, hook_vals=M.data, U=U, R=R, iters=info["iters"], ndof=info["ndof"])
+
+
 if __name__ == "__main__":
     fixtures = dict(elements=elements, split=split_cases, hindfoot=hindfoot_solve, block=block_solves, patch=patch,
-                    post=post, materials=materials_case)
+                    post=post, materials=materials_case, actions=actions, spring_hook=spring_hook)
     for name in (sys.argv[1:] or list(fixtures)):
         fixtures[name]()

@@ -3,7 +3,7 @@ reference itself (tests/golden/) and, at larger sizes, the CPU oracle and size-i
 
 Tolerances: FP64 operator products 1e-12 relative; solutions at CG tolerance 1e-10 within 1e-7 relative
 L2 of the reference's; mixed / refined precision at rel-res 1e-8 within 1e-6 (displacement) and 1e-5
-(von Mises), the bar of the task statement."""
+(von Mises) against the FP64 reference solution."""
 import os
 
 import numpy as np

@@ -185,3 +185,65 @@ def test_oracle_material_mixing(golden):
         E, nu, active, F, ser = O.mix_materials(cls, z["L"], shape, groups, **kw)
         for a, key in ((E, "E"), (nu, "nu"), (active, "active"), (F, "F"), (ser, "ser")):
             np.testing.assert_array_equal(a, z[f"{name}_{key}"])
+
+
+# ------------------------------------------------------------------------ spring hook and surgical actions
+def spring_hook_inputs(z):
+    """Springs and bone-node sets of the spring_hook fixture in the reference's hook form."""
+    names = ["talus", "calcaneus", "navicular"]
+    bn = np.split(z["bone_nodes"], np.cumsum(z["bone_len"])[:-1])
+    bone_nodes = dict(zip(names, bn))
+    springs = [dict(a=a, b=b, k=float(k), A=names[e[0]], B=names[e[1]])
+               for a, b, k, e in zip(z["spring_a"], z["spring_b"], z["spring_k"], z["spring_ends"])]
+    return springs, bone_nodes
+
+
+def test_oracle_spring_hook_matches_reference(golden):
+    z = golden("spring_hook")
+    og = O.OGrid(z["xe"], z["ye"], z["ze"])
+    springs, bone_nodes = spring_hook_inputs(z)
+    hook = O.spring_matrix_cn(og.node_xyz[z["orig"]], springs, bone_nodes)
+    cells = np.flatnonzero(z["active"])
+    nused = np.unique(z["cn"][cells])
+    nmap = -np.ones(len(z["orig"]), np.int64)
+    nmap[nused] = np.arange(len(nused))
+    M = hook(nmap, 3 * len(nused)).tocoo()
+    got = {(3 * nused[r // 3] + r % 3, 3 * nused[c // 3] + c % 3): v for r, c, v in zip(M.row, M.col, M.data)}
+    ref = dict(zip(zip(z["hook_rows"], z["hook_cols"]), z["hook_vals"]))
+    assert set(got) == set(ref)
+    scale = np.abs(z["hook_vals"]).max()
+    assert max(abs(got[k] - ref[k]) for k in ref) <= 1e-13 * scale
+
+
+def test_oracle_solve_with_spring_hook(golden):
+    z = golden("spring_hook")
+    og = O.OGrid(z["xe"], z["ye"], z["ze"])
+    springs, bone_nodes = spring_hook_inputs(z)
+    hook = O.spring_matrix_cn(og.node_xyz[z["orig"]], springs, bone_nodes)
+    U, info, R = O.solve_cn(og, z["lam"], z["mu"], z["active"], z["cn"], z["orig"],
+                            (z["fixed_nodes"], z["fixed_area"]), [(z["load_nodes"], z["load_area"], z["load_t"])],
+                            hook, _groups(z), tol=1e-10)
+    ok = ~np.isnan(z["U"])
+    assert (np.isnan(U) == ~ok).all()
+    assert np.linalg.norm(U[ok] - z["U"][ok]) / np.linalg.norm(z["U"][ok]) < 1e-7
+    assert abs(info["iters"] - int(z["iters"])) <= 3
+
+
+def action_problem(z, action):
+    from comech_b200 import synth
+    nx, ny, nz, h, seed = z["case"]
+    return synth.hindfoot_problem(int(nx), int(ny), int(nz), h=float(h), seed=int(seed), action=action)
+
+
+def action_digest(P):
+    return np.array([P["lam"].sum(), P["mu"].sum(), P["active"].sum(), P["cn"].sum(), len(P["orig"]),
+                     P["fixed"][1].sum(), P["loads"][0][1].sum(), P["extra"].node_coo()[4].sum()], float)
+
+
+@pytest.mark.parametrize("action", ["resection", "osteotomy", "interposition", "fusion", "load"])
+def test_action_instances_match_the_fixture(golden, action):
+    """The generator still makes the instances the reference solved for the actions fixture."""
+    z = golden("actions")
+    P = action_problem(z, action)
+    np.testing.assert_allclose(action_digest(P), z[f"{action}_digest"], rtol=1e-12, atol=0)
+    assert len(P["orig"]) == len(z[f"{action}_U"])
