@@ -121,16 +121,46 @@ def make_problem(seed, dims=WORKLOAD):
     return synth.hindfoot_problem(dims["nx"], dims["ny"], dims["nz"], h=dims["h"], seed=seed)
 
 
-def cpu_oracle_step(dims, seed=0):
-    """One solve_cn + cell_stress of the CPU oracle; returns (seconds, ndof)."""
+def cpu_oracle_run(dims, seed=0, P=None):
+    """One solve_cn + cell_stress of the CPU oracle on the generator's instance at ``dims``: seconds per phase
+    (assembly with penalties and extra entries, multigrid set-up, PCG, stress), dofs, iterations, and the
+    solution (U, von Mises) for the parity checks."""
     from oracle import fe_oracle as O
-    P = make_problem(seed, dims)
+    P = make_problem(seed, dims) if P is None else P
     g = O.OGrid(P["grid"].xe, P["grid"].ye, P["grid"].ze)
     t = time.perf_counter()
     U, info, R = O.solve_cn(g, P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"], P["extra"],
                             P["node_groups"], tol=TOL)
-    O.cell_stress(g, P["lam"], P["mu"], U, np.flatnonzero(P["active"]), P["cn"], nan_to_zero=True)
-    return time.perf_counter() - t, info["ndof"], info["iters"]
+    t1 = time.perf_counter()
+    _, vm, _ = O.cell_stress(g, P["lam"], P["mu"], U, np.flatnonzero(P["active"]), P["cn"], nan_to_zero=True)
+    t2 = time.perf_counter()
+    return dict(t=t2 - t, t_assemble=info["t_assemble"], t_setup=info["t_setup"], t_pcg=info["t_pcg"],
+                t_stress=t2 - t1, ndof=int(info["ndof"]), iters=int(info["iters"]), U=U, vm=vm)
+
+
+def cpu_oracle_step(dims, seed=0):
+    """One solve_cn + cell_stress of the CPU oracle; returns (seconds, ndof, iterations)."""
+    r = cpu_oracle_run(dims, seed)
+    return r["t"], r["ndof"], r["iters"]
+
+
+def extrapolate(sample, ndof, iters):
+    """Oracle seconds of a solve of ``ndof`` dofs in ``iters`` iterations from a measured sample: the assembly,
+    multigrid set-up and stress phases scale with the dofs, the PCG phase with dofs x iterations."""
+    r = ndof / sample["ndof"]
+    return ((sample["t_assemble"] + sample["t_setup"] + sample["t_stress"]) * r
+            + sample["t_pcg"] * r * iters / sample["iters"])
+
+
+def parity(U, vm, Uo, vmo):
+    """Displacement and von Mises rel-L2 of a device solution against the oracle's (used nodes, active cells)."""
+    U = np.asarray(U).reshape(-1, 3)
+    Uo = np.asarray(Uo).reshape(-1, 3)
+    ok = ~np.isnan(Uo)
+    if not (np.isnan(U) == ~ok).all():
+        return {"error": "used-node masks differ"}
+    return {"disp_rel_l2": float(np.linalg.norm(U[ok] - Uo[ok]) / np.linalg.norm(Uo[ok])),
+            "vm_rel_l2": float(np.linalg.norm(np.asarray(vm) - vmo) / np.linalg.norm(vmo))}
 
 
 def workload_ndof():
