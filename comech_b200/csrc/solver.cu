@@ -2248,6 +2248,30 @@ int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int3
   return h->sync_out();
 }
 
+int feb_benchmark_apply_set(FebHandle* h, int32_t prec, int32_t nbuf, const void* const* u, void* const* y,
+                            int32_t nrep, float* ms) {
+  if (!h || nbuf < 1 || !u || !y || nrep < 1 || !ms) {
+    set_last_error("feb_benchmark_apply_set: bad argument");
+    return FEB_ERR_ARG;
+  }
+  for (int b = 0; b < nbuf; ++b)
+    if (!u[b] || !y[b]) { set_last_error("feb_benchmark_apply_set: null buffer %d", b); return FEB_ERR_ARG; }
+  FEB_TRY(h->sync_in());
+  FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+  for (int i = 0; i < nrep; ++i) {
+    const int b = i % nbuf;
+    if (prec == 0) h->apply<double>(0, (const double*)u[b], (double*)y[b], nullptr);
+    else h->apply<float>(0, (const float*)u[b], (float*)y[b], nullptr);
+  }
+  FEB_CUDA(cudaEventRecord(h->ev1, h->s));
+  FEB_CUDA(cudaEventSynchronize(h->ev1));
+  float t = 0.f;
+  FEB_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+  *ms = t / nrep;
+  FEB_TRY(check_tc_status(h));
+  return h->sync_out();
+}
+
 int feb_destroy(FebHandle* h) {
   if (!h) return FEB_OK;
   delete h;

@@ -367,6 +367,10 @@ FEB_API int feb_net_to_nodes(FebNetGrid net, const double* hn, const float* pred
 
 /* Benchmark hook: average device time (CUDA events on the handle's stream) of nrep level-0 products. */
 FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms);
+/* Benchmark hook: the same over nbuf (u, y) pairs used in turn, so that a set of buffers larger than the L2
+   cache makes every product read its operands from HBM. */
+FEB_API int feb_benchmark_apply_set(FebHandle* h, int32_t prec, int32_t nbuf, const void* const* u, void* const* y,
+                                    int32_t nrep, float* ms);
 
 /* Kernels launched by this library since it was loaded (graph launches count their kernel nodes). */
 FEB_API int64_t feb_launch_count(void);
