@@ -73,7 +73,7 @@ struct LevelParams;
 //   r = r_in - t            -> r_out (if given)
 //   d' = a1 u + a2 Dinv r   -> d_out (if given);  x_out = x_in + d' (x_in may be null: zero)
 // with (a1, a2) = (0, c_init) for k < 0 and (a1[k], a2[k]) of the level's Chebyshev parameters otherwise.
-// With neither d_out nor x_out the step is the residual update r_out = r_in - K u.
+// With neither d_out nor x_out the step is the residual update r_out = r_in - K u (lp may then be null).
 template <typename T>
 struct SmoothArgs {
   const T* r_in = nullptr;

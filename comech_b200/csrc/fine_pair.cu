@@ -191,9 +191,11 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   T (*sMat)[MW] = reinterpret_cast<T (*)[MW]>(smem_raw + 4 * sizeof(V2<T>) * 3 * WY * 32);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   T a1 = T(0), a2 = T(0);
-  if constexpr (SMOOTH) {
-    a1 = S.k < 0 ? T(0) : T(S.lp->a1[S.k]);
-    a2 = S.k < 0 ? T(S.lp->c_init) : T(S.lp->a2[S.k]);
+  if constexpr (SMOOTH) {   // the Chebyshev coefficients (a residual-only step carries no parameters)
+    if (S.lp && (S.d_out || S.x_out)) {
+      a1 = S.k < 0 ? T(0) : T(S.lp->a1[S.k]);
+      a2 = S.k < 0 ? T(S.lp->c_init) : T(S.lp->a2[S.k]);
+    }
   }
   const int64_t ntiles = (int64_t)nbx * nby * nbz;
   if (blockIdx.x >= ntiles) {   // split copies: finished from the sparse accumulator alone
