@@ -240,6 +240,83 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
+def timed_steps(fn, steps, flush, dist=None, clocks=None):
+    """Device time of ``steps`` calls of fn (CUDA events on the current stream, L2 flushed before each); the
+    barrier and synchronisation bracket the whole timed region.  Returns (per-step ms, last result)."""
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out, ms = None, []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        flush_l2(flush)
+        ev0.record()
+        out = fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        ms.append(ev0.elapsed_time(ev1))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    return ms, out
+
+
+def special_nodes(P, g):
+    """Grid nodes of the level-0 operator that receive a sparse contribution (ground springs, extra entries,
+    corners of cells touching split copies) plus the split copies: the nodes that go through the accumulator."""
+    cells = np.flatnonzero(P["active"])
+    irr = cells[(P["cn"][cells] != g.cell_nodes[cells]).any(1)]
+    nr = P["extra"].node_coo()[0]
+    nodes = np.unique(np.concatenate([np.asarray(P["fixed"][0]), P["cn"][irr].ravel(), nr]))
+    return int(np.count_nonzero(nodes < g.nnode)) + (len(P["orig"]) - g.nnode), len(irr)
+
+
+def ku_roofline(P, d, lib, engine, _lib, pk, pk_kind):
+    """The level-0 operator (sparse pass + paired-row kernel) timed on a rotating set of operand buffers
+    larger than L2, with its algorithmic bytes."""
+    import ctypes as C
+    import torch
+    g = P["grid"]
+    ntotal = len(P["orig"])
+    nact = int(P["active"].sum())
+    n_spec, n_irr = special_nodes(P, g)
+    n_pen = len(P["fixed"][0])
+    n_extra = P["extra"].node_coo()[4].size
+    npair = (g.nx + 1) * ((g.ny + 1) // 2 + 1) * (g.nz + 1)
+    pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"], pen_node=d["pen_node"],
+                        pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
+    roof = {}
+    try:
+        for name, dt, sv in (("fp32", torch.float32, 4), ("fp64", torch.float64, 8)):
+            nbuf = max(2, int(np.ceil(3 * 126e6 / (6 * ntotal * sv))))      # the set exceeds L2 three times over
+            us = [torch.randn(3 * ntotal, dtype=dt, device="cuda") for _ in range(nbuf)]
+            ys = [torch.empty_like(u) for u in us]
+            up = (C.c_void_p * nbuf)(*[u.data_ptr() for u in us])
+            yp = (C.c_void_p * nbuf)(*[y.data_ptr() for y in ys])
+            ms = C.c_float()
+            for nrep in (2 * nbuf, 20 * nbuf):
+                _lib.check(lib.feb_benchmark_apply_set(pr.h, 0 if sv == 8 else 1, nbuf, up, yp, nrep, C.byref(ms)))
+            # u, y; cell-pair words (2 bytes per pair of node rows); the sparse part: irregular cells (8 node ids +
+            # 2 material values), penalties (node + 3 values), extra entries (column + value), and the
+            # accumulator of the special nodes (atomic adds, then read and cleared by the owners)
+            alg = (6 * ntotal * sv + 2 * npair + n_irr * (32 + 2 * sv) + n_pen * (4 + 3 * sv) + n_extra * (8 + sv)
+                   + n_spec * 3 * sv * 3)
+            roof[name] = dict(ms=ms.value, bytes=alg, gbs=alg / (ms.value * 1e-3) / 1e9, nbuf=nbuf)
+            del us, ys
+    finally:
+        pr.close()
+    r32 = roof["fp32"]
+    return {"bound": "hbm", "achieved": round(r32["gbs"], 1), "peak": pk, "unit": "GB/s",
+            "frac": round(r32["gbs"] / pk, 4), "traffic": ku_traffic(),
+            "kernel": "level-0 K.u FP32 (k_fine_sparse + k_fine_pair), operands rotated over "
+                      f"{r32['nbuf']} buffer sets (> L2)",
+            "peak_kind": pk_kind, "ms_per_launch": round(r32["ms"], 4), "algorithmic_bytes": r32["bytes"],
+            "active_cells": nact,
+            "fp64": {"achieved": round(roof["fp64"]["gbs"], 1), "frac": round(roof["fp64"]["gbs"] / pk, 4),
+                     "ms_per_launch": round(roof["fp64"]["ms"], 4), "algorithmic_bytes": roof["fp64"]["bytes"]}}
+
+
 def run_ours(args, rank, world, dist):
     import torch
     from comech_b200 import engine, _lib
@@ -247,6 +324,7 @@ def run_ours(args, rank, world, dist):
     dev = torch.cuda.current_device()
     P = make_problem(seed=rank_seed(rank))
     d = device_inputs(P)
+    g = P["grid"]
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
     prec = args.precision
     warm = None
@@ -257,82 +335,60 @@ def run_ours(args, rank, world, dist):
         except RuntimeError:
             if args.warm == "on":
                 raise
-    for _ in range(args.warmup):
-        device_solve(P, d, prec)
-    torch.cuda.synchronize()
-    # ---------------------------------------------------------------- timed: device-resident inputs
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    step_ms = []
-    launches0 = lib.feb_launch_count()
-    with Clocks(dev) as clk:
-        if dist:
-            dist.barrier()
+    # the metric's configuration (learned start when the packaged network is present), then the same solve
+    # from a zero start and the plain FP64 GMG-PCG; every arm is the mean of the same number of timed steps
+    arms = [("headline", prec, warm)]
+    if warm is not None:
+        arms.append(("zero_start", prec, None))
+    arms.append(("plain_fp64", "fp64", None))
+    res = {}
+    launches = 0
+    clk_summary = None
+    for name, pr_, w_ in arms:
+        for _ in range(args.warmup):
+            device_solve(P, d, pr_, warm=w_)
         torch.cuda.synchronize()
-        for _ in range(args.steps):
-            flush_l2(flush)
-            ev0.record()
-            U, vm, info = device_solve(P, d, prec)
-            ev1.record()
-            torch.cuda.synchronize()
-            step_ms.append(ev0.elapsed_time(ev1))
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-    launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
-    t_total = reduce_max(sum(step_ms) / 1e3, dist)
+        launches0 = lib.feb_launch_count()
+        if name == "headline":
+            with Clocks(dev) as clk:
+                ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist)
+            clk_summary = clk.summary()
+            launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
+        else:
+            ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist)
+        U, vm, info = out
+        res[name] = dict(ms=ms, U=U.cpu().numpy(), vm=vm, info=info)
+    t_total = reduce_max(sum(res["headline"]["ms"]) / 1e3, dist)
     value = t_total / (args.steps * world)
-    mixed_info = info
-    U_mixed = U.cpu().numpy()
-    g0 = P["grid"]
-    # ---------------------------------------------------------------- plain FP64 GMG-PCG, same inputs
-    device_solve(P, d, "fp64")
-    torch.cuda.synchronize()
-    fp64_ms = []
-    for _ in range(max(1, min(args.steps, 3))):
-        flush_l2(flush)
-        ev0.record()
-        U64, vm64, info64 = device_solve(P, d, "fp64")
-        ev1.record()
-        torch.cuda.synchronize()
-        fp64_ms.append(ev0.elapsed_time(ev1))
-    U64h = U64.cpu().numpy()
-    ok = ~np.isnan(U64h)
-    # ---------------------------------------------------------------- the learned start, measured beside
+    mean_s = {k: reduce_max(sum(v["ms"]) / 1e3, dist) / (args.steps * world) for k, v in res.items()}
+    hinfo = res["headline"]["info"]
+    U64h = res["plain_fp64"]["U"]
+    vm64 = res["plain_fp64"]["vm"]
+    par64 = {}
+    for k in res:
+        if k != "plain_fp64":
+            par64[k] = parity(res[k]["U"], res[k]["vm"].cpu().numpy(), U64h, vm64.cpu().numpy())
     learned = None
     if warm is not None:
-        try:
-            device_solve(P, d, prec, warm=warm)
-            torch.cuda.synchronize()
-            w_ms = []
-            for _ in range(max(1, min(args.steps, 3))):
-                flush_l2(flush)
-                ev0.record()
-                _, _, infw = device_solve(P, d, prec, warm=warm)
-                ev1.record()
-                torch.cuda.synchronize()
-                w_ms.append(ev0.elapsed_time(ev1))
-            nc = g0.nx * g0.ny * g0.nz
-            torch.cuda.synchronize()
-            ev0.record()
-            x0w = warm.predict_x0(g0, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
-                                  d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
-            ev1.record()
-            torch.cuda.synchronize()
-            t_pred = ev0.elapsed_time(ev1)
-            xw = x0w.view(-1, 3).cpu().numpy()
-            Ur = U64h.reshape(-1, 3)
-            okn = ok.reshape(-1, 3).all(1)
-            learned = {"s_per_solve": round(min(w_ms) / 1e3, 5), "steps_ms": [round(t, 2) for t in w_ms],
-                       "iters": int(infw.iters), "relres": infw.relres, "prediction_ms": round(t_pred, 3),
-                       "x0_used": int(infw.x0_used), "x0_scale": float(infw.x0_scale),
-                       "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn])),
-                       "network": "3D conv encoder-decoder, 4.26M parameters, trained on 2000 FP64 solves of the "
-                                  "96x64x48 generator; start = x0 + M(f - K x0), scaled to its energy-optimal multiple"}
-        except _lib.FebError as e:     # a network pass whose tensor-core wait ran out
-            learned = {"error": str(e)}
-
-    disp_rel = float(np.linalg.norm(U_mixed[ok] - U64h[ok]) / np.linalg.norm(U64h[ok]))
-    vm_rel = float(torch.linalg.norm(vm - vm64).item() / torch.linalg.norm(vm64).item())
+        nc = g.nx * g.ny * g.nz
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        x0w = warm.predict_x0(g, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
+                              d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
+        ev1.record()
+        torch.cuda.synchronize()
+        xw = x0w.view(-1, 3).cpu().numpy()
+        Ur = U64h.reshape(-1, 3)
+        okn = ~np.isnan(Ur).any(1)
+        zi = res["zero_start"]["info"]
+        learned = {"iters": int(hinfo.iters), "zero_start_iters": int(zi.iters),
+                   "s_per_solve": round(mean_s["headline"], 5), "zero_start_s_per_solve": round(mean_s["zero_start"], 5),
+                   "prediction_ms": round(ev0.elapsed_time(ev1), 3), "x0_used": int(hinfo.x0_used),
+                   "x0_scale": float(hinfo.x0_scale),
+                   "prediction_rel_l2": float(np.linalg.norm(xw[okn] - Ur[okn]) / np.linalg.norm(Ur[okn])),
+                   "network": "3D conv encoder-decoder, 4.26M parameters, trained on 2000 FP64 solves of the "
+                              "96x64x48 generator; start = x0 + M(f - K x0), scaled to its energy-optimal multiple"}
     # ---------------------------------------------------------------- e2e through the public API
     pinned = {}
     for k in ("lam", "mu", "cn", "orig"):
@@ -344,13 +400,12 @@ def run_ours(args, rank, world, dist):
     act.numpy()[...] = P["active"]
     pinned["active"] = act.numpy()
     cells_h = np.flatnonzero(P["active"])
-    g = P["grid"]
 
     def e2e_step():
         t_a = time.perf_counter()
         U, inf, R = engine.solve_cn(g, pinned["lam"], pinned["mu"], pinned["active"], pinned["cn"], pinned["orig"],
                                     P["fixed"], P["loads"], P["extra"], P["node_groups"], tol=TOL, maxiter=800,
-                                    precision=prec, keep_device=True)
+                                    precision=prec, keep_device=True, warm_start=warm)
         t_b = time.perf_counter()
         sig, vmh, eps = engine.cell_stress_cn(g, pinned["lam"], pinned["mu"], U, cells_h, pinned["cn"],
                                               device=inf["device"])
@@ -362,7 +417,7 @@ def run_ours(args, rank, world, dist):
     e2e_step()
     torch.cuda.synchronize()
     e2e_s = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(max(1, min(args.steps, 5))):
         flush_l2(flush)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -374,71 +429,64 @@ def run_ours(args, rank, world, dist):
            + P["loads"][0][0].size * 32 + nact * 8 + P["fixed"][0].size * 32 + P["extra"].node_coo()[4].size * 24)
     d2h = ntotal * 24 + nact * 13 * 8
     e2e_val = reduce_max(sum(e2e_s) / len(e2e_s), dist) / world
-    # ---------------------------------------------------------------- roofline of the K.u operator
+    # ---------------------------------------------------------------- roofline of the level-0 operator
     pk, pk_kind = peaks()
-    pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"], pen_node=d["pen_node"],
-                        pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
-    import ctypes as C
-    roof = {}
-    try:
-        used = pr.used_mask()[1]
-        n_irr = int(np.count_nonzero((P["cn"][cells_h] != g.cell_nodes[cells_h]).any(1)))
-        n_pen = len(P["fixed"][0])
-        n_extra = P["extra"].node_coo()[4].size
-        for name, dt, sv in (("fp32", torch.float32, 4), ("fp64", torch.float64, 8)):
-            u = torch.randn(3 * ntotal, dtype=dt, device="cuda")
-            y = torch.empty_like(u)
-            ms = C.c_float()
-            _lib.check(lib.feb_benchmark_apply(pr.h, 0 if sv == 8 else 1, C.c_void_p(u.data_ptr()),
-                                               C.c_void_p(y.data_ptr()), 5, C.byref(ms)))
-            _lib.check(lib.feb_benchmark_apply(pr.h, 0 if sv == 8 else 1, C.c_void_p(u.data_ptr()),
-                                               C.c_void_p(y.data_ptr()), 50, C.byref(ms)))
-            alg = (3 * ntotal * sv * 2 + nact * 2 * sv + n_irr * (32 + 2 * sv) + n_pen * (4 + 3 * sv)
-                   + n_extra * (8 + sv))
-            roof[name] = dict(ms=ms.value, bytes=alg, gbs=alg / (ms.value * 1e-3) / 1e9)
-    finally:
-        pr.close()
-    traffic = ku_traffic()
-    r32 = roof["fp32"]
-    roofline = {"bound": "hbm", "achieved": round(r32["gbs"], 1), "peak": pk, "unit": "GB/s",
-                "frac": round(r32["gbs"] / pk, 4), "traffic": traffic, "kernel": "K.u FP32 (k_fine_struct + sparse pass)",
-                "peak_kind": pk_kind, "ms_per_launch": round(r32["ms"], 4), "algorithmic_bytes": r32["bytes"],
-                "fp64": {"achieved": round(roof["fp64"]["gbs"], 1), "frac": round(roof["fp64"]["gbs"] / pk, 4),
-                         "ms_per_launch": round(roof["fp64"]["ms"], 4)}}
-    # ---------------------------------------------------------------- CPU baseline (rank 0, N = 1)
+    roofline = ku_roofline(P, d, lib, engine, _lib, pk, pk_kind)
+    # ---------------------------------------------------------------- CPU baseline and oracle parity (rank 0, N = 1)
     cpu = None
+    parity_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        secs, nd, iters = cpu_oracle_step(SAMPLE_BIG)
-        scale = mixed_info.ndof / nd
-        cpu = {"value": round(secs * scale, 2), "unit": "s/solve", "cores": 1, "kind": "port",
-               "sample": (f"oracle solve_cn + cell_stress, hindfoot {SAMPLE_BIG['nx']}x{SAMPLE_BIG['ny']}x"
-                          f"{SAMPLE_BIG['nz']} h={SAMPLE_BIG['h']} ({nd} dofs, {iters} iters, {secs:.1f} s), scaled "
-                          f"x{scale:.2f} by dofs to the workload")}
+        Ps = make_problem(0, SAMPLE_BIG)
+        smp = cpu_oracle_run(SAMPLE_BIG, P=Ps)
+        ds = device_inputs(Ps)
+        parity_oracle = {"workload": (f"hindfoot {SAMPLE_BIG['nx']}x{SAMPLE_BIG['ny']}x{SAMPLE_BIG['nz']} "
+                                      f"h={SAMPLE_BIG['h']} ({smp['ndof']} dofs, oracle {smp['iters']} iterations)")}
+        for name, pr_, w_ in arms:
+            Us, vms, _ = device_solve(Ps, ds, pr_, warm=w_)
+            parity_oracle[name] = parity(Us.cpu().numpy(), vms.cpu().numpy(), smp["U"], smp["vm"])
+        it_w = int(res["plain_fp64"]["info"].iters)
+        est = extrapolate(smp, int(hinfo.ndof), it_w)
+        cpu = {"value": round(est, 2), "unit": "s/solve", "cores": 1, "kind": "port",
+               "sample": (f"oracle solve_cn + cell_stress (NumPy/SciPy, single-threaded sparse kernels) on hindfoot "
+                          f"{SAMPLE_BIG['nx']}x{SAMPLE_BIG['ny']}x{SAMPLE_BIG['nz']} h={SAMPLE_BIG['h']}: {smp['ndof']} "
+                          f"dofs, {smp['iters']} iterations, {smp['t']:.1f} s (assembly {smp['t_assemble']:.1f}, "
+                          f"multigrid set-up {smp['t_setup']:.1f}, PCG {smp['t_pcg']:.1f}, stress "
+                          f"{smp['t_stress']:.1f}); set-up and stress scaled by dofs, PCG by dofs x iterations to "
+                          f"{int(hinfo.ndof)} dofs and {it_w} iterations (the FP64 solve's count on the workload)")}
+    if args.cpu_full and rank == 0:
+        full = cpu_oracle_run(WORKLOAD, P=P)
+        cpu_full = {"s_per_solve": round(full["t"], 2), "iters": full["iters"], "ndof": full["ndof"],
+                    "phases_s": {k: round(full[k], 2) for k in ("t_assemble", "t_setup", "t_pcg", "t_stress")},
+                    "cores": 1}
+        parity_full = {k: parity(v["U"], v["vm"].cpu().numpy(), full["U"], full["vm"]) for k, v in res.items()}
+    else:
+        cpu_full = parity_full = None
     return dict(
         metric=METRIC, value=round(value, 5), unit="s/solve", n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=round(1e3 * t_total / args.steps, 3), higher_is_better=False, scaling="weak", vs_baseline=None,
-        dtype="f32 inner / f64 refinement" if prec == "refine" else ("f64" if prec == "fp64" else "f64 CG / f32 V-cycle"),
+        dtype=("f32 inner / f64 refinement" if prec == "refine" else
+               ("f64" if prec == "fp64" else "f64 CG / f32 V-cycle")),
         data="synthetic (seeded hindfoot generator)",
         config={"workload": (f"hindfoot {WORKLOAD['nx']}x{WORKLOAD['ny']}x{WORKLOAD['nz']} h={WORKLOAD['h']}mm "
-                             f"(C2 generator)"), "ndof": int(mixed_info.ndof),
-                "precision": prec,
-                "warm_start": ("zero; the learned start (the metric's learned+mixed) is measured beside in "
-                               "learned_warm_start (a few percent of the iterations at most)" if warm is not None
-                               else "zero (no trained network found)"), "tol": TOL,
-                "iters": int(mixed_info.iters), "sweeps": int(mixed_info.sweeps), "relres": mixed_info.relres,
-                "levels": int(mixed_info.levels), "l2": "flushed (256 MB write) before every step",
-                "parallelism": f"independent solves x{world}"},
-        plain_fp64={"s_per_solve": round(min(fp64_ms) / 1e3, 5), "iters": int(info64.iters),
-                    "relres": info64.relres},
-        speedup_vs_plain_fp64=round(min(fp64_ms) / 1e3 / value, 3) if world == 1 else None,
-        learned_warm_start=learned,
-        parity_vs_fp64={"disp_rel_l2": disp_rel, "vm_rel_l2": vm_rel},
-        stage_ms={"setup": round(mixed_info.t_setup_ms, 3), "solve": round(mixed_info.t_solve_ms, 3),
-                  "setup_stages": dict(zip(SETUP_STAGES, (round(float(v), 3) for v in mixed_info.t_stage_ms)))},
+                             f"(C2 generator)"), "ndof": int(hinfo.ndof), "precision": prec,
+                "warm_start": ("learned (packaged network), prediction inside the step" if warm is not None
+                               else "zero (no trained network found)"),
+                "tol": TOL, "iters": int(hinfo.iters), "sweeps": int(hinfo.sweeps), "relres": hinfo.relres,
+                "levels": int(hinfo.levels), "ku_kernel": ["per-cell", "paired-row", "tensor-core"][int(hinfo.ku_kind)],
+                "l2": "flushed (256 MB write) before every step", "parallelism": f"independent solves x{world}"},
+        arms_s_per_solve={k: round(v, 5) for k, v in mean_s.items()},
+        arms_iters={k: int(v["info"].iters) for k, v in res.items()},
+        plain_fp64={"s_per_solve": round(mean_s["plain_fp64"], 5), "iters": int(res["plain_fp64"]["info"].iters),
+                    "relres": res["plain_fp64"]["info"].relres},
+        speedup_vs_plain_fp64=round(mean_s["plain_fp64"] / value, 3) if world == 1 else None,
+        learned_warm_start=learned, parity_vs_fp64=par64, parity_vs_oracle=parity_oracle,
+        cpu_full=cpu_full, parity_vs_oracle_full=parity_full,
+        stage_ms={"setup": round(hinfo.t_setup_ms, 3), "solve": round(hinfo.t_solve_ms, 3),
+                  "setup_stages": dict(zip(SETUP_STAGES, (round(float(v), 3) for v in hinfo.t_stage_ms)))},
         e2e={"value": round(e2e_val, 5), "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
              "d2h_bytes_per_step": int(d2h), "iters": int(infe["iters"]), "relres": infe["relres"],
              "t_host": infe["t_host"], "steps_s": [round(t, 4) for t in e2e_s]},
-        roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk.summary(),
+        roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk_summary,
     )
 
 
@@ -469,6 +517,11 @@ def run_profile(args):
                 "t_stage_ms": [round(float(v), 2) for v in info.t_stage_ms]}
     pr = engine.Problem(P["grid"], _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
+    if args.mode == "ku-rot":
+        pr.close()
+        pk, pk_kind = peaks()
+        return {"mode": "ku-rot", "pair_config": os.environ.get("FEB_PAIR_CONFIG"),
+                "roofline": ku_roofline(P, d, _lib.load(), engine, _lib, pk, pk_kind)}
     out = {"mode": "ku"}
     try:
         ntotal = len(P["orig"])
@@ -646,7 +699,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "refine"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "post", "batch"], default="full",
+    ap.add_argument("--cpu-full", action="store_true",
+                    help="also run the CPU oracle on the full workload (minutes): true CPU time and parity at full size")
+    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "ku-rot", "post", "batch"], default="full",
                     help="solve-once / ku: one device solve or a few K.u products of the workload (profiling); "
                          "post: the rows around the solve, device against the CPU oracle; batch: 64 uneven "
                          "instances with seeded actions, one at a time and 8 / 16 in flight")

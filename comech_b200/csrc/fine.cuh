@@ -86,8 +86,9 @@ struct SmoothArgs {
 };
 
 struct PairConfig {
-  int wy = 16;       // warps per CTA (2 node rows each); 16 only on the cubic SRI path in FP32
-  int zchunk = 16;   // node planes per CTA
+  int wy = 16;            // warps per CTA of products (2 node rows each); 16 only on the cubic SRI path in FP32
+  int zchunk = 16;        // node planes per CTA of products
+  int zchunk_smooth = 16; // node planes per CTA of the smoothing steps (always 8 warps per CTA)
 };
 
 // y = K u (S null) or the smoother step S; returns a status
@@ -97,6 +98,10 @@ int launch_fine_pair(const PairView<T>& F, const FineView<T>& G, const T* u, T* 
 // sets the shared-memory limits of every paired-kernel variant of this model on the current device (call
 // before any stream capture)
 int prepare_fine_pair(int mode, bool cube);
+// resident CTAs per SM of the paired kernel (smoothing variant) and its x-y tiles per node plane
+template <typename T>
+int fine_pair_blocks_per_sm(int mode, bool cube, int wy, bool smooth);
+int fine_pair_tiles_xy(int nxn, int nyn, int wy);
 template <int W>
 void launch_mat_ids(const double* mat_s, int64_t ncell, unsigned long long* keys, double* vals, uint8_t* ids,
                     int* status, cudaStream_t s);

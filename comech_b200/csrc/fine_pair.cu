@@ -131,42 +131,57 @@ __device__ __forceinline__ void pair_modal(P2<T> (&X)[8], P2<T> (&Y)[8], P2<T> (
     }
 }
 
-// per-node smoother update of one node: t = K u at the node (u = the direction d_in), all 3 components
+// Operands of the smoother update at one node, loaded a step before they are used: residual before the
+// product, iterate, direction (the product's input) and the symmetric block-Jacobi inverse.
 template <typename T>
-struct NodeUpd {
-  const PairView<T>& F;
-  const SmoothArgs<T>& S;
-  T a1, a2;
-  __device__ __forceinline__ void run(int64_t n, const T (&t)[3], const T* __restrict__ u) const {
-    T r[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) r[c] = S.r_in[3 * n + c] - t[c];
-    if (S.r_out) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) S.r_out[3 * n + c] = r[c];
-    }
-    if (!S.d_out && !S.x_out) return;
-    const int64_t nt = F.ntotal;
-    const T* D = F.dinv6;
-    const T d00 = D[n], d11 = D[nt + n], d22 = D[2 * nt + n], d01 = D[3 * nt + n], d02 = D[4 * nt + n],
-            d12 = D[5 * nt + n];
-    T z[3];
-    z[0] = d00 * r[0] + d01 * r[1] + d02 * r[2];
-    z[1] = d01 * r[0] + d11 * r[1] + d12 * r[2];
-    z[2] = d02 * r[0] + d12 * r[1] + d22 * r[2];
-    T dn[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) dn[c] = a2 * z[c] + (a1 != T(0) ? a1 * u[3 * n + c] : T(0));
-    if (S.d_out) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) S.d_out[3 * n + c] = dn[c];
-    }
-    if (S.x_out) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) S.x_out[3 * n + c] = (S.x_in ? S.x_in[3 * n + c] : T(0)) + dn[c];
-    }
-  }
+struct NodeOps {
+  T r[3], x[3], d[3], D[6];
 };
+
+template <typename T>
+__device__ __forceinline__ void load_node_ops(const PairView<T>& F, const SmoothArgs<T>& S, const T* __restrict__ u,
+                                              bool need_dir, int n, NodeOps<T>& o) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    o.r[c] = S.r_in[3 * n + c];
+    o.x[c] = S.x_in ? S.x_in[3 * n + c] : T(0);
+    o.d[c] = need_dir ? u[3 * n + c] : T(0);
+  }
+  if (S.d_out || S.x_out) {
+    const T* D = F.dinv6 + n;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o.D[q] = D[(size_t)q * F.ntotal];
+  }
+}
+
+// smoother update of one node from t = K u at the node and its operands
+template <typename T>
+__device__ __forceinline__ void node_update(const SmoothArgs<T>& S, T a1, T a2, int n, const T (&t)[3],
+                                            const NodeOps<T>& o) {
+  T r[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) r[c] = o.r[c] - t[c];
+  if (S.r_out) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S.r_out[3 * n + c] = r[c];
+  }
+  if (!S.d_out && !S.x_out) return;
+  T z[3];
+  z[0] = o.D[0] * r[0] + o.D[3] * r[1] + o.D[4] * r[2];
+  z[1] = o.D[3] * r[0] + o.D[1] * r[1] + o.D[5] * r[2];
+  z[2] = o.D[4] * r[0] + o.D[5] * r[1] + o.D[2] * r[2];
+  T dn[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dn[c] = a2 * z[c] + a1 * o.d[c];
+  if (S.d_out) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S.d_out[3 * n + c] = dn[c];
+  }
+  if (S.x_out) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S.x_out[3 * n + c] = o.x[c] + dn[c];
+  }
+}
 
 template <typename T, int MODE, bool CUBE, int WY>
 constexpr size_t pair_smem_bytes() {
@@ -182,6 +197,8 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   constexpr bool HAS12 = (MODE != MAT_ISO_SRI);
   constexpr int OY = 2 * WY - 2;
   constexpr int MW = CUBE ? 2 : W;
+  // FP32 smoothing loads the epilogue operands one step ahead; FP64 (no register room) loads them in finish()
+  constexpr bool PREF = SMOOTH && std::is_same<T, float>::value;
   using V = P2<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // forward: (sum, diff) x-edge of the lower row per component; backward: (mean, diff) x-edge force of the
@@ -205,7 +222,9 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
 #pragma unroll
     for (int c = 0; c < 3; ++c) { t[c] = F.tsp[3 * n + c]; F.tsp[3 * n + c] = T(0); }
     if constexpr (SMOOTH) {
-      NodeUpd<T>{F, S, a1, a2}.run(n, t, u);
+      NodeOps<T> o;
+      load_node_ops(F, S, u, a1 != T(0), (int)n, o);
+      node_update(S, a1, a2, (int)n, t, o);
     } else {
 #pragma unroll
       for (int c = 0; c < 3; ++c) y[3 * n + c] = t[c];
@@ -231,10 +250,12 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   const bool in0 = xin && r0 >= 0 && r0 < F.nyn, in1 = xin && r1 < F.nyn;
   const bool own_x = lane >= 1 && lane <= kXOwn && i < F.nxn;
   const bool own0 = own_x && w >= 1 && r0 < F.nyn, own1 = own_x && w <= WY - 2 && r1 < F.nyn;
-  const int64_t plane = (int64_t)F.nxn * F.nyn;
-  const int64_t n0base = in0 ? i + (int64_t)F.nxn * r0 : 0, n1base = in1 ? i + (int64_t)F.nxn * r1 : 0;
-  const int64_t cpl = (int64_t)F.nxn * F.mp;
-  const int64_t cbase = (xin && m < F.mp) ? i + (int64_t)F.nxn * m : -1;
+  // 32-bit node offsets (feb_create keeps 3 x nodes below 2^31)
+  const int plane = F.nxn * F.nyn;
+  const int n0base = in0 ? i + F.nxn * r0 : 0, n1base = in1 ? i + F.nxn * r1 : 0;
+  const int cpl = F.nxn * F.mp;
+  const int cbase = (xin && m < F.mp) ? i + F.nxn * m : -1;
+  const bool need_dir = SMOOTH && a1 != T(0);
   // geometry of the general path: this thread's x width and its two rows' y widths
   V ga(T(1)), gb(T(1)), gia(T(1)), gib(T(1));
   if constexpr (!CUBE) {
@@ -246,8 +267,9 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
 
   auto load_plane = [&](int k, V (&v)[3]) {
     const bool kin = k >= 0 && k < F.nzn;
-    const T* p0 = u + 3 * (n0base + plane * k);
-    const T* p1 = u + 3 * (n1base + plane * k);
+    const int pk = plane * k;
+    const T* p0 = u + 3 * (n0base + pk);
+    const T* p1 = u + 3 * (n1base + pk);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v[c] = V((kin && in0) ? p0[c] : T(0), (kin && in1) ? p1[c] : T(0));
   };
@@ -281,7 +303,8 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   };
   // finishes node plane kk: y-edge totals (lower share + the share from the pair below), x back-transform,
   // epilogue of the owned nodes
-  auto finish = [&](int kk, int sl, const V (&Lw)[3][2], const T (&Uhi)[3][2], uint32_t flags) {
+  auto finish = [&](int kk, int sl, const V (&Lw)[3][2], const T (&Uhi)[3][2], uint32_t flags, const NodeOps<T>& o0,
+                    const NodeOps<T>& o1) {
     V tot[3][2];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -299,7 +322,7 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
       out[c] = lo + left;
     }
     if (kk < K0 || kk >= K1) return;
-    const int64_t n0 = n0base + plane * kk, n1 = n1base + plane * kk;
+    const int n0 = n0base + plane * kk, n1 = n1base + plane * kk;
     T t0[3] = {out[0].lo(), out[1].lo(), out[2].lo()}, t1[3] = {out[0].hi(), out[1].hi(), out[2].hi()};
     if (own0 && (flags & 0x80u)) {
 #pragma unroll
@@ -309,10 +332,13 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
 #pragma unroll
       for (int c = 0; c < 3; ++c) { t1[c] += F.tsp[3 * n1 + c]; F.tsp[3 * n1 + c] = T(0); }
     }
-    if constexpr (SMOOTH) {
-      const NodeUpd<T> up{F, S, a1, a2};
-      if (own0) up.run(n0, t0, u);
-      if (own1) up.run(n1, t1, u);
+    if constexpr (PREF) {
+      if (own0) node_update(S, a1, a2, n0, t0, o0);
+      if (own1) node_update(S, a1, a2, n1, t1, o1);
+    } else if constexpr (SMOOTH) {
+      NodeOps<T> o;
+      if (own0) { load_node_ops(F, S, u, need_dir, n0, o); node_update(S, a1, a2, n0, t0, o); }
+      if (own1) { load_node_ops(F, S, u, need_dir, n1, o); node_update(S, a1, a2, n1, t1, o); }
     } else {
       if (own0) {
 #pragma unroll
@@ -329,6 +355,15 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   V Fk[3][4], topc[3][4], Lw[3][2];
   T Uhi[3][2];
   uint32_t cells_c, cells_n, flags_prev = 0u;
+  NodeOps<T> op0, op1, on0, on1;   // operands of the plane finished this step, and of the next one
+  auto prefetch = [&](int kk, NodeOps<T>& o0, NodeOps<T>& o1) {
+    if constexpr (PREF) {
+      if (kk >= K0 && kk < K1) {
+        if (own0) load_node_ops(F, S, u, need_dir, n0base + plane * kk, o0);
+        if (own1) load_node_ops(F, S, u, need_dir, n1base + plane * kk, o1);
+      }
+    }
+  };
   {   // prologue: face of plane K0-1
     V v0[3], E[3][2];
     load_plane(K0 - 1, v0);
@@ -347,17 +382,20 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
       Uhi[c][0] = Uhi[c][1] = T(0);
     }
   }
+  prefetch(K0 - 1, op0, op1);
   for (int k = K0 - 1; k < K1; ++k) {
-    // (a) x-edge of plane k+1; prefetch plane k+3 and the cells of layer k+1
+    // (a) x-edge of plane k+1; prefetch plane k+3, the cells of layer k+1 and the epilogue operands of plane k
     V E[3][2];
     edge(vn, E);
     put_edge(slot(k + 1), E);
     load_plane(k + 3, vq);
     cells_n = load_cells(k + 1);
+    prefetch(k, on0, on1);
     __syncthreads();
     // (b) finish plane k-1
-    if (k > K0 - 1) finish(k - 1, slot(k - 1), Lw, Uhi, flags_prev);
+    if (k > K0 - 1) finish(k - 1, slot(k - 1), Lw, Uhi, flags_prev, op0, op1);
     flags_prev = cells_c;
+    if constexpr (PREF) { op0 = on0; op1 = on1; }
     // (c) faces of plane k+1, z butterfly -> modal coefficients of cell layer k
     V Fk1[3][4];
     face(slot(k + 1), E, Fk1);
@@ -419,7 +457,7 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
     cells_c = cells_n;
   }
   __syncthreads();
-  finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev);
+  finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev, op0, op1);
 }
 
 template <typename T, int MODE, bool CUBE, int WY, bool SMOOTH>
@@ -445,10 +483,7 @@ int prepare_pair_kernel() {
 template <typename T, int MODE>
 int prepare_pair_precision(bool cube) {
   if constexpr (MODE == MAT_ISO_SRI && std::is_same<T, float>::value) {
-    if (cube) {
-      FEB_TRY((prepare_pair_kernel<T, MODE, true, 16, false>()));
-      FEB_TRY((prepare_pair_kernel<T, MODE, true, 16, true>()));
-    }
+    if (cube) FEB_TRY((prepare_pair_kernel<T, MODE, true, 16, false>()));
   }
   if constexpr (MODE == MAT_ISO_SRI) {
     if (cube) {
@@ -464,10 +499,11 @@ int prepare_pair_precision(bool cube) {
 template <typename T, int MODE, bool SMOOTH>
 int launch_pair_wy(const PairView<T>& F, const T* u, T* y, const SmoothArgs<T>& A, const int* skip, PairConfig cfg,
                    cudaStream_t s) {
-  const int zc = std::max(1, cfg.zchunk);
+  if (SMOOTH) cfg.wy = 8;   // the smoothing variants need the register room of 8-warp CTAs
+  const int zc = std::max(1, SMOOTH ? cfg.zchunk_smooth : cfg.zchunk);
   if constexpr (MODE == MAT_ISO_SRI) {
     if (F.cube) {
-      if constexpr (std::is_same<T, float>::value) {
+      if constexpr (std::is_same<T, float>::value && !SMOOTH) {
         if (cfg.wy == 16) return launch_pair_kernel<T, MODE, true, 16, SMOOTH>(F, u, y, A, skip, zc, s);
       }
       return launch_pair_kernel<T, MODE, true, 8, SMOOTH>(F, u, y, A, skip, zc, s);
@@ -600,6 +636,38 @@ int launch_fine_pair(const PairView<T>& F, const FineView<T>& G, const T* u, T* 
   if (S) return launch_pair_wy<T, MODE, true>(F, u, y, *S, skip, cfg, s);
   return launch_pair_wy<T, MODE, false>(F, u, y, SmoothArgs<T>{}, skip, cfg, s);
 }
+
+template <typename T, int MODE, bool CUBE, int WY, bool SMOOTH>
+int pair_occupancy() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_fine_pair<T, MODE, CUBE, WY, SMOOTH>, 32 * WY,
+                                                    pair_smem_bytes<T, MODE, CUBE, WY>()) != cudaSuccess)
+    return 1;
+  return std::max(nb, 1);
+}
+
+template <typename T, bool SMOOTH>
+int pair_occupancy_mode(int mode, bool cube) {
+  if (mode == MAT_ISO_SRI && cube) return pair_occupancy<T, MAT_ISO_SRI, true, 8, SMOOTH>();
+  switch (mode) {
+    case MAT_ISO_SRI: return pair_occupancy<T, MAT_ISO_SRI, false, 8, SMOOTH>();
+    case MAT_ISO_FULL: return pair_occupancy<T, MAT_ISO_FULL, false, 8, SMOOTH>();
+    default: return pair_occupancy<T, MAT_ORTHO, false, 8, SMOOTH>();
+  }
+}
+
+template <typename T>
+int fine_pair_blocks_per_sm(int mode, bool cube, int wy, bool smooth) {
+  if (smooth) return pair_occupancy_mode<T, true>(mode, cube);
+  if constexpr (std::is_same<T, float>::value) {
+    if (wy == 16 && mode == MAT_ISO_SRI && cube) return pair_occupancy<T, MAT_ISO_SRI, true, 16, false>();
+  }
+  return pair_occupancy_mode<T, false>(mode, cube);
+}
+template int fine_pair_blocks_per_sm<float>(int, bool, int, bool);
+template int fine_pair_blocks_per_sm<double>(int, bool, int, bool);
+
+int fine_pair_tiles_xy(int nxn, int nyn, int wy) { return div_up(nxn, kXOwn) * div_up(nyn, 2 * wy - 2); }
 
 int prepare_fine_pair(int mode, bool cube) {
   switch (mode) {

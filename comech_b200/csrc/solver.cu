@@ -1248,22 +1248,56 @@ int tune_one(FebHandle* h, KuConfig* best, T* u, T* y) {
   return FEB_OK;
 }
 
-// launch shape of the paired kernel: warps per CTA x node planes per CTA
+// z chunks that fill 1 to 4 whole waves of resident CTAs, plus a few fixed sizes
 template <typename T>
-int tune_pair(FebHandle* h, PairConfig* best, T* u, T* y) {
-  std::vector<PairConfig> cand;
+std::vector<int> wave_chunks(FebHandle* h, int wy, bool smooth) {
+  int sms = kSmCount, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = fine_pair_blocks_per_sm<T>(h->mode, h->P32.cube, wy, smooth);
+  const int txy = fine_pair_tiles_xy(h->nx + 1, h->ny + 1, wy);
+  const int nzn = h->nz + 1;
+  std::vector<int> zcs = {8, 16, 32};
+  for (int waves = 1; waves <= 4; ++waves) {
+    const int nbz = std::max(1, (waves * sms * per_sm) / std::max(txy, 1));
+    zcs.push_back(std::max(2, div_up(nzn, nbz)));
+  }
+  std::sort(zcs.begin(), zcs.end());
+  zcs.erase(std::unique(zcs.begin(), zcs.end()), zcs.end());
+  return zcs;
+}
+
+// launch shapes of the paired kernel: products (warps per CTA x node planes per CTA) and smoothing steps
+// (node planes per CTA at 8 warps), each timed on this operator
+template <typename T>
+int tune_pair(FebHandle* h, PairConfig* best, T* u, T* y, T* y2, T* y3) {
+  PairConfig& slot = std::is_same<T, double>::value ? h->pc64 : h->pc32;
   const bool wide = std::is_same<T, float>::value && h->P32.cube;
+  float best_ms = 1e30f;
   for (int wy : {8, 16}) {
     if (wy == 16 && !wide) continue;
-    for (int zc : {8, 12, 16, 24, 32, 48}) cand.push_back(PairConfig{wy, zc});
+    for (int zc : wave_chunks<T>(h, wy, false)) {
+      slot.wy = wy;
+      slot.zchunk = zc;
+      float ms = 0.f;
+      FEB_TRY(time_apply<T>(h, u, y, &ms));
+      if (ms < best_ms) { best_ms = ms; best->wy = wy; best->zchunk = zc; }
+    }
   }
-  float best_ms = 1e30f;
-  PairConfig& slot = std::is_same<T, double>::value ? h->pc64 : h->pc32;
-  for (const PairConfig& c : cand) {
-    slot = c;
+  slot.wy = best->wy;
+  slot.zchunk = best->zchunk;
+  SmoothArgs<T> A;
+  A.r_in = u; A.r_out = y; A.x_in = u; A.x_out = y2; A.d_out = y3;   // no parameters: a1 = a2 = 0, same traffic
+  best_ms = 1e30f;
+  for (int zc : wave_chunks<T>(h, 8, true)) {
+    slot.zchunk_smooth = zc;
+    for (int w = 0; w < 2; ++w) h->pair_run<T>(u, nullptr, &A, nullptr);
+    FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+    for (int r = 0; r < 3; ++r) h->pair_run<T>(u, nullptr, &A, nullptr);
+    FEB_CUDA(cudaEventRecord(h->ev1, h->s));
+    FEB_CUDA(cudaEventSynchronize(h->ev1));
     float ms = 0.f;
-    FEB_TRY(time_apply<T>(h, u, y, &ms));
-    if (ms < best_ms) { best_ms = ms; *best = c; }
+    FEB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (ms < best_ms) { best_ms = ms; best->zchunk_smooth = zc; }
   }
   slot = *best;
   return FEB_OK;
@@ -1294,31 +1328,39 @@ int autotune_ku(FebHandle* h) {
     }
   }
   if (h->tc_ok && env_tc() == 1) h->ku32 = KuConfig{16, 16, 1};
-  if (penv && *penv) {
-    int wy = 8, zc = 16;
-    if (std::sscanf(penv, "%d,%d", &wy, &zc) == 2) {
-      h->pc32 = PairConfig{(wy == 16 && h->P32.cube) ? 16 : 8, zc};
-      h->pc64 = PairConfig{8, zc};
+  if (penv && *penv) {      // "wy,zchunk[,zchunk_smooth]"
+    int wy = 8, zc = 16, zs = 0;
+    const int got = std::sscanf(penv, "%d,%d,%d", &wy, &zc, &zs);
+    if (got >= 2) {
+      if (got < 3) zs = zc;
+      h->pc32 = PairConfig{(wy == 16 && h->P32.cube) ? 16 : 8, zc, zs};
+      h->pc64 = PairConfig{8, zc, zs};
       ppinned = true;
     }
   }
   const bool need_cell = !h->pair_ok && !pinned, need_pair = h->pair_ok && !ppinned;
   if (!need_cell && !need_pair) return FEB_OK;
   const size_t n = 3 * (size_t)h->ntotal;
-  double *u64 = nullptr, *y64 = nullptr;
+  double *u64 = nullptr, *y64 = nullptr, *y2 = nullptr, *y3 = nullptr;
   FEB_TRY(h->pool.zeros(&u64, n));
   FEB_TRY(h->pool.alloc(&y64, n));
+  if (need_pair) {
+    FEB_TRY(h->pool.alloc(&y2, n));
+    FEB_TRY(h->pool.alloc(&y3, n));
+  }
   Tuned t{h->ku32, h->ku64, h->pc32, h->pc64};
   if (need_cell) {
     FEB_TRY(tune_one<float>(h, &t.k32, (float*)u64, (float*)y64));
     FEB_TRY(tune_one<double>(h, &t.k64, u64, y64));
   }
   if (need_pair) {
-    FEB_TRY(tune_pair<float>(h, &t.p32, (float*)u64, (float*)y64));
-    FEB_TRY(tune_pair<double>(h, &t.p64, u64, y64));
+    FEB_TRY(tune_pair<float>(h, &t.p32, (float*)u64, (float*)y64, (float*)y2, (float*)y3));
+    FEB_TRY(tune_pair<double>(h, &t.p64, u64, y64, y2, y3));
   }
   h->pool.free(u64);
   h->pool.free(y64);
+  h->pool.free(y2);
+  h->pool.free(y3);
   h->ku32 = t.k32;
   h->ku64 = t.k64;
   h->pc32 = t.p32;
