@@ -357,22 +357,27 @@ def test_inputs_and_targets_of_a_hindfoot():
 
 def test_packaged_network_on_held_out_instances():
     """The network shipped in comech_b200/weights (trained on seeds 1000-2999 of the 96x64x48 generator against the
-    strain energy of its error plus 0.2 x the relative squared error) on three instances it never saw (an
-    osteotomy, an interposition, a fusion).
+    strain energy of its error plus 0.2 x the relative squared error) on six instances it never saw, one per
+    action.  Three starts of the same mixed-precision solve are compared: zero; the network's prediction; and the
+    same preparation from x0 = 0, i.e. one preconditioner application to the load scaled to its energy-optimal
+    multiple (a start that needs no network).  The preparation (a K product, a V-cycle, a K product and two dot
+    products) costs about one CG iteration.
 
-    Bars, from the 200-instance held-out study of comech_b200.warm_train:
-    - its prediction is within 90 % relative L2 of the FP64 solution (median 57 %, at most 73 %: the energy term
-      leaves rigid motions to the squared-error term, and the solve's springs and rigid-mode correction to CG);
-    - the mixed-precision solve started from it (smoothed once by the preconditioner, scaled to its
-      energy-optimal multiple) converges to rel-res 1e-8;
-    - it takes at most 8 more iterations than the zero start (per instance -6 to +5, mean -1.7).
+    Measured on 20 held-out instances (seeds 5000-5019): mean iterations 73.45 from zero, 72.15 from the learned
+    start, 72.90 from the preconditioned load.  The learned start saves about one iteration, which its preparation
+    costs again, so it gives no net gain on this hindfoot family: the count is set by the slow inter-bone modes
+    that the Krylov space finds within a few iterations whatever the start.
 
-    So the learned start is safe, and its gain over the zero start is about 2 iterations in 63."""
+    Bars: the prediction is within 90 % relative L2 of the FP64 solution; every solve converges; per instance the
+    learned start takes at most 8 more iterations than the zero start; and on average over the six it takes no
+    more than one iteration more than the zero start (it does not slow the solve down)."""
     import os
+    import torch
     from comech_b200 import warm_train as W
     assert os.path.exists(warmnet.WEIGHTS), "packaged network missing"
     net = warmnet.default_net()
-    for seed in (5000, 5001, 5002):
+    counts = []
+    for seed in range(5000, 5006):
         _, P = W.make_instance(seed)
         ln, lz = W.load_parts(P)
         U64, _ = W.solve(P, "fp64")
@@ -380,13 +385,17 @@ def test_packaged_network_on_held_out_instances():
         x0 = net.predict_x0(P["grid"], P["lam"], P["mu"], P["active"], P["orig"], P["fixed"][0], ln, lz,
                             len(P["orig"]))
         _, i1 = W.solve(P, "mixed", x0)
+        _, i2 = W.solve(P, "mixed", torch.zeros_like(x0))
         Ur = host(U64).reshape(-1, 3)
         ok = np.isfinite(Ur).all(1)
         pr = host(x0).reshape(-1, 3)
         assert np.linalg.norm(pr[ok] - Ur[ok]) < 0.9 * np.linalg.norm(Ur[ok])
-        assert i0.flag == 0 and i1.flag == 0 and i1.relres < 1e-8
+        assert i0.flag == 0 and i1.flag == 0 and i2.flag == 0 and i1.relres < 1e-8
         assert i1.x0_used == 1 and i1.x0_scale > 0
         assert i1.iters <= i0.iters + 8, (seed, i0.iters, i1.iters)
+        counts.append((i0.iters, i1.iters, i2.iters))
+    c = np.array(counts, float)
+    assert c[:, 1].mean() <= c[:, 0].mean() + 1.0, counts
 
 
 def test_edge_loss_and_head_gradient():
