@@ -489,23 +489,26 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       if (lane == src) { a0 += s0; a1 += s1; a2 += s2; }
     }
   }
-  if (L.tn_ptr && valid) {      // rank-1 terms: lane-parallel dot and axpy, the node's pairs split over the warps
-    const int pe = L.tn_ptr[n + 1];
-    for (int p = L.tn_ptr[n] + w; p < pe; p += 4) {
-      const int t = L.tn_term[p], eb = L.t_ptr[t], ee = L.t_ptr[t + 1];
-      T d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-      int e = eb;
-      for (; e + 3 < ee; e += 4) {
-        d0 += L.t_val[e] * u[L.t_dof[e]];
-        d1 += L.t_val[e + 1] * u[L.t_dof[e + 1]];
-        d2 += L.t_val[e + 2] * u[L.t_dof[e + 2]];
-        d3 += L.t_val[e + 3] * u[L.t_dof[e + 3]];
+  if (L.tn_ptr) {      // rank-1 terms: for each (node, term) pair of the 32 nodes, the whole warp forms the
+                       // term's dot v_t.u (lanes over its entries); the 4 warps take every 4th pair of a node
+    int pb = 0, pe = 0;
+    if (valid) { pb = L.tn_ptr[n]; pe = L.tn_ptr[n + 1]; }
+    unsigned todo = __ballot_sync(0xffffffffu, pe > pb);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int b0 = __shfl_sync(0xffffffffu, pb, src), b1 = __shfl_sync(0xffffffffu, pe, src);
+      for (int p = b0 + w; p < b1; p += 4) {
+        const int t = L.tn_term[p], eb = L.t_ptr[t], ee = L.t_ptr[t + 1];
+        T d = 0;
+        for (int e = eb + lane; e < ee; e += 32) d += L.t_val[e] * u[L.t_dof[e]];
+        const T dot = L.t_lam[t] * warp_sum(d);
+        if (lane == src) {
+          a0 += dot * L.tn_coef[3 * p];
+          a1 += dot * L.tn_coef[3 * p + 1];
+          a2 += dot * L.tn_coef[3 * p + 2];
+        }
       }
-      for (; e < ee; ++e) d0 += L.t_val[e] * u[L.t_dof[e]];
-      const T dot = L.t_lam[t] * ((d0 + d1) + (d2 + d3));
-      a0 += dot * L.tn_coef[3 * p];
-      a1 += dot * L.tn_coef[3 * p + 1];
-      a2 += dot * L.tn_coef[3 * p + 2];
     }
   }
   red[w][0][lane] = a0; red[w][1][lane] = a1; red[w][2][lane] = a2;
