@@ -271,6 +271,88 @@ __global__ void k_cells_to_stencil(const double* __restrict__ KeC, double* __res
   for (int t = 0; t < 9; ++t) A[(size_t)(o * 9 + t) * n + J] = acc[t];
 }
 
+// Galerkin basis of a coarse cell on a uniform fine grid with even cell counts: every coarse cell holds 2 x 2 x 2
+// fine cells of equal widths (a, b, c), and its prolongation weights are the same (1, 1/2, 0 per axis).  Hence
+// P_f^T K_f P_f of the fine cell at sub-position f is lam_f BL[f] + mu_f BM[f] with 16 constant 24 x 24
+// matrices (isotropic models), computed here once: out[(2 f + m) * 576 + 24 row + col], m = 0 (lam), 1 (mu).
+template <int MODE>
+__global__ void k_galerkin_basis(double a, double b, double c, double* __restrict__ out) {
+  const int f = blockIdx.x >> 1, m = blockIdx.x & 1;   // sub-position, material part
+  const int q = threadIdx.x;                              // column: coarse corner q / 3, component q % 3
+  if (q >= 24) return;
+  const int fx = f & 1, fy = (f >> 1) & 1, fz = (f >> 2) & 1;
+  const int ca = q / 3, s = q % 3;
+  auto w = [](int p, int corner) { return p == 1 ? 0.5 : ((p == 0) == (corner == 0) ? 1.0 : 0.0); };
+  double u[3][8], fo[3][8];
+  for (int l = 0; l < 8; ++l) {
+    const double v = w(fx + (l & 1), ca & 1) * w(fy + ((l >> 1) & 1), (ca >> 1) & 1) * w(fz + ((l >> 2) & 1), (ca >> 2) & 1);
+    for (int r = 0; r < 3; ++r) u[r][l] = (r == s) ? v : 0.0;
+  }
+  double mat[2] = {m == 0 ? 1.0 : 0.0, m == 1 ? 1.0 : 0.0};
+  Material<double> mt = make_material<double, MODE>(mat);
+  hex8_apply(u, a, b, c, 1.0 / a, 1.0 / b, 1.0 / c, mt, fo);
+  for (int cb = 0; cb < 8; ++cb)
+    for (int r = 0; r < 3; ++r) {
+      double acc = 0.0;
+      for (int l = 0; l < 8; ++l)
+        acc += w(fx + (l & 1), cb & 1) * w(fy + ((l >> 1) & 1), (cb >> 1) & 1) * w(fz + ((l >> 2) & 1), (cb >> 2) & 1) *
+               fo[r][l];
+      out[(size_t)blockIdx.x * 576 + (3 * cb + r) * 24 + q] = acc;
+    }
+}
+
+// Level-1 stencil A1[J][o] (27 blocks of 3 x 3) summed directly over the coarse cells holding J and J + o and
+// their 8 fine cells: sum_C sum_f lam_f BL[f][la][lb] + mu_f BM[f][la][lb] (same sums as k_galerkin_cells +
+// k_cells_to_stencil, without the 576-value coarse-cell matrices in memory).
+__global__ void __launch_bounds__(27 * 8)
+k_galerkin_direct(const double* __restrict__ mat_all, int fnx, int fny, const double* __restrict__ basis,
+                  double* __restrict__ A, int cnx, int cny, int cnz) {
+  extern __shared__ double sbasis[];   // 16 x 576
+  for (int t = threadIdx.y * 27 + threadIdx.x; t < 16 * 576; t += 27 * 8) sbasis[t] = basis[t];
+  __syncthreads();
+  const int o = threadIdx.x;
+  const int64_t n = (int64_t)cnx * cny * cnz;
+  const int64_t J = blockIdx.x * (int64_t)8 + threadIdx.y;
+  if (J >= n) return;
+  const int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+  const int jc[3] = {jx, jy, jz}, nn[3] = {cnx, cny, cnz};
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int I[3][2], aJ[3][2], aK[3][2], cnt[3];
+  bool ok = true;
+  for (int d = 0; d < 3; ++d) {
+    cnt[d] = 0;
+    const int K = jc[d] + od[d];
+    if (K < 0 || K >= nn[d]) { ok = false; break; }
+    for (int iv = jc[d] - 1; iv <= jc[d]; ++iv) {
+      if (iv < 0 || iv >= nn[d] - 1) continue;
+      if (K < iv || K > iv + 1) continue;
+      I[d][cnt[d]] = iv; aJ[d][cnt[d]] = jc[d] - iv; aK[d][cnt[d]] = K - iv; ++cnt[d];
+    }
+  }
+  if (ok) {
+    for (int cz = 0; cz < cnt[2]; ++cz)
+      for (int cy = 0; cy < cnt[1]; ++cy)
+        for (int cx = 0; cx < cnt[0]; ++cx) {
+          const int la = aJ[0][cx] + 2 * aJ[1][cy] + 4 * aJ[2][cz];
+          const int lb = aK[0][cx] + 2 * aK[1][cy] + 4 * aK[2][cz];
+          for (int f = 0; f < 8; ++f) {
+            const int fi = 2 * I[0][cx] + (f & 1), fj = 2 * I[1][cy] + ((f >> 1) & 1), fk = 2 * I[2][cz] + ((f >> 2) & 1);
+            const double* p = mat_all + 2 * (fi + (int64_t)fnx * (fj + (int64_t)fny * fk));
+            const double lam = p[0], mu = p[1];
+            if (lam == 0.0 && mu == 0.0) continue;
+            const double* BL = sbasis + (2 * f) * 576 + (3 * la) * 24 + 3 * lb;
+            const double* BM = BL + 576;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+              for (int qq = 0; qq < 3; ++qq) acc[3 * r + qq] += lam * BL[24 * r + qq] + mu * BM[24 * r + qq];
+          }
+        }
+  }
+  for (int t = 0; t < 9; ++t) A[(size_t)(o * 9 + t) * n + J] = acc[t];
+}
+
 __device__ __forceinline__ int64_t grid_pos(int64_t node, int64_t fnnode, const int* orig_copy) {
   return node < fnnode ? node : (int64_t)orig_copy[node - fnnode];
 }
@@ -629,6 +711,22 @@ void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, con
   dim3 blk2(27, 8);
   k_cells_to_stencil<<<div_up(n, 8), blk2, 0, s>>>(KeC, A1, cnx, cny, cnz); note_launch();
 }
+
+template <int MODE>
+int launch_galerkin_direct(const double* mat_all, int fnx, int fny, double a, double b, double c, double* basis,
+                           double* A1, int cnx, int cny, int cnz, cudaStream_t s) {
+  if (MODE == MAT_ORTHO) return FEB_ERR_ARG;
+  k_galerkin_basis<MODE><<<16, 32, 0, s>>>(a, b, c, basis); note_launch();
+  const int smem = 16 * 576 * sizeof(double);
+  FEB_TRY(set_dyn_smem((const void*)k_galerkin_direct, smem));
+  const int64_t n = (int64_t)cnx * cny * cnz;
+  k_galerkin_direct<<<div_up(n, 8), dim3(27, 8), smem, s>>>(mat_all, fnx, fny, basis, A1, cnx, cny, cnz); note_launch();
+  return FEB_OK;
+}
+template int launch_galerkin_direct<MAT_ISO_SRI>(const double*, int, int, double, double, double, double*, double*, int,
+                                                 int, int, cudaStream_t);
+template int launch_galerkin_direct<MAT_ISO_FULL>(const double*, int, int, double, double, double, double*, double*, int,
+                                                  int, int, cudaStream_t);
 
 void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
                              const int* pen_node, const double* pen_k, double* A1, int cnx, int cny, int cnz,

@@ -98,6 +98,12 @@ template <int MODE>
 void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, const TransferDev& P, double* KeC,
                            double* A1, int cnx, int cny, int cnz, cudaStream_t s);
 
+// Level-1 stencil of a uniform fine grid (cell widths a, b, c) with even cell counts, isotropic models: summed
+// directly from the fine cells' (lam, mu) and 16 constant sub-cell matrices (basis: 16 x 576 doubles of scratch).
+template <int MODE>
+int launch_galerkin_direct(const double* mat_all, int fnx, int fny, double a, double b, double c, double* basis,
+                           double* A1, int cnx, int cny, int cnz, cudaStream_t s);
+
 // Fold diagonal penalties / local extra entries of level 0 into the level-1 stencil.
 void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
                              const int* pen_node, const double* pen_k, double* A1, int cnx, int cny, int cnz,

@@ -1786,15 +1786,40 @@ int build_hierarchy(FebHandle* h) {
     g_prof.mark("Lk kept mask + count", H.s);
     FEB_TRY(H.pool.zeros(&C.A64, 243 * (size_t)C.ntotal));
     if (l == 0) {
-      double* KeC = nullptr;
-      FEB_TRY(H.pool.alloc(&KeC, 576 * (size_t)(C.nx - 1) * (C.ny - 1) * (C.nz - 1)));
-      switch (H.mode) {
-        case MAT_ISO_SRI: launch_galerkin_cells<MAT_ISO_SRI>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
-        case MAT_ISO_FULL: launch_galerkin_cells<MAT_ISO_FULL>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
-        default: launch_galerkin_cells<MAT_ORTHO>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+      // uniform widths per axis, even cell counts, isotropic model: the stencil is summed directly from the
+      // fine cells' materials (FEB_GALERKIN_DIRECT=0 keeps the coarse-cell matrices); otherwise coarse-cell
+      // matrices first, then the node stencil
+      auto uniform = [](const std::vector<double>& e) {
+        const double w0 = e[1] - e[0];
+        for (size_t i = 0; i + 1 < e.size(); ++i)
+          if (std::fabs((e[i + 1] - e[i]) - w0) > 1e-12 * std::fabs(w0)) return false;
+        return w0 > 0.0;
+      };
+      const char* genv = std::getenv("FEB_GALERKIN_DIRECT");
+      const bool direct = !(genv && genv[0] == '0') && H.mode != MAT_ORTHO && uniform(H.xe) && uniform(H.ye) &&
+                          uniform(H.ze) && H.nx % 2 == 0 && H.ny % 2 == 0 && H.nz % 2 == 0 &&
+                          C.nx == H.nx / 2 + 1 && C.ny == H.ny / 2 + 1 && C.nz == H.nz / 2 + 1;
+      if (direct) {
+        double* basis = nullptr;
+        FEB_TRY(H.pool.alloc(&basis, 16 * 576));
+        const double a = H.xe[1] - H.xe[0], b = H.ye[1] - H.ye[0], c = H.ze[1] - H.ze[0];
+        if (H.mode == MAT_ISO_SRI)
+          FEB_TRY(launch_galerkin_direct<MAT_ISO_SRI>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+        else
+          FEB_TRY(launch_galerkin_direct<MAT_ISO_FULL>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+        FEB_CUDA(cudaGetLastError());
+        H.pool.free(basis);
+      } else {
+        double* KeC = nullptr;
+        FEB_TRY(H.pool.alloc(&KeC, 576 * (size_t)(C.nx - 1) * (C.ny - 1) * (C.nz - 1)));
+        switch (H.mode) {
+          case MAT_ISO_SRI: launch_galerkin_cells<MAT_ISO_SRI>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+          case MAT_ISO_FULL: launch_galerkin_cells<MAT_ISO_FULL>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+          default: launch_galerkin_cells<MAT_ORTHO>(H.F64, H.mat_all, F.P, KeC, C.A64, C.nx, C.ny, C.nz, H.s); break;
+        }
+        FEB_CUDA(cudaGetLastError());
+        H.pool.free(KeC);
       }
-      FEB_CUDA(cudaGetLastError());
-      H.pool.free(KeC);
       launch_galerkin_penalty(F.P, F.nx, F.ny, F.nnode, H.orig_copy, H.npen, H.F64.pen_node, H.F64.pen_k, C.A64, C.nx,
                               C.ny, C.nz, C.ntotal, H.s);
       launch_galerkin_local(F.P, F.nx, F.ny, F.nnode, H.orig_copy, H.nlocal, H.loc_r, H.loc_c, H.loc_v, C.A64, C.nx,
