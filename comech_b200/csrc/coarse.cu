@@ -353,6 +353,57 @@ k_galerkin_direct(const double* __restrict__ mat_all, int fnx, int fny, const do
   for (int t = 0; t < 9; ++t) A[(size_t)(o * 9 + t) * n + J] = acc[t];
 }
 
+// Interior patterns: for the offsets o = 13..26 the blocks summed over the coarse cells holding J and J + o and
+// all 8 fine cells of each (one thread per (m, o, entry)).
+__global__ void k_sym_pattern(const double* __restrict__ basis, double* __restrict__ pat) {
+  const int t = threadIdx.x;   // 0..251
+  if (t >= 252) return;
+  const int m = t / 126, e = t % 126, q = e / 9, rc = e % 9, r = rc / 3, cc = rc % 3;
+  const int o = 13 + q;
+  const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+  int la_ax[3][2], lb_ax[3][2], cnt[3];
+  for (int d = 0; d < 3; ++d) {
+    cnt[d] = 0;
+    for (int iv = -1; iv <= 0; ++iv) {   // cells [jc + iv, jc + iv + 1] holding jc and jc + od
+      const int la = -iv, lb = od[d] - iv;
+      if (lb < 0 || lb > 1) continue;
+      la_ax[d][cnt[d]] = la; lb_ax[d][cnt[d]] = lb; ++cnt[d];
+    }
+  }
+  double acc = 0.0;
+  for (int cz = 0; cz < cnt[2]; ++cz)
+    for (int cy = 0; cy < cnt[1]; ++cy)
+      for (int cx = 0; cx < cnt[0]; ++cx) {
+        const int la = la_ax[0][cx] + 2 * la_ax[1][cy] + 4 * la_ax[2][cz];
+        const int lb = lb_ax[0][cx] + 2 * lb_ax[1][cy] + 4 * lb_ax[2][cz];
+        for (int f = 0; f < 8; ++f) acc += basis[(2 * f + m) * 576 + (3 * la + r) * 24 + 3 * lb + cc];
+      }
+  pat[t] = acc;
+}
+
+__global__ void k_sym_tags(const double* __restrict__ S64, int cnx, int cny, int cnz,
+                           const uint16_t* __restrict__ cellpair, int fnxn, int mp, const double* __restrict__ mtab,
+                           const double* __restrict__ pat, uint8_t* __restrict__ tag) {
+  const int64_t n = (int64_t)cnx * cny * cnz;
+  const int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (J >= n) return;
+  const int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  // fine cell (2 jx, 2 jy, 2 jz): row 2 jy is the upper byte of row pair m = jy
+  uint32_t id = 0;
+  if (jy < mp) id = (cellpair[2 * jx + (int64_t)fnxn * (jy + (int64_t)mp * (2 * jz))] >> 8) & 0x7fu;
+  uint8_t t = 0;
+  if (id > 0) {
+    const double lam = mtab[2 * id], mu = mtab[2 * id + 1];
+    double scale = 0.0;
+    for (int e = 0; e < 126; ++e) scale = fmax(scale, fabs(lam * pat[e]) + fabs(mu * pat[126 + e]));
+    bool same = scale > 0.0;
+    for (int e = 0; e < 126 && same; ++e)
+      same = fabs(S64[(size_t)e * n + J] - (lam * pat[e] + mu * pat[126 + e])) <= 1e-12 * scale;
+    t = same ? (uint8_t)id : 0;
+  }
+  tag[J] = t;
+}
+
 __device__ __forceinline__ int64_t grid_pos(int64_t node, int64_t fnnode, const int* orig_copy) {
   return node < fnnode ? node : (int64_t)orig_copy[node - fnnode];
 }
@@ -520,13 +571,23 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       const int* __restrict__ skip) {
   if (skip && *skip) return;
   __shared__ T red[4][3][32];
+  __shared__ T spat[2][126];
+  __shared__ T smat[128][2];
   const int lane = threadIdx.x, w = threadIdx.y;
+  const bool cmp = L.tag != nullptr;
+  if (cmp) {
+    const int tid = w * 32 + lane;
+    for (int e = tid; e < 252; e += 128) spat[e / 126][e % 126] = L.pat[e];
+    for (int e = tid; e < 256; e += 128) smat[e / 2][e % 2] = L.tmat[e];
+    __syncthreads();
+  }
   const int i = blockIdx.x * 32 + lane, j = blockIdx.y, k = blockIdx.z;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const bool valid = i < nx;
   const int ic = valid ? i : nx - 1;
   const int n = ic + nx * (j + ny * k);
   const int64_t N = L.n;
+  const int tn = cmp ? L.tag[n] : 0;
   T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
@@ -541,10 +602,26 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
     const int mf = vf ? n + off : n, mb = vb ? n - off : n;
     T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
     T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
-    const T f0 = B[n], f1 = B[N + n], f2 = B[2 * N + n], f3 = B[3 * N + n], f4 = B[4 * N + n],
-            f5 = B[5 * N + n], f6 = B[6 * N + n], f7 = B[7 * N + n], f8 = B[8 * N + n];
-    const T g0 = B[mb], g1 = B[N + mb], g2 = B[2 * N + mb], g3 = B[3 * N + mb], g4 = B[4 * N + mb],
-            g5 = B[5 * N + mb], g6 = B[6 * N + mb], g7 = B[7 * N + mb], g8 = B[8 * N + mb];
+    T fv[9], gv[9];
+    const int tm = cmp ? L.tag[mb] : 0;
+    if (tn) {
+      const T lam = smat[tn][0], mu = smat[tn][1];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) fv[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
+    } else {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) fv[t] = B[t * N + n];
+    }
+    if (tm) {
+      const T lam = smat[tm][0], mu = smat[tm][1];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) gv[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
+    } else {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) gv[t] = B[t * N + mb];
+    }
+    const T f0 = fv[0], f1 = fv[1], f2 = fv[2], f3 = fv[3], f4 = fv[4], f5 = fv[5], f6 = fv[6], f7 = fv[7], f8 = fv[8];
+    const T g0 = gv[0], g1 = gv[1], g2 = gv[2], g3 = gv[3], g4 = gv[4], g5 = gv[5], g6 = gv[6], g7 = gv[7], g8 = gv[8];
     if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
     if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
     a0 += f0 * uf0 + f1 * uf1 + f2 * uf2 + g0 * ub0 + g3 * ub1 + g6 * ub2;
@@ -727,6 +804,16 @@ template int launch_galerkin_direct<MAT_ISO_SRI>(const double*, int, int, double
                                                  int, int, cudaStream_t);
 template int launch_galerkin_direct<MAT_ISO_FULL>(const double*, int, int, double, double, double, double*, double*, int,
                                                   int, int, cudaStream_t);
+
+void launch_sym_pattern(const double* basis, double* pat, cudaStream_t s) {
+  k_sym_pattern<<<1, 256, 0, s>>>(basis, pat); note_launch();
+}
+void launch_sym_tags(const double* S64, int cnx, int cny, int cnz, const uint16_t* cellpair, int fnxn, int mp,
+                     const double* mtab, const double* pat, uint8_t* tag, cudaStream_t s) {
+  const int64_t n = (int64_t)cnx * cny * cnz;
+  k_sym_tags<<<div_up(n, kThreads), kThreads, 0, s>>>(S64, cnx, cny, cnz, cellpair, fnxn, mp, mtab, pat, tag);
+  note_launch();
+}
 
 void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,
                              const int* pen_node, const double* pen_k, double* A1, int cnx, int cny, int cnz,

@@ -57,6 +57,12 @@ struct SymView {
   const int* t_dof;
   const T* t_val;
   const T* t_lam;
+  // compressed stencil: tag[n] > 0 marks a node whose stored half stencil is lam pat[0] + mu pat[1] with
+  // (lam, mu) = tmat[2 tag], tmat[2 tag + 1] (all cells around it of one material); such blocks are formed
+  // on the fly instead of read.  tag == nullptr: every block is read.
+  const uint8_t* tag = nullptr;
+  const T* tmat = nullptr;  // [128][2]
+  const T* pat = nullptr;   // [2][126]
 };
 
 // Fused level kernels: EPI_APPLY y = A u; EPI_RESID r = b - A u; EPI_CHEB Chebyshev step with ping-pong
@@ -103,6 +109,15 @@ void launch_galerkin_cells(const FineView<double>& F, const double* mat_all, con
 template <int MODE>
 int launch_galerkin_direct(const double* mat_all, int fnx, int fny, double a, double b, double c, double* basis,
                            double* A1, int cnx, int cny, int cnz, cudaStream_t s);
+
+// Interior half-stencil patterns of the uniform level-1 node from the Galerkin basis of
+// launch_galerkin_direct: pat[m][126] (m = 0 lam, 1 mu), same layout as the half storage.
+void launch_sym_pattern(const double* basis, double* pat, cudaStream_t s);
+// Tags of the compressed level-1 stencil: node J gets the material id of fine cell (2 jx, 2 jy, 2 jz) (read
+// from the paired kernel's cell-pair words) when its stored FP64 half stencil S64 equals lam pat[0] + mu pat[1]
+// to 1e-12 (relative), else 0.
+void launch_sym_tags(const double* S64, int cnx, int cny, int cnz, const uint16_t* cellpair, int fnxn, int mp,
+                     const double* mtab, const double* pat, uint8_t* tag, cudaStream_t s);
 
 // Fold diagonal penalties / local extra entries of level 0 into the level-1 stencil.
 void launch_galerkin_penalty(const TransferDev& P, int fnx, int fny, int64_t fnnode, const int* orig_copy, int npen,

@@ -565,6 +565,9 @@ struct Level {
   float *t_val32 = nullptr, *t_lam32 = nullptr, *tn_coef32 = nullptr;
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
+  uint8_t* tag = nullptr;                 // compressed stencil (level 1): material tag per node, 0 = stored
+  double *pat64 = nullptr, *tmat64 = nullptr;
+  float *pat32 = nullptr, *tmat32 = nullptr;
   AxisHost ax[3];                         // transfer to the next level
   TransferDev P{};
   double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr, *t64 = nullptr, *e64 = nullptr;
@@ -820,6 +823,11 @@ struct FebHandle {
     S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
     S.t_ptr = V.t_ptr; S.t_dof = V.t_dof; S.t_val = tval<T>(V); S.t_lam = tlam<T>(V);
     S.Dinv = dinv<T>(V);
+    if (V.tag) {
+      S.tag = V.tag;
+      if constexpr (std::is_same<T, double>::value) { S.pat = V.pat64; S.tmat = V.tmat64; }
+      else { S.pat = V.pat32; S.tmat = V.tmat32; }
+    }
     return S;
   }
   template <typename T> static const T* symS(const Level& V);
@@ -1807,6 +1815,12 @@ int build_hierarchy(FebHandle* h) {
           FEB_TRY(launch_galerkin_direct<MAT_ISO_SRI>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
         else
           FEB_TRY(launch_galerkin_direct<MAT_ISO_FULL>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+        // interior patterns of the compressed level-1 stencil (tags follow once the half stencil exists)
+        const char* cenv = std::getenv("FEB_SYM_COMPRESS");
+        if (H.pair_ok && !(cenv && cenv[0] == '0')) {
+          FEB_TRY(H.pool.alloc(&C.pat64, 252));
+          launch_sym_pattern(basis, C.pat64, H.s);
+        }
         FEB_CUDA(cudaGetLastError());
         H.pool.free(basis);
       } else {
@@ -1844,6 +1858,18 @@ int build_hierarchy(FebHandle* h) {
     g_prof.mark("Lk sparse project + upload", H.s);
     FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)C.ntotal));
     launch_stencil_to_sym<double>(C.A64, C.ntotal, C.S64, H.s);
+    if (C.pat64) {   // compressed level-1 stencil: tags of the uniform nodes, patterns and material table in T
+      FEB_TRY(H.pool.alloc(&C.tag, C.ntotal));
+      launch_sym_tags(C.S64, C.nx, C.ny, C.nz, H.P32.cellpair, H.nx + 1, H.P32.mp, H.P32.mtab, C.pat64, C.tag, H.s);
+      C.tmat64 = const_cast<double*>(H.P32.mtab);
+      if (f32) {
+        FEB_TRY(H.pool.alloc(&C.pat32, 252));
+        FEB_TRY(H.pool.alloc(&C.tmat32, 2 * kMaxMatIds));
+        launch_convert<double, float>(C.pat64, C.pat32, 252, nullptr, H.s);
+        launch_convert<double, float>(C.tmat64, C.tmat32, 2 * kMaxMatIds, nullptr, H.s);
+      }
+      FEB_CUDA(cudaGetLastError());
+    }
     if (f32) {
       FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)C.ntotal));
       launch_stencil_to_sym<float>(C.A64, C.ntotal, C.S32, H.s);

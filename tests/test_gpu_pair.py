@@ -127,3 +127,21 @@ def test_direct_galerkin_matches_cell_matrices(monkeypatch, precision):
     assert rel(res["1"][0][ok], res["0"][0][ok]) < 1e-9
     assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= 1
     assert res["1"][1]["lmax"] == pytest.approx(res["0"][1]["lmax"], rel=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_compressed_level1_stencil_matches_stored(monkeypatch, precision):
+    """Level-1 blocks formed on the fly at nodes inside one material (FEB_SYM_COMPRESS=1, the default) and read
+    from the stored stencil everywhere (FEB_SYM_COMPRESS=0): the same solve within 1e-9, iterations within 1."""
+    P = synth.hindfoot_problem(48, 34, 28, h=80.0 / 48, seed=7)
+    g = P["grid"]
+    args = (P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"], P["extra"], P["node_groups"])
+    res = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("FEB_SYM_COMPRESS", flag)
+        U, info, R = engine.solve_cn(g, *args, tol=1e-10, precision=precision)
+        assert info["flag"] == 0 and info["relres"] < 1e-10
+        res[flag] = (U, info)
+    ok = ~np.isnan(res["0"][0])
+    assert rel(res["1"][0][ok], res["0"][0][ok]) < 1e-9
+    assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= 1
