@@ -132,7 +132,9 @@ def test_direct_galerkin_matches_cell_matrices(monkeypatch, precision):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_compressed_level1_stencil_matches_stored(monkeypatch, precision):
     """Level-1 blocks formed on the fly at nodes inside one material (FEB_SYM_COMPRESS=1, the default) and read
-    from the stored stencil everywhere (FEB_SYM_COMPRESS=0): the same solve within 1e-9, iterations within 1."""
+    from the stored stencil everywhere (FEB_SYM_COMPRESS=0): the same solve within 1e-9; iterations within 1 in
+    FP64, within 3 with the FP32 V-cycle (whose blocks differ from the rounded stored ones in the last bit, and
+    whose iteration count moves by a few with such rounding)."""
     P = synth.hindfoot_problem(48, 34, 28, h=80.0 / 48, seed=7)
     g = P["grid"]
     args = (P["lam"], P["mu"], P["active"], P["cn"], P["orig"], P["fixed"], P["loads"], P["extra"], P["node_groups"])
@@ -144,4 +146,4 @@ def test_compressed_level1_stencil_matches_stored(monkeypatch, precision):
         res[flag] = (U, info)
     ok = ~np.isnan(res["0"][0])
     assert rel(res["1"][0][ok], res["0"][0][ok]) < 1e-9
-    assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= 1
+    assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= (1 if precision == "fp64" else 3)
