@@ -49,37 +49,34 @@ __global__ void k_symmetrize(double* __restrict__ M, int nd) {
   M[j * nd + i] = v;
 }
 
-// Invert the pivot block in shared memory (scalar Gauss-Jordan, SPD so no pivoting).
-__global__ void k_gj_pivot(double* __restrict__ M, int nd, int k0, int bs, double* __restrict__ Dinv,
-                           int* __restrict__ status) {
+// Invert the pivot block in shared memory (scalar Gauss-Jordan, SPD so no pivoting), one thread per element:
+// each sweep step p reads a_ip, a_pj, a_pp, then every thread rewrites its own element
+// (a_ij -= a_ip a_pj / a_pp; a_pj /= a_pp; a_ip = -a_ip / a_pp; a_pp = 1 / a_pp).
+__global__ void __launch_bounds__(GJ_B * GJ_B)
+k_gj_pivot(double* __restrict__ M, int nd, int k0, int bs, double* __restrict__ Dinv, int* __restrict__ status) {
   __shared__ double a[GJ_B][GJ_B + 1];
-  const int t = threadIdx.x;
-  for (int e = t; e < bs * bs; e += blockDim.x) a[e / bs][e % bs] = M[(size_t)(k0 + e / bs) * nd + k0 + e % bs];
+  const int i = threadIdx.y, j = threadIdx.x;
+  const bool in = i < bs && j < bs;
+  if (in) a[i][j] = M[(size_t)(k0 + i) * nd + k0 + j];
   __syncthreads();
   for (int p = 0; p < bs; ++p) {
     double piv = a[p][p];
+    const double aip = in ? a[i][p] : 0.0, apj = in ? a[p][j] : 0.0, aij = in ? a[i][j] : 0.0;
     __syncthreads();
     if (!(piv > 0.0) || !isfinite(piv)) {
-      if (t == 0) atomicExch(status, FEB_ERR_COARSE);
+      if (i == 0 && j == 0) atomicExch(status, FEB_ERR_COARSE);
       piv = 1.0;
     }
-    double ip = 1.0 / piv;
-    // sweep on p: a_pp <- 1/a_pp; a_pj <- a_pj / a_pp; a_ij <- a_ij - a_ip a_pj / a_pp; a_ip <- -a_ip / a_pp
-    for (int e = t; e < bs * bs; e += blockDim.x) {
-      int i = e / bs, j = e % bs;
-      if (i != p && j != p) a[i][j] -= a[i][p] * a[p][j] * ip;
+    const double ip = 1.0 / piv;
+    if (in) {
+      if (i != p && j != p) a[i][j] = aij - aip * apj * ip;
+      else if (i == p && j != p) a[p][j] = apj * ip;
+      else if (j == p && i != p) a[i][p] = -aip * ip;
+      else a[p][p] = ip;
     }
-    __syncthreads();
-    for (int e = t; e < bs; e += blockDim.x) {
-      if (e != p) {
-        a[p][e] *= ip;
-        a[e][p] *= -ip;
-      }
-    }
-    if (t == 0) a[p][p] = ip;
     __syncthreads();
   }
-  for (int e = t; e < bs * bs; e += blockDim.x) Dinv[e] = a[e / bs][e % bs];
+  if (in) Dinv[i * bs + j] = a[i][j];
 }
 
 // Trow[r][j] = sum_q Dinv[r][q] M[k0+q][j] for all j (pivot-block rows of the sweep)
@@ -230,7 +227,7 @@ void launch_dense_invert(double* M, int nd, double* scratch, int* status, cudaSt
   double* Tcol = Trow + (size_t)GJ_B * nd;
   for (int k0 = 0; k0 < nd; k0 += GJ_B) {
     int bs = std::min(GJ_B, nd - k0);
-    k_gj_pivot<<<1, 256, 0, s>>>(M, nd, k0, bs, Dinv, status); note_launch();
+    k_gj_pivot<<<1, dim3(GJ_B, GJ_B), 0, s>>>(M, nd, k0, bs, Dinv, status); note_launch();
     dim3 g1(div_up(nd, 128), bs);
     k_gj_row<<<g1, 128, 0, s>>>(M, nd, k0, bs, Dinv, Trow); note_launch();
     k_gj_colcopy<<<g1, 128, 0, s>>>(M, nd, k0, bs, Tcol); note_launch();

@@ -1183,17 +1183,21 @@ int upload_transfer(Pool& pool, Level& V) {
 }
 
 // 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients
+// The iteration runs in the precision of the V-cycle that uses the estimate (FP32 for the mixed and refined
+// precisions, as the reference GPU path runs it in its multigrid dtype, rb/gpusolve.py:84-97).
+template <typename T>
 int power_iteration(FebHandle* h, int l) {
   Level& V = h->L[l];
   const int64_t n = 3 * V.ntotal;
-  launch_random_start(V.x64, V.used, V.ntotal, h->opt.seed + 7919ull * (uint64_t)l, h->s);
-  launch_dot_partial<double, double>(V.x64, V.x64, n, h->partials, nullptr, h->s);
+  T *x = FebHandle::vx<T>(V), *t = FebHandle::vt<T>(V), *d = FebHandle::vd<T>(V);
+  launch_random_start<T>(x, V.used, V.ntotal, h->opt.seed + 7919ull * (uint64_t)l, h->s);
+  launch_dot_partial<T, T>(x, x, n, h->partials, nullptr, h->s);
   launch_finalize(FIN_POWER0, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
   for (int it = 0; it < 12; ++it) {
-    h->apply<double>(l, V.x64, V.t64, nullptr);
-    launch_bj_apply_norm(V.Dinv64, V.t64, V.d64, V.ntotal, h->partials, h->s);
+    h->apply<T>(l, x, t, nullptr);
+    launch_bj_apply_norm<T>(FebHandle::dinv<T>(V), t, d, V.ntotal, h->partials, h->s);
     launch_finalize(FIN_POWER, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
-    launch_scale(V.d64, V.x64, h->lp + l, n, h->s);
+    launch_scale<T>(d, x, h->lp + l, n, h->s);
   }
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
@@ -1917,7 +1921,7 @@ int build_hierarchy(FebHandle* h) {
     FEB_TRY(level_vectors<double>(H.pool, V, true, f32));
   }
   g_prof.mark("level work vectors", H.s);
-  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(power_iteration(h, k));
+  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(f32 ? power_iteration<float>(h, k) : power_iteration<double>(h, k));
   H.stage_mark();   // 6: work vectors, power iterations
   g_prof.mark("power iterations", H.s);
   FEB_TRY(build_dense(h));

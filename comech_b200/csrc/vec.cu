@@ -213,33 +213,35 @@ __device__ __forceinline__ uint64_t splitmix(uint64_t z) {
 }
 
 // standard normal start vector of the power iteration (Box-Muller on a counter-based hash), 0 where masked out
-__global__ void k_random_start(double* __restrict__ x, const uint8_t* __restrict__ mask, int64_t nn, uint64_t seed) {
+template <typename T>
+__global__ void k_random_start(T* __restrict__ x, const uint8_t* __restrict__ mask, int64_t nn, uint64_t seed) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= 3 * nn) return;
   uint64_t h = splitmix(seed ^ splitmix((uint64_t)i));
   double u1 = ((h >> 11) + 1.0) * (1.0 / 9007199254740993.0);
   double u2 = (splitmix(h) >> 11) * (1.0 / 9007199254740992.0);
   double g = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-  x[i] = (mask == nullptr || mask[i / 3]) ? g : 0.0;
+  x[i] = (mask == nullptr || mask[i / 3]) ? T(g) : T(0);
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_bj_apply_norm(const double* __restrict__ D, const double* __restrict__ v, double* __restrict__ y, int64_t nn,
+k_bj_apply_norm(const T* __restrict__ D, const T* __restrict__ v, T* __restrict__ y, int64_t nn,
                 double* __restrict__ partials) {
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < nn; i += (int64_t)gridDim.x * kThreads) {
-    double z0, z1, z2;
+    T z0, z1, z2;
     bj(D, nn, i, v[3 * i], v[3 * i + 1], v[3 * i + 2], z0, z1, z2);
     y[3 * i] = z0; y[3 * i + 1] = z1; y[3 * i + 2] = z2;
-    s += z0 * z0 + z1 * z1 + z2 * z2;
+    s += double(z0) * double(z0) + double(z1) * double(z1) + double(z2) * double(z2);
   }
   s = block_sum(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-__global__ void k_scale(const double* __restrict__ y, double* __restrict__ x, const LevelParams* __restrict__ lp,
-                        int64_t n) {
-  const double inv = lp->inv;
+template <typename T>
+__global__ void k_scale(const T* __restrict__ y, T* __restrict__ x, const LevelParams* __restrict__ lp, int64_t n) {
+  const T inv = T(lp->inv);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] = y[i] * inv;
 }
@@ -342,18 +344,26 @@ void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, 
   k_residual<T><<<grid_for(n), kThreads, 0, s>>>(b, Ax, r, n, skip); note_launch();
 }
 
-void launch_random_start(double* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s) {
-  k_random_start<<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(x, mask, nn, seed); note_launch();
+template <typename T>
+void launch_random_start(T* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s) {
+  k_random_start<T><<<div_up(3 * nn, kThreads), kThreads, 0, s>>>(x, mask, nn, seed); note_launch();
 }
 
-void launch_bj_apply_norm(const double* Dinv, const double* v, double* y, int64_t nn, double* partials,
-                          cudaStream_t s) {
-  k_bj_apply_norm<<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials); note_launch();
+template <typename T>
+void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s) {
+  k_bj_apply_norm<T><<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials); note_launch();
 }
 
-void launch_scale(const double* y, double* x, const LevelParams* lp, int64_t n, cudaStream_t s) {
-  k_scale<<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n); note_launch();
+template <typename T>
+void launch_scale(const T* y, T* x, const LevelParams* lp, int64_t n, cudaStream_t s) {
+  k_scale<T><<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n); note_launch();
 }
+template void launch_random_start<float>(float*, const uint8_t*, int64_t, uint64_t, cudaStream_t);
+template void launch_random_start<double>(double*, const uint8_t*, int64_t, uint64_t, cudaStream_t);
+template void launch_bj_apply_norm<float>(const float*, const float*, float*, int64_t, double*, cudaStream_t);
+template void launch_bj_apply_norm<double>(const double*, const double*, double*, int64_t, double*, cudaStream_t);
+template void launch_scale<float>(const float*, float*, const LevelParams*, int64_t, cudaStream_t);
+template void launch_scale<double>(const double*, double*, const LevelParams*, int64_t, cudaStream_t);
 
 template <typename Ts, typename Td>
 void launch_convert(const Ts* src, Td* dst, int64_t n, const int* skip, cudaStream_t s) {

@@ -57,10 +57,12 @@ template <typename T>
 void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s);
 
 // power iteration
-void launch_random_start(double* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s);
-void launch_bj_apply_norm(const double* Dinv, const double* v, double* y, int64_t nn, double* partials,
-                          cudaStream_t s);
-void launch_scale(const double* y, double* x, const LevelParams* lp, int64_t n, cudaStream_t s);
+template <typename T>
+void launch_random_start(T* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s);
+template <typename T>
+void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s);
+template <typename T>
+void launch_scale(const T* y, T* x, const LevelParams* lp, int64_t n, cudaStream_t s);
 
 // conversions and small helpers
 template <typename Ts, typename Td>
