@@ -564,6 +564,18 @@ __global__ void k_stencil_to_sym(const double* __restrict__ A, int64_t n, T* __r
 // its slots' loads in flight together.  Partial sums meet in shared memory; warps 0..2 then each finish
 // one component of the 32 nodes.  Entries the stencil cannot hold (per-node CSR) are summed by the warps
 // cooperatively: warp w takes the nodes of its 32 with entries whose lane is w mod 4.
+// lam_t v_t.u of every rank-1 term, one warp per term (lanes over its entries)
+template <typename T>
+__global__ void k_term_dots(SymView<T> L, int nterms, const T* __restrict__ u, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int t = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (t >= nterms) return;
+  T d = 0;
+  for (int e = L.t_ptr[t] + lane; e < L.t_ptr[t + 1]; e += 32) d += L.t_val[e] * u[L.t_dof[e]];
+  d = warp_sum(d);
+  if (lane == 0) L.tdot[t] = L.t_lam[t] * d;
+}
+
 template <typename T, int EPI>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
@@ -648,26 +660,14 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       if (lane == src) { a0 += s0; a1 += s1; a2 += s2; }
     }
   }
-  if (L.tn_ptr) {      // rank-1 terms: for each (node, term) pair of the 32 nodes, the whole warp forms the
-                       // term's dot v_t.u (lanes over its entries); the 4 warps take every 4th pair of a node
-    int pb = 0, pe = 0;
-    if (valid) { pb = L.tn_ptr[n]; pe = L.tn_ptr[n + 1]; }
-    unsigned todo = __ballot_sync(0xffffffffu, pe > pb);
-    while (todo) {
-      const int src = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int b0 = __shfl_sync(0xffffffffu, pb, src), b1 = __shfl_sync(0xffffffffu, pe, src);
-      for (int p = b0 + w; p < b1; p += 4) {
-        const int t = L.tn_term[p], eb = L.t_ptr[t], ee = L.t_ptr[t + 1];
-        T d = 0;
-        for (int e = eb + lane; e < ee; e += 32) d += L.t_val[e] * u[L.t_dof[e]];
-        const T dot = L.t_lam[t] * warp_sum(d);
-        if (lane == src) {
-          a0 += dot * L.tn_coef[3 * p];
-          a1 += dot * L.tn_coef[3 * p + 1];
-          a2 += dot * L.tn_coef[3 * p + 2];
-        }
-      }
+  if (L.tn_ptr && valid) {   // rank-1 terms: the term's dot lam_t v_t.u comes from k_term_dots; the node's
+                             // pairs are split over the 4 warps
+    const int pe = L.tn_ptr[n + 1];
+    for (int p = L.tn_ptr[n] + w; p < pe; p += 4) {
+      const T dot = L.tdot[L.tn_term[p]];
+      a0 += dot * L.tn_coef[3 * p];
+      a1 += dot * L.tn_coef[3 * p + 1];
+      a2 += dot * L.tn_coef[3 * p + 2];
     }
   }
   red[w][0][lane] = a0; red[w][1][lane] = a1; red[w][2][lane] = a2;
@@ -709,6 +709,9 @@ template <typename T>
 void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
                 const LevelParams* lp, int k, const int* skip, cudaStream_t s) {
   const dim3 g(div_up(L.nx, 32), L.ny, L.nz), blk(32, 4);
+  if (L.tn_ptr && L.nterms > 0) {
+    k_term_dots<T><<<div_up(L.nterms, 8), 256, 0, s>>>(L, L.nterms, u, skip); note_launch();
+  }
   if (epi == EPI_APPLY) {
     k_sym<T, EPI_APPLY><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
   } else if (epi == EPI_RESID) {

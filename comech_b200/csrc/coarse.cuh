@@ -57,6 +57,8 @@ struct SymView {
   const int* t_dof;
   const T* t_val;
   const T* t_lam;
+  int nterms = 0;
+  T* tdot = nullptr;        // per term lam_t v_t.u of the current product (formed by k_term_dots before k_sym)
   // compressed stencil: tag[n] > 0 marks a node whose stored half stencil is lam pat[0] + mu pat[1] with
   // (lam, mu) = tmat[2 tag], tmat[2 tag + 1] (all cells around it of one material); such blocks are formed
   // on the fly instead of read.  tag == nullptr: every block is read.

@@ -565,6 +565,8 @@ struct Level {
   float *t_val32 = nullptr, *t_lam32 = nullptr, *tn_coef32 = nullptr;
   double* Dinv64 = nullptr;
   float* Dinv32 = nullptr;
+  double* tdot64 = nullptr;               // per-term dots of the current product (rank-1 terms)
+  float* tdot32 = nullptr;
   uint8_t* tag = nullptr;                 // compressed stencil (level 1): material tag per node, 0 = stored
   double *pat64 = nullptr, *tmat64 = nullptr;
   float *pat32 = nullptr, *tmat32 = nullptr;
@@ -635,6 +637,8 @@ int upload_terms(Pool& pool, const Terms& T, int64_t nnode, Level& V) {
   FEB_TRY(pool.upload(&V.tn_term, term.data(), term.size()));
   FEB_TRY(pool.upload(&V.tn_coef64, coef.data(), coef.size()));
   FEB_TRY(pool.upload(&V.tn_coef32, coef32.data(), coef32.size()));
+  FEB_TRY(pool.alloc(&V.tdot64, T.size()));
+  FEB_TRY(pool.alloc(&V.tdot32, T.size()));
   return FEB_OK;
 }
 
@@ -822,6 +826,8 @@ struct FebHandle {
     S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
     S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
     S.t_ptr = V.t_ptr; S.t_dof = V.t_dof; S.t_val = tval<T>(V); S.t_lam = tlam<T>(V);
+    S.nterms = V.nterms;
+    if constexpr (std::is_same<T, double>::value) S.tdot = V.tdot64; else S.tdot = V.tdot32;
     S.Dinv = dinv<T>(V);
     if (V.tag) {
       S.tag = V.tag;
@@ -1820,8 +1826,8 @@ int build_hierarchy(FebHandle* h) {
         else
           FEB_TRY(launch_galerkin_direct<MAT_ISO_FULL>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
         // interior patterns of the compressed level-1 stencil (tags follow once the half stencil exists)
-        const char* cenv = std::getenv("FEB_SYM_COMPRESS");
-        if (H.pair_ok && !(cenv && cenv[0] == '0')) {
+        const char* cenv = std::getenv("FEB_SYM_COMPRESS");   // opt-in: measured slower on the hindfoot
+        if (H.pair_ok && cenv && cenv[0] == '1') {
           FEB_TRY(H.pool.alloc(&C.pat64, 252));
           launch_sym_pattern(basis, C.pat64, H.s);
         }

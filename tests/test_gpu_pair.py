@@ -131,8 +131,8 @@ def test_direct_galerkin_matches_cell_matrices(monkeypatch, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_compressed_level1_stencil_matches_stored(monkeypatch, precision):
-    """Level-1 blocks formed on the fly at nodes inside one material (FEB_SYM_COMPRESS=1, the default) and read
-    from the stored stencil everywhere (FEB_SYM_COMPRESS=0): the same solve within 1e-9; iterations within 1 in
+    """Level-1 blocks formed on the fly at nodes inside one material (FEB_SYM_COMPRESS=1) and read from the
+    stored stencil everywhere (FEB_SYM_COMPRESS=0, the default): the same solve within 1e-9; iterations within 1 in
     FP64, within 3 with the FP32 V-cycle (whose blocks differ from the rounded stored ones in the last bit, and
     whose iteration count moves by a few with such rounding)."""
     P = synth.hindfoot_problem(48, 34, 28, h=80.0 / 48, seed=7)
