@@ -90,8 +90,9 @@ def test_pair_operator_matches_reference_assembly(golden, monkeypatch):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "refine"])
 def test_fused_vcycle_matches_unfused(monkeypatch, precision):
-    """The same split-node solve with the fused level-0 smoother and with the unfused kernels: same
-    iteration count within 2 and solutions within 1e-8 of each other (each within its own 1e-10 residual)."""
+    """The same split-node solve with the fused level-0 smoother and with the unfused kernels: iteration counts
+    within 2 in FP64 (within 5 % with FP32 V-cycles) and solutions within 1e-8 of each other (each within its own
+    1e-10 residual)."""
     monkeypatch.setenv("FEB_KU_TC", "0")
     P = synth.hindfoot_problem(40, 28, 24, h=2.0, seed=5)
     g = P["grid"]
@@ -106,7 +107,9 @@ def test_fused_vcycle_matches_unfused(monkeypatch, precision):
     ok = ~np.isnan(res["0"][0])
     assert (np.isnan(res["1"][0]) == ~ok).all()
     assert rel(res["1"][0][ok], res["0"][0][ok]) < 1e-8
-    assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= 2
+    # FP32 V-cycles: the count moves by a few with summation order (refinement sums several sweeps)
+    bar = 2 if precision == "fp64" else max(3, int(0.05 * res["0"][1]["iters"]))
+    assert abs(res["1"][1]["iters"] - res["0"][1]["iters"]) <= bar
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
