@@ -514,7 +514,9 @@ def run_profile(args):
                 "warm_start": warm is not None, "x0_used": int(info.x0_used), "iters": int(info.iters),
                 "sweeps": int(info.sweeps), "relres": info.relres, "t_setup_ms": round(info.t_setup_ms, 2),
                 "t_solve_ms": round(info.t_solve_ms, 2), "ndof": int(info.ndof), "ku_shape": list(info.ku_shape),
-                "t_stage_ms": [round(float(v), 2) for v in info.t_stage_ms]}
+                "t_stage_ms": [round(float(v), 2) for v in info.t_stage_ms],
+                "lmax": [round(float(v), 6) for v in info.lmax[:max(int(info.levels) - 1, 0)]],
+                "level_dofs": [int(v) for v in info.level_dofs[:int(info.levels)]]}
     pr = engine.Problem(P["grid"], _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], options=dict(max_levels=0))
     if args.mode == "ku-rot":
@@ -554,33 +556,40 @@ def batch_instance(seed):
 
 
 def run_batch(args):
-    """64 independent instances of uneven size and seeded action, solved on one GPU one at a time and with 8 / 16
-    solves in flight (comech_b200.batch).  Times are wall-clock around the whole batch through the public API
-    (host inputs, uploads, solves, downloads), after one warm-up pass."""
+    """64 independent instances of uneven size and seeded action on one GPU: the host thread pool (1, 8 and 16
+    whole solve_cn calls in flight) against the batched launch (comech_b200.batch mode "graph": set-up on 16
+    threads, then ONE feb_solve_batch graph launch for all instances, then the downloads).  Times are
+    wall-clock around the whole batch through the public API (host inputs, uploads, set-up, solves, downloads),
+    after one warm-up pass."""
     import multiprocessing as mp
     n = args.batch_n
     with mp.get_context("spawn").Pool(max(1, min(16, (os.cpu_count() or 2) - 1))) as pool:
         items = pool.map(batch_instance, range(n))
     import torch
     from comech_b200 import batch
-    batch.solve_batch(items[:4], precision=args.precision, tol=TOL, concurrency=4)      # warm-up
+    batch.solve_batch(items[:4], precision=args.precision, tol=TOL, concurrency=4, mode="threads")   # warm-up
+    batch.solve_batch(items[:4], precision=args.precision, tol=TOL, concurrency=4, mode="graph")
     out = {"mode": "batch", "instances": n, "precision": args.precision, "tol": TOL,
            "dims": sorted({(P["grid"].nx, P["grid"].ny, P["grid"].nz) for P in items})[:: max(1, n // 8)],
            "actions": list(BATCH_ACTIONS)}
     runs = {}
-    for conc in (1, 8, 16):
+    for name, mode, conc in (("threads_1", "threads", 1), ("threads_8", "threads", 8), ("threads_16", "threads", 16),
+                             ("graph", "graph", 16)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = batch.solve_batch(items, precision=args.precision, tol=TOL, concurrency=conc)
+        res = batch.solve_batch(items, precision=args.precision, tol=TOL, concurrency=conc, mode=mode)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        runs[conc] = dict(seconds=round(dt, 3), solves_per_s=round(n / dt, 2),
+        runs[name] = dict(seconds=round(dt, 3), solves_per_s=round(n / dt, 2),
                           iters_median=float(np.median([r[1]["iters"] for r in res])),
                           relres_max=float(max(r[1]["relres"] for r in res)),
                           flags=sorted({int(r[1]["flag"]) for r in res}))
+        if mode == "graph":
+            runs[name]["phases_s"] = res[0][1]["batch"]
     out["ndof_total"] = int(sum(r[1]["ndof"] for r in res))
-    out["runs"] = {str(k): v for k, v in runs.items()}
-    out["speedup_16_vs_1"] = round(runs[1]["seconds"] / runs[16]["seconds"], 2)
+    out["runs"] = runs
+    out["speedup_threads16_vs_1"] = round(runs["threads_1"]["seconds"] / runs["threads_16"]["seconds"], 2)
+    out["speedup_graph_vs_threads16"] = round(runs["threads_16"]["seconds"] / runs["graph"]["seconds"], 2)
     return out
 
 

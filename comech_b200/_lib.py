@@ -15,7 +15,7 @@ ERRORS = {-1: "FEB_ERR_ARG", -2: "FEB_ERR_CUDA", -3: "FEB_ERR_BREAKDOWN", -4: "F
 MAT_ISO_SRI, MAT_ISO_FULL, MAT_ORTHO = 0, 1, 2
 PREC = {"fp64": 0, "mixed": 1, "refine": 2}
 
-EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_solve", "feb_apply",
+EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_solve", "feb_solve_batch", "feb_apply", "feb_precondition",
            "feb_export_solution", "feb_used_nodes", "feb_destroy", "feb_accumulate_nodal", "feb_cell_stress",
            "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_benchmark_apply_set", "feb_launch_count", "feb_last_error",
            "feb_region_forces", "feb_rigid_fit", "feb_relative_displacement", "feb_sample_cells",
@@ -98,6 +98,8 @@ def load():
     lib.feb_set_rigid_groups.argtypes = [P, C.c_int32, P, P]
     lib.feb_solve.argtypes = [P, P, P, P, C.POINTER(FebInfo)]
     lib.feb_apply.argtypes = [P, C.c_int32, P, P]
+    lib.feb_precondition.argtypes = [P, P, P]
+    lib.feb_solve_batch.argtypes = [P, C.c_int32, P, P, P, P]
     lib.feb_export_solution.argtypes = [P, P, P]
     lib.feb_used_nodes.argtypes = [P, C.POINTER(C.c_int64), P]
     lib.feb_destroy.argtypes = [P]

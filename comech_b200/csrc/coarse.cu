@@ -89,6 +89,60 @@ __global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __rest
   rc[3 * J] = s0; rc[3 * J + 1] = s1; rc[3 * J + 2] = s2;
 }
 
+// r_c = P^T r_f for even coarsening: coarse node J gathers fine nodes 2 J + a, a in {-1, 0, 1} per axis, with
+// weight 1 (a = 0) or 1/2 (a = +-1)
+template <typename T>
+__global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, const T* __restrict__ rf,
+                                T* __restrict__ rc, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int jx = blockIdx.x * blockDim.x + threadIdx.x, jy = blockIdx.y, jz = blockIdx.z;
+  if (jx >= cnx) return;
+  T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+  for (int c = -1; c <= 1; ++c) {
+    const int fk = 2 * jz + c;
+    if (fk < 0 || fk >= fnz) continue;
+#pragma unroll
+    for (int b = -1; b <= 1; ++b) {
+      const int fj = 2 * jy + b;
+      if (fj < 0 || fj >= fny) continue;
+#pragma unroll
+      for (int a = -1; a <= 1; ++a) {
+        const int fi = 2 * jx + a;
+        if (fi < 0 || fi >= fnx) continue;
+        const T w = T((a ? 0.5 : 1.0) * (b ? 0.5 : 1.0) * (c ? 0.5 : 1.0));
+        const int64_t f = fi + (int64_t)fnx * (fj + (int64_t)fny * fk);
+        s0 += w * rf[3 * f]; s1 += w * rf[3 * f + 1]; s2 += w * rf[3 * f + 2];
+      }
+    }
+  }
+  const int64_t J = jx + (int64_t)cnx * (jy + (int64_t)cny * jz);
+  rc[3 * J] = s0; rc[3 * J + 1] = s1; rc[3 * J + 2] = s2;
+}
+
+// x_f += P x_c on used fine nodes for even coarsening: per axis an even fine node takes its coarse node, an odd
+// one the mean of its two neighbours
+template <typename T>
+__global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, const uint8_t* __restrict__ used,
+                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
+  if (pi >= fnx) return;
+  const int64_t n = pi + (int64_t)fnx * (pj + (int64_t)fny * pk);
+  if (!used[n]) return;
+  const int ni = (pi & 1) + 1, nj = (pj & 1) + 1, nk = (pk & 1) + 1;
+  const T wi = T(ni == 2 ? 0.5 : 1.0), wj = T(nj == 2 ? 0.5 : 1.0), wk = T(nk == 2 ? 0.5 : 1.0);
+  T s0 = 0, s1 = 0, s2 = 0;
+  for (int c = 0; c < nk; ++c)
+    for (int b = 0; b < nj; ++b)
+      for (int a = 0; a < ni; ++a) {
+        const int64_t K = (pi >> 1) + a + (int64_t)cnx * ((pj >> 1) + b + (int64_t)cny * ((pk >> 1) + c));
+        const T w = wi * wj * wk;
+        s0 += w * xc[3 * K]; s1 += w * xc[3 * K + 1]; s2 += w * xc[3 * K + 2];
+      }
+  xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+}
+
 template <typename T>
 __global__ void k_restrict_copies(TransferDev P, int fnx, int fny, int64_t fnnode, int64_t fntotal,
                                   const int* __restrict__ orig_copy, const T* __restrict__ rf, T* __restrict__ rc,
@@ -756,8 +810,12 @@ void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int*
 template <typename T>
 void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                      const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s) {
-  int64_t nc = (int64_t)P.ax[0].nc * P.ax[1].nc * P.ax[2].nc;
-  k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
+  if (P.even) {
+    k_restrict_even<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(
+        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, rf, rc, skip); note_launch();
+  } else {
+    k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
+  }
   if (fntotal > fnnode)
     k_restrict_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
                                                                                  orig_copy, rf, rc, skip); note_launch();
@@ -768,7 +826,12 @@ template <typename T>
 void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
                         cudaStream_t s) {
-  k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip); note_launch();
+  if (P.even) {
+    k_prolong_even<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P.ax[0].nc, P.ax[1].nc, fnx, fny, used, xc, xf,
+                                                                     skip); note_launch();
+  } else {
+    k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip); note_launch();
+  }
   if (fntotal > fnnode) {
     k_prolong_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
                                                                                orig_copy, xc, xf, skip); note_launch();

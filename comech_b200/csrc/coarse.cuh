@@ -18,6 +18,8 @@ struct AxisDev {
 
 struct TransferDev {
   AxisDev ax[3];
+  int even = 0;   // 1: every axis coarsens 2 n - 1 -> n nodes with weights 1 and 1/2 (uniform spacing, even cell
+                  // counts); the transfers then index directly instead of reading the axis tables
 };
 
 // Structured level (>= 1): nodes nx*ny*nz (x fastest), stencil A[o*9 + 3r + c][n], o = (dx+1) + 3(dy+1) + 9(dz+1)

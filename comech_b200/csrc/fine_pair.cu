@@ -30,6 +30,14 @@ namespace feb {
 namespace {
 
 constexpr int kXOwn = 30;
+#ifndef FEB_PAIR_MINB
+#define FEB_PAIR_MINB 1
+#endif
+#ifndef FEB_PAIR_UNROLL
+#define FEB_PAIR_UNROLL 1
+#endif
+// FP32 marches two planes per trip (no register copies between planes)
+constexpr bool kPairUnroll = FEB_PAIR_UNROLL != 0;
 
 template <typename T>
 using V2 = typename Vec2<T>::type;
@@ -189,7 +197,7 @@ constexpr size_t pair_smem_bytes() {
 }
 
 template <typename T, int MODE, bool CUBE, int WY, bool SMOOTH>
-__global__ void __launch_bounds__(32 * WY, 1)
+__global__ void __launch_bounds__(32 * WY, FEB_PAIR_MINB)
 k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArgs<T> S, const int* __restrict__ skip,
             int zchunk, int nbx, int nby, int nbz) {
   if (skip && *skip) return;
@@ -351,11 +359,13 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
     }
   };
 
-  V vn[3], vp[3], vq[3];
-  V Fk[3][4], topc[3][4], Lw[3][2];
+  // Planes alternate between two register sets (input planes, faces, cell words, epilogue operands), and the
+  // march takes two planes per trip, so no set is ever copied into the other.
+  V va[3], vb[3];
+  V Fa[3][4], Fb[3][4], topc[3][4], Lw[3][2];
   T Uhi[3][2];
-  uint32_t cells_c, cells_n, flags_prev = 0u;
-  NodeOps<T> op0, op1, on0, on1;   // operands of the plane finished this step, and of the next one
+  uint32_t ca, cb = 0u, flags_prev = 0u;
+  NodeOps<T> oa0, oa1, ob0, ob1;
   auto prefetch = [&](int kk, NodeOps<T>& o0, NodeOps<T>& o1) {
     if constexpr (PREF) {
       if (kk >= K0 && kk < K1) {
@@ -367,13 +377,13 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   {   // prologue: face of plane K0-1
     V v0[3], E[3][2];
     load_plane(K0 - 1, v0);
-    load_plane(K0, vn);
-    load_plane(K0 + 1, vp);
-    cells_c = load_cells(K0 - 1);
+    load_plane(K0, va);
+    load_plane(K0 + 1, vb);
+    ca = load_cells(K0 - 1);
     edge(v0, E);
     put_edge(slot(K0 - 1), E);
     __syncthreads();
-    face(slot(K0 - 1), E, Fk);
+    face(slot(K0 - 1), E, Fa);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -382,33 +392,35 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
       Uhi[c][0] = Uhi[c][1] = T(0);
     }
   }
-  prefetch(K0 - 1, op0, op1);
-  for (int k = K0 - 1; k < K1; ++k) {
+  prefetch(K0 - 1, oa0, oa1);
+  // one step of the march at plane k: vin holds plane k+1 (and receives plane k+3), Fin the face of plane k,
+  // Fout receives the face of plane k+1; cin holds the cell word of layer k, cout receives layer k+1; oin
+  // holds the epilogue operands of plane k-1, oout receives those of plane k
+  auto step = [&](int k, V (&vin)[3], V (&Fin)[3][4], V (&Fout)[3][4], uint32_t cin, uint32_t& cout,
+                  NodeOps<T>& oin0, NodeOps<T>& oin1, NodeOps<T>& oout0, NodeOps<T>& oout1) {
     // (a) x-edge of plane k+1; prefetch plane k+3, the cells of layer k+1 and the epilogue operands of plane k
     V E[3][2];
-    edge(vn, E);
+    edge(vin, E);
     put_edge(slot(k + 1), E);
-    load_plane(k + 3, vq);
-    cells_n = load_cells(k + 1);
-    prefetch(k, on0, on1);
+    load_plane(k + 3, vin);
+    cout = load_cells(k + 1);
+    prefetch(k, oout0, oout1);
     __syncthreads();
     // (b) finish plane k-1
-    if (k > K0 - 1) finish(k - 1, slot(k - 1), Lw, Uhi, flags_prev, op0, op1);
-    flags_prev = cells_c;
-    if constexpr (PREF) { op0 = on0; op1 = on1; }
+    if (k > K0 - 1) finish(k - 1, slot(k - 1), Lw, Uhi, flags_prev, oin0, oin1);
+    flags_prev = cin;
     // (c) faces of plane k+1, z butterfly -> modal coefficients of cell layer k
-    V Fk1[3][4];
-    face(slot(k + 1), E, Fk1);
+    face(slot(k + 1), E, Fout);
     V X[8], Y[8], Z[8];
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-      X[l] = Fk[0][l] + Fk1[0][l]; X[l + 4] = Fk1[0][l] - Fk[0][l];
-      Y[l] = Fk[1][l] + Fk1[1][l]; Y[l + 4] = Fk1[1][l] - Fk[1][l];
-      Z[l] = Fk[2][l] + Fk1[2][l]; Z[l + 4] = Fk1[2][l] - Fk[2][l];
+      X[l] = Fin[0][l] + Fout[0][l]; X[l + 4] = Fout[0][l] - Fin[0][l];
+      Y[l] = Fin[1][l] + Fout[1][l]; Y[l + 4] = Fout[1][l] - Fin[1][l];
+      Z[l] = Fin[2][l] + Fout[2][l]; Z[l + 4] = Fout[2][l] - Fin[2][l];
     }
     // (d) element core of the two cells (i, r0, k), (i, r1, k)
     V FX[8], FY[8], FZ[8];
-    const int id0 = (lane < 31) ? int(cells_c & 0x7fu) : 0, id1 = (lane < 31) ? int((cells_c >> 8) & 0x7fu) : 0;
+    const int id0 = (lane < 31) ? int(cin & 0x7fu) : 0, id1 = (lane < 31) ? int((cin >> 8) & 0x7fu) : 0;
     if constexpr (CUBE) {
       const V L16(sMat[id0][0], sMat[id1][0]), M48(sMat[id0][1], sMat[id1][1]);
       cube_sri_core<T>(X, Y, Z, L16, M48, FX, FY, FZ);
@@ -447,17 +459,36 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
       }
       sB[sl][c][w][lane] = mk2<T>(U[0].hi(), U[1].hi());
     }
-    // (g) advance
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-#pragma unroll
-      for (int l = 0; l < 4; ++l) Fk[c][l] = Fk1[c][l];
-      vn[c] = vp[c]; vp[c] = vq[c];
+  };
+  if constexpr (kPairUnroll && std::is_same<T, float>::value) {
+    int k = K0 - 1;
+    for (; k + 1 < K1; k += 2) {
+      step(k, va, Fa, Fb, ca, cb, oa0, oa1, ob0, ob1);
+      step(k + 1, vb, Fb, Fa, cb, ca, ob0, ob1, oa0, oa1);
     }
-    cells_c = cells_n;
+    if (k < K1) {   // odd number of steps: the last one runs on the first set
+      step(k, va, Fa, Fb, ca, cb, oa0, oa1, ob0, ob1);
+      __syncthreads();
+      finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev, ob0, ob1);
+    } else {
+      __syncthreads();
+      finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev, oa0, oa1);
+    }
+  } else {   // FP64: one plane per trip, the second set copied into the first (no register room for both)
+    for (int k = K0 - 1; k < K1; ++k) {
+      step(k, va, Fa, Fb, ca, cb, oa0, oa1, ob0, ob1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const V t = va[c]; va[c] = vb[c]; vb[c] = t;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) Fa[c][l] = Fb[c][l];
+      }
+      ca = cb;
+      if constexpr (PREF) { oa0 = ob0; oa1 = ob1; }
+    }
+    __syncthreads();
+    finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev, oa0, oa1);
   }
-  __syncthreads();
-  finish(K1 - 1, slot(K1 - 1), Lw, Uhi, flags_prev, op0, op1);
 }
 
 template <typename T, int MODE, bool CUBE, int WY, bool SMOOTH>

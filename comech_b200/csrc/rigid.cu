@@ -87,6 +87,59 @@ k_ztr_partial(RigidView Z, const T* __restrict__ r, double* __restrict__ part, c
   }
 }
 
+// zr = Z^T r from the partials, coef = Einv zr (when Einv is given); run by one block
+__device__ void ztr_finish(const RigidView& Z, int nblk, const double* part, const double* __restrict__ Einv,
+                           double* __restrict__ zr, double* __restrict__ coef) {
+  const int nc = 6 * Z.ngroups;
+  for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+    int g = t / 6, m = t % 6;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += ((const volatile double*)part)[((size_t)g * nblk + b) * 6 + m];
+    zr[t] = s;
+  }
+  __syncthreads();
+  if (Einv == nullptr) return;
+  for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < nc; ++q) s += Einv[(size_t)t * nc + q] * ((const volatile double*)zr)[q];
+    coef[t] = s;
+  }
+}
+
+// k_ztr_partial with ztr_finish in the block that arrives last (counted on ctr after a fence that publishes
+// the block's partials; the counter is re-armed for the next use)
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_ztr_fused(RigidView Z, const T* __restrict__ r, double* part, const double* __restrict__ Einv, double* zr,
+            double* coef, unsigned int* ctr, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int g = blockIdx.y;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int e = Z.off[g] + blockIdx.x * kThreads + threadIdx.x; e < Z.off[g + 1]; e += gridDim.x * kThreads) {
+    const int64_t n = Z.nodes[e];
+    const double rx = Z.rho[3 * e], ry = Z.rho[3 * e + 1], rz = Z.rho[3 * e + 2];
+    double r0 = double(r[3 * n]), r1 = double(r[3 * n + 1]), r2 = double(r[3 * n + 2]);
+    s[0] += r0; s[1] += r1; s[2] += r2;
+    s[3] += -rz * r1 + ry * r2;
+    s[4] += rz * r0 - rx * r2;
+    s[5] += -ry * r0 + rx * r1;
+  }
+  for (int m = 0; m < 6; ++m) {
+    double v = block_sum(s[m]);
+    if (threadIdx.x == 0) part[((size_t)g * gridDim.x + blockIdx.x) * 6 + m] = v;
+    __syncthreads();
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ctr, 1u) == gridDim.x * gridDim.y - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  ztr_finish(Z, gridDim.x, part, Einv, zr, coef);
+  if (threadIdx.x == 0) *ctr = 0u;
+}
+
 // coef = Einv (Z^T r); one block
 __global__ void k_ztr_finish(RigidView Z, int nblk, const double* __restrict__ part, const double* __restrict__ Einv,
                              double* __restrict__ zr, double* __restrict__ coef, const int* __restrict__ skip) {
@@ -150,11 +203,15 @@ void launch_centroids(const RigidView& Z, double* cen, double* part, cudaStream_
 
 template <typename T>
 void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, double* zr, double* coef,
-                        const double* Einv, const int* skip, cudaStream_t s) {
+                        const double* Einv, const int* skip, cudaStream_t s, unsigned int* ctr) {
   int nb = rigid_blocks(Z);
   dim3 g(nb, Z.ngroups);
-  k_ztr_partial<T><<<g, kThreads, 0, s>>>(Z, r, part, skip); note_launch();
-  k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, Einv, zr, coef, skip); note_launch();
+  if (ctr) {
+    k_ztr_fused<T><<<g, kThreads, 0, s>>>(Z, r, part, Einv, zr, coef, ctr, skip); note_launch();
+  } else {
+    k_ztr_partial<T><<<g, kThreads, 0, s>>>(Z, r, part, skip); note_launch();
+    k_ztr_finish<<<1, kThreads, 0, s>>>(Z, nb, part, Einv, zr, coef, skip); note_launch();
+  }
   if (Einv) k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip); note_launch();
 }
 
@@ -176,8 +233,8 @@ void launch_z_column(const RigidView& Z, int col, double* v, cudaStream_t s) {
 }
 
 template void launch_rigid_apply<float>(const RigidView&, const float*, float*, double*, double*, double*,
-                                        const double*, const int*, cudaStream_t);
+                                        const double*, const int*, cudaStream_t, unsigned int*);
 template void launch_rigid_apply<double>(const RigidView&, const double*, double*, double*, double*, double*,
-                                         const double*, const int*, cudaStream_t);
+                                         const double*, const int*, cudaStream_t, unsigned int*);
 
 }  // namespace feb

@@ -22,10 +22,11 @@ void launch_rigid_rho(const RigidView& Z, double* rho, cudaStream_t s);
 int rigid_blocks(const RigidView& Z);
 // part: rigid_blocks * ngroups * 6 doubles (scratch)
 void launch_centroids(const RigidView& Z, double* cen, double* part, cudaStream_t s);
-// z += Z Einv Z^T r   (part: rigid_blocks * ngroups * 6 doubles; zr, coef: 6 ngroups)
+// z += Z Einv Z^T r   (part: rigid_blocks * ngroups * 6 doubles; zr, coef: 6 ngroups).  ctr (optional): a
+// zeroed counter; the reduction is then finished by its last block instead of a second launch.
 template <typename T>
 void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, double* zr, double* coef,
-                        const double* Einv, const int* skip, cudaStream_t s);
+                        const double* Einv, const int* skip, cudaStream_t s, unsigned int* ctr = nullptr);
 // zr = Z^T r
 void launch_ztr(const RigidView& Z, const double* r, double* part, double* zr, cudaStream_t s);
 // v += column col of Z

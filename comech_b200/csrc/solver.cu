@@ -136,6 +136,8 @@ struct AxisHost {
 };
 
 // 1-D prolongation from every other node plus the last one with linear weights (fe/gmg.py:7-26)
+int env_flag(const char* name);   // 1 when the variable is set to anything but "" or "0"
+
 AxisHost make_axis(const std::vector<double>& c) {
   AxisHost A;
   const int n = (int)c.size();
@@ -735,6 +737,7 @@ struct FebHandle {
   CgState* st = nullptr;      // outer CG
   CgState* sti = nullptr;     // inner CG (refinement)
   double* partials = nullptr;
+  unsigned int* ctr = nullptr;   // arrival counter of the last-block reductions (zero between launches)
   double* sc = nullptr;       // refinement scaling
   int* status = nullptr;
   CgState* st_h = nullptr;    // pinned
@@ -953,22 +956,23 @@ struct FebHandle {
     smooth<T>(l, b, x, false, skip);
   }
 
-  // z = M r for the CG of precision T (FP64 CG with an FP64 or FP32 V-cycle, FP32 CG with FP32)
+  // z = M r for the CG of precision T (FP64 CG with an FP64 or FP32 V-cycle, FP32 CG with FP32); rf_ready:
+  // the FP32 copy of r (rf) was written by the CG update already
   template <typename T>
-  void precondition(const T* r_, T* z_, const int* skip) {
+  void precondition(const T* r_, T* z_, const int* skip, bool rf_ready = false) {
     const int64_t n = 3 * ntotal;
     if constexpr (std::is_same<T, double>::value) {
       if (opt.precision == FEB_PREC_FP64) {
         vcycle<double>(0, r_, z_, skip);
       } else {
-        launch_convert<double, float>(r_, rf, n, skip, s);
+        if (!rf_ready) launch_convert<double, float>(r_, rf, n, skip, s);
         vcycle<float>(0, rf, zf, skip);
         launch_convert<float, double>(zf, z_, n, skip, s);
       }
     } else {
       vcycle<float>(0, r_, z_, skip);
     }
-    if (has_rigid) launch_rigid_apply<T>(Z, r_, z_, zpart, zr, zcoef, Einv, skip, s);
+    if (has_rigid) launch_rigid_apply<T>(Z, r_, z_, zpart, zr, zcoef, Einv, skip, s, ctr + 1);
   }
 
   // one CG iteration (SciPy order: z = M r, beta, p, q = A p, alpha, x, r, convergence)
@@ -976,15 +980,14 @@ struct FebHandle {
   void cg_body(CgState* S, T* x_, T* r_, T* z_, T* p_, T* q_) {
     const int* skip = &S->done;
     const int64_t n = 3 * ntotal;
-    precondition<T>(r_, z_, skip);
-    launch_dot_partial<T, T>(r_, z_, n, partials, skip, s);
-    launch_finalize(FIN_RZ, partials, S, nullptr, 0, skip, s);
+    // the mixed precision's FP32 copy of r is written by the x/r update (and by cg_start before the loop)
+    const bool mixed = std::is_same<T, double>::value && opt.precision != FEB_PREC_FP64;
+    precondition<T>(r_, z_, skip, mixed);
+    launch_dot_finalize<T, T>(FIN_RZ, r_, z_, n, partials, ctr, S, skip, s);
     launch_update_p<T>(z_, p_, S, n, skip, s);
     apply<T>(0, p_, q_, skip);
-    launch_dot_partial<T, T>(p_, q_, n, partials, skip, s);
-    launch_finalize(FIN_ALPHA, partials, S, nullptr, 0, skip, s);
-    launch_update_xr<T>(p_, q_, x_, r_, S, n, partials, skip, s);
-    launch_finalize(FIN_CONV, partials, S, nullptr, 0, skip, s);
+    launch_dot_finalize<T, T>(FIN_ALPHA, p_, q_, n, partials, ctr, S, skip, s);
+    launch_update_xr_conv<T>(p_, q_, x_, r_, mixed ? rf : nullptr, S, n, partials, ctr, skip, s);
   }
 
   // one CG iteration captured as a graph; with use_graphs == 2 the iteration is the body of a device-side
@@ -1083,6 +1086,10 @@ struct FebHandle {
     launch_dot_partial<T, T>(r_, r_, n, partials, nullptr, s);
     launch_finalize(FIN_INIT, partials, S, nullptr, 0, nullptr, s);
     launches += has_x0 ? 6 : 2;
+    if (std::is_same<T, double>::value && opt.precision != FEB_PREC_FP64) {   // FP32 copy for the first V-cycle
+      launch_convert<double, float>((const double*)r_, rf, n, nullptr, s);
+      launches += 1;
+    }
     return FEB_OK;
   }
 
@@ -1185,12 +1192,22 @@ int upload_transfer(Pool& pool, Level& V) {
     FEB_TRY(pool.upload(&ivc, c.data(), c.size()));
     D.ca = ca; D.cb = cb; D.wa = wa; D.wb = wb; D.cidx = cidx; D.iv_first = ivf; D.iv_count = ivc;
   }
+  // even coarsening on every axis: 2 nc - 1 fine nodes, odd fine nodes halfway between their coarse neighbours
+  bool even = true;
+  for (int d = 0; d < 3 && even; ++d) {
+    const AxisHost& A = V.ax[d];
+    even = A.nf == 2 * A.nc - 1;
+    for (int i = 0; i < A.nf && even; ++i) {
+      if (i % 2 == 0) even = A.ca[i] == i / 2 && A.wa[i] == 1.0 && (A.wb[i] == 0.0 || A.cb[i] == A.ca[i]);
+      else even = A.ca[i] == i / 2 && A.cb[i] == i / 2 + 1 && std::fabs(A.wa[i] - 0.5) < 1e-12 &&
+                  std::fabs(A.wb[i] - 0.5) < 1e-12;
+    }
+  }
+  V.P.even = even ? 1 : 0;
   return FEB_OK;
 }
 
-// 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients
-// The iteration runs in the precision of the V-cycle that uses the estimate (FP32 for the mixed and refined
-// precisions, as the reference GPU path runs it in its multigrid dtype, rb/gpusolve.py:84-97).
+// 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients, in precision T.
 template <typename T>
 int power_iteration(FebHandle* h, int l) {
   Level& V = h->L[l];
@@ -1927,7 +1944,11 @@ int build_hierarchy(FebHandle* h) {
     FEB_TRY(level_vectors<double>(H.pool, V, true, f32));
   }
   g_prof.mark("level work vectors", H.s);
-  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(f32 ? power_iteration<float>(h, k) : power_iteration<double>(h, k));
+  // The power steps run in FP64 for every precision: on the 160 x 112 x 96 hindfoot the FP32 estimate cost the
+  // mixed solve 5 iterations (78 against 73; FP64 V-cycle 72).  FEB_POWER_FP32=1 runs them in the V-cycle's
+  // precision instead (as rb/gpusolve.py:84-97 does in its multigrid dtype).
+  const bool pw32 = f32 && env_flag("FEB_POWER_FP32");
+  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(pw32 ? power_iteration<float>(h, k) : power_iteration<double>(h, k));
   H.stage_mark();   // 6: work vectors, power iterations
   g_prof.mark("power iterations", H.s);
   FEB_TRY(build_dense(h));
@@ -1980,6 +2001,93 @@ void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
 int env_flag(const char* name) {
   const char* v = std::getenv(name);
   return v && *v && std::strcmp(v, "0") != 0;
+}
+
+// the parts of FebInfo that describe the handle (hierarchy, smoother estimates, kernel shapes, set-up times)
+int fill_handle_info(FebHandle& H, FebInfo& inf) {
+  inf.t_setup_ms = H.t_setup_ms;
+  inf.levels = H.coarsest + 1;
+  inf.ndof = H.ndof;
+  inf.coarse_n = H.nd;
+  std::vector<LevelParams> lp(kMaxLevels);
+  FEB_CUDA(cudaMemcpyAsync(lp.data(), H.lp, kMaxLevels * sizeof(LevelParams), cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamSynchronize(H.s));
+  for (int l = 0; l <= H.coarsest && l < 8; ++l) {
+    inf.level_dofs[l] = H.L[l].ndof;
+    inf.lmax[l] = l < H.coarsest ? lp[l].lmax : 0.0;
+  }
+  inf.kernel_launches = H.launches;
+  for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
+  inf.ku_shape[0] = H.ku32.tc ? 0 : H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
+  inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
+  inf.ku_kind = (H.tc_ok && H.ku32.tc) ? 2 : (H.pair_ok ? 1 : 0);
+  if (H.pair_ok) {
+    if (!(H.tc_ok && H.ku32.tc)) { inf.ku_shape[0] = H.pc32.wy; inf.ku_shape[1] = H.pc32.zchunk; }
+    inf.ku_shape[2] = H.pc64.wy; inf.ku_shape[3] = H.pc64.zchunk;
+  }
+  return FEB_OK;
+}
+
+// One instance of a batched solve as three pieces of graph G: the start (device-side stop threshold from ||f||,
+// the start vector, ||r0||), a device-side while loop of CG iterations (the loop's condition is the instance's
+// own convergence flag), and the finish (result copy, true residual, state read-back into pinned memory).
+int add_batch_instance(FebHandle& H, cudaGraph_t G, const double* f_in, const double* x0_in, double* xout,
+                       double tol) {
+  const int64_t n = 3 * H.ntotal;
+  const bool mixed = H.opt.precision != FEB_PREC_FP64;
+  CgState init{};
+  init.tol2 = tol * tol;
+  init.maxiter = H.opt.maxiter;
+  *H.st_h = init;   // read by the graph's first node when the graph runs
+  // start
+  cudaGraph_t pre = nullptr;
+  FEB_CUDA(cudaStreamBeginCapture(H.s, cudaStreamCaptureModeThreadLocal));
+  FEB_CUDA(cudaMemcpyAsync(H.st, H.st_h, sizeof(CgState), cudaMemcpyHostToDevice, H.s));
+  k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(f_in, H.L[0].used, H.ntotal, H.fb);
+  launch_dot_partial<double, double>(H.fb, H.fb, n, H.partials, nullptr, H.s);
+  launch_finalize(FIN_THR, H.partials, H.st, nullptr, 0, nullptr, H.s);
+  if (x0_in) {
+    k_masked_copy<<<div_up(n, kThreads), kThreads, 0, H.s>>>(x0_in, H.L[0].used, H.ntotal, H.x);
+    H.apply<double>(0, H.x, H.q, nullptr);
+    launch_residual<double>(H.fb, H.q, H.r, n, nullptr, H.s);
+  } else {
+    FEB_CUDA(cudaMemsetAsync(H.x, 0, n * sizeof(double), H.s));
+    FEB_CUDA(cudaMemcpyAsync(H.r, H.fb, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+  }
+  launch_dot_partial<double, double>(H.r, H.r, n, H.partials, nullptr, H.s);
+  launch_finalize(FIN_INIT, H.partials, H.st, nullptr, 0, nullptr, H.s);
+  if (mixed) launch_convert<double, float>(H.r, H.rf, n, nullptr, H.s);
+  FEB_CUDA(cudaStreamEndCapture(H.s, &pre));
+  cudaGraphNode_t npre, ncond, npost;
+  FEB_CUDA(cudaGraphAddChildGraphNode(&npre, G, nullptr, 0, pre));
+  FEB_CUDA(cudaGraphDestroy(pre));
+  // iterations
+  cudaGraphConditionalHandle cond;
+  FEB_CUDA(cudaGraphConditionalHandleCreate(&cond, G, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  FEB_CUDA(cudaGraphAddNode(&ncond, G, &npre, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  FEB_CUDA(cudaStreamBeginCaptureToGraph(H.s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  H.cg_body<double>(H.st, H.x, H.r, H.z, H.p, H.q);
+  launch_set_condition(cond, H.st, H.s);
+  FEB_CUDA(cudaStreamEndCapture(H.s, &body));
+  // finish
+  cudaGraph_t post = nullptr;
+  FEB_CUDA(cudaStreamBeginCapture(H.s, cudaStreamCaptureModeThreadLocal));
+  FEB_CUDA(cudaMemcpyAsync(xout, H.x, n * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
+  H.apply<double>(0, xout, H.q, nullptr);
+  launch_residual<double>(H.fb, H.q, H.r, n, nullptr, H.s);
+  launch_dot_partial<double, double>(H.r, H.r, n, H.partials, nullptr, H.s);
+  launch_finalize(FIN_TRUE, H.partials, H.st, nullptr, 0, nullptr, H.s);
+  FEB_CUDA(cudaMemcpyAsync(H.st_h, H.st, sizeof(CgState), cudaMemcpyDeviceToHost, H.s));
+  FEB_CUDA(cudaStreamEndCapture(H.s, &post));
+  FEB_CUDA(cudaGraphAddChildGraphNode(&npost, G, &ncond, 1, post));
+  FEB_CUDA(cudaGraphDestroy(post));
+  return FEB_OK;
 }
 
 }  // namespace
@@ -2042,6 +2150,7 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
     if ((st = h->pool.zeros(&h->st, 1)) != FEB_OK) break;
     if ((st = h->pool.zeros(&h->sti, 1)) != FEB_OK) break;
     if ((st = h->pool.alloc(&h->partials, kRedBlocks)) != FEB_OK) break;
+    if ((st = h->pool.zeros(&h->ctr, 4)) != FEB_OK) break;
     if ((st = h->pool.zeros(&h->sc, 4)) != FEB_OK) break;
     if ((st = h->pool.zeros(&h->status, 1)) != FEB_OK) break;
     if (!(h->st_h = g_pinned.take())) { st = FEB_ERR_CUDA; set_last_error("cudaMallocHost"); break; }
@@ -2276,25 +2385,7 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   float ms = 0.f;
   cudaEventElapsedTime(&ms, H.ev0, H.ev1);
   inf.t_solve_ms = ms;
-  inf.t_setup_ms = H.t_setup_ms;
-  inf.levels = H.coarsest + 1;
-  inf.ndof = H.ndof;
-  inf.coarse_n = H.nd;
-  std::vector<LevelParams> lp(kMaxLevels);
-  FEB_CUDA(cudaMemcpy(lp.data(), H.lp, kMaxLevels * sizeof(LevelParams), cudaMemcpyDeviceToHost));
-  for (int l = 0; l <= H.coarsest && l < 8; ++l) {
-    inf.level_dofs[l] = H.L[l].ndof;
-    inf.lmax[l] = l < H.coarsest ? lp[l].lmax : 0.0;
-  }
-  inf.kernel_launches = H.launches;
-  for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
-  inf.ku_shape[0] = H.ku32.tc ? 0 : H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
-  inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
-  inf.ku_kind = (H.tc_ok && H.ku32.tc) ? 2 : (H.pair_ok ? 1 : 0);
-  if (H.pair_ok) {
-    if (!(H.tc_ok && H.ku32.tc)) { inf.ku_shape[0] = H.pc32.wy; inf.ku_shape[1] = H.pc32.zchunk; }
-    inf.ku_shape[2] = H.pc64.wy; inf.ku_shape[3] = H.pc64.zchunk;
-  }
+  FEB_TRY(fill_handle_info(H, inf));
   if (info) *info = inf;
   FEB_TRY(H.sync_out());
   if (st != FEB_OK) {
@@ -2304,11 +2395,92 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   return FEB_OK;
 }
 
+int feb_solve_batch(FebHandle* const* hs, int32_t n, const double* const* f, const double* const* x0,
+                    double* const* x, FebInfo* info) {
+  if (!hs || n < 0 || (n > 0 && (!f || !x))) { set_last_error("feb_solve_batch: bad argument"); return FEB_ERR_ARG; }
+  if (n == 0) return FEB_OK;
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i] || !f[i] || !x[i]) { set_last_error("feb_solve_batch: null handle or vector at %d", i); return FEB_ERR_ARG; }
+    if (hs[i]->coarsest < 0) { set_last_error("feb_solve_batch: handle %d built with max_levels = 0", i); return FEB_ERR_ARG; }
+    if (hs[i]->opt.precision == FEB_PREC_REFINE) {
+      set_last_error("feb_solve_batch: handle %d uses the refined precision (host-driven sweeps); use feb_solve", i);
+      return FEB_ERR_ARG;
+    }
+    for (int j = 0; j < i; ++j)
+      if (hs[j] == hs[i]) { set_last_error("feb_solve_batch: handle %d given twice", i); return FEB_ERR_ARG; }
+  }
+  FebHandle& H0 = *hs[0];
+  const long long before = g_launches.load();
+  cudaGraph_t G = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  int st = FEB_OK;
+  auto fail = [&](int code) {
+    if (ex) cudaGraphExecDestroy(ex);
+    if (G) cudaGraphDestroy(G);
+    g_launches.store(before);
+    return code;
+  };
+  if (cudaGraphCreate(&G, 0) != cudaSuccess) { set_last_error("cudaGraphCreate"); return FEB_ERR_CUDA; }
+  for (int i = 0; i < n; ++i) {
+    FebHandle& H = *hs[i];
+    if ((st = H.sync_in()) != FEB_OK) return fail(st);
+    if ((st = add_batch_instance(H, G, f[i], x0 ? x0[i] : nullptr, x[i], H.opt.tol)) != FEB_OK) return fail(st);
+  }
+  g_launches.store(before);   // captured kernels are counted below, once per run
+  if (cudaGraphInstantiate(&ex, G, 0) != cudaSuccess) { set_last_error("feb_solve_batch: graph instantiation failed"); return fail(FEB_ERR_CUDA); }
+  // every instance's stream has reached its inputs (sync_in); the batch runs on instance 0's stream after all
+  for (int i = 1; i < n; ++i) {
+    if (cudaEventRecord(hs[i]->ev_sync, hs[i]->s) != cudaSuccess ||
+        cudaStreamWaitEvent(H0.s, hs[i]->ev_sync, 0) != cudaSuccess) { set_last_error("feb_solve_batch: stream join"); return fail(FEB_ERR_CUDA); }
+  }
+  cudaEventRecord(H0.ev0, H0.s);
+  if (cudaGraphLaunch(ex, H0.s) != cudaSuccess) { set_last_error("feb_solve_batch: graph launch failed"); return fail(FEB_ERR_CUDA); }
+  cudaEventRecord(H0.ev1, H0.s);
+  if (cudaEventSynchronize(H0.ev1) != cudaSuccess) {
+    set_last_error("feb_solve_batch: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(FEB_ERR_CUDA);
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, H0.ev0, H0.ev1);
+  int first_err = FEB_OK;
+  for (int i = 0; i < n; ++i) {
+    FebHandle& H = *hs[i];
+    const CgState S = *H.st_h;
+    FebInfo inf{};
+    inf.iters = S.it; inf.flag = S.flag; inf.sweeps = 1;
+    inf.relres = S.fn2 > 0 ? std::sqrt(S.rtrue / S.fn2) : 0.0;
+    inf.t_solve_ms = ms;    // the whole batch: the instances run concurrently
+    inf.x0_used = x0 && x0[i] ? 1 : 0;
+    inf.x0_scale = inf.x0_used ? 1.f : 0.f;
+    H.launches = 0;
+    if ((st = fill_handle_info(H, inf)) != FEB_OK) return fail(st);
+    if (info) info[i] = inf;
+    if (S.status != FEB_OK && first_err == FEB_OK) first_err = S.status;
+    if ((st = H.sync_out()) != FEB_OK) return fail(st);
+  }
+  if (ex) cudaGraphExecDestroy(ex);
+  cudaGraphDestroy(G);
+  if (first_err != FEB_OK) {
+    set_last_error(first_err == FEB_ERR_BREAKDOWN ? "CG breakdown: p^T K p <= 0" : "non-finite residual");
+    return first_err;
+  }
+  return FEB_OK;
+}
+
 int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y) {
   if (!h || !u || !y) { set_last_error("feb_apply: null argument"); return FEB_ERR_ARG; }
   FEB_TRY(h->sync_in());
   if (prec == 0) h->apply<double>(0, (const double*)u, (double*)y, nullptr);
   else h->apply<float>(0, (const float*)u, (float*)y, nullptr);
+  FEB_CUDA(cudaGetLastError());
+  return h->sync_out();
+}
+
+int feb_precondition(FebHandle* h, const double* r, double* z) {
+  if (!h || !r || !z) { set_last_error("feb_precondition: null argument"); return FEB_ERR_ARG; }
+  if (h->coarsest < 0) { set_last_error("feb_precondition: handle built with max_levels = 0 (operator only)"); return FEB_ERR_ARG; }
+  FEB_TRY(h->sync_in());
+  h->precondition<double>(r, z, nullptr);
   FEB_CUDA(cudaGetLastError());
   return h->sync_out();
 }

@@ -24,15 +24,8 @@ k_dot_partial(const Ta* __restrict__ a, const Tb* __restrict__ b, int64_t n, dou
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-// Sums the partials in a fixed order (deterministic) and runs the scalar step of the caller.
-__global__ void __launch_bounds__(kThreads)
-k_finalize(int kind, const double* __restrict__ partials, int np, CgState* st, LevelParams* lp, int deg,
-           const int* __restrict__ skip) {
-  if (skip && *skip) return;
-  double s = 0.0;
-  for (int i = threadIdx.x; i < np; i += kThreads) s += partials[i];
-  s = block_sum(s);
-  if (threadIdx.x != 0) return;
+// The scalar step of a reduction's caller, given the reduction's value s (thread 0 only).
+__device__ void finalize_step(int kind, double s, CgState* st, LevelParams* lp, int deg) {
   switch (kind) {
     case FIN_RZ:
       st->rz = s;
@@ -66,6 +59,13 @@ k_finalize(int kind, const double* __restrict__ partials, int np, CgState* st, L
       else if (s < st->thr2) { st->done = 1; st->flag = 0; }
       else if (st->maxiter <= 0) { st->done = 1; st->flag = st->maxiter; }
       break;
+    case FIN_THR:   // stop threshold from ||f||^2; a zero right-hand side stops before the first iteration
+      st->fn2 = s;
+      st->thr2 = s > 0.0 ? st->tol2 * s : INFINITY;
+      break;
+    case FIN_TRUE:
+      st->rtrue = s;
+      break;
     case FIN_POWER0:
       lp->xnorm = sqrt(s);
       break;
@@ -90,6 +90,58 @@ k_finalize(int kind, const double* __restrict__ partials, int np, CgState* st, L
   }
 }
 
+// Sums the partials in a fixed order (deterministic) and runs the scalar step of the caller.
+__global__ void __launch_bounds__(kThreads)
+k_finalize(int kind, const double* __restrict__ partials, int np, CgState* st, LevelParams* lp, int deg,
+           const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += kThreads) s += partials[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) finalize_step(kind, s, st, lp, deg);
+}
+
+// Last-block finalisation of a grid reduction: every block has stored its partial; the block that arrives
+// last (counted on `ctr`, after a fence that publishes the partial) sums all partials in the same fixed order
+// as k_finalize, runs the scalar step and re-arms the counter.  Block-uniform; no block waits for another.
+__device__ __forceinline__ void last_block_finalize(int kind, double* partials, unsigned int* ctr, CgState* st) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) s += ((volatile double*)partials)[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) {
+    finalize_step(kind, s, st, nullptr, 0);
+    *ctr = 0u;
+  }
+}
+
+// dot product with the caller's scalar step in the last block (FIN_RZ, FIN_ALPHA)
+template <typename Ta, typename Tb>
+__global__ void __launch_bounds__(kThreads)
+k_dot_finalize(int kind, const Ta* __restrict__ a, const Tb* __restrict__ b, int64_t n, double* partials,
+               unsigned int* ctr, CgState* st, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    s0 += double(a[i]) * double(b[i]);
+    s1 += double(a[i + stride]) * double(b[i + stride]);
+    s2 += double(a[i + 2 * stride]) * double(b[i + 2 * stride]);
+    s3 += double(a[i + 3 * stride]) * double(b[i + 3 * stride]);
+  }
+  for (; i < n; i += stride) s0 += double(a[i]) * double(b[i]);
+  double s = block_sum((s0 + s1) + (s2 + s3));
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  last_block_finalize(kind, partials, ctr, st);
+}
+
 template <typename T>
 __global__ void k_update_p(const T* __restrict__ z, T* __restrict__ p, const CgState* __restrict__ st, int64_t n,
                            const int* __restrict__ skip) {
@@ -99,10 +151,13 @@ __global__ void k_update_p(const T* __restrict__ z, T* __restrict__ p, const CgS
     p[i] = z[i] + beta * p[i];
 }
 
+// x += alpha p, r -= alpha q, partial ||r||^2; rf (optional) receives r in FP32 for the next FP32 V-cycle;
+// with ctr the last block runs the convergence step (FIN_CONV) itself
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_update_xr(const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x, T* __restrict__ r,
-            const CgState* __restrict__ st, int64_t n, double* __restrict__ partials, const int* __restrict__ skip) {
+            float* __restrict__ rf, CgState* st, int64_t n, double* partials, unsigned int* ctr,
+            const int* __restrict__ skip) {
   if (skip && *skip) return;
   const T alpha = T(st->alpha);
   double s0 = 0.0, s1 = 0.0;
@@ -114,6 +169,7 @@ k_update_xr(const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
     x[i] = x0 + alpha * p0; x[i + stride] = x1 + alpha * p1;
     const T r0 = ra - alpha * q0, r1 = rb - alpha * q1;
     r[i] = r0; r[i + stride] = r1;
+    if (rf) { rf[i] = float(r0); rf[i + stride] = float(r1); }
     s0 += double(r0) * double(r0);
     s1 += double(r1) * double(r1);
   }
@@ -121,10 +177,12 @@ k_update_xr(const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
     x[i] += alpha * p[i];
     T ri = r[i] - alpha * q[i];
     r[i] = ri;
+    if (rf) rf[i] = float(ri);
     s0 += double(ri) * double(ri);
   }
   double s = block_sum(s0 + s1);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (ctr) last_block_finalize(FIN_CONV, partials, ctr, st);
 }
 
 template <typename T>
@@ -312,7 +370,20 @@ void launch_update_p(const T* z, T* p, const CgState* st, int64_t n, const int* 
 template <typename T>
 void launch_update_xr(const T* p, const T* q, T* x, T* r, const CgState* st, int64_t n, double* partials,
                       const int* skip, cudaStream_t s) {
-  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, st, n, partials, skip); note_launch();
+  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, nullptr, const_cast<CgState*>(st), n, partials, nullptr,
+                                                 skip); note_launch();
+}
+
+template <typename T>
+void launch_update_xr_conv(const T* p, const T* q, T* x, T* r, float* rf, CgState* st, int64_t n, double* partials,
+                           unsigned int* ctr, const int* skip, cudaStream_t s) {
+  k_update_xr<T><<<kRedBlocks, kThreads, 0, s>>>(p, q, x, r, rf, st, n, partials, ctr, skip); note_launch();
+}
+
+template <typename Ta, typename Tb>
+void launch_dot_finalize(int kind, const Ta* a, const Tb* b, int64_t n, double* partials, unsigned int* ctr,
+                         CgState* st, const int* skip, cudaStream_t s) {
+  k_dot_finalize<Ta, Tb><<<kRedBlocks, kThreads, 0, s>>>(kind, a, b, n, partials, ctr, st, skip); note_launch();
 }
 
 template <typename T>
@@ -410,6 +481,14 @@ template void launch_dot_partial<double, double>(const double*, const double*, i
 template void launch_dot_partial<float, float>(const float*, const float*, int64_t, double*, const int*,
                                                cudaStream_t);
 template void launch_convert<double, float>(const double*, float*, int64_t, const int*, cudaStream_t);
+template void launch_update_xr_conv<double>(const double*, const double*, double*, double*, float*, CgState*, int64_t,
+                                            double*, unsigned int*, const int*, cudaStream_t);
+template void launch_update_xr_conv<float>(const float*, const float*, float*, float*, float*, CgState*, int64_t,
+                                           double*, unsigned int*, const int*, cudaStream_t);
+template void launch_dot_finalize<double, double>(int, const double*, const double*, int64_t, double*, unsigned int*,
+                                                  CgState*, const int*, cudaStream_t);
+template void launch_dot_finalize<float, float>(int, const float*, const float*, int64_t, double*, unsigned int*,
+                                                CgState*, const int*, cudaStream_t);
 template void launch_convert<float, double>(const float*, double*, int64_t, const int*, cudaStream_t);
 
 }  // namespace feb

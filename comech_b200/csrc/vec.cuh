@@ -11,6 +11,9 @@ constexpr int kRedBlocks = 4 * kSmCount;   // partial sums per reduction
 struct CgState {
   double rz, rz_old, pq, alpha, beta, rr, thr2;
   int it, done, flag, status, maxiter, pad;
+  double tol2;   // batched solves: thr2 = tol2 ||f||^2 is formed on the device (FIN_THR)
+  double fn2;    // ||f||^2 (FIN_THR)
+  double rtrue;  // ||f - K x||^2 of the result (FIN_TRUE)
 };
 
 // Per-level smoother parameters written by the power iteration.
@@ -29,7 +32,8 @@ template <typename Ta, typename Tb>
 void launch_dot_partial(const Ta* a, const Tb* b, int64_t n, double* partials, const int* skip, cudaStream_t s);
 
 // kinds of the single-block finalisation kernel
-enum FinKind : int { FIN_RZ = 0, FIN_ALPHA = 1, FIN_CONV = 2, FIN_INIT = 3, FIN_POWER0 = 4, FIN_POWER = 5 };
+enum FinKind : int { FIN_RZ = 0, FIN_ALPHA = 1, FIN_CONV = 2, FIN_INIT = 3, FIN_POWER0 = 4, FIN_POWER = 5,
+                     FIN_THR = 6, FIN_TRUE = 7 };
 void launch_finalize(int kind, const double* partials, CgState* st, LevelParams* lp, int deg, const int* skip,
                      cudaStream_t s);
 
@@ -38,6 +42,15 @@ void launch_update_p(const T* z, T* p, const CgState* st, int64_t n, const int* 
 template <typename T>
 void launch_update_xr(const T* p, const T* q, T* x, T* r, const CgState* st, int64_t n, double* partials,
                       const int* skip, cudaStream_t s);
+// the CG's x/r update with the convergence step (FIN_CONV) in its last block; rf (optional) receives r in
+// FP32.  ctr: a zeroed counter, re-armed by the kernel, used by one reduction at a time on the stream.
+template <typename T>
+void launch_update_xr_conv(const T* p, const T* q, T* x, T* r, float* rf, CgState* st, int64_t n, double* partials,
+                           unsigned int* ctr, const int* skip, cudaStream_t s);
+// a.b with the step `kind` (FIN_RZ, FIN_ALPHA) in the last block
+template <typename Ta, typename Tb>
+void launch_dot_finalize(int kind, const Ta* a, const Tb* b, int64_t n, double* partials, unsigned int* ctr,
+                         CgState* st, const int* skip, cudaStream_t s);
 
 // Chebyshev smoother pieces (Dinv SoA [9][nn], vectors AoS [3 nn])
 template <typename T>

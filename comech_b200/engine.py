@@ -178,6 +178,12 @@ class Problem:
         _lib.check(_lib.load().feb_solve(self.h, _ptr(f), _ptr(x0), _ptr(x), C.byref(info)))
         return x, info
 
+    def precondition(self, r):
+        """z = M r (one V-cycle plus the rigid-mode correction; FP64 full-layout device vectors)."""
+        z = self.torch.empty_like(r)
+        _lib.check(_lib.load().feb_precondition(self.h, _ptr(r), _ptr(z)))
+        return z
+
     def apply(self, u):
         y = self.torch.empty_like(u)
         prec = 0 if u.dtype == self.torch.float64 else 1
@@ -204,7 +210,10 @@ def _info_dict(info, t0, extra=None):
              lmax=[float(info.lmax[i]) for i in range(max(int(info.levels) - 1, 0))],
              kernel_launches=int(info.kernel_launches), ku_shape=list(info.ku_shape), ku_kind=int(info.ku_kind),
              t_stage_ms=[round(float(v), 3) for v in info.t_stage_ms], device=f"cuda:{_torch().cuda.current_device()}",
-             x0_used=bool(info.x0_used), x0_scale=float(info.x0_scale), t_wall=round(time.perf_counter() - t0, 4))
+             x0_used=bool(info.x0_used), x0_scale=float(info.x0_scale), t_wall=round(time.perf_counter() - t0, 4),
+             # the reference GPU path's keys (rb/gpusolve.py:285): hierarchy set-up seconds and the attempt that
+             # succeeded (the device path makes one attempt: a failure raises, there is no CPU retry)
+             t_hier=round(info.t_setup_ms / 1e3, 2), gpu_attempt=0)
     if extra:
         d.update(extra)
     return d
@@ -231,11 +240,25 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
     info, reactions R).  ``warm_start``: True (the packaged network) or a ``warmnet.WarmNet`` predicts the initial
     guess when no ``x0`` is given; the solve falls back to a zero start if the guess's residual is not below
     ||f|| (info["x0_used"])."""
+    ctx = prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra, node_groups, tol, maxiter, aniso,
+                     precision=precision, x0=x0, options=options, warm_start=warm_start)
+    try:
+        x, info = ctx["P"].solve(ctx["f"], ctx["x0"])
+        ctx["stamps"].append(("solve", time.perf_counter()))
+        return finish_cn(ctx, x, info, keep_device=keep_device)
+    finally:
+        if not keep_device:
+            ctx["P"].close()
+
+
+def prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups=None, tol=1e-6, maxiter=800,
+               aniso=None, *, precision="fp64", x0=None, options=None, warm_start=None):
+    """The part of solve_cn before the solve: the operator and its hierarchy (a Problem), the rigid groups, the
+    right-hand side and the start.  Returns a context for finish_cn; the caller closes ctx["P"]."""
     if aniso is not None:
         raise NotImplementedError("laminate (aniso) joint cells are not supported by the device solver")
     t0 = time.perf_counter()
     stamps = [("start", t0)]
-    ncell = g.nx * g.ny * g.nz
     orig = np.asarray(orig)
     ntotal = len(orig)
     fn, fa = fixed
@@ -267,21 +290,42 @@ def solve_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_groups
             stamps.append(("warm_start", time.perf_counter()))
         else:
             x0d = None
-        x, info = P.solve(f, x0d)
-        stamps.append(("solve", time.perf_counter()))
-        Ud = P.export(x)
-        U = _host(Ud.view(ntotal, 3))
-        stamps.append(("download", time.perf_counter()))
-        R = np.zeros((ntotal, 3))
-        np.add.at(R, fn, -(fa[:, None] * K_GROUND) * U[fn])
-        stamps.append(("reactions", time.perf_counter()))
-        d = _info_dict(info, t0, dict(t_host={b[0]: round(b[1] - a[1], 4) for a, b in zip(stamps, stamps[1:])}))
-        if keep_device:
-            d["device"] = dict(U=Ud, mat=P.mat, cn=P.cn, problem=P)
-        return U, d, R
-    finally:
-        if not keep_device:
-            P.close()
+    except BaseException:
+        P.close()
+        raise
+    return dict(P=P, f=f, x0=x0d, fn=fn, fa=fa, ntotal=ntotal, stamps=stamps, t0=t0)
+
+
+def finish_cn(ctx, x, info, keep_device=False):
+    """The part of solve_cn after the solve: U (NaN on unused nodes), reactions of the ground springs, info."""
+    P, fn, fa, ntotal, stamps = ctx["P"], ctx["fn"], ctx["fa"], ctx["ntotal"], ctx["stamps"]
+    Ud = P.export(x)
+    U = _host(Ud.view(ntotal, 3))
+    stamps.append(("download", time.perf_counter()))
+    R = np.zeros((ntotal, 3))
+    np.add.at(R, fn, -(fa[:, None] * K_GROUND) * U[fn])
+    stamps.append(("reactions", time.perf_counter()))
+    d = _info_dict(info, ctx["t0"], dict(t_host={b[0]: round(b[1] - a[1], 4) for a, b in zip(stamps, stamps[1:])}))
+    if keep_device:
+        d["device"] = dict(U=Ud, mat=P.mat, cn=P.cn, problem=P)
+    return U, d, R
+
+
+def solve_batch_device(problems, fs, x0s=None):
+    """One feb_solve_batch call: problems (Problem), right-hand sides and optional starts (device tensors, full
+    layout).  Returns [(x, FebInfo)] in order."""
+    torch = _torch()
+    n = len(problems)
+    xs = [torch.empty_like(f) for f in fs]
+    infos = (_lib.FebInfo * n)()
+    hs = (C.c_void_p * n)(*[P.h.value for P in problems])
+    fp = (C.c_void_p * n)(*[f.data_ptr() for f in fs])
+    xp = (C.c_void_p * n)(*[x.data_ptr() for x in xs])
+    x0p = None
+    if x0s is not None:
+        x0p = (C.c_void_p * n)(*[(x.data_ptr() if x is not None else 0) for x in x0s])
+    _lib.check(_lib.load().feb_solve_batch(hs, n, fp, x0p, xp, infos))
+    return [(xs[i], infos[i]) for i in range(n)]
 
 
 def _used_from_grid(g, active):
@@ -429,12 +473,12 @@ def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, A_op=N
     """GMG-preconditioned CG for an assembled matrix on compact dofs (fe/gmg.py:120-137, the plugin point
     that rb/rbfe.py:21-27 swaps).  Compatibility path: the fine level applies A as a sparse matrix on the
     device and the coarse levels are its Galerkin products on the structured grid; node ``i`` of A sits at
-    grid node ``used_nodes[i]`` (split copies share their grid node, rb/splitfe.py:153).  Z, when given,
-    must be the per-group rigid-body modes of fe/solver.py:177-199.  Returns (x, info)."""
+    grid node ``used_nodes[i]`` (split copies share their grid node, rb/splitfe.py:153).  A Z made of the
+    per-group rigid-body modes of fe/solver.py:177-199 runs on the device with the rest of the solve; with any
+    other Z, or with a separate Krylov operator A_op, the V-cycle still runs on the device (feb_precondition) and
+    SciPy's cg drives the iteration on the host (_pcg_host_operator).  Returns (x, info)."""
     import scipy.sparse as sp
     from .grid import Grid
-    if A_op is not None:
-        raise NotImplementedError("A_op is not supported by the device solver")
     t0 = time.perf_counter()
     xe, ye, ze = grid_edges
     g = Grid(xe, ye, ze)
@@ -456,8 +500,18 @@ def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, A_op=N
     P = Problem(g, _lib.MAT_ISO_SRI, np.zeros(2 * ncell), np.zeros(ncell, bool), cn=None, orig=orig, extra_coo=coo,
                 precision=precision, tol=tol, maxiter=maxiter, options=options, mark_used=node_of)
     try:
-        if Z is not None:
-            P.set_rigid_groups([node_of[gr] for gr in _rigid_groups_from_Z(Z, n_c)])
+        groups = None
+        if Z is not None and A_op is None:
+            try:
+                groups = _rigid_groups_from_Z(Z, n_c)
+            except NotImplementedError:
+                groups = None
+        if A_op is not None or (Z is not None and groups is None):
+            # a separate Krylov operator, or a Z other than per-group rigid modes: host Krylov loop
+            return _pcg_host_operator(P, A, A if A_op is None else A_op, b, x0, Z, tol, maxiter, node_of, len(orig),
+                                      t0)
+        if groups is not None:
+            P.set_rigid_groups([node_of[gr] for gr in groups])
         bf = np.zeros((len(orig), 3)); bf[node_of] = np.asarray(b, np.float64).reshape(-1, 3)
         f = _dev(bf.ravel(), np.float64)
         x0d = None
@@ -469,3 +523,37 @@ def pcg_gmg(A, b, used_nodes, grid_edges, tol=1e-7, maxiter=500, x0=None, A_op=N
         return xh, _info_dict(info, t0)
     finally:
         P.close()
+
+
+def _pcg_host_operator(P, A, A_op, b, x0, Z, tol, maxiter, node_of, ntot, t0):
+    """pcg_gmg with a separate Krylov operator A_op (fe/gmg.py:127-136): the preconditioner is still built from A
+    (the device V-cycle, plus the rigid-mode correction whose coarse matrix Z^T A_op Z is formed with A_op as the
+    reference forms it), and SciPy's cg runs the iteration with A_op, a host operator, so each iteration moves r to
+    the device and M r back.  Returns (x, info) like the device path."""
+    import scipy.sparse.linalg as spla
+    torch = _torch()
+    n = A.shape[0]
+    dofs = (3 * node_of[:, None] + np.arange(3)[None, :]).ravel()
+
+    def vcycle(r):
+        rf = np.zeros(3 * ntot); rf[dofs] = np.asarray(r, np.float64).ravel()
+        return _host(P.precondition(_dev(rf, np.float64)))[dofs]
+
+    if Z is not None:
+        # P carries no rigid groups here: the correction is applied on the host with A_op, as fe/gmg.py:127-135
+        Zd = Z.toarray() if hasattr(Z, "toarray") else np.asarray(Z)
+        AZ = np.column_stack([A_op @ Zd[:, i] for i in range(Zd.shape[1])])
+        Ec = Zd.T @ AZ
+        Einv = np.linalg.pinv(0.5 * (Ec + Ec.T))
+        M = spla.LinearOperator((n, n), matvec=lambda r: vcycle(r) + Zd @ (Einv @ (Zd.T @ r)))
+    else:
+        M = spla.LinearOperator((n, n), matvec=vcycle)
+    it = [0]
+    x, flag = spla.cg(A_op, np.asarray(b, np.float64), x0=x0, rtol=tol, maxiter=maxiter, M=M,
+                      callback=lambda xk: it.__setitem__(0, it[0] + 1))
+    torch.cuda.synchronize()
+    r = np.asarray(b, np.float64) - A_op @ x
+    bn = np.linalg.norm(b)
+    return x, dict(iters=it[0], flag=int(flag), relres=float(np.linalg.norm(r) / (bn if bn > 0 else 1.0)),
+                   levels=None, krylov="host (A_op)", t_wall=round(time.perf_counter() - t0, 4), t_hier=None,
+                   gpu_attempt=0)

@@ -137,8 +137,26 @@ FEB_API int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* o
  * Unused nodes of x are left 0. */
 FEB_API int feb_solve(FebHandle* h, const double* f, const double* x0, double* x, FebInfo* info);
 
+/* Solves n independent systems K_i x_i = f_i, one per handle, as ONE CUDA graph launch: per instance a
+ * device-side start (stop threshold tol ||f_i|| formed on the device), a device-side while loop of CG iterations
+ * whose condition is the instance's own convergence flag (instances stop independently), and a finish (x_i, true
+ * residual).  The instances run concurrently on the device; small grids that leave most SMs idle alone share
+ * the GPU.  Replaces the per-process engine pool of exp/rb_run_engine_v4.py:113-147, where every process solved
+ * one (foot, action) instance with rb/splitfe.py:123-158.
+ * hs: n distinct handles (FP64 or mixed precision; the refined precision's host-driven sweeps need feb_solve);
+ * f[i], x[i]: [dev] full layout of handle i; x0: NULL (zero starts) or n starts (NULL entries allowed), used as
+ * given; info: NULL or n entries (t_solve_ms is the batch's time).  The graph runs on hs[0]'s stream after all
+ * callers' streams; each caller's stream continues after the batch. */
+FEB_API int feb_solve_batch(FebHandle* const* hs, int32_t n, const double* const* f, const double* const* x0,
+                            double* const* x, FebInfo* info);
+
 /* y = K u on the level-0 operator (full layout), prec = 0 FP64 / 1 FP32 (test and benchmark hook). */
 FEB_API int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y);
+
+/* z = M r: one application of the solve's preconditioner (V-cycle in the handle's precision plus the rigid-mode
+ * correction), FP64 full-layout r and z on the device.  Replaces the M LinearOperator of fe/gmg.py:125-135 for a
+ * Krylov loop run by the caller (pcg_gmg with a separate A_op, fe/gmg.py:136). */
+FEB_API int feb_precondition(FebHandle* h, const double* r, double* z);
 
 /* U[node][c] = x for used nodes, NaN for unused ones (the reference's U, rb/splitfe.py:154). */
 FEB_API int feb_export_solution(FebHandle* h, const double* x, double* U);

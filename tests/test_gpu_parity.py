@@ -272,6 +272,52 @@ def test_pcg_gmg_on_assembled_matrix(golden):
     x, info = engine.pcg_gmg(K, f, z["orig"][nused], (g.xe, g.ye, g.ze), tol=1e-10, maxiter=800, Z=Zm)
     assert info["flag"] == 0
     assert rel(x, z["U"][nused].ravel()) < 1e-7
+    assert info["gpu_attempt"] == 0 and info["t_hier"] >= 0.0
+
+
+def _assembled(golden):
+    from oracle import fe_oracle as O
+    z, g = _hindfoot(golden)
+    og = O.OGrid(z["xe"], z["ye"], z["ze"])
+    cells = np.flatnonzero(z["active"])
+    K, nmap, nused = O.assemble(og, z["lam"], z["mu"], cells, z["cn"], O.kl_sri(og))
+    n = K.shape[0]
+    kd = np.zeros(n)
+    for c in range(3):
+        np.add.at(kd, 3 * nmap[z["fixed_nodes"]] + c, z["fixed_area"] * 1e6)
+    K = K + O.sp.diags(kd) + _springs(z)(nmap, n)
+    f = np.zeros(n)
+    for c in range(3):
+        np.add.at(f, 3 * nmap[z["load_nodes"]] + c, z["load_area"] * z["load_t"][c])
+    Zm = O.rigid_modes(og.node_xyz[z["orig"]], nmap, n, _groups(z))
+    return z, g, K, f, Zm, nused
+
+
+def test_pcg_gmg_with_separate_krylov_operator(golden):
+    """pcg_gmg(A_op=...) (fe/gmg.py:127-136): the preconditioner comes from A, the Krylov iteration and the
+    rigid-mode coarse matrix from A_op.  With A_op a LinearOperator of the same matrix the solution is the
+    reference's; with A_op = 1.01 A it is the reference's divided by 1.01."""
+    import scipy.sparse.linalg as spla
+    z, g, K, f, Zm, nused = _assembled(golden)
+    n = K.shape[0]
+    Aop = spla.LinearOperator((n, n), matvec=lambda v: K @ v)
+    x, info = engine.pcg_gmg(K, f, z["orig"][nused], (g.xe, g.ye, g.ze), tol=1e-10, maxiter=800, Z=Zm, A_op=Aop)
+    assert info["flag"] == 0 and info["relres"] < 1e-9
+    assert rel(x, z["U"][nused].ravel()) < 1e-7
+    x2, info2 = engine.pcg_gmg(K, f, z["orig"][nused], (g.xe, g.ye, g.ze), tol=1e-10, maxiter=800, A_op=1.01 * K)
+    assert info2["flag"] == 0
+    assert rel(1.01 * x2, z["U"][nused].ravel()) < 1e-7
+
+
+def test_pcg_gmg_with_general_coarse_columns(golden):
+    """A Z that is not the per-group rigid-mode layout (here: the rigid modes mixed by a random orthogonal
+    matrix, same span) runs through the host Krylov loop with the device V-cycle; same solution."""
+    z, g, K, f, Zm, nused = _assembled(golden)
+    Zd = Zm.toarray() if hasattr(Zm, "toarray") else np.asarray(Zm)
+    Q, _ = np.linalg.qr(np.random.default_rng(0).standard_normal((Zd.shape[1], Zd.shape[1])))
+    x, info = engine.pcg_gmg(K, f, z["orig"][nused], (g.xe, g.ye, g.ze), tol=1e-10, maxiter=800, Z=Zd @ Q)
+    assert info["flag"] == 0
+    assert rel(x, z["U"][nused].ravel()) < 1e-7
 
 
 def test_plugin_swaps_reference_style_modules(golden):
