@@ -475,6 +475,7 @@ def run_ours(args, rank, world, dist):
                 "levels": int(hinfo.levels), "ku_kernel": ["per-cell", "paired-row", "tensor-core"][int(hinfo.ku_kind)],
                 "l2": "flushed (256 MB write) before every step", "parallelism": f"independent solves x{world}"},
         arms_s_per_solve={k: round(v, 5) for k, v in mean_s.items()},
+        arms_step_ms={k: [round(x, 2) for x in v["ms"]] for k, v in res.items()},
         arms_iters={k: int(v["info"].iters) for k, v in res.items()},
         plain_fp64={"s_per_solve": round(mean_s["plain_fp64"], 5), "iters": int(res["plain_fp64"]["info"].iters),
                     "relres": res["plain_fp64"]["info"].relres},

@@ -22,7 +22,7 @@ EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_sol
            "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
            "feb_mix_materials", "feb_net_conv", "feb_net_wgrad", "feb_net_colsum", "feb_net_weights", "feb_net_head",
            "feb_net_adam", "feb_net_sumsq", "feb_net_inputs", "feb_net_targets", "feb_net_to_nodes",
-           "feb_net_head_grad", "feb_net_loss", "feb_net_energy_loss"]
+           "feb_net_head_grad", "feb_net_loss", "feb_net_energy_loss", "feb_label_lattice"]
 
 GATHER_SHIFT, GATHER_DOWN, GATHER_ONE, GATHER_UP = 0, 1, 2, 3
 
@@ -100,6 +100,7 @@ def load():
     lib.feb_apply.argtypes = [P, C.c_int32, P, P]
     lib.feb_precondition.argtypes = [P, P, P]
     lib.feb_solve_batch.argtypes = [P, C.c_int32, P, P, P, P]
+    lib.feb_label_lattice.argtypes = [P, P, C.c_int32, P, C.c_int32, P, C.c_int32, P, P]
     lib.feb_export_solution.argtypes = [P, P, P]
     lib.feb_used_nodes.argtypes = [P, C.POINTER(C.c_int64), P]
     lib.feb_destroy.argtypes = [P]

@@ -13,7 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfeb200.so")
-SOURCES = ["fine.cu", "fine_pair.cu", "fine_tc.cu", "coarse.cu", "vec.cu", "dense.cu", "rigid.cu", "stress.cu", "post.cu", "split.cu", "materials.cu", "net.cu", "solver.cu"]
+SOURCES = ["fine.cu", "fine_pair.cu", "fine_tc.cu", "coarse.cu", "vec.cu", "dense.cu", "rigid.cu", "stress.cu", "post.cu", "split.cu", "materials.cu", "net.cu", "labels.cu", "solver.cu"]
+# per-file flags: the labelling kernel rounds every product and sum on its own, like NumPy's elementwise operations
+FILE_FLAGS = {"labels.cu": ["-fmad=false"]}
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -37,7 +39,7 @@ def _compile(src, force, extra):
     obj = os.path.join(BUILD, src.replace(".cu", ".o"))
     if not force and not _stale(obj, _deps(src)):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(src, []) + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"

@@ -770,7 +770,16 @@ struct FebHandle {
   double t_setup_ms = 0.0;
   int launches = 0;
 
+  // side streams of set-up work that runs per level (power iterations), with their join events
+  static constexpr int kAux = kMaxLevels;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t aux_ev[kAux] = {};
+
   ~FebHandle() {
+    for (int i = 0; i < kAux; ++i) {
+      if (aux[i]) { cudaStreamSynchronize(aux[i]); cudaStreamDestroy(aux[i]); }
+      if (aux_ev[i]) cudaEventDestroy(aux_ev[i]);
+    }
     if (g_outer) cudaGraphExecDestroy(g_outer);
     if (g_inner) cudaGraphExecDestroy(g_inner);
     g_pinned.give(st_h);
@@ -1208,22 +1217,52 @@ int upload_transfer(Pool& pool, Level& V) {
 }
 
 // 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients, in precision T.
+// (on h->s, with the reduction scratch `part`)
 template <typename T>
-int power_iteration(FebHandle* h, int l) {
+int power_iteration(FebHandle* h, int l, double* part) {
   Level& V = h->L[l];
   const int64_t n = 3 * V.ntotal;
   T *x = FebHandle::vx<T>(V), *t = FebHandle::vt<T>(V), *d = FebHandle::vd<T>(V);
   launch_random_start<T>(x, V.used, V.ntotal, h->opt.seed + 7919ull * (uint64_t)l, h->s);
-  launch_dot_partial<T, T>(x, x, n, h->partials, nullptr, h->s);
-  launch_finalize(FIN_POWER0, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
+  launch_dot_partial<T, T>(x, x, n, part, nullptr, h->s);
+  launch_finalize(FIN_POWER0, part, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
   for (int it = 0; it < 12; ++it) {
     h->apply<T>(l, x, t, nullptr);
-    launch_bj_apply_norm<T>(FebHandle::dinv<T>(V), t, d, V.ntotal, h->partials, h->s);
-    launch_finalize(FIN_POWER, h->partials, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
+    launch_bj_apply_norm<T>(FebHandle::dinv<T>(V), t, d, V.ntotal, part, h->s);
+    launch_finalize(FIN_POWER, part, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
     launch_scale<T>(d, x, h->lp + l, n, h->s);
   }
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
+}
+
+// The levels' power iterations touch disjoint buffers (each level's vectors, stencil, term dots and its own
+// reduction scratch), so level k runs on side stream k and the handle's stream joins them all: the set-up
+// waits for the slowest level (level 0) instead of their sum.
+template <typename T>
+int power_iterations(FebHandle* h) {
+  FebHandle& H = *h;
+  const int nl = H.coarsest;
+  if (nl <= 0) return FEB_OK;
+  double* part = nullptr;
+  FEB_TRY(H.pool.alloc(&part, (size_t)kRedBlocks * nl));
+  FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
+  cudaStream_t main = H.s;
+  int st = FEB_OK;
+  for (int k = 0; k < nl && st == FEB_OK; ++k) {
+    if (!H.aux[k]) {
+      FEB_CUDA(cudaStreamCreateWithFlags(&H.aux[k], cudaStreamNonBlocking));
+      FEB_CUDA(cudaEventCreateWithFlags(&H.aux_ev[k], cudaEventDisableTiming));
+    }
+    FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
+    H.s = H.aux[k];
+    st = power_iteration<T>(h, k, part + (size_t)kRedBlocks * k);
+    H.s = main;
+    FEB_CUDA(cudaEventRecord(H.aux_ev[k], H.aux[k]));
+  }
+  for (int k = 0; k < nl; ++k) FEB_CUDA(cudaStreamWaitEvent(main, H.aux_ev[k], 0));
+  H.pool.free(part);
+  return st;
 }
 
 // ------------------------------------------------------------------------------------------------ autotuner
@@ -1948,7 +1987,7 @@ int build_hierarchy(FebHandle* h) {
   // mixed solve 5 iterations (78 against 73; FP64 V-cycle 72).  FEB_POWER_FP32=1 runs them in the V-cycle's
   // precision instead (as rb/gpusolve.py:84-97 does in its multigrid dtype).
   const bool pw32 = f32 && env_flag("FEB_POWER_FP32");
-  for (int k = 0; k < H.coarsest; ++k) FEB_TRY(pw32 ? power_iteration<float>(h, k) : power_iteration<double>(h, k));
+  FEB_TRY(pw32 ? power_iterations<float>(h) : power_iterations<double>(h));
   H.stage_mark();   // 6: work vectors, power iterations
   g_prof.mark("power iterations", H.s);
   FEB_TRY(build_dense(h));

@@ -258,3 +258,90 @@ def hindfoot_problem(nx=160, ny=112, nz=96, h=0.5, seed=0, action="none", n_liga
                 nsplit=nsplit, fixed=(fn, fa), loads=loads, extra=springs, node_groups=groups,
                 contact=np.isin(cells, bottom), bridge=bridge, action=action,
                 name=f"hindfoot {nx}x{ny}x{nz} h={h} seed={seed} action={action}")
+
+
+def synthetic_template(seed=0, h=1.0):
+    """A seeded stand-in for the engine's label template (rb/rbgeom.py:127-181 builds the real one from the CT
+    atlas, which is not distributed): calcaneus below and talus above the subtalar joint, each a cortical shell
+    around cancellous bone, three cartilage facets (posterior, middle, anterior) in the joint, tibia above the
+    talus, a navicular in front, soft tissue around, in the template frame of the real one (joint inside
+    labels.JOINT_BOX).  Distance maps of the subtalar region, facet frames and footprints are derived from the
+    raster the way the real template derives them.  Returns a labels.Template."""
+    from scipy import ndimage
+    from .labels import Template, FACETS, SOFT
+    rng = np.random.default_rng(seed)
+    o = np.array([-112.0, -40.0, 0.0])
+    shape = (int(round(136 / h)), int(round(80 / h)), int(round(110 / h)))
+    x = o[0] + (np.arange(shape[0]) + 0.5) * h
+    y = o[1] + (np.arange(shape[1]) + 0.5) * h
+    z = o[2] + (np.arange(shape[2]) + 0.5) * h
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    lab = np.zeros(shape, np.int8)
+
+    def ell(c, r, p=2.0):
+        return (np.abs((X - c[0]) / r[0]) ** p + np.abs((Y - c[1]) / r[1]) ** p + np.abs((Z - c[2]) / r[2]) ** p) <= 1.0
+
+    j = lambda s: s * (1.0 + 0.06 * rng.uniform(-1, 1))
+    lab[ell((-50.0, 0.0, 52.0), (62.0, 32.0, 52.0))] = SOFT
+    # the subtalar joint: a tilted surface z_j(x, y) with a gap of 2 g between the bones
+    g = 1.2
+    zj = 56.0 + j(0.12) * (X + 45.0) - 0.05 * Y
+    cal = ell((-58.0, 0.0, 40.0), (j(42.0), j(17.0), j(22.0)), 2.4) & (Z < zj - g)
+    tal = ell((-44.0, 2.0, 66.0), (j(22.0), j(15.0), j(14.0)), 2.2) & (Z > zj + g)
+    for mask, cort, canc in ((cal, 1, 53), (tal, 2, 52)):
+        inner = ndimage.binary_erosion(mask, iterations=max(1, int(round(1.5 / h))))
+        lab[mask] = cort
+        lab[inner] = canc
+    tib = ell((-40.0, 0.0, 102.0), (j(12.0), j(12.0), j(20.0))) & ~tal
+    lab[tib] = 4
+    lab[ell((-40.0, 0.0, 104.0), (7.0, 7.0, 20.0)) & tib] = 13
+    nav = ell((-8.0, 4.0, 58.0), (j(8.0), j(12.0), j(10.0))) & ~tal & ~cal
+    lab[nav] = 40
+    lab[ell((-44.0, 2.0, 86.5), (16.0, 11.0, 2.0)) & ~tal & ~tib] = 5          # ankle cartilage
+    # facets: cartilage in the joint gap, elliptical patches centred where talus and calcaneus come closest
+    gap = ~cal & ~tal & (lab == SOFT) & (np.abs(Z - zj) <= g)
+    for name, cxy, ab in (("post", (-56.0, -3.0), (j(11.0), j(8.5))), ("mid", (-37.0, 8.0), (j(6.0), j(4.2))),
+                          ("ant", (-28.0, 9.0), (j(4.2), j(3.6)))):
+        patch = gap & (((X - cxy[0]) / ab[0]) ** 2 + ((Y - cxy[1]) / ab[1]) ** 2 <= 1.0)
+        lab[patch] = FACETS[name]
+    # subtalar region and distance maps (rb/rbgeom.py:140-150)
+    sub_box = ((-100.0, 10.0), (-30.0, 38.0), (10.0, 100.0))
+    i0, i1 = (int(round((b - o[0]) / h)) for b in sub_box[0])
+    j0, j1 = (int(round((b - o[1]) / h)) for b in sub_box[1])
+    k0, k1 = (int(round((b - o[2]) / h)) for b in sub_box[2])
+    S = lab[i0:i1, j0:j1, k0:k1].astype(np.int16)
+    talS = np.isin(S, (2, 52)); calS = np.isin(S, (1, 53))
+    dt = (ndimage.distance_transform_edt(~talS) * h).astype(np.float16).astype(np.float32)
+    dc = (ndimage.distance_transform_edt(~calS) * h).astype(np.float16).astype(np.float32)
+    so = np.array([o[0] + i0 * h, o[1] + j0 * h, o[2] + k0 * h])
+    grad = np.stack(np.gradient(dc - dt), -1)
+    facets = {}
+    for name, b in FACETS.items():
+        P = (np.argwhere(S == b) + 0.5) * h + so
+        c = P.mean(0)
+        gv = grad[S == b]
+        gv = gv / (np.linalg.norm(gv, axis=1, keepdims=True) + 1e-9)
+        n = gv.mean(0); n /= np.linalg.norm(n)
+        e1 = np.array([1.0, 0, 0]) - n[0] * n; e1 /= np.linalg.norm(e1)
+        e2 = np.cross(n, e1)
+        if e2[1] < 0:
+            e2 = -e2
+        u = (P - c) @ e1; v = (P - c) @ e2; w = (P - c) @ n
+        res = 0.25
+        ua, va = np.floor(u.min()) - 2, np.floor(v.min()) - 2
+        nu_, nv_ = int((np.ceil(u.max()) + 2 - ua) / res), int((np.ceil(v.max()) + 2 - va) / res)
+        F0 = np.zeros((nu_, nv_), bool)
+        for du in np.arange(-h / 2 + res / 2, h / 2, res):
+            for dv in np.arange(-h / 2 + res / 2, h / 2, res):
+                iu = np.clip(((u + du - ua) / res).astype(int), 0, nu_ - 1)
+                iv = np.clip(((v + dv - va) / res).astype(int), 0, nv_ - 1)
+                F0[iu, iv] = True
+        F0 = ndimage.binary_fill_holes(ndimage.binary_closing(F0, np.ones((5, 5)), iterations=2))
+        gw = (dt.astype(float) + dc.astype(float))[S == b]
+        facets[name] = dict(c=c, n=n, e1=e1, e2=e2, ua=float(ua), va=float(va), res=res, F0=F0,
+                            a0=float(u.max() - u.min()) / 2, b0=float(v.max() - v.min()) / 2,
+                            uc=float((u.max() + u.min()) / 2), vc=float((v.max() + v.min()) / 2),
+                            wmax=float(np.abs(w).max()), gap=float(np.median(gw)),
+                            xyz_lo=P.min(0) - h / 2, xyz_hi=P.max(0) + h / 2)
+    static = {2, 52, 4, 13, 3, 54, 5, 6, 7}
+    return Template(lab, o, h, dt, dc, so, facets, static)

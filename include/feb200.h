@@ -258,6 +258,63 @@ FEB_API int feb_mix_materials(int32_t nx, int32_t ny, int32_t nz, int32_t ns3, c
                               const double* class_mu, const double* class_M, double* F, double* E, double* nu,
                               uint8_t* active, uint8_t* ser, void* stream);
 
+/* ---- voxel labelling of a foot lattice (rb/rbgeom.py:493-524 label_lattice, :358-464 label_points) ---------- */
+/* One facet of the template (rb/rbgeom.py:152-171): centre c, normal n, in-plane axes e1 (anterior) and e2
+ * (medial), footprint raster F0 [dev] uint8 nu x nv (row-major, origin (ua, va), pixel res), semi-axes a0 b0,
+ * centre (uc, vc) in the plane, cartilage half-thickness wmax, median joint gap, bounding box. */
+typedef struct FebLabelFacet {
+  double c[3], n[3], e1[3], e2[3];
+  double ua, va, res, a0, b0, uc, vc, wmax, gap;
+  double xyz_lo[3], xyz_hi[3];
+  const uint8_t* F0;
+  int32_t nu, nv;
+} FebLabelFacet;
+
+/* A front grown over a facet from its edge (rb/rbgeom.py:332-342): inside when (u - uc) d0 + (v - vc) d1 <= thr;
+ * on = 0 when the covered fraction is 0.  The host forms d (unit) and thr (the fraction's quantile over the scaled
+ * footprint's pixel centres). */
+typedef struct FebLabelGrown {
+  int32_t on, pad;
+  double d[2];
+  double thr;
+} FebLabelGrown;
+
+/* Template, foot and action of one labelling call.  Template (rb/rbgeom.py:183-218): lab [dev] int8 lnx x lny x lnz
+ * (x slowest; origin o, spacing h), dt / dc [dev] float32 snx x sny x snz distances to talus / calcaneus (origin so,
+ * spacing h), facets post, mid, ant, scale centre c0, shear (z_ref, x_w0, x_w1), osteotomy plane (x_cut0, z_cut0,
+ * cut_slope, z_frag_top), static_mask bit b = body b never moves with the fragment.  Foot (rb/rbgeom.py:55-73):
+ * scale, facet factors fa / fb (post, mid, ant: size / nominal), ant_mode, ctype (0 none, 1 I, 2 II, 3 III, 4 IV),
+ * rtype (0 none, 1-4 R1-R4), sust_y, post_dome, tan_align = tan(align in rad) with align_on = (align != 0),
+ * cov_mid, fib_frac and the grown fronts of the coalitions (g_cov_mid, g_cov_post).  Action (rb/rbgeom.py:86-93):
+ * resect, interp, fusion, osteo, defect fronts (g_d_mid, g_d_post); void_fill = (defect_fill == "void"). */
+typedef struct FebLabelParams {
+  const int8_t* lab;
+  int32_t lnx, lny, lnz, pad0;
+  double o[3], h;
+  const float* dt;
+  const float* dc;
+  int32_t snx, sny, snz, pad1;
+  double so[3];
+  FebLabelFacet facet[3];
+  double c0[3], z_ref, x_w0, x_w1, x_cut0, z_cut0, cut_slope, z_frag_top;
+  uint32_t static_mask[4];
+  double scale, fa[3], fb[3];
+  int32_t ant_mode, ctype;
+  double sust_y, post_dome, tan_align;
+  int32_t align_on, rtype;
+  double cov_mid, fib_frac;
+  FebLabelGrown g_cov_mid, g_cov_post, g_d_mid, g_d_post;
+  int32_t resect, interp, fusion, void_fill;
+  double osteo;
+} FebLabelParams;
+
+/* Labels of the lattice sx x sy x sz (world frame; [dev] float64 nx, ny, nz) into L [dev] int16 nx x ny x nz
+ * (z fastest): equal to rb/rbgeom.py:358 label_points at every lattice point.  One thread per point: the inverse
+ * map into the template (scale, fragment shift, alignment shear, local warps by 3 fixed-point steps), the raster
+ * lookup, the fragment relabelling and the subtalar edits, in FP64 in the reference's operation order. */
+FEB_API int feb_label_lattice(const FebLabelParams* p, const double* sx, int32_t nx, const double* sy, int32_t ny,
+                              const double* sz, int32_t nz, int16_t* L, void* stream);
+
 /* ---------------------------------------------------------------------------------------------------------
  * Learned warm start: a 3D convolutional encoder-decoder whose prediction is the PCG initial guess.  The
  * reference has no counterpart (its PCG starts from x0 = 0 or a caller's x0, fe/gmg.py:120-137); these entry

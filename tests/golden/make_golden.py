@@ -324,8 +324,48 @@ def spring_hook():
          hook_rows=rows, hook_cols=cols, hook_vals=M.data, U=U, R=R, iters=info["iters"], ndof=info["ndof"])
 
 
+from label_cases import LABEL_CASES   # noqa: E402  (shared with the tests)
+
+
+
+def labels():
+    """label_lattice (rb/rbgeom.py:493-524) on seeded synthetic templates (comech_b200.synth.synthetic_template)
+    for feet and actions that exercise every branch of label_points; the template is handed to the reference as
+    an rbgeom.Template carrying the generated fields."""
+    import rbgeom as RB
+    from comech_b200 import labels as LB
+    out = {}
+    for seed in (0, 1):
+        T = synth.synthetic_template(seed)
+        RT = object.__new__(RB.Template)
+        for k in ("lab", "o", "h", "dt", "dc", "so", "facets", "c0", "z_ref", "x_w0", "x_w1", "x_cut0", "z_cut0",
+                  "cut_slope", "z_frag_top", "static_bodies"):
+            setattr(RT, k, getattr(T, k))
+        rng = np.random.default_rng(50 + seed)
+        # a whole-foot lattice and a fine lattice over the joint, offset from the raster
+        hx = 1.3 + 0.1 * seed
+        lat = {"foot": (np.arange(-104.0, 14.0, hx) + rng.uniform(0, 1), np.arange(-36.0, 36.0, hx) + rng.uniform(0, 1),
+                        np.arange(4.0, 104.0, hx) + rng.uniform(0, 1)),
+               "joint": (np.arange(-76.0, -14.0, 0.6) + rng.uniform(0, 0.5), np.arange(-26.0, 26.0, 0.6) + rng.uniform(0, 0.5),
+                         np.arange(40.0, 76.0, 0.6) + rng.uniform(0, 0.5))}
+        for name, fk, ak, fill in LABEL_CASES:
+            foot, act = RB.Foot(**fk), RB.Action(**ak)
+            for ln, (sx, sy, sz) in lat.items():
+                key = f"s{seed}_{name}_{ln}"
+                out[key] = RB.label_lattice(sx, sy, sz, foot, act, T=RT, defect_fill=fill).astype(np.int16)
+                if name == "default" or ln == "joint":
+                    out[f"s{seed}_{ln}_sx"], out[f"s{seed}_{ln}_sy"], out[f"s{seed}_{ln}_sz"] = sx, sy, sz
+        # a few scattered points through label_points itself
+        P = np.column_stack([rng.uniform(-80, -10, 4000), rng.uniform(-25, 25, 4000), rng.uniform(35, 80, 4000)])
+        out[f"s{seed}_points"] = P
+        for name, fk, ak, fill in LABEL_CASES:
+            out[f"s{seed}_{name}_pts"] = RB.label_points(P, RB.Foot(**fk), RB.Action(**ak), T=RT, defect_fill=fill)
+    save("labels", **out)
+
+
 if __name__ == "__main__":
     fixtures = dict(elements=elements, split=split_cases, hindfoot=hindfoot_solve, block=block_solves, patch=patch,
-                    post=post, materials=materials_case, actions=actions, spring_hook=spring_hook)
+                    post=post, materials=materials_case, actions=actions, spring_hook=spring_hook,
+                    labels=labels)
     for name in (sys.argv[1:] or list(fixtures)):
         fixtures[name]()

@@ -49,8 +49,9 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
+    from comech_b200 import labels
     structs = [_lib.FebGrid, _lib.FebOperator, _lib.FebOptions, _lib.FebInfo, _lib.FebNetGrid, _lib.FebConv,
-               _lib.FebWgrad]
+               _lib.FebWgrad, labels.FebLabelFacet, labels.FebLabelGrown, labels.FebLabelParams]
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for st in structs:
         lines.append(f'printf("{st.__name__} %zu\\n", sizeof({st.__name__}));')
