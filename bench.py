@@ -243,19 +243,28 @@ def flush_l2(buf):
 def timed_steps(fn, steps, flush, dist=None, clocks=None):
     """Device time of ``steps`` calls of fn (CUDA events on the current stream, L2 flushed before each); the
     barrier and synchronisation bracket the whole timed region.  Returns (per-step ms, last result)."""
+    import gc
     import torch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out, ms = None, []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    for _ in range(steps):
-        flush_l2(flush)
-        ev0.record()
-        out = fn()
-        ev1.record()
-        torch.cuda.synchronize()
-        ms.append(ev0.elapsed_time(ev1))
+    # the interpreter's cyclic collector is run between steps, not inside them: a collection pass over the
+    # step's large host arrays stalls the host thread that issues the step's launches
+    gc.collect()
+    gc.disable()
+    try:
+        for _ in range(steps):
+            flush_l2(flush)
+            ev0.record()
+            out = fn()
+            ev1.record()
+            torch.cuda.synchronize()
+            ms.append(ev0.elapsed_time(ev1))
+            gc.collect()
+    finally:
+        gc.enable()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -417,13 +426,20 @@ def run_ours(args, rank, world, dist):
     e2e_step()
     torch.cuda.synchronize()
     e2e_s = []
-    for _ in range(max(1, min(args.steps, 5))):
-        flush_l2(flush)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        Ue, vme, infe = e2e_step()
-        torch.cuda.synchronize()
-        e2e_s.append(time.perf_counter() - t0)
+    import gc
+    gc.collect()
+    gc.disable()            # as in timed_steps: the cyclic collector runs between steps
+    try:
+        for _ in range(max(1, min(args.steps, 5))):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Ue, vme, infe = e2e_step()
+            torch.cuda.synchronize()
+            e2e_s.append(time.perf_counter() - t0)
+            gc.collect()
+    finally:
+        gc.enable()
     ncell, ntotal, nact = g.ncell, len(P["orig"]), len(cells_h)
     h2d = (2 * ncell * 8 + ncell + ncell * 64 + ntotal * 8 + 8 * sum(len(x) for x in P["node_groups"])
            + P["loads"][0][0].size * 32 + nact * 8 + P["fixed"][0].size * 32 + P["extra"].node_coo()[4].size * 24)

@@ -630,18 +630,21 @@ __global__ void k_term_dots(SymView<T> L, int nterms, const T* __restrict__ u, c
   if (lane == 0) L.tdot[t] = L.t_lam[t] * d;
 }
 
-template <typename T, int EPI>
+// CMP: the level carries the compressed single-material blocks (tags); without them the pattern code is not
+// compiled into the kernel at all.  Offsets within the stencil planes are 32-bit (126 n < 2^31 is checked at
+// launch).
+template <typename T, int EPI, bool CMP>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
       T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
       const int* __restrict__ skip) {
   if (skip && *skip) return;
   __shared__ T red[4][3][32];
-  __shared__ T spat[2][126];
-  __shared__ T smat[128][2];
+  __shared__ T spat[2][CMP ? 126 : 1];
+  __shared__ T smat[CMP ? 128 : 1][2];
   const int lane = threadIdx.x, w = threadIdx.y;
-  const bool cmp = L.tag != nullptr;
-  if (cmp) {
+  constexpr bool cmp = CMP;
+  if constexpr (CMP) {
     const int tid = w * 32 + lane;
     for (int e = tid; e < 252; e += 128) spat[e / 126][e % 126] = L.pat[e];
     for (int e = tid; e < 256; e += 128) smat[e / 2][e % 2] = L.tmat[e];
@@ -652,8 +655,9 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
   const bool valid = i < nx;
   const int ic = valid ? i : nx - 1;
   const int n = ic + nx * (j + ny * k);
-  const int64_t N = L.n;
-  const int tn = cmp ? L.tag[n] : 0;
+  const int N = (int)L.n;
+  int tn = 0;
+  if constexpr (CMP) tn = L.tag[n];
   T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
@@ -662,29 +666,30 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
     const int o = 13 + q;
     const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
     const int off = dx + nx * (dy + ny * dz);
-    const T* B = L.S + (size_t)(q * 9) * N;
+    const T* __restrict__ B = L.S + q * 9 * N;
     const bool vf = ic + dx >= 0 && ic + dx < nx && j + dy >= 0 && j + dy < ny && k + dz < nz;
     const bool vb = q > 0 && ic - dx >= 0 && ic - dx < nx && j - dy >= 0 && j - dy < ny && k - dz >= 0;
     const int mf = vf ? n + off : n, mb = vb ? n - off : n;
     T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
     T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
     T fv[9], gv[9];
-    const int tm = cmp ? L.tag[mb] : 0;
-    if (tn) {
-      const T lam = smat[tn][0], mu = smat[tn][1];
+    int tm = 0;
+    if constexpr (CMP) tm = L.tag[mb];
+    auto stored = [&](int m, T (&v)[9]) {
 #pragma unroll
-      for (int t = 0; t < 9; ++t) fv[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
+      for (int t = 0; t < 9; ++t) v[t] = B[t * N + m];
+    };
+    if constexpr (CMP) {
+      auto formed = [&](int tg, T (&v)[9]) {
+        const T lam = smat[tg][0], mu = smat[tg][1];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) v[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
+      };
+      if (tn) formed(tn, fv); else stored(n, fv);
+      if (tm) formed(tm, gv); else stored(mb, gv);
     } else {
-#pragma unroll
-      for (int t = 0; t < 9; ++t) fv[t] = B[t * N + n];
-    }
-    if (tm) {
-      const T lam = smat[tm][0], mu = smat[tm][1];
-#pragma unroll
-      for (int t = 0; t < 9; ++t) gv[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
-    } else {
-#pragma unroll
-      for (int t = 0; t < 9; ++t) gv[t] = B[t * N + mb];
+      stored(n, fv);
+      stored(mb, gv);
     }
     const T f0 = fv[0], f1 = fv[1], f2 = fv[2], f3 = fv[3], f4 = fv[4], f5 = fv[5], f6 = fv[6], f7 = fv[7], f8 = fv[8];
     const T g0 = gv[0], g1 = gv[1], g2 = gv[2], g3 = gv[3], g4 = gv[4], g5 = gv[5], g6 = gv[6], g7 = gv[7], g8 = gv[8];
@@ -733,7 +738,7 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
     if constexpr (EPI == EPI_CHEB) {
       rold0 = r[3 * n]; rold1 = r[3 * n + 1]; rold2 = r[3 * n + 2];
       uc = u[3 * n + c]; xc = x[3 * n + c];
-      D0 = L.Dinv[(3 * c) * N + n]; D1 = L.Dinv[(3 * c + 1) * N + n]; D2 = L.Dinv[(3 * c + 2) * N + n];
+      D0 = L.Dinv[(3 * c) * N + n]; D1 = L.Dinv[(3 * c + 1) * N + n]; D2 = L.Dinv[(3 * c + 2) * N + n];   // 9 N < 2^31
     }
   }
   __syncthreads();
@@ -766,13 +771,22 @@ void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r
   if (L.tn_ptr && L.nterms > 0) {
     k_term_dots<T><<<div_up(L.nterms, 8), 256, 0, s>>>(L, L.nterms, u, skip); note_launch();
   }
-  if (epi == EPI_APPLY) {
-    k_sym<T, EPI_APPLY><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
-  } else if (epi == EPI_RESID) {
-    k_sym<T, EPI_RESID><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
-  } else {
-    k_sym<T, EPI_CHEB><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip); note_launch();
+  if (126 * L.n >= (int64_t)INT32_MAX) {   // stencil-plane offsets are 32-bit; never reached by a coarse level
+    fprintf(stderr, "launch_sym: level of %lld nodes exceeds the 32-bit stencil offsets\n", (long long)L.n);
+    return;
   }
+  const bool cmp = L.tag != nullptr;
+  if (epi == EPI_APPLY) {
+    if (cmp) k_sym<T, EPI_APPLY, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    else k_sym<T, EPI_APPLY, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+  } else if (epi == EPI_RESID) {
+    if (cmp) k_sym<T, EPI_RESID, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    else k_sym<T, EPI_RESID, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+  } else {
+    if (cmp) k_sym<T, EPI_CHEB, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    else k_sym<T, EPI_CHEB, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+  }
+  note_launch();
 }
 
 template <typename T>

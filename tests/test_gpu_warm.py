@@ -363,10 +363,14 @@ def test_packaged_network_on_held_out_instances():
     multiple (a start that needs no network).  The preparation (a K product, a V-cycle, a K product and two dot
     products) costs about one CG iteration.
 
-    Measured on 20 held-out instances (seeds 5000-5019): mean iterations 73.45 from zero, 72.15 from the learned
-    start, 72.90 from the preconditioned load.  The learned start saves about one iteration, which its preparation
-    costs again, so it gives no net gain on this hindfoot family: the count is set by the slow inter-bone modes
-    that the Krylov space finds within a few iterations whatever the start.
+    Measured on 20 held-out instances (seeds 5000-5019): mean iterations in the mixed precision 73.45 from zero,
+    72.15 from the learned start, 72.90 from the preconditioned load; in FP64 (no run-to-run rounding noise)
+    69.35 from zero, 69.00 from the learned start, 68.35 from the preconditioned load.  So the learned start
+    saves at most about one iteration, which its preparation costs again, and a start that needs no network does
+    as well: no net gain on this hindfoot family.  The count is set by the slow inter-bone modes (bones held
+    only by soft tissue, cartilage and springs) that the Krylov space finds within a few iterations whatever
+    the start; a start shortens the solve only by the log of its energy-norm error reduction over the
+    per-iteration rate (about 0.75).
 
     Bars: the prediction is within 90 % relative L2 of the FP64 solution; every solve converges; per instance the
     learned start takes at most 8 more iterations than the zero start; and on average over the six it takes no
