@@ -197,6 +197,11 @@ def device_inputs(P):
 
 
 SOLVER_OPTIONS = {}
+# The oracle's FP64 solve of the full 160x112x96 workload (bench.py --cpu-full, one B200 box's host core):
+# 72 iterations, 284.3 s (assembly 30.1, multigrid set-up 17.5, PCG 235.4, stress 1.3).  The reference arm
+# extrapolates its bounded samples to this iteration count.
+ORACLE_FULL_ITERS = 72
+ORACLE_FULL_S = 284.3
 
 
 def device_solve(P, d, precision, x0=None, warm=None):
@@ -240,9 +245,10 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
-def timed_steps(fn, steps, flush, dist=None, clocks=None):
+def timed_steps(fn, steps, flush, dist=None, clocks=None, per_step=None):
     """Device time of ``steps`` calls of fn (CUDA events on the current stream, L2 flushed before each); the
-    barrier and synchronisation bracket the whole timed region.  Returns (per-step ms, last result)."""
+    barrier and synchronisation bracket the whole timed region.  Returns (per-step ms, last result);
+    ``per_step(result)`` (optional) is appended to the list ``timed_steps.details`` after each step."""
     import gc
     import torch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -262,6 +268,8 @@ def timed_steps(fn, steps, flush, dist=None, clocks=None):
             ev1.record()
             torch.cuda.synchronize()
             ms.append(ev0.elapsed_time(ev1))
+            if per_step is not None:
+                timed_steps.details.append(per_step(out))
             gc.collect()
     finally:
         gc.enable()
@@ -353,18 +361,23 @@ def run_ours(args, rank, world, dist):
     res = {}
     launches = 0
     clk_summary = None
+    step_info = {}
+    info_of = lambda out: (round(out[2].t_setup_ms, 2), round(out[2].t_solve_ms, 2), int(out[2].iters))
     for name, pr_, w_ in arms:
         for _ in range(args.warmup):
             device_solve(P, d, pr_, warm=w_)
         torch.cuda.synchronize()
         launches0 = lib.feb_launch_count()
+        timed_steps.details = []
         if name == "headline":
             with Clocks(dev) as clk:
-                ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist)
+                ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist,
+                                      per_step=info_of)
             clk_summary = clk.summary()
             launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
         else:
-            ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist)
+            ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist, per_step=info_of)
+        step_info[name] = timed_steps.details
         U, vm, info = out
         res[name] = dict(ms=ms, U=U.cpu().numpy(), vm=vm, info=info)
     t_total = reduce_max(sum(res["headline"]["ms"]) / 1e3, dist)
@@ -492,6 +505,7 @@ def run_ours(args, rank, world, dist):
                 "l2": "flushed (256 MB write) before every step", "parallelism": f"independent solves x{world}"},
         arms_s_per_solve={k: round(v, 5) for k, v in mean_s.items()},
         arms_step_ms={k: [round(x, 2) for x in v["ms"]] for k, v in res.items()},
+        arms_step_setup_solve_iters=step_info,
         arms_iters={k: int(v["info"].iters) for k, v in res.items()},
         plain_fp64={"s_per_solve": round(mean_s["plain_fp64"], 5), "iters": int(res["plain_fp64"]["info"].iters),
                     "relres": res["plain_fp64"]["info"].relres},
@@ -703,12 +717,7 @@ def run_reference(args, rank, world):
         cpu_oracle_run(SAMPLE_SMALL)
     runs = [cpu_oracle_run(dims) for _ in range(args.steps)]
     full_ndof = workload_ndof()
-    # iterations of the workload: the oracle's count grows slowly with size; take it from the two samples'
-    # counts, log-linear in dofs (48 at 87k, 60 at 340k dofs measured; the device FP64 solve takes 72 at 5.1M)
-    small = runs[0] if dims is SAMPLE_SMALL else cpu_oracle_run(SAMPLE_SMALL)
-    big = runs[0] if dims is SAMPLE_BIG else cpu_oracle_run(SAMPLE_BIG)
-    slope = (big["iters"] - small["iters"]) / np.log(big["ndof"] / small["ndof"])
-    full_iters = int(round(big["iters"] + slope * np.log(full_ndof / big["ndof"])))
+    full_iters = ORACLE_FULL_ITERS
     est = [extrapolate(r, full_ndof, full_iters) for r in runs]
     value = float(np.mean(est))
     r0 = runs[0]
@@ -716,8 +725,9 @@ def run_reference(args, rank, world):
             f"{dims['nx']}x{dims['ny']}x{dims['nz']} h={dims['h']} ({r0['ndof']} dofs, {r0['iters']} iterations, "
             f"{r0['t']:.1f} s: assembly {r0['t_assemble']:.1f}, set-up {r0['t_setup']:.1f}, PCG {r0['t_pcg']:.1f}, "
             f"stress {r0['t_stress']:.1f}), mean of {len(runs)} steps, each extrapolated to {full_ndof} dofs and "
-            f"{full_iters} iterations (set-up phases by dofs, PCG by dofs x iterations); the full solve takes "
-            f"minutes, which the steps x warm-up protocol cannot time")
+            f"{full_iters} iterations (set-up phases by dofs, PCG by dofs x iterations; the oracle's own count on the "
+            f"full workload, measured with --cpu-full, where the whole solve took {ORACLE_FULL_S} s); the full solve "
+            f"takes minutes, which the steps x warm-up protocol cannot time")
     return dict(metric=METRIC, value=round(value, 3), unit="s/solve", n_gpus=world, steps=args.steps,
                 warmup=args.warmup, ms_per_step=round(1e3 * float(np.mean([r["t"] for r in runs])), 1),
                 higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64",

@@ -26,10 +26,10 @@ void set_last_error(const char* fmt, ...);
     }                                                                                    \
   } while (0)
 
-#define FEB_TRY(call)              \
-  do {                             \
-    int s_ = (call);               \
-    if (s_ != FEB_OK) return s_;   \
+#define FEB_TRY(call)                          \
+  do {                                         \
+    const int feb_try_st_ = (call);            \
+    if (feb_try_st_ != FEB_OK) return feb_try_st_; \
   } while (0)
 
 // host-side count of kernel launches issued by the library (feb_launch_count)

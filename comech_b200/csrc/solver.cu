@@ -82,6 +82,48 @@ namespace {
 constexpr int kMaxLevels = 8;
 
 // ------------------------------------------------------------------------------------------------ memory
+// Set-up uploads go through one process-wide pinned staging ring: a host copy into pinned memory, then an
+// asynchronous DMA, so an upload neither stalls the host on the stream nor runs at pageable-copy speed.  Each
+// staged copy records an event; before the ring wraps, the host waits for the copies issued since the last
+// wrap (any stream).  Requests larger than the ring are copied directly.
+class PinnedStaging {
+ public:
+  int copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!buf_) {
+      if (cudaMallocHost(&buf_, kCap) != cudaSuccess) { buf_ = nullptr; cudaGetLastError(); }
+    }
+    if (!buf_ || bytes > kCap) {
+      FEB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+      return FEB_OK;
+    }
+    if (off_ + bytes > kCap) {      // wrap: every copy out of the ring so far has to be done
+      for (size_t i = 0; i < used_; ++i) FEB_CUDA(cudaEventSynchronize(ev_[i]));
+      used_ = 0;
+      off_ = 0;
+    }
+    if (used_ == ev_.size()) {
+      cudaEvent_t e;
+      FEB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev_.push_back(e);
+    }
+    char* at = static_cast<char*>(buf_) + off_;
+    std::memcpy(at, src, bytes);
+    FEB_CUDA(cudaMemcpyAsync(dst, at, bytes, cudaMemcpyHostToDevice, s));
+    FEB_CUDA(cudaEventRecord(ev_[used_++], s));
+    off_ += (bytes + 255) & ~size_t(255);
+    return FEB_OK;
+  }
+
+ private:
+  static constexpr size_t kCap = size_t(32) << 20;
+  std::mutex mu_;
+  void* buf_ = nullptr;             // kept until the process exits
+  size_t off_ = 0, used_ = 0;
+  std::vector<cudaEvent_t> ev_;
+};
+PinnedStaging g_staging;
+
 class Pool {
  public:
   explicit Pool(cudaStream_t s) : s_(s) {}
@@ -107,7 +149,7 @@ class Pool {
   template <typename T>
   int upload(T** p, const T* h, size_t n) {
     FEB_TRY(alloc(p, n));
-    if (n) FEB_CUDA(cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, s_));
+    if (n) FEB_TRY(g_staging.copy(*p, h, n * sizeof(T), s_));
     return FEB_OK;
   }
   void free(void* p) {
@@ -726,6 +768,11 @@ struct FebHandle {
   int *loc_r = nullptr, *loc_c = nullptr;
   double* loc_v = nullptr;
   double* mat_all = nullptr;
+  // level-1 stencil summed directly from the fine cells, launched on a side stream while the host prepares the
+  // penalties and extra entries (A1_early, ready at A1_ev; basis: its sub-cell matrices)
+  double* A1_early = nullptr;
+  double* A1_basis = nullptr;
+  cudaEvent_t A1_ev = nullptr;
   std::vector<Level> L;
   int coarsest = 0;
   // dense coarsest level
@@ -780,6 +827,7 @@ struct FebHandle {
       if (aux[i]) { cudaStreamSynchronize(aux[i]); cudaStreamDestroy(aux[i]); }
       if (aux_ev[i]) cudaEventDestroy(aux_ev[i]);
     }
+    if (A1_ev) cudaEventDestroy(A1_ev);
     if (g_outer) cudaGraphExecDestroy(g_outer);
     if (g_inner) cudaGraphExecDestroy(g_inner);
     g_pinned.give(st_h);
@@ -1237,15 +1285,16 @@ int power_iteration(FebHandle* h, int l, double* part) {
 }
 
 // The levels' power iterations touch disjoint buffers (each level's vectors, stencil, term dots and its own
-// reduction scratch), so level k runs on side stream k and the handle's stream joins them all: the set-up
-// waits for the slowest level (level 0) instead of their sum.
+// reduction scratch), so level k runs on side stream k (power_fork); the handle's stream meanwhile builds the
+// dense coarsest level, which reads none of them, and then joins the side streams (power_join): the set-up
+// waits for the slowest of these chains instead of their sum.  No allocation is made on a side stream.
 template <typename T>
-int power_iterations(FebHandle* h) {
+int power_fork(FebHandle* h, double** part) {
   FebHandle& H = *h;
   const int nl = H.coarsest;
+  *part = nullptr;
   if (nl <= 0) return FEB_OK;
-  double* part = nullptr;
-  FEB_TRY(H.pool.alloc(&part, (size_t)kRedBlocks * nl));
+  FEB_TRY(H.pool.alloc(part, (size_t)kRedBlocks * nl));
   FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
   cudaStream_t main = H.s;
   int st = FEB_OK;
@@ -1256,13 +1305,18 @@ int power_iterations(FebHandle* h) {
     }
     FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
     H.s = H.aux[k];
-    st = power_iteration<T>(h, k, part + (size_t)kRedBlocks * k);
+    st = power_iteration<T>(h, k, *part + (size_t)kRedBlocks * k);
     H.s = main;
     FEB_CUDA(cudaEventRecord(H.aux_ev[k], H.aux[k]));
   }
-  for (int k = 0; k < nl; ++k) FEB_CUDA(cudaStreamWaitEvent(main, H.aux_ev[k], 0));
-  H.pool.free(part);
   return st;
+}
+
+int power_join(FebHandle* h, double* part) {
+  FebHandle& H = *h;
+  for (int k = 0; k < H.coarsest; ++k) FEB_CUDA(cudaStreamWaitEvent(H.s, H.aux_ev[k], 0));
+  H.pool.free(part);
+  return FEB_OK;
 }
 
 // ------------------------------------------------------------------------------------------------ autotuner
@@ -1585,6 +1639,42 @@ int setup_tc(FebHandle* h) {
   return FEB_OK;
 }
 
+// the level-1 stencil can be summed directly from the fine cells: uniform widths per axis, even cell counts,
+// isotropic model (FEB_GALERKIN_DIRECT=0 keeps the coarse-cell matrices)
+bool galerkin_direct_ok(const FebHandle& H) {
+  auto uniform = [](const std::vector<double>& e) {
+    const double w0 = e[1] - e[0];
+    for (size_t i = 0; i + 1 < e.size(); ++i)
+      if (std::fabs((e[i + 1] - e[i]) - w0) > 1e-12 * std::fabs(w0)) return false;
+    return w0 > 0.0;
+  };
+  const char* genv = std::getenv("FEB_GALERKIN_DIRECT");
+  return !(genv && genv[0] == '0') && H.mode != MAT_ORTHO && uniform(H.xe) && uniform(H.ye) && uniform(H.ze) &&
+         H.nx % 2 == 0 && H.ny % 2 == 0 && H.nz % 2 == 0;
+}
+
+// Starts the level-1 stencil of a grid that will surely be coarsened on a side stream (the last one of the
+// handle's side streams), right after the cells are prepared; build_hierarchy joins it.
+template <int MODE>
+int launch_level1_early(FebHandle& H) {
+  const int cx = H.nx / 2 + 1, cy = H.ny / 2 + 1, cz = H.nz / 2 + 1;
+  const int64_t n1 = (int64_t)cx * cy * cz;
+  FEB_TRY(H.pool.zeros(&H.A1_early, 243 * (size_t)n1));
+  FEB_TRY(H.pool.alloc(&H.A1_basis, 16 * 576));
+  const int k = FebHandle::kAux - 1;
+  if (!H.aux[k]) {
+    FEB_CUDA(cudaStreamCreateWithFlags(&H.aux[k], cudaStreamNonBlocking));
+    FEB_CUDA(cudaEventCreateWithFlags(&H.aux_ev[k], cudaEventDisableTiming));
+  }
+  if (!H.A1_ev) FEB_CUDA(cudaEventCreateWithFlags(&H.A1_ev, cudaEventDisableTiming));
+  FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
+  FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
+  const double a = H.xe[1] - H.xe[0], b = H.ye[1] - H.ye[0], c = H.ze[1] - H.ze[0];
+  FEB_TRY(launch_galerkin_direct<MODE>(H.mat_all, H.nx, H.ny, a, b, c, H.A1_basis, H.A1_early, cx, cy, cz, H.aux[k]));
+  FEB_CUDA(cudaEventRecord(H.A1_ev, H.aux[k]));
+  return FEB_OK;
+}
+
 template <int W>
 int setup_level0(FebHandle* h, const FebOperator* op) {
   FebHandle& H = *h;
@@ -1664,6 +1754,11 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     FEB_CUDA(cudaMemcpyAsync(oc.data(), H.orig_copy, oc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
     FEB_CUDA(cudaStreamSynchronize(s));
     H.orig_copy_h.assign(oc.begin(), oc.end());
+  }
+  // a grid far above the coarsest size always gets level 1: its stencil starts now, beside the host work below
+  if (H.opt.max_levels >= 2 && 3 * H.nnode > 8 * (int64_t)H.opt.min_dofs && galerkin_direct_ok(H)) {
+    if (H.mode == MAT_ISO_SRI) FEB_TRY(launch_level1_early<MAT_ISO_SRI>(H));
+    else FEB_TRY(launch_level1_early<MAT_ISO_FULL>(H));
   }
   H.stage_mark();   // 1: cells, irregular list, copies
   g_prof.mark("L0 cells/irregular/copies", s);
@@ -1774,6 +1869,9 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   FEB_TRY(setup_pair<W>(h, mat_s64));
   H.stage_mark();   // 3: used nodes, level-0 diagonal blocks, paired-row operator
   g_prof.mark("L0 local upload, diag blocks, pair operator", s);
+  // the autotuner's timings must not share the GPU with the early level-1 stencil: wait for it first (the
+  // host work of stage 2 is longer than the stencil, so this wait is normally already satisfied)
+  if (H.A1_early) FEB_CUDA(cudaStreamWaitEvent(s, H.A1_ev, 0));
   FEB_TRY(setup_tc(h));
   FEB_TRY(autotune_ku(h));
   H.stage_mark();   // 4: K.u autotuning (first handle of a grid shape only)
@@ -1858,29 +1956,30 @@ int build_hierarchy(FebHandle* h) {
     FEB_TRY(count_mask(h, C.used, C.ntotal, &kept));
     C.ndof = 3 * kept;
     g_prof.mark("Lk kept mask + count", H.s);
-    FEB_TRY(H.pool.zeros(&C.A64, 243 * (size_t)C.ntotal));
+    const bool early = l == 0 && H.A1_early && C.nx == H.nx / 2 + 1 && C.ny == H.ny / 2 + 1 && C.nz == H.nz / 2 + 1;
+    if (early) {          // the stencil was started on a side stream during the level-0 set-up
+      C.A64 = H.A1_early;
+      H.A1_early = nullptr;
+      FEB_CUDA(cudaStreamWaitEvent(H.s, H.A1_ev, 0));
+    } else {
+      FEB_TRY(H.pool.zeros(&C.A64, 243 * (size_t)C.ntotal));
+    }
     if (l == 0) {
       // uniform widths per axis, even cell counts, isotropic model: the stencil is summed directly from the
-      // fine cells' materials (FEB_GALERKIN_DIRECT=0 keeps the coarse-cell matrices); otherwise coarse-cell
-      // matrices first, then the node stencil
-      auto uniform = [](const std::vector<double>& e) {
-        const double w0 = e[1] - e[0];
-        for (size_t i = 0; i + 1 < e.size(); ++i)
-          if (std::fabs((e[i + 1] - e[i]) - w0) > 1e-12 * std::fabs(w0)) return false;
-        return w0 > 0.0;
-      };
-      const char* genv = std::getenv("FEB_GALERKIN_DIRECT");
-      const bool direct = !(genv && genv[0] == '0') && H.mode != MAT_ORTHO && uniform(H.xe) && uniform(H.ye) &&
-                          uniform(H.ze) && H.nx % 2 == 0 && H.ny % 2 == 0 && H.nz % 2 == 0 &&
-                          C.nx == H.nx / 2 + 1 && C.ny == H.ny / 2 + 1 && C.nz == H.nz / 2 + 1;
+      // fine cells' materials; otherwise coarse-cell matrices first, then the node stencil
+      const bool direct = galerkin_direct_ok(H) && C.nx == H.nx / 2 + 1 && C.ny == H.ny / 2 + 1 &&
+                          C.nz == H.nz / 2 + 1;
       if (direct) {
-        double* basis = nullptr;
-        FEB_TRY(H.pool.alloc(&basis, 16 * 576));
-        const double a = H.xe[1] - H.xe[0], b = H.ye[1] - H.ye[0], c = H.ze[1] - H.ze[0];
-        if (H.mode == MAT_ISO_SRI)
-          FEB_TRY(launch_galerkin_direct<MAT_ISO_SRI>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
-        else
-          FEB_TRY(launch_galerkin_direct<MAT_ISO_FULL>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+        double* basis = H.A1_basis;
+        H.A1_basis = nullptr;
+        if (!early) {
+          if (!basis) FEB_TRY(H.pool.alloc(&basis, 16 * 576));
+          const double a = H.xe[1] - H.xe[0], b = H.ye[1] - H.ye[0], c = H.ze[1] - H.ze[0];
+          if (H.mode == MAT_ISO_SRI)
+            FEB_TRY(launch_galerkin_direct<MAT_ISO_SRI>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+          else
+            FEB_TRY(launch_galerkin_direct<MAT_ISO_FULL>(H.mat_all, H.nx, H.ny, a, b, c, basis, C.A64, C.nx, C.ny, C.nz, H.s));
+        }
         // interior patterns of the compressed level-1 stencil (tags follow once the half stencil exists)
         const char* cenv = std::getenv("FEB_SYM_COMPRESS");   // opt-in: measured slower on the hindfoot
         if (H.pair_ok && cenv && cenv[0] == '1') {
@@ -1987,10 +2086,14 @@ int build_hierarchy(FebHandle* h) {
   // mixed solve 5 iterations (78 against 73; FP64 V-cycle 72).  FEB_POWER_FP32=1 runs them in the V-cycle's
   // precision instead (as rb/gpusolve.py:84-97 does in its multigrid dtype).
   const bool pw32 = f32 && env_flag("FEB_POWER_FP32");
-  FEB_TRY(pw32 ? power_iterations<float>(h) : power_iterations<double>(h));
-  H.stage_mark();   // 6: work vectors, power iterations
-  g_prof.mark("power iterations", H.s);
-  FEB_TRY(build_dense(h));
+  double* part = nullptr;
+  const int pst = pw32 ? power_fork<float>(h, &part) : power_fork<double>(h, &part);
+  if (pst != FEB_OK) { power_join(h, part); return pst; }
+  H.stage_mark();   // 6: work vectors, power iterations started on the side streams
+  g_prof.mark("power iterations (launched)", H.s);
+  const int dst = build_dense(h);   // concurrent with the power iterations
+  FEB_TRY(power_join(h, part));
+  FEB_TRY(dst);
   H.stage_mark();   // 7: dense coarsest level and its inverse
   g_prof.mark("dense coarsest inverse", H.s);
   for (int k = 1; k <= H.coarsest; ++k) {      // the full stencils only feed the Galerkin products
