@@ -184,8 +184,9 @@ FEB_API int feb_cell_stress(const FebGrid* grid, int32_t mat_mode, const double*
  * feb_cell_stress.  Its scratch (grid edges and cell widths) is one fixed file-scope device array:
  * at most 4096 cells per axis (larger grids: FEB_ERR_ARG), 192 KB held on every GPU that loads the
  * library until exit.  The first call on a device looks up that array's address with the device
- * current; make it before any stream capture.  All calls share the array: calls that overlap on the
- * GPU race, so order them on one stream.  No counterpart in the reference (its stress recovery is NumPy). */
+ * current.  Every call copies the grid edges from the caller's (pageable) host arrays into that array, so
+ * no call may be made under stream capture: a captured copy would read the host arrays when the graph
+ * replays.  All calls share the array: calls that overlap on the GPU race, so order them on one stream.  No counterpart in the reference (its stress recovery is NumPy). */
 FEB_API int feb_cell_stress_noalloc(const FebGrid* grid, int32_t mat_mode, const double* mat, const double* U,
                                     int64_t ncells, const int64_t* cells, const int64_t* cn, int32_t nan_to_zero,
                                     double* sig, double* vm, double* eps, void* stream);
