@@ -209,22 +209,30 @@ def device_solve(P, d, precision, x0=None, warm=None):
     trained warmnet.WarmNet) the network's prediction is the initial guess, computed inside the step."""
     from comech_b200 import engine, _lib
     g = P["grid"]
+    t = [time.perf_counter()]          # host time stamps of the phases (no synchronisation added)
     pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], precision=precision, tol=TOL,
                         maxiter=800, options=SOLVER_OPTIONS)
+    t.append(time.perf_counter())
     try:
         pr.set_rigid_groups(d["g_nodes"], offsets=d["g_off"])
+        t.append(time.perf_counter())
         f = pr.rhs([(d["l_nodes"], d["l_vals"])])
         if warm is not None and x0 is None:
             nc = g.nx * g.ny * g.nz
             x0 = warm.predict_x0(g, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
                                  d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
+        t.append(time.perf_counter())
         x, info = pr.solve(f, x0)
+        t.append(time.perf_counter())
         U = pr.export(x)
         sig, vm, eps = engine._stress(g, _lib.MAT_ISO_SRI, d["mat"], U, d["cells"], d["cn"], True, to_host=False)
+        t.append(time.perf_counter())
         return U, vm, info
     finally:
         pr.close()
+        t.append(time.perf_counter())
+        device_solve.host_ms = [round(1e3 * (b - a), 2) for a, b in zip(t, t[1:])]
 
 
 KU_PROFILE = os.path.join(HERE, "profiles", "k_fine_struct_fp32_hindfoot_160x112x96.md")
@@ -362,7 +370,10 @@ def run_ours(args, rank, world, dist):
     launches = 0
     clk_summary = None
     step_info = {}
-    info_of = lambda out: (round(out[2].t_setup_ms, 2), round(out[2].t_solve_ms, 2), int(out[2].iters))
+    # per step: device set-up and solve ms, iterations, and the host ms of create / rigid groups / rhs (+ the
+    # learned start) / solve / export + stress / close
+    info_of = lambda out: (round(out[2].t_setup_ms, 2), round(out[2].t_solve_ms, 2), int(out[2].iters),
+                           getattr(device_solve, "host_ms", None))
     for name, pr_, w_ in arms:
         for _ in range(args.warmup):
             device_solve(P, d, pr_, warm=w_)
@@ -624,6 +635,50 @@ def run_batch(args):
     return out
 
 
+LABEL_BENCH_CASES = [
+    ("plain foot", {}, {}),
+    ("coalition R2, resection", dict(ctype="I", rtype="R2", cov_mid=0.4), dict(resect=1, d_post=0.25)),
+    ("warps, valgus, osteotomy", dict(sust_y=14.0, post_dome=3.0, align=6.0), dict(osteo=5.0)),
+]
+
+
+def run_labels(args):
+    """Voxel labelling of the FE lattice (rb/rbgeom.py:493-524) on the seeded synthetic template: a 160 x 112 x 96
+    lattice at 0.5 mm over the hindfoot, for a plain foot, a coalition with its resection, and warps with a valgus
+    shear and an osteotomy.  Device: labels.label_lattice from host lattice axes to host labels (template already
+    on the device), median of 5 after a warm-up; CPU: the oracle's label_lattice, one run each; the labels are
+    compared."""
+    import torch
+    from comech_b200 import labels as LB, synth
+    from oracle import label_oracle as LO
+    T = synth.synthetic_template(0)
+    D = LB.DeviceTemplate(T)
+    sx = -100.0 + 0.5 * np.arange(160) + 0.13
+    sy = -28.0 + 0.5 * np.arange(112) + 0.21
+    sz = 20.0 + 0.5 * np.arange(96) + 0.07
+    rows, plain = [], None
+    for name, fk, ak in LABEL_BENCH_CASES:
+        foot, act = LB.Foot(**fk), LB.Action(**ak)
+        LB.label_lattice(sx, sy, sz, foot, act, device_template=D)
+        ts = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Ld = LB.label_lattice(sx, sy, sz, foot, act, device_template=D)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        Lo = LO.label_lattice(sx, sy, sz, foot, act, T)
+        tc = time.perf_counter() - t0
+        if plain is None:
+            plain = Lo
+        dev = float(np.median(ts))
+        rows.append(dict(case=name, device_ms=round(1e3 * dev, 3), cpu_s=round(tc, 3), speedup=round(tc / dev, 1),
+                         mismatches=int((Ld != Lo).sum()), edited_vs_plain=int((Lo != plain).sum())))
+    return {"mode": "labels", "lattice": [len(sx), len(sy), len(sz)], "points": int(len(sx) * len(sy) * len(sz)),
+            "cases": rows}
+
+
 def run_post(args):
     """The rows around the solve on the workload: region forces, rigid fit, relative displacement, resampling on a
     2-mm analysis grid, split connectivity and material mixing.  Device: the public calls from host arrays (inputs
@@ -750,7 +805,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-full", action="store_true",
                     help="also run the CPU oracle on the full workload (minutes): true CPU time and parity at full size")
-    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "ku-rot", "post", "batch"], default="full",
+    ap.add_argument("--mode", choices=["full", "solve-once", "ku", "ku-rot", "post", "batch", "labels"], default="full",
                     help="solve-once / ku: one device solve or a few K.u products of the workload (profiling); "
                          "post: the rows around the solve, device against the CPU oracle; batch: 64 uneven "
                          "instances with seeded actions, one at a time and 8 / 16 in flight")
@@ -789,6 +844,8 @@ def main():
             out = run_ours(args, rank, world, dist)
         elif args.mode == "post":
             out = run_post(args)
+        elif args.mode == "labels":
+            out = run_labels(args)
         else:
             out = run_profile(args)
         if dist:

@@ -544,6 +544,49 @@ __global__ void k_axpy_inplace(double* x, const double* y, int64_t n, double a) 
   if (i < n) x[i] += a * y[i];
 }
 
+// Rigid groups: per group (one CTA each) the number of its nodes that are used; a node id out of range sets
+// *bad.  Then the used nodes of the kept groups are compacted in their given order (one CTA per group, a
+// block-wide scan per chunk of 1024 entries).
+__global__ void __launch_bounds__(1024)
+k_group_count(const int64_t* __restrict__ nodes, const int64_t* __restrict__ off, const uint8_t* __restrict__ used,
+              int64_t ntotal, int* __restrict__ count, int* __restrict__ bad) {
+  const int g = blockIdx.x;
+  int c = 0;
+  for (int64_t e = off[g] + threadIdx.x; e < off[g + 1]; e += blockDim.x) {
+    const int64_t n = nodes[e];
+    if (n < 0 || n >= ntotal) { atomicExch(bad, 1); continue; }
+    c += used[n] ? 1 : 0;
+  }
+  c = block_sum(c);
+  if (threadIdx.x == 0) count[g] = c;
+}
+
+__global__ void __launch_bounds__(1024)
+k_group_compact(const int64_t* __restrict__ nodes, const int64_t* __restrict__ off, const uint8_t* __restrict__ used,
+                const int* __restrict__ dst_off, int64_t* __restrict__ out) {
+  const int g = blockIdx.x;
+  if (dst_off[g] < 0) return;           // dropped group
+  __shared__ int warp_tot[32];
+  __shared__ int base;
+  if (threadIdx.x == 0) base = dst_off[g];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int64_t e0 = off[g]; e0 < off[g + 1]; e0 += blockDim.x) {
+    const int64_t e = e0 + threadIdx.x;
+    const bool keep = e < off[g + 1] && used[nodes[e]];
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    const int before = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) warp_tot[w] = __popc(m);
+    __syncthreads();
+    int prefix = 0, total = 0;
+    for (int q = 0; q < nw; ++q) { prefix += q < w ? warp_tot[q] : 0; total += warp_tot[q]; }
+    if (keep) out[base + prefix + before] = nodes[e];
+    __syncthreads();
+    if (threadIdx.x == 0) base += total;
+    __syncthreads();
+  }
+}
+
 __global__ void k_masked_copy(const double* __restrict__ src, const uint8_t* __restrict__ used, int64_t n,
                               double* __restrict__ dst) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -2348,33 +2391,36 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   if (H.g_outer) { cudaGraphExecDestroy(H.g_outer); H.g_outer = nullptr; }
   if (H.g_inner) { cudaGraphExecDestroy(H.g_inner); H.g_inner = nullptr; }
   if (ngroups == 0) return FEB_OK;
-  // keep used nodes of every group, drop groups with fewer than 4 (rb/splitfe.py:105-112)
-  const int64_t total = offsets[ngroups];
-  std::vector<int64_t> nh(total);
-  FEB_CUDA(cudaMemcpyAsync(nh.data(), nodes, total * sizeof(int64_t), cudaMemcpyDeviceToHost, H.s));
-  std::vector<uint8_t> used(H.ntotal);
-  FEB_CUDA(cudaMemcpyAsync(used.data(), H.L[0].used, H.ntotal, cudaMemcpyDeviceToHost, H.s));
+  // keep used nodes of every group, drop groups with fewer than 4 (rb/splitfe.py:105-112); the filtering and
+  // the compaction run on the device, the host sees the per-group counts only
+  std::vector<int64_t> off_in(offsets, offsets + ngroups + 1);
+  int64_t* d_off_in = nullptr;
+  int *d_count = nullptr, *d_dst = nullptr;
+  FEB_TRY(H.pool.upload(&d_off_in, off_in.data(), off_in.size()));
+  FEB_TRY(H.pool.zeros(&d_count, (size_t)ngroups + 1));     // counts, then the out-of-range flag
+  k_group_count<<<ngroups, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, H.ntotal, d_count, d_count + ngroups);
+  note_launch();
+  std::vector<int> cnt(ngroups + 1);
+  FEB_CUDA(cudaMemcpyAsync(cnt.data(), d_count, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, H.s));
   FEB_CUDA(cudaStreamSynchronize(H.s));
-  std::vector<int> off(1, 0);
-  std::vector<int64_t> kept;
+  if (cnt[ngroups]) { set_last_error("feb_set_rigid_groups: a group node is out of range"); return FEB_ERR_ARG; }
+  std::vector<int> off(1, 0), dst(ngroups, -1);
   for (int g = 0; g < ngroups; ++g) {
-    std::vector<int64_t> gn;
-    for (int64_t e = offsets[g]; e < offsets[g + 1]; ++e) {
-      int64_t n = nh[e];
-      if (n < 0 || n >= H.ntotal) { set_last_error("group node %lld out of range", (long long)n); return FEB_ERR_ARG; }
-      if (used[n]) gn.push_back(n);
-    }
-    if (gn.size() < 4) continue;
-    kept.insert(kept.end(), gn.begin(), gn.end());
-    off.push_back((int)kept.size());
+    if (cnt[g] < 4) continue;
+    dst[g] = off.back();
+    off.push_back(off.back() + cnt[g]);
   }
   const int G = (int)off.size() - 1;
   if (G == 0) return FEB_OK;
+  const int64_t nkept = off.back();
   int* doff;
   int64_t* dnodes;
   double* cen;
+  FEB_TRY(H.pool.upload(&d_dst, dst.data(), dst.size()));
   FEB_TRY(H.pool.upload(&doff, off.data(), off.size()));
-  FEB_TRY(H.pool.upload(&dnodes, kept.data(), kept.size()));
+  FEB_TRY(H.pool.alloc(&dnodes, (size_t)nkept));
+  k_group_compact<<<ngroups, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, d_dst, dnodes);
+  note_launch();
   FEB_TRY(H.pool.alloc(&cen, 3 * (size_t)G));
   RigidView& Z = H.Z;
   Z.ngroups = G; Z.off = doff; Z.nodes = dnodes; Z.cen = cen;
@@ -2384,26 +2430,32 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   FEB_TRY(H.pool.alloc(&H.zpart, (size_t)rigid_blocks(Z) * G * 6));
   launch_centroids(Z, cen, H.zpart, H.s);
   double* rho = nullptr;
-  FEB_TRY(H.pool.alloc(&rho, 3 * kept.size()));
+  FEB_TRY(H.pool.alloc(&rho, 3 * (size_t)nkept));
   Z.rho = rho;
   launch_rigid_rho(Z, rho, H.s);
   FEB_TRY(H.pool.alloc(&H.zr, nc));
   FEB_TRY(H.pool.alloc(&H.zcoef, nc));
-  // Ec = Z^T K Z column by column (FP64 matrix-free K)
+  // Ec = Z^T K Z column by column (FP64 matrix-free K); the columns stay on the device until one read-back
   std::vector<double> Ec((size_t)nc * nc);
-  double *col, *kcol;
+  double *col, *kcol, *Ecd;
   FEB_TRY(H.pool.alloc(&col, 3 * (size_t)H.ntotal));
   FEB_TRY(H.pool.alloc(&kcol, 3 * (size_t)H.ntotal));
+  FEB_TRY(H.pool.alloc(&Ecd, (size_t)nc * nc));
   for (int c = 0; c < nc; ++c) {
     FEB_CUDA(cudaMemsetAsync(col, 0, 3 * (size_t)H.ntotal * sizeof(double), H.s));
     launch_z_column(Z, c, col, H.s);
     H.apply<double>(0, col, kcol, nullptr);
     launch_ztr(Z, kcol, H.zpart, H.zr, H.s);
-    FEB_CUDA(cudaMemcpyAsync(&Ec[(size_t)c * nc], H.zr, nc * sizeof(double), cudaMemcpyDeviceToHost, H.s));
+    FEB_CUDA(cudaMemcpyAsync(Ecd + (size_t)c * nc, H.zr, nc * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
   }
+  FEB_CUDA(cudaMemcpyAsync(Ec.data(), Ecd, Ec.size() * sizeof(double), cudaMemcpyDeviceToHost, H.s));
   FEB_CUDA(cudaStreamSynchronize(H.s));
   H.pool.free(col);
   H.pool.free(kcol);
+  H.pool.free(Ecd);
+  H.pool.free(d_off_in);
+  H.pool.free(d_count);
+  H.pool.free(d_dst);
   std::vector<double> Es((size_t)nc * nc);
   for (int i = 0; i < nc; ++i)
     for (int j = 0; j < nc; ++j) Es[(size_t)i * nc + j] = 0.5 * (Ec[(size_t)i * nc + j] + Ec[(size_t)j * nc + i]);

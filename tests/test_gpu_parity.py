@@ -359,3 +359,28 @@ def test_split_connectivity_on_device_bit_exact(golden, case):
     assert (cn == z[f"{case}_cn"]).all()
     assert (orig == z[f"{case}_orig"]).all()
     assert ns == int(z[f"{case}_nsplit"])
+
+
+def test_rigid_groups_filtering_on_the_device(golden):
+    """feb_set_rigid_groups keeps the used nodes of every group in their given order and drops groups with fewer
+    than 4 of them (rb/splitfe.py:105-112): adding a group of unused nodes and a 3-node group, and unused nodes
+    inside a real group, leaves the solve unchanged; a node id out of range is an argument error."""
+    from comech_b200 import _lib
+    z, g = _hindfoot(golden)
+    args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
+            [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z))
+    groups = _groups(z)
+    U0, i0, _ = engine.solve_cn(*args, groups, tol=1e-10)
+    used = np.zeros(len(z["orig"]), bool)
+    used[np.unique(z["cn"][np.flatnonzero(z["active"])])] = True
+    unused = np.flatnonzero(~used)
+    padded = [np.concatenate([unused[:5], np.asarray(gr), unused[5:9]]) for gr in groups]
+    extra = padded + [unused[10:40], np.asarray(groups[0])[:3]]
+    U1, i1, _ = engine.solve_cn(*args, extra, tol=1e-10)
+    assert i1["flag"] == 0 and abs(i1["iters"] - i0["iters"]) <= 1
+    ok = np.isfinite(U0)
+    assert rel(U1[ok], U0[ok]) < 1e-10
+    with engine.Problem(g, _lib.MAT_ISO_SRI, np.concatenate([z["lam"], z["mu"]]), z["active"], cn=z["cn"],
+                        orig=z["orig"], options=dict(max_levels=0)) as P:
+        with pytest.raises(_lib.FebError):
+            P.set_rigid_groups([np.array([0, 1, 2, len(z["orig"]) + 5])])
