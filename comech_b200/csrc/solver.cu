@@ -228,15 +228,18 @@ void coo_merge(Entries& E) {
     any_or |= key[i];
     any_and &= key[i];
   }
-  std::vector<uint32_t> cnt(1 << 16);
-  for (int shift = 0; shift < 64; shift += 16) {
-    if ((((any_or ^ any_and) >> shift) & 0xFFFF) == 0) continue;     // digit constant over all keys
+  // LSD radix sort with 11-bit digits (the histogram stays in L1); digits constant over all keys are skipped
+  constexpr int kBits = 11;
+  constexpr uint64_t kMask = (1u << kBits) - 1;
+  std::vector<uint32_t> cnt(size_t(1) << kBits);
+  for (int shift = 0; shift < 64; shift += kBits) {
+    if ((((any_or ^ any_and) >> shift) & kMask) == 0) continue;
     std::fill(cnt.begin(), cnt.end(), 0u);
-    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> shift) & 0xFFFF]++;
+    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> shift) & kMask]++;
     uint32_t sum = 0;
     for (auto& c : cnt) { const uint32_t t = c; c = sum; sum += t; }
     for (size_t i = 0; i < n; ++i) {
-      const uint32_t at = cnt[(key[i] >> shift) & 0xFFFF]++;
+      const uint32_t at = cnt[(key[i] >> shift) & kMask]++;
       k2[at] = key[i];
       i2[at] = idx[i];
     }
@@ -612,6 +615,7 @@ int upload_csr(Pool& pool, const Entries& E, Csr& C) {
   std::vector<int> rd, rp, cl;
   std::vector<double> v;
   std::vector<float> vf;
+  cl.reserve(E.size()); v.reserve(E.size()); vf.reserve(E.size());
   for (size_t e = 0; e < E.size(); ++e) {
     if (rd.empty() || rd.back() != E.r[e]) { rd.push_back((int)E.r[e]); rp.push_back((int)e); }
     cl.push_back((int)E.c[e]);
@@ -1822,6 +1826,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   std::vector<int> pn;
   std::vector<double> pk;
   std::vector<float> pkf;
+  pn.reserve(op->npen); pk.reserve(3 * op->npen); pkf.reserve(3 * op->npen);
   for (int64_t e2 = 0; e2 < op->npen; ++e2) {
     int64_t node = op->pen_node[e2];
     if (node < 0 || node >= H.ntotal) { set_last_error("penalty node %lld out of range", (long long)node); return FEB_ERR_ARG; }
@@ -1859,13 +1864,21 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   const int gx = H.nx + 1, gy = H.ny + 1;
   auto pos = [&](int64_t node) { return node < H.nnode ? node : H.orig_copy_h[node - H.nnode]; };
   std::vector<char> is_local(ex.size());
+  // grid coordinates by 32-bit unsigned division (grid node ids are below 2^31): two divisions per node
+  const uint32_t ugx = (uint32_t)gx, ugy = (uint32_t)gy;
+  auto coords = [&](int64_t node, int& x, int& y, int& z) {
+    const uint32_t a = (uint32_t)pos(node), q = a / ugx;
+    x = int(a - q * ugx); z = int(q / ugy); y = int(q - (uint32_t)z * ugy);
+  };
   for (size_t e2 = 0; e2 < ex.size(); ++e2) {
-    int64_t a = pos(ex.r[e2] / 3), b = pos(ex.c[e2] / 3);
-    int da = int(a % gx) - int(b % gx), db = int((a / gx) % gy) - int((b / gx) % gy), dc = int(a / ((int64_t)gx * gy)) - int(b / ((int64_t)gx * gy));
-    is_local[e2] = std::abs(da) <= 1 && std::abs(db) <= 1 && std::abs(dc) <= 1;
+    int ax, ay, az, bx, by, bz;
+    coords(ex.r[e2] / 3, ax, ay, az);
+    coords(ex.c[e2] / 3, bx, by, bz);
+    is_local[e2] = std::abs(ax - bx) <= 1 && std::abs(ay - by) <= 1 && std::abs(az - bz) <= 1;
   }
+  g_prof.mark("L0 extra classify", s);
   std::vector<char> taken = factor_nonlocal(ex, is_local, V.terms);
-  g_prof.mark("L0 extra classify + factor", s);
+  g_prof.mark("L0 extra factor", s);
   for (size_t e2 = 0; e2 < ex.size(); ++e2) {
     if (taken[e2]) continue;
     Entries& dst = is_local[e2] ? loc : V.nonlocal;
