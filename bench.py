@@ -235,7 +235,7 @@ def device_solve(P, d, precision, x0=None, warm=None):
         device_solve.host_ms = [round(1e3 * (b - a), 2) for a, b in zip(t, t[1:])]
 
 
-KU_PROFILE = os.path.join(HERE, "profiles", "k_fine_struct_fp32_hindfoot_160x112x96.md")
+KU_PROFILE = os.path.join(HERE, "profiles", "k_fine_pair_apply_fp32_hindfoot_160x112x96.md")
 
 
 def ku_traffic():
