@@ -43,7 +43,7 @@ class FebOptions(C.Structure):
     _fields_ = [("precision", C.c_int32), ("maxiter", C.c_int32), ("tol", C.c_double), ("min_dofs", C.c_int32),
                 ("max_levels", C.c_int32), ("cheb_degree", C.c_int32), ("check_every", C.c_int32),
                 ("inner_tol", C.c_double), ("inner_maxiter", C.c_int32), ("use_graphs", C.c_int32),
-                ("seed", C.c_uint64), ("x0_mode", C.c_int32), ("pad_", C.c_int32)]
+                ("seed", C.c_uint64), ("x0_mode", C.c_int32), ("level_kernel", C.c_int32)]
 
 
 class FebInfo(C.Structure):

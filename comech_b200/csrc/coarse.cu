@@ -442,6 +442,7 @@ __global__ void k_sym_tags(const double* __restrict__ S64, int cnx, int cny, int
   const int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (J >= n) return;
   const int jx = int(J % cnx), jy = int((J / cnx) % cny), jz = int(J / ((int64_t)cnx * cny));
+  const int64_t np = sym_np(cnx, cny, cnz), P = jx + (int64_t)sym_nxp(cnx) * (jy + (int64_t)cny * jz);
   // fine cell (2 jx, 2 jy, 2 jz): row 2 jy is the upper byte of row pair m = jy
   uint32_t id = 0;
   if (jy < mp) id = (cellpair[2 * jx + (int64_t)fnxn * (jy + (int64_t)mp * (2 * jz))] >> 8) & 0x7fu;
@@ -452,7 +453,7 @@ __global__ void k_sym_tags(const double* __restrict__ S64, int cnx, int cny, int
     for (int e = 0; e < 126; ++e) scale = fmax(scale, fabs(lam * pat[e]) + fabs(mu * pat[126 + e]));
     bool same = scale > 0.0;
     for (int e = 0; e < 126 && same; ++e)
-      same = fabs(S64[(size_t)e * n + J] - (lam * pat[e] + mu * pat[126 + e])) <= 1e-12 * scale;
+      same = fabs(S64[(size_t)e * np + P] - (lam * pat[e] + mu * pat[126 + e])) <= 1e-12 * scale;
     t = same ? (uint8_t)id : 0;
   }
   tag[J] = t;
@@ -600,12 +601,18 @@ __global__ void k_block_inverse(const double* __restrict__ D, int64_t n, double*
   }
 }
 
+// one thread per padded position p; padding positions (i >= nx) are written zero
 template <typename T>
-__global__ void k_stencil_to_sym(const double* __restrict__ A, int64_t n, T* __restrict__ S) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  for (int o = 13; o < 27; ++o)
-    for (int t = 0; t < 9; ++t) S[(size_t)((o - 13) * 9 + t) * n + i] = T(A[(size_t)(o * 9 + t) * n + i]);
+__global__ void k_stencil_to_sym(const double* __restrict__ A, int nx, int nxp, int64_t n, int64_t np,
+                                 T* __restrict__ S) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int64_t row = p / nxp;
+  const int i = int(p - row * nxp);
+  const int64_t m = row * nx + i;
+  for (int q = 0; q < 14; ++q)
+    for (int t = 0; t < 9; ++t)
+      S[(size_t)(q * 9 + t) * np + p] = i < nx ? T(A[(size_t)((q + 13) * 9 + t) * n + m]) : T(0);
 }
 
 // Stencil product of a symmetric half-stored level with a fused epilogue.
@@ -630,10 +637,60 @@ __global__ void k_term_dots(SymView<T> L, int nterms, const T* __restrict__ u, c
   if (lane == 0) L.tdot[t] = L.t_lam[t] * d;
 }
 
+// Slot Q (offset o = 13 + Q) of one node: the forward block stored at the node times u at n + off, and, for
+// Q > 0, the forward block stored at n - off, transposed, times u there.  Out-of-range neighbours are clamped
+// to the node itself and their u zeroed, so the loads carry no branches.  Q is a compile-time constant: the
+// offsets, the bounds tests and the plane offsets fold.  CMP: blocks of tagged (single-material) nodes are
+// formed from the patterns sp[2][126] and the material table sm[128][2] (shared memory) instead of read.
+template <typename T, bool CMP, int Q>
+__device__ __forceinline__ void sym_slot(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
+                                         int k, int tn, const T* sp, const T* sm, T& a0, T& a1, T& a2) {
+  constexpr int o = 13 + Q;
+  constexpr int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+  const int nx = L.nx, ny = L.ny, nz = L.nz, nxp = L.nxp, NP = (int)L.np;
+  const int off = dx + nx * (dy + ny * dz), offp = dx + nxp * (dy + ny * dz);
+  const T* __restrict__ B = L.S + (size_t)Q * 9 * NP;
+  bool vf = true, vb = Q > 0;
+  if constexpr (dx > 0) { vf = vf && ic + 1 < nx; vb = vb && ic >= 1; }
+  if constexpr (dx < 0) { vf = vf && ic >= 1; vb = vb && ic + 1 < nx; }
+  if constexpr (dy > 0) { vf = vf && j + 1 < ny; vb = vb && j >= 1; }
+  if constexpr (dy < 0) { vf = vf && j >= 1; vb = vb && j + 1 < ny; }
+  if constexpr (dz > 0) { vf = vf && k + 1 < nz; vb = vb && k >= 1; }
+  const int mf = vf ? n + off : n;
+  T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
+  if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
+  T fv[9];
+  auto stored = [&](int m, T (&v)[9]) {     // m: padded position
+#pragma unroll
+    for (int t = 0; t < 9; ++t) v[t] = B[(size_t)t * NP + m];
+  };
+  auto formed = [&](int tg, T (&v)[9]) {
+    const T lam = sm[2 * tg], mu = sm[2 * tg + 1];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) v[t] = lam * sp[9 * Q + t] + mu * sp[126 + 9 * Q + t];
+  };
+  if constexpr (CMP) { if (tn) formed(tn, fv); else stored(pn, fv); }
+  else stored(pn, fv);
+  a0 += fv[0] * uf0 + fv[1] * uf1 + fv[2] * uf2;
+  a1 += fv[3] * uf0 + fv[4] * uf1 + fv[5] * uf2;
+  a2 += fv[6] * uf0 + fv[7] * uf1 + fv[8] * uf2;
+  if constexpr (Q > 0) {
+    const int mb = vb ? n - off : n, pb = vb ? pn - offp : pn;
+    T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
+    if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
+    T gv[9];
+    if constexpr (CMP) { const int tm = L.tag[mb]; if (tm) formed(tm, gv); else stored(pb, gv); }
+    else stored(pb, gv);
+    a0 += gv[0] * ub0 + gv[3] * ub1 + gv[6] * ub2;
+    a1 += gv[1] * ub0 + gv[4] * ub1 + gv[7] * ub2;
+    a2 += gv[2] * ub0 + gv[5] * ub1 + gv[8] * ub2;
+  }
+}
+
 // CMP: the level carries the compressed single-material blocks (tags); without them the pattern code is not
-// compiled into the kernel at all.  Offsets within the stencil planes are 32-bit (126 n < 2^31 is checked at
-// launch).
-template <typename T, int EPI, bool CMP>
+// compiled into the kernel at all.  Offsets within the stencil planes are 32-bit (126 x the padded node count
+// < 2^31 is checked at launch).
+template <typename T, int EPI, bool CMP, bool CT>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
       T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
@@ -643,7 +700,6 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
   __shared__ T spat[2][CMP ? 126 : 1];
   __shared__ T smat[CMP ? 128 : 1][2];
   const int lane = threadIdx.x, w = threadIdx.y;
-  constexpr bool cmp = CMP;
   if constexpr (CMP) {
     const int tid = w * 32 + lane;
     for (int e = tid; e < 252; e += 128) spat[e / 126][e % 126] = L.pat[e];
@@ -656,48 +712,62 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
   const int ic = valid ? i : nx - 1;
   const int n = ic + nx * (j + ny * k);
   const int N = (int)L.n;
+  const int nxp = L.nxp, NP = (int)L.np;          // row-padded stencil planes
+  const int pn = ic + nxp * (j + ny * k);
   int tn = 0;
   if constexpr (CMP) tn = L.tag[n];
   T a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const int q = w + 4 * t;
-    if (q > 13) break;                                     // warp-uniform (t == 3, w >= 2)
-    const int o = 13 + q;
-    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
-    const int off = dx + nx * (dy + ny * dz);
-    const T* __restrict__ B = L.S + q * 9 * N;
-    const bool vf = ic + dx >= 0 && ic + dx < nx && j + dy >= 0 && j + dy < ny && k + dz < nz;
-    const bool vb = q > 0 && ic - dx >= 0 && ic - dx < nx && j - dy >= 0 && j - dy < ny && k - dz >= 0;
-    const int mf = vf ? n + off : n, mb = vb ? n - off : n;
-    T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
-    T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
-    T fv[9], gv[9];
-    int tm = 0;
-    if constexpr (CMP) tm = L.tag[mb];
-    auto stored = [&](int m, T (&v)[9]) {
-#pragma unroll
-      for (int t = 0; t < 9; ++t) v[t] = B[t * N + m];
-    };
-    if constexpr (CMP) {
-      auto formed = [&](int tg, T (&v)[9]) {
-        const T lam = smat[tg][0], mu = smat[tg][1];
-#pragma unroll
-        for (int t = 0; t < 9; ++t) v[t] = lam * spat[0][9 * q + t] + mu * spat[1][9 * q + t];
-      };
-      if (tn) formed(tn, fv); else stored(n, fv);
-      if (tm) formed(tm, gv); else stored(mb, gv);
-    } else {
-      stored(n, fv);
-      stored(mb, gv);
+  const T* sp = CMP ? &spat[0][0] : nullptr;
+  const T* sm = CMP ? &smat[0][0] : nullptr;
+  if constexpr (CT) {
+    // the 14 slots over the 4 warps (warp-uniform switch): 0 4 8 12 | 1 5 9 13 | 2 6 10 | 3 7 11
+#define FEB_SLOT(Q) sym_slot<T, CMP, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, a0, a1, a2)
+    switch (w) {
+      case 0: FEB_SLOT(0); FEB_SLOT(4); FEB_SLOT(8); FEB_SLOT(12); break;
+      case 1: FEB_SLOT(1); FEB_SLOT(5); FEB_SLOT(9); FEB_SLOT(13); break;
+      case 2: FEB_SLOT(2); FEB_SLOT(6); FEB_SLOT(10); break;
+      default: FEB_SLOT(3); FEB_SLOT(7); FEB_SLOT(11); break;
     }
-    const T f0 = fv[0], f1 = fv[1], f2 = fv[2], f3 = fv[3], f4 = fv[4], f5 = fv[5], f6 = fv[6], f7 = fv[7], f8 = fv[8];
-    const T g0 = gv[0], g1 = gv[1], g2 = gv[2], g3 = gv[3], g4 = gv[4], g5 = gv[5], g6 = gv[6], g7 = gv[7], g8 = gv[8];
-    if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
-    if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
-    a0 += f0 * uf0 + f1 * uf1 + f2 * uf2 + g0 * ub0 + g3 * ub1 + g6 * ub2;
-    a1 += f3 * uf0 + f4 * uf1 + f5 * uf2 + g1 * ub0 + g4 * ub1 + g7 * ub2;
-    a2 += f6 * uf0 + f7 * uf1 + f8 * uf2 + g2 * ub0 + g5 * ub1 + g8 * ub2;
+#undef FEB_SLOT
+  } else {
+    // the same slots with the slot index a run-time value (the loop keeps every slot's loads in flight together)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int q = w + 4 * t;
+      if (q > 13) break;                                     // warp-uniform (t == 3, w >= 2)
+      const int o = 13 + q;
+      const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+      const int off = dx + nx * (dy + ny * dz), offp = dx + nxp * (dy + ny * dz);
+      const T* __restrict__ B = L.S + q * 9 * NP;
+      const bool vf = ic + dx >= 0 && ic + dx < nx && j + dy >= 0 && j + dy < ny && k + dz < nz;
+      const bool vb = q > 0 && ic - dx >= 0 && ic - dx < nx && j - dy >= 0 && j - dy < ny && k - dz >= 0;
+      const int mf = vf ? n + off : n, mb = vb ? n - off : n, pb = vb ? pn - offp : pn;
+      T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
+      T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
+      T fv[9], gv[9];
+      auto stored = [&](int m, T (&v)[9]) {     // m: padded position
+#pragma unroll
+        for (int tt = 0; tt < 9; ++tt) v[tt] = B[tt * NP + m];
+      };
+      if constexpr (CMP) {
+        auto formed = [&](int tg, T (&v)[9]) {
+          const T lam = sm[2 * tg], mu = sm[2 * tg + 1];
+#pragma unroll
+          for (int tt = 0; tt < 9; ++tt) v[tt] = lam * sp[9 * q + tt] + mu * sp[126 + 9 * q + tt];
+        };
+        const int tm = L.tag[mb];
+        if (tn) formed(tn, fv); else stored(pn, fv);
+        if (tm) formed(tm, gv); else stored(pb, gv);
+      } else {
+        stored(pn, fv);
+        stored(pb, gv);
+      }
+      if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
+      if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
+      a0 += fv[0] * uf0 + fv[1] * uf1 + fv[2] * uf2 + gv[0] * ub0 + gv[3] * ub1 + gv[6] * ub2;
+      a1 += fv[3] * uf0 + fv[4] * uf1 + fv[5] * uf2 + gv[1] * ub0 + gv[4] * ub1 + gv[7] * ub2;
+      a2 += fv[6] * uf0 + fv[7] * uf1 + fv[8] * uf2 + gv[2] * ub0 + gv[5] * ub1 + gv[8] * ub2;
+    }
   }
   if (L.node_ptr) {
     int beg = 0, end = 0;
@@ -771,27 +841,30 @@ void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r
   if (L.tn_ptr && L.nterms > 0) {
     k_term_dots<T><<<div_up(L.nterms, 8), 256, 0, s>>>(L, L.nterms, u, skip); note_launch();
   }
-  if (126 * L.n >= (int64_t)INT32_MAX) {   // stencil-plane offsets are 32-bit; never reached by a coarse level
+  if (126 * L.np >= (int64_t)INT32_MAX) {  // stencil-plane offsets are 32-bit; never reached by a coarse level
     fprintf(stderr, "launch_sym: level of %lld nodes exceeds the 32-bit stencil offsets\n", (long long)L.n);
     return;
   }
   const bool cmp = L.tag != nullptr;
+  const bool ct = L.slots == 2 || (L.slots == 0 && std::is_same<T, float>::value);
+#define FEB_SYM(E, C, CT_) k_sym<T, E, C, CT_><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip)
+#define FEB_SYM2(E, C) do { if (ct) FEB_SYM(E, C, true); else FEB_SYM(E, C, false); } while (0)
   if (epi == EPI_APPLY) {
-    if (cmp) k_sym<T, EPI_APPLY, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
-    else k_sym<T, EPI_APPLY, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    if (cmp) FEB_SYM2(EPI_APPLY, true); else FEB_SYM2(EPI_APPLY, false);
   } else if (epi == EPI_RESID) {
-    if (cmp) k_sym<T, EPI_RESID, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
-    else k_sym<T, EPI_RESID, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    if (cmp) FEB_SYM2(EPI_RESID, true); else FEB_SYM2(EPI_RESID, false);
   } else {
-    if (cmp) k_sym<T, EPI_CHEB, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
-    else k_sym<T, EPI_CHEB, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip);
+    if (cmp) FEB_SYM2(EPI_CHEB, true); else FEB_SYM2(EPI_CHEB, false);
   }
+#undef FEB_SYM2
+#undef FEB_SYM
   note_launch();
 }
 
 template <typename T>
-void launch_stencil_to_sym(const double* A, int64_t n, T* S, cudaStream_t s) {
-  k_stencil_to_sym<T><<<div_up(n, kThreads), kThreads, 0, s>>>(A, n, S); note_launch();
+void launch_stencil_to_sym(const double* A, int nx, int ny, int nz, T* S, cudaStream_t s) {
+  const int64_t n = (int64_t)nx * ny * nz, np = sym_np(nx, ny, nz);
+  k_stencil_to_sym<T><<<div_up(np, kThreads), kThreads, 0, s>>>(A, nx, sym_nxp(nx), n, np, S); note_launch();
 }
 
 template void launch_sym<float>(const SymView<float>&, int, const float*, float*, const float*, float*, float*,
@@ -805,8 +878,8 @@ void launch_galerkin_axis(const AxisDev& ax, int d, const double* Ain, int inx, 
   note_launch();
 }
 
-template void launch_stencil_to_sym<float>(const double*, int64_t, float*, cudaStream_t);
-template void launch_stencil_to_sym<double>(const double*, int64_t, double*, cudaStream_t);
+template void launch_stencil_to_sym<float>(const double*, int, int, int, float*, cudaStream_t);
+template void launch_stencil_to_sym<double>(const double*, int, int, int, double*, cudaStream_t);
 
 template <typename T>
 void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s) {

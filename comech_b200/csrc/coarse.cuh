@@ -36,13 +36,22 @@ template <typename T>
 void launch_stencil_apply(const StencilView<T>& L, const T* u, T* y, const int* skip, cudaStream_t s);
 
 // Symmetric half storage of a stencil level: blocks of the offsets o = 13..26 (self and the 13 "forward"
-// neighbours) as S[(o-13)*9 + 3r + c][n]; the block of a backward offset o' < 13 is the transpose of the
-// forward block stored at the neighbour.  Entries the stencil cannot hold are a per-node CSR:
+// neighbours) as S[(o-13)*9 + 3r + c][p]; the block of a backward offset o' < 13 is the transpose of the
+// forward block stored at the neighbour.  The node axis p is row-padded: p = i + nxp (j + ny k) with
+// nxp = nx rounded up to a multiple of 4 (padding zero), so that every row of every plane starts 16-byte
+// aligned.  Entries the stencil cannot hold are a per-node CSR (natural node ids):
 // entries node_ptr[n] .. node_ptr[n+1] with row component ent_r, column dof ent_col, value ent_v.
+__host__ __device__ inline int sym_nxp(int nx) { return (nx + 3) & ~3; }
+__host__ __device__ inline int64_t sym_np(int nx, int ny, int nz) { return (int64_t)sym_nxp(nx) * ny * nz; }
+
 template <typename T>
 struct SymView {
   int nx, ny, nz;
   int64_t n;
+  int nxp = 0;             // padded row length of S
+  int64_t np = 0;          // padded node count: the stride of S's planes
+  int slots = 0;           // the product's slot index: 0 compile-time in FP32, run-time in FP64; 1 run-time;
+                           // 2 compile-time
   const T* S;
   const int* node_ptr;     // nullptr when there are no such entries
   const int8_t* ent_r;
@@ -76,9 +85,9 @@ struct LevelParams;
 template <typename T>
 void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
                 const LevelParams* lp, int k, const int* skip, cudaStream_t s);
-// full [243][n] FP64 stencil -> half storage in T
+// full [243][n] FP64 stencil of an nx x ny x nz level -> row-padded half storage in T ([126][sym_np])
 template <typename T>
-void launch_stencil_to_sym(const double* A, int64_t n, T* S, cudaStream_t s);
+void launch_stencil_to_sym(const double* A, int nx, int ny, int nz, T* S, cudaStream_t s);
 
 template <typename T>
 void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,
@@ -118,8 +127,8 @@ int launch_galerkin_direct(const double* mat_all, int fnx, int fny, double a, do
 // launch_galerkin_direct: pat[m][126] (m = 0 lam, 1 mu), same layout as the half storage.
 void launch_sym_pattern(const double* basis, double* pat, cudaStream_t s);
 // Tags of the compressed level-1 stencil: node J gets the material id of fine cell (2 jx, 2 jy, 2 jz) (read
-// from the paired kernel's cell-pair words) when its stored FP64 half stencil S64 equals lam pat[0] + mu pat[1]
-// to 1e-12 (relative), else 0.
+// from the paired kernel's cell-pair words) when its stored FP64 half stencil S64 (row-padded) equals
+// lam pat[0] + mu pat[1] to 1e-12 (relative), else 0.
 void launch_sym_tags(const double* S64, int cnx, int cny, int cnz, const uint16_t* cellpair, int fnxn, int mp,
                      const double* mtab, const double* pat, uint8_t* tag, cudaStream_t s);
 

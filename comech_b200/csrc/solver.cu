@@ -13,9 +13,11 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -55,7 +57,11 @@ struct SetupProfile {
 };
 thread_local SetupProfile g_prof;
 
-void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// kernels recorded into a graph by this thread are not launches: they count when the graph runs
+thread_local bool g_capturing = false;
+void note_launch(int n) {
+  if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
 
 int set_dyn_smem(const void* kernel, int bytes) {
   static std::mutex mu;
@@ -215,7 +221,7 @@ struct Entries {
 };
 
 // Sorts entries by (row, col) and sums duplicates: LSD radix sort of the packed key row << 32 | col
-// (dofs < 2^31, feb_create checks 3 nnode_total), 16-bit digits, digits that never vary skipped.
+// (dofs < 2^31, feb_create checks 3 nnode_total), 11-bit digits, digits that never vary skipped.
 void coo_merge(Entries& E) {
   const size_t n = E.size();
   if (n == 0) return;
@@ -769,17 +775,64 @@ class PinnedSlots {
   std::vector<CgState*> free_;   // blocks stay allocated until the process exits
 };
 static PinnedSlots g_pinned;
+
+// Streams and events of closed handles are kept, per device, for the next handle: creating them can wait on
+// the driver's resource manager, which a concurrent monitoring query (nvidia-smi, NVML) holds for milliseconds,
+// so a warm process creates none.  Every event is timing-enabled.
+class StreamCache {
+ public:
+  cudaStream_t stream() {
+    const int dev = device();
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      auto& v = streams_[dev];
+      if (!v.empty()) { cudaStream_t st = v.back(); v.pop_back(); return st; }
+    }
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    return st;
+  }
+  cudaEvent_t event() {
+    const int dev = device();
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      auto& v = events_[dev];
+      if (!v.empty()) { cudaEvent_t e = v.back(); v.pop_back(); return e; }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+  }
+  // a stream is given back idle (the caller synchronised it)
+  void give(cudaStream_t st) {
+    if (!st) return;
+    std::lock_guard<std::mutex> lock(mu_);
+    streams_[device()].push_back(st);
+  }
+  void give(cudaEvent_t e) {
+    if (!e) return;
+    std::lock_guard<std::mutex> lock(mu_);
+    events_[device()].push_back(e);
+  }
+
+ private:
+  static int device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) { cudaGetLastError(); d = 0; }
+    return d;
+  }
+  std::mutex mu_;
+  std::map<int, std::vector<cudaStream_t>> streams_;   // kept until the process exits
+  std::map<int, std::vector<cudaEvent_t>> events_;
+};
+static StreamCache g_streams;
 }  // namespace feb
 
-static cudaStream_t make_stream() {
-  cudaStream_t st = nullptr;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-  return st;
-}
+static cudaStream_t make_stream() { return feb::g_streams.stream(); }
 
 struct FebHandle {
   explicit FebHandle(cudaStream_t caller_) : caller(caller_), s(make_stream()), pool(s) {
-    cudaEventCreateWithFlags(&ev_sync, cudaEventDisableTiming);
+    ev_sync = g_streams.event();
   }
   cudaStream_t caller;
   cudaStream_t s;
@@ -846,6 +899,12 @@ struct FebHandle {
   cudaGraphExec_t g_outer = nullptr, g_inner = nullptr;
   int g_outer_nodes = 0, g_inner_nodes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t tev0 = nullptr, tev1 = nullptr;   // the autotuner's timings (ev0 marks the set-up's start)
+  int tune_events() {
+    if (!tev0 && !(tev0 = g_streams.event())) { set_last_error("cudaEventCreate"); return FEB_ERR_CUDA; }
+    if (!tev1 && !(tev1 = g_streams.event())) { set_last_error("cudaEventCreate"); return FEB_ERR_CUDA; }
+    return FEB_OK;
+  }
   KuConfig ku32{}, ku64{};   // launch shapes of the fine K.u (autotuned per grid shape)
   // paired-row level-0 kernels (fine_pair.cu): used when every regular cell's material fits the id table
   bool pair_ok = false;
@@ -862,6 +921,7 @@ struct FebHandle {
     if (stage_n <= kStages) cudaEventRecord(stage_ev[stage_n++], s);
   }
   double t_setup_ms = 0.0;
+  double t_pre_ms = 0.0;    // host time of feb_create before the device-timed set-up (pool reservation, handle)
   int launches = 0;
 
   // side streams of set-up work that runs per level (power iterations), with their join events
@@ -869,22 +929,75 @@ struct FebHandle {
   cudaStream_t aux[kAux] = {};
   cudaEvent_t aux_ev[kAux] = {};
 
+  // Set-up work still running when feb_create returns: the power iterations (aux streams) and the dense
+  // coarsest level with its inverse (dense_s).  The caller's next steps (rigid groups, loads, a start value)
+  // overlap them on the device; settle() joins them into s before anything reads their results.
+  bool pending = false;
+  int coarse_fail = 0;                    // the coarsest-level matrix was not positive definite
+  cudaStream_t dense_s = nullptr;
+  cudaEvent_t dense_ev = nullptr;
+  int* dense_st = nullptr;                // device status of the inverse, copied to dense_st_h (pinned)
+  CgState* dense_st_h = nullptr;
+  std::vector<void*> deferred_free;       // buffers the deferred work reads, freed on s once joined
+
+  int coarse_error() {
+    set_last_error("coarsest-level matrix (%d dofs) is not positive definite", nd);
+    return FEB_ERR_COARSE;
+  }
+  // joins the deferred set-up into s, frees what only it needed, completes the set-up times and reports a
+  // failed coarsest-level inverse (then and on every later call)
+  int settle() {
+    if (!pending) return coarse_fail ? coarse_error() : FEB_OK;
+    pending = false;
+    for (int k = 0; k < coarsest; ++k) FEB_CUDA(cudaStreamWaitEvent(s, aux_ev[k], 0));
+    FEB_CUDA(cudaStreamWaitEvent(s, dense_ev, 0));
+    for (void* p : deferred_free) pool.free(p);
+    deferred_free.clear();
+    FEB_CUDA(cudaEventSynchronize(dense_ev));
+    for (int k = 0; k < coarsest; ++k) FEB_CUDA(cudaEventSynchronize(aux_ev[k]));
+    // stage 6: from the end of the enqueue to the end of the slowest deferred chain; the set-up's span
+    float t = 0.f, tail = 0.f, span = (float)t_setup_ms;
+    auto upto = [&](cudaEvent_t e) {
+      if (cudaEventElapsedTime(&t, stage_ev[6], e) == cudaSuccess) tail = std::max(tail, t);
+      if (cudaEventElapsedTime(&t, ev0, e) == cudaSuccess) span = std::max(span, t);
+    };
+    upto(dense_ev);
+    for (int k = 0; k < coarsest; ++k) upto(aux_ev[k]);
+    cudaGetLastError();
+    stage_ms[6] = tail;
+    t_setup_ms = span;
+    coarse_fail = *reinterpret_cast<volatile int*>(dense_st_h) != 0;
+    return coarse_fail ? coarse_error() : FEB_OK;
+  }
+
+  // the level-0 products share their sparse-part accumulators with the level-0 power iteration: a product on
+  // s waits (on the device) for that chain while it may still run
+  int wait_fine() {
+    if (pending && coarsest > 0) FEB_CUDA(cudaStreamWaitEvent(s, aux_ev[0], 0));
+    return FEB_OK;
+  }
+
   ~FebHandle() {
+    if (dense_s) { cudaStreamSynchronize(dense_s); g_streams.give(dense_s); }
+    g_streams.give(dense_ev);
+    g_pinned.give(dense_st_h);
     for (int i = 0; i < kAux; ++i) {
-      if (aux[i]) { cudaStreamSynchronize(aux[i]); cudaStreamDestroy(aux[i]); }
-      if (aux_ev[i]) cudaEventDestroy(aux_ev[i]);
+      if (aux[i]) { cudaStreamSynchronize(aux[i]); g_streams.give(aux[i]); }
+      g_streams.give(aux_ev[i]);
     }
-    if (A1_ev) cudaEventDestroy(A1_ev);
+    g_streams.give(A1_ev);
     if (g_outer) cudaGraphExecDestroy(g_outer);
     if (g_inner) cudaGraphExecDestroy(g_inner);
     g_pinned.give(st_h);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
+    g_streams.give(ev0);
+    g_streams.give(tev0);
+    g_streams.give(tev1);
+    g_streams.give(ev1);
     pool.release();
     cudaStreamSynchronize(s);
-    if (ev_sync) cudaEventDestroy(ev_sync);
-    for (auto& e : stage_ev) if (e) cudaEventDestroy(e);
-    cudaStreamDestroy(s);
+    g_streams.give(ev_sync);
+    for (auto& e : stage_ev) g_streams.give(e);
+    g_streams.give(s);
   }
 
   // ---------------------------------------------------------------------------------------------- operators
@@ -926,9 +1039,11 @@ struct FebHandle {
     }
   }
   template <typename T>
-  static SymView<T> symview(const Level& V) {
+  SymView<T> symview(const Level& V) const {
     SymView<T> S;
     S.nx = V.nx; S.ny = V.ny; S.nz = V.nz; S.n = V.nnode;
+    S.nxp = sym_nxp(V.nx); S.np = sym_np(V.nx, V.ny, V.nz);
+    S.slots = opt.level_kernel;
     S.S = symS<T>(V);
     S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
     S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
@@ -1098,7 +1213,10 @@ struct FebHandle {
   // while loop (conditional graph node): the whole CG then runs as one graph launch
   int capture(CgState* S, bool inner, cudaGraphExec_t* exec, int* nodes) {
     if (*exec) return FEB_OK;
-    const long long before = g_launches.load();
+    struct Capturing {
+      Capturing() { g_capturing = true; }
+      ~Capturing() { g_capturing = false; }
+    } capturing;
     cudaGraph_t g = nullptr;
     if (opt.use_graphs >= 2) {
       FEB_CUDA(cudaGraphCreate(&g, 0));
@@ -1129,10 +1247,16 @@ struct FebHandle {
       FEB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
       *nodes = (int)nn;
     }
-    g_launches.store(before);   // captured kernels are counted when the graph runs
     FEB_CUDA(cudaGraphInstantiate(exec, g, 0));
     FEB_CUDA(cudaGraphDestroy(g));
     return FEB_OK;
+  }
+
+  // the CG iteration graph, captured ahead of the first solve (feb_set_rigid_groups does it beside its products)
+  int prepare_graphs() {
+    if (!opt.use_graphs || coarsest < 0) return FEB_OK;
+    return opt.precision == FEB_PREC_REFINE ? capture(sti, true, &g_inner, &g_inner_nodes)
+                                            : capture(st, false, &g_outer, &g_outer_nodes);
   }
 
   // runs CG iterations until S->done; returns the final host copy of the state
@@ -1347,8 +1471,9 @@ int power_fork(FebHandle* h, double** part) {
   int st = FEB_OK;
   for (int k = 0; k < nl && st == FEB_OK; ++k) {
     if (!H.aux[k]) {
-      FEB_CUDA(cudaStreamCreateWithFlags(&H.aux[k], cudaStreamNonBlocking));
-      FEB_CUDA(cudaEventCreateWithFlags(&H.aux_ev[k], cudaEventDisableTiming));
+      H.aux[k] = g_streams.stream();
+      H.aux_ev[k] = g_streams.event();   // timed: the set-up's span ends at the slowest chain
+      if (!H.aux[k] || !H.aux_ev[k]) { set_last_error("side stream / event creation failed"); return FEB_ERR_CUDA; }
     }
     FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
     H.s = H.aux[k];
@@ -1392,11 +1517,12 @@ int env_tc() {
 template <typename T>
 int time_apply(FebHandle* h, T* u, T* y, float* ms) {
   for (int w = 0; w < 2; ++w) h->apply<T>(0, u, y, nullptr);
-  FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+  FEB_TRY(h->tune_events());
+  FEB_CUDA(cudaEventRecord(h->tev0, h->s));
   for (int r = 0; r < 3; ++r) h->apply<T>(0, u, y, nullptr);
-  FEB_CUDA(cudaEventRecord(h->ev1, h->s));
-  FEB_CUDA(cudaEventSynchronize(h->ev1));
-  FEB_CUDA(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  FEB_CUDA(cudaEventRecord(h->tev1, h->s));
+  FEB_CUDA(cudaEventSynchronize(h->tev1));
+  FEB_CUDA(cudaEventElapsedTime(ms, h->tev0, h->tev1));
   return FEB_OK;
 }
 
@@ -1466,12 +1592,13 @@ int tune_pair(FebHandle* h, PairConfig* best, T* u, T* y, T* y2, T* y3) {
   for (int zc : wave_chunks<T>(h, 8, true)) {
     slot.zchunk_smooth = zc;
     for (int w = 0; w < 2; ++w) h->pair_run<T>(u, nullptr, &A, nullptr);
-    FEB_CUDA(cudaEventRecord(h->ev0, h->s));
+    FEB_TRY(h->tune_events());
+    FEB_CUDA(cudaEventRecord(h->tev0, h->s));
     for (int r = 0; r < 3; ++r) h->pair_run<T>(u, nullptr, &A, nullptr);
-    FEB_CUDA(cudaEventRecord(h->ev1, h->s));
-    FEB_CUDA(cudaEventSynchronize(h->ev1));
+    FEB_CUDA(cudaEventRecord(h->tev1, h->s));
+    FEB_CUDA(cudaEventSynchronize(h->tev1));
     float ms = 0.f;
-    FEB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    FEB_CUDA(cudaEventElapsedTime(&ms, h->tev0, h->tev1));
     if (ms < best_ms) { best_ms = ms; best->zchunk_smooth = zc; }
   }
   slot = *best;
@@ -1710,10 +1837,11 @@ int launch_level1_early(FebHandle& H) {
   FEB_TRY(H.pool.alloc(&H.A1_basis, 16 * 576));
   const int k = FebHandle::kAux - 1;
   if (!H.aux[k]) {
-    FEB_CUDA(cudaStreamCreateWithFlags(&H.aux[k], cudaStreamNonBlocking));
-    FEB_CUDA(cudaEventCreateWithFlags(&H.aux_ev[k], cudaEventDisableTiming));
+    H.aux[k] = g_streams.stream();
+    H.aux_ev[k] = g_streams.event();   // timed: the set-up's span ends at the slowest chain
+    if (!H.aux[k] || !H.aux_ev[k]) { set_last_error("side stream / event creation failed"); return FEB_ERR_CUDA; }
   }
-  if (!H.A1_ev) FEB_CUDA(cudaEventCreateWithFlags(&H.A1_ev, cudaEventDisableTiming));
+  if (!H.A1_ev && !(H.A1_ev = g_streams.event())) { set_last_error("cudaEventCreate"); return FEB_ERR_CUDA; }
   FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
   FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
   const double a = H.xe[1] - H.xe[0], b = H.ye[1] - H.ye[0], c = H.ze[1] - H.ze[0];
@@ -1721,6 +1849,77 @@ int launch_level1_early(FebHandle& H) {
   FEB_CUDA(cudaEventRecord(H.A1_ev, H.aux[k]));
   return FEB_OK;
 }
+
+// The host pipeline of the extra entries (bounds check, merge, local / non-local classification, rank-1
+// factoring) runs on a worker thread beside the cells stage and the early level-1 stencil.  The
+// classification needs the split copies' grid positions, which the cells stage reads back: the worker waits
+// for ready() (or gives up when the set-up fails first).  The used-node filter is applied by the caller
+// afterwards, on the merged entries; dropping entries commutes with merging, so only when an entry is
+// actually dropped are the classification and the factoring redone.
+class ExtraPrep {
+ public:
+  Entries ex;                    // merged, every entry in range
+  std::vector<char> is_local;    // both nodes within one cell of each other
+  std::vector<char> taken;       // entries represented by `terms`
+  Terms terms;
+  char err[160] = {};            // bounds error (empty: none)
+
+  void start(const FebOperator* op, int64_t nnode, int64_t ntotal, int gx, int gy,
+             const std::vector<int64_t>* orig_copy) {
+    std::shared_future<void> go = ready_.get_future().share();
+    th_ = std::thread([this, op, nnode, ntotal, gx, gy, orig_copy, go]() {
+      ex.r.reserve(op->nextra); ex.c.reserve(op->nextra); ex.v.reserve(op->nextra);
+      for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
+        const int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
+        if (rr < 0 || cc < 0 || rr >= 3 * ntotal || cc >= 3 * ntotal) {
+          snprintf(err, sizeof(err), "extra entry (%lld, %lld) out of range", (long long)rr, (long long)cc);
+          return;
+        }
+        ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
+      }
+      coo_merge(ex);
+      go.wait();
+      if (!ok_.load(std::memory_order_acquire)) return;
+      classify(nnode, gx, gy, *orig_copy);
+      taken = factor_nonlocal(ex, is_local, terms);
+    });
+  }
+  // the split copies' positions are in place (called once, on success)
+  void ready() {
+    ok_.store(true, std::memory_order_release);
+    release();
+  }
+  void join() {
+    release();
+    if (th_.joinable()) th_.join();
+  }
+  ~ExtraPrep() { join(); }
+
+  // grid coordinates by 32-bit unsigned division (grid node ids are below 2^31): two divisions per node
+  void classify(int64_t nnode, int gx, int gy, const std::vector<int64_t>& orig_copy) {
+    const uint32_t ugx = (uint32_t)gx, ugy = (uint32_t)gy;
+    auto coords = [&](int64_t node, int& x, int& y, int& z) {
+      const uint32_t a = (uint32_t)(node < nnode ? node : orig_copy[node - nnode]), q = a / ugx;
+      x = int(a - q * ugx); z = int(q / ugy); y = int(q - (uint32_t)z * ugy);
+    };
+    is_local.assign(ex.size(), 0);
+    for (size_t e2 = 0; e2 < ex.size(); ++e2) {
+      int ax, ay, az, bx, by, bz;
+      coords(ex.r[e2] / 3, ax, ay, az);
+      coords(ex.c[e2] / 3, bx, by, bz);
+      is_local[e2] = std::abs(ax - bx) <= 1 && std::abs(ay - by) <= 1 && std::abs(az - bz) <= 1;
+    }
+  }
+
+ private:
+  void release() {
+    if (!released_) { released_ = true; ready_.set_value(); }
+  }
+  std::promise<void> ready_;
+  std::atomic<bool> ok_{false};
+  bool released_ = false;
+  std::thread th_;
+};
 
 template <int W>
 int setup_level0(FebHandle* h, const FebOperator* op) {
@@ -1731,6 +1930,8 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   V.nx = H.nx + 1; V.ny = H.ny + 1; V.nz = H.nz + 1;
   V.nnode = H.nnode; V.ntotal = H.ntotal;
   V.coord[0] = H.xe; V.coord[1] = H.ye; V.coord[2] = H.ze;
+  ExtraPrep xp;
+  if (op->nextra > 0) xp.start(op, H.nnode, H.ntotal, H.nx + 1, H.ny + 1, &H.orig_copy_h);
   // per-axis widths
   std::vector<double> w64[3], iw64[3];
   std::vector<float> w32[3], iw32[3];
@@ -1802,6 +2003,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
     FEB_CUDA(cudaStreamSynchronize(s));
     H.orig_copy_h.assign(oc.begin(), oc.end());
   }
+  xp.ready();
   // a grid far above the coarsest size always gets level 1: its stencil starts now, beside the host work below
   if (H.opt.max_levels >= 2 && 3 * H.nnode > 8 * (int64_t)H.opt.min_dofs && galerkin_direct_ok(H)) {
     if (H.mode == MAT_ISO_SRI) FEB_TRY(launch_level1_early<MAT_ISO_SRI>(H));
@@ -1843,42 +2045,32 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   FEB_TRY(H.pool.upload(&pen_k32, pkf.data(), pkf.size()));
   // extra matrix: all entries applied on level 0; local ones folded into the level-1 stencil on the
   // device, non-local ones projected through the levels on the host
-  Entries ex;
-  ex.r.reserve(op->nextra); ex.c.reserve(op->nextra); ex.v.reserve(op->nextra);
-  for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
-    int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
-    if (rr < 0 || cc < 0 || rr >= 3 * H.ntotal || cc >= 3 * H.ntotal) {
-      set_last_error("extra entry (%lld, %lld) out of range", (long long)rr, (long long)cc);
-      return FEB_ERR_ARG;
-    }
-    if (!used_h[rr / 3] || !used_h[cc / 3]) continue;
-    ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
+  g_prof.mark("L0 penalties", s);
+  xp.join();
+  if (xp.err[0]) { set_last_error("%s", xp.err); return FEB_ERR_ARG; }
+  Entries& ex = xp.ex;
+  std::vector<char>& is_local = xp.is_local;
+  std::vector<char>& taken = xp.taken;
+  V.terms = std::move(xp.terms);
+  // entries on unused nodes are dropped (fe/solver.py:213-215); rare, and then the worker's classification
+  // and factoring of the dropped set are redone on what remains
+  size_t keep = 0;
+  for (size_t e2 = 0; e2 < ex.size(); ++e2) keep += used_h[ex.r[e2] / 3] && used_h[ex.c[e2] / 3];
+  if (keep < ex.size()) {
+    Entries f;
+    f.r.reserve(keep); f.c.reserve(keep); f.v.reserve(keep);
+    for (size_t e2 = 0; e2 < ex.size(); ++e2)
+      if (used_h[ex.r[e2] / 3] && used_h[ex.c[e2] / 3]) { f.r.push_back(ex.r[e2]); f.c.push_back(ex.c[e2]); f.v.push_back(ex.v[e2]); }
+    ex = std::move(f);
+    xp.classify(H.nnode, H.nx + 1, H.ny + 1, H.orig_copy_h);
+    V.terms = Terms();
+    taken = factor_nonlocal(ex, is_local, V.terms);
   }
-  g_prof.mark("L0 penalties + extra read", s);
-  coo_merge(ex);
-  g_prof.mark("L0 extra merge", s);
+  g_prof.mark("L0 extra entries (worker joined, used filter)", s);
   Csr c0;
   FEB_TRY(upload_csr(H.pool, ex, c0));
   g_prof.mark("L0 extra CSR upload", s);
   Entries loc;
-  const int gx = H.nx + 1, gy = H.ny + 1;
-  auto pos = [&](int64_t node) { return node < H.nnode ? node : H.orig_copy_h[node - H.nnode]; };
-  std::vector<char> is_local(ex.size());
-  // grid coordinates by 32-bit unsigned division (grid node ids are below 2^31): two divisions per node
-  const uint32_t ugx = (uint32_t)gx, ugy = (uint32_t)gy;
-  auto coords = [&](int64_t node, int& x, int& y, int& z) {
-    const uint32_t a = (uint32_t)pos(node), q = a / ugx;
-    x = int(a - q * ugx); z = int(q / ugy); y = int(q - (uint32_t)z * ugy);
-  };
-  for (size_t e2 = 0; e2 < ex.size(); ++e2) {
-    int ax, ay, az, bx, by, bz;
-    coords(ex.r[e2] / 3, ax, ay, az);
-    coords(ex.c[e2] / 3, bx, by, bz);
-    is_local[e2] = std::abs(ax - bx) <= 1 && std::abs(ay - by) <= 1 && std::abs(az - bz) <= 1;
-  }
-  g_prof.mark("L0 extra classify", s);
-  std::vector<char> taken = factor_nonlocal(ex, is_local, V.terms);
-  g_prof.mark("L0 extra factor", s);
   for (size_t e2 = 0; e2 < ex.size(); ++e2) {
     if (taken[e2]) continue;
     Entries& dst = is_local[e2] ? loc : V.nonlocal;
@@ -1947,40 +2139,52 @@ int build_dense(FebHandle* h) {
     if (mask[i]) { cmap[i] = (int)klist.size(); klist.push_back((int)i); }
   H.nd = 3 * (int)klist.size();
   if (H.nd == 0) { set_last_error("empty coarsest level"); return FEB_ERR_ARG; }
+  // buffers are allocated (stream-ordered) on s; the assembly and the inverse run on dense_s from here, and
+  // feb_create returns without waiting for them (FebHandle::settle joins them)
   FEB_TRY(H.pool.upload(&H.cmap, cmap.data(), cmap.size()));
   FEB_TRY(H.pool.upload(&H.klist, klist.data(), klist.size()));
   FEB_TRY(H.pool.zeros(&H.Minv, (size_t)H.nd * H.nd));
   FEB_TRY(H.pool.alloc(&H.bd, H.nd));
   FEB_TRY(H.pool.alloc(&H.xd, H.nd));
-  if (H.coarsest == 0) {
-    switch (H.mode) {
-      case MAT_ISO_SRI: launch_dense_from_fine<MAT_ISO_SRI>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
-      case MAT_ISO_FULL: launch_dense_from_fine<MAT_ISO_FULL>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
-      default: launch_dense_from_fine<MAT_ORTHO>(H.F64, H.cmap, H.Minv, H.nd, H.s); break;
-    }
-  } else {
-    launch_dense_from_stencil(V.A64, V.nx, V.ny, V.nz, H.cmap, H.Minv, H.nd, H.s);
-    if (V.sparse.size()) {
-      std::vector<int> rr(V.sparse.r.begin(), V.sparse.r.end()), cc(V.sparse.c.begin(), V.sparse.c.end());
-      int *dr, *dc;
-      double* dv;
-      FEB_TRY(H.pool.upload(&dr, rr.data(), rr.size()));
-      FEB_TRY(H.pool.upload(&dc, cc.data(), cc.size()));
-      FEB_TRY(H.pool.upload(&dv, V.sparse.v.data(), V.sparse.v.size()));
-      launch_dense_add_entries((int)rr.size(), dr, dc, dv, H.cmap, H.Minv, H.nd, H.s);
-    }
-    launch_dense_add_terms(V.nterms, V.t_ptr, V.t_dof, V.t_val64, V.t_lam64, H.cmap, H.Minv, H.nd, H.s);
+  int *dr = nullptr, *dc = nullptr;
+  double* dv = nullptr;
+  if (H.coarsest > 0 && V.sparse.size()) {
+    std::vector<int> rr(V.sparse.r.begin(), V.sparse.r.end()), cc(V.sparse.c.begin(), V.sparse.c.end());
+    FEB_TRY(H.pool.upload(&dr, rr.data(), rr.size()));
+    FEB_TRY(H.pool.upload(&dc, cc.data(), cc.size()));
+    FEB_TRY(H.pool.upload(&dv, V.sparse.v.data(), V.sparse.v.size()));
   }
   double* scratch = nullptr;
   FEB_TRY(H.pool.alloc(&scratch, dense_scratch_doubles(H.nd)));
-  FEB_CUDA(cudaMemsetAsync(H.status, 0, sizeof(int), H.s));
-  launch_dense_invert(H.Minv, H.nd, scratch, H.status, H.s);
+  if (!H.dense_st) FEB_TRY(H.pool.zeros(&H.dense_st, 1));
+  if (!H.dense_st_h && !(H.dense_st_h = g_pinned.take())) { set_last_error("cudaMallocHost"); return FEB_ERR_CUDA; }
+  if (!H.dense_s) {
+    H.dense_s = g_streams.stream();
+    H.dense_ev = g_streams.event();
+    if (!H.dense_s || !H.dense_ev) { set_last_error("side stream / event creation failed"); return FEB_ERR_CUDA; }
+  }
+  FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
+  FEB_CUDA(cudaStreamWaitEvent(H.dense_s, H.ev_sync, 0));
+  cudaStream_t ds = H.dense_s;
+  if (H.coarsest == 0) {
+    switch (H.mode) {
+      case MAT_ISO_SRI: launch_dense_from_fine<MAT_ISO_SRI>(H.F64, H.cmap, H.Minv, H.nd, ds); break;
+      case MAT_ISO_FULL: launch_dense_from_fine<MAT_ISO_FULL>(H.F64, H.cmap, H.Minv, H.nd, ds); break;
+      default: launch_dense_from_fine<MAT_ORTHO>(H.F64, H.cmap, H.Minv, H.nd, ds); break;
+    }
+  } else {
+    launch_dense_from_stencil(V.A64, V.nx, V.ny, V.nz, H.cmap, H.Minv, H.nd, ds);
+    if (dr) launch_dense_add_entries((int)V.sparse.size(), dr, dc, dv, H.cmap, H.Minv, H.nd, ds);
+    launch_dense_add_terms(V.nterms, V.t_ptr, V.t_dof, V.t_val64, V.t_lam64, H.cmap, H.Minv, H.nd, ds);
+  }
+  FEB_CUDA(cudaMemsetAsync(H.dense_st, 0, sizeof(int), ds));
+  launch_dense_invert(H.Minv, H.nd, scratch, H.dense_st, ds);
   FEB_CUDA(cudaGetLastError());
-  int st = 0;
-  FEB_CUDA(cudaMemcpyAsync(&st, H.status, sizeof(int), cudaMemcpyDeviceToHost, H.s));
-  FEB_CUDA(cudaStreamSynchronize(H.s));
-  H.pool.free(scratch);
-  if (st != 0) { set_last_error("coarsest-level matrix (%d dofs) is not positive definite", H.nd); return FEB_ERR_COARSE; }
+  FEB_CUDA(cudaMemcpyAsync(H.dense_st_h, H.dense_st, sizeof(int), cudaMemcpyDeviceToHost, ds));
+  FEB_CUDA(cudaEventRecord(H.dense_ev, ds));
+  H.pending = true;
+  for (void* p : {(void*)scratch, (void*)dr, (void*)dc, (void*)dv})
+    if (p) H.deferred_free.push_back(p);
   return FEB_OK;
 }
 
@@ -2077,8 +2281,8 @@ int build_hierarchy(FebHandle* h) {
     FEB_TRY(upload_node_csr(H.pool, C.sparse, C.nnode, C));
     FEB_TRY(upload_terms(H.pool, C.terms, C.nnode, C));
     g_prof.mark("Lk sparse project + upload", H.s);
-    FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)C.ntotal));
-    launch_stencil_to_sym<double>(C.A64, C.ntotal, C.S64, H.s);
+    FEB_TRY(H.pool.alloc(&C.S64, 126 * (size_t)sym_np(C.nx, C.ny, C.nz)));
+    launch_stencil_to_sym<double>(C.A64, C.nx, C.ny, C.nz, C.S64, H.s);
     if (C.pat64) {   // compressed level-1 stencil: tags of the uniform nodes, patterns and material table in T
       FEB_TRY(H.pool.alloc(&C.tag, C.ntotal));
       launch_sym_tags(C.S64, C.nx, C.ny, C.nz, H.P32.cellpair, H.nx + 1, H.P32.mp, H.P32.mtab, C.pat64, C.tag, H.s);
@@ -2092,8 +2296,8 @@ int build_hierarchy(FebHandle* h) {
       FEB_CUDA(cudaGetLastError());
     }
     if (f32) {
-      FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)C.ntotal));
-      launch_stencil_to_sym<float>(C.A64, C.ntotal, C.S32, H.s);
+      FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)sym_np(C.nx, C.ny, C.nz)));
+      launch_stencil_to_sym<float>(C.A64, C.nx, C.ny, C.nz, C.S32, H.s);
     }
     g_prof.mark("Lk half stencils", H.s);
     l += 1;
@@ -2147,16 +2351,29 @@ int build_hierarchy(FebHandle* h) {
   if (pst != FEB_OK) { power_join(h, part); return pst; }
   H.stage_mark();   // 6: work vectors, power iterations started on the side streams
   g_prof.mark("power iterations (launched)", H.s);
-  const int dst = build_dense(h);   // concurrent with the power iterations
-  FEB_TRY(power_join(h, part));
-  FEB_TRY(dst);
-  H.stage_mark();   // 7: dense coarsest level and its inverse
-  g_prof.mark("dense coarsest inverse", H.s);
-  for (int k = 1; k <= H.coarsest; ++k) {      // the full stencils only feed the Galerkin products
-    H.pool.free(H.L[k].A64);
-    H.L[k].A64 = nullptr;
-    if (f32) { H.pool.free(H.L[k].S64); H.L[k].S64 = nullptr; }
+  // the dense coarsest level runs on its own stream beside the power iterations; neither is waited for
+  // here: the caller's next steps overlap them, and settle() joins them (stage 6's time is measured there)
+  const int dst = build_dense(h);
+  if (dst != FEB_OK) { power_join(h, part); return dst; }
+  H.pending = true;
+  H.deferred_free.push_back(part);
+  if (g_prof.on) {
+    FEB_TRY(H.settle());
+    g_prof.mark("dense coarsest inverse, power iterations (joined)", H.s);
   }
+  // the full stencils only feed the Galerkin products and the dense level; the FP64 half stencils of an FP32
+  // V-cycle only the power iterations: all are released once the deferred work is joined
+  for (int k = 1; k <= H.coarsest; ++k) {
+    H.deferred_free.push_back(H.L[k].A64);
+    H.L[k].A64 = nullptr;
+    if (f32 && !pw32) { H.deferred_free.push_back(H.L[k].S64); H.L[k].S64 = nullptr; }
+  }
+  if (!H.pending) {                              // joined above (set-up profiling)
+    for (void* p : H.deferred_free) H.pool.free(p);
+    H.deferred_free.clear();
+  }
+  if (f32 && pw32)
+    for (int k = 1; k <= H.coarsest; ++k) { H.pool.free(H.L[k].S64); H.L[k].S64 = nullptr; }
   return FEB_OK;
 }
 
@@ -2173,7 +2390,10 @@ int check_tc_status(FebHandle* h) {
 // The device's default stream-ordered pool serves every allocation of a handle.  Freed memory stays mapped
 // (release threshold at its maximum) for the next handle, and the pool is reserved up front in one block of
 // about twice the largest set-up seen (at least ~3 KB per node): growing it piece by piece during set-up
-// costs up to hundreds of milliseconds per new peak, in whichever stage happens to need the memory.
+// costs up to hundreds of milliseconds per new peak, in whichever stage happens to need the memory.  The
+// used-memory peak drifts a little from one set-up to the next (whether a block freed on one stream is
+// reused by another depends on timing), so the pool is grown only on a real shortage, reserved memory below
+// 1.25 x that peak or below the size estimate, not whenever the peak passes half of the reservation.
 void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   int dev = 0;
   cudaMemPool_t mp;
@@ -2184,6 +2404,7 @@ void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &have);
   cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &high);
   const uint64_t nodes = (uint64_t)std::max(nnode, nnode_total);
+  if (have >= std::max<uint64_t>(high + high / 4, nodes * 3072ull)) return;
   uint64_t want = std::max<uint64_t>(2 * high, nodes * 3072ull);
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) want = std::min<uint64_t>(want, have + free_b / 2);
@@ -2215,7 +2436,8 @@ int fill_handle_info(FebHandle& H, FebInfo& inf) {
     inf.lmax[l] = l < H.coarsest ? lp[l].lmax : 0.0;
   }
   inf.kernel_launches = H.launches;
-  for (int i = 0; i < 8; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
+  for (int i = 0; i < 7; ++i) inf.t_stage_ms[i] = H.stage_ms[i];
+  inf.t_stage_ms[7] = H.t_pre_ms;
   inf.ku_shape[0] = H.ku32.tc ? 0 : H.ku32.ty; inf.ku_shape[1] = H.ku32.zchunk;
   inf.ku_shape[2] = H.ku64.ty; inf.ku_shape[3] = H.ku64.zchunk;
   inf.ku_kind = (H.tc_ok && H.ku32.tc) ? 2 : (H.pair_ok ? 1 : 0);
@@ -2311,6 +2533,7 @@ void feb_default_options(FebOptions* o) {
   o->use_graphs = 2;
   o->seed = 0;
   o->x0_mode = 2;
+  o->level_kernel = 0;
 }
 
 int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt, void* stream, FebHandle** out) {
@@ -2321,6 +2544,7 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   *out = nullptr;
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) { set_last_error("feb_create: empty grid"); return FEB_ERR_ARG; }
   if (op->mat_mode < 0 || op->mat_mode > 2) { set_last_error("feb_create: bad mat_mode"); return FEB_ERR_ARG; }
+  const auto t_entry = std::chrono::steady_clock::now();
   reserve_pool((int64_t)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1), op->nnode_total, (cudaStream_t)stream);
   FebHandle* h = new FebHandle((cudaStream_t)stream);
   if (opt) h->opt = *opt; else feb_default_options(&h->opt);
@@ -2333,11 +2557,13 @@ int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt
   h->nnode = (int64_t)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1);
   h->ntotal = op->nnode_total > 0 ? op->nnode_total : h->nnode;
   if (h->ntotal < h->nnode || h->ntotal > INT32_MAX / 3) { delete h; set_last_error("feb_create: bad nnode_total"); return FEB_ERR_ARG; }
-  cudaEventCreate(&h->ev0);
-  cudaEventCreate(&h->ev1);
-  for (auto& e : h->stage_ev) cudaEventCreate(&e);
+  h->ev0 = g_streams.event();
+  h->ev1 = g_streams.event();
+  for (auto& e : h->stage_ev) e = g_streams.event();
+  if (!h->s || !h->ev_sync || !h->ev0 || !h->ev1) { delete h; set_last_error("feb_create: stream / event creation failed"); return FEB_ERR_CUDA; }
   if (h->sync_in() != FEB_OK) { delete h; return FEB_ERR_CUDA; }
   cudaEventRecord(h->ev0, h->s);
+  h->t_pre_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_entry).count();
   h->stage_mark();   // 0: start
   g_prof.start(env_flag("FEB_PROFILE_SETUP") != 0);
   int st = FEB_OK;
@@ -2454,6 +2680,7 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   FEB_TRY(H.pool.alloc(&col, 3 * (size_t)H.ntotal));
   FEB_TRY(H.pool.alloc(&kcol, 3 * (size_t)H.ntotal));
   FEB_TRY(H.pool.alloc(&Ecd, (size_t)nc * nc));
+  FEB_TRY(H.wait_fine());
   for (int c = 0; c < nc; ++c) {
     FEB_CUDA(cudaMemsetAsync(col, 0, 3 * (size_t)H.ntotal * sizeof(double), H.s));
     launch_z_column(Z, c, col, H.s);
@@ -2461,6 +2688,17 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
     launch_ztr(Z, kcol, H.zpart, H.zr, H.s);
     FEB_CUDA(cudaMemcpyAsync(Ecd + (size_t)c * nc, H.zr, nc * sizeof(double), cudaMemcpyDeviceToDevice, H.s));
   }
+  // while the device forms the columns: the solve's iteration graph, with the rigid-mode correction (its
+  // pseudo-inverse is written into Einv below, before any solve reads it)
+  FEB_TRY(H.pool.alloc(&H.Einv, (size_t)nc * nc));
+  H.has_rigid = true;
+  auto undo = [&](int code) {            // no rigid correction, and no graph that applies one
+    H.has_rigid = false;
+    if (H.g_outer) { cudaGraphExecDestroy(H.g_outer); H.g_outer = nullptr; }
+    if (H.g_inner) { cudaGraphExecDestroy(H.g_inner); H.g_inner = nullptr; }
+    return code;
+  };
+  if (const int cst = H.prepare_graphs(); cst != FEB_OK) return undo(cst);
   FEB_CUDA(cudaMemcpyAsync(Ec.data(), Ecd, Ec.size() * sizeof(double), cudaMemcpyDeviceToHost, H.s));
   FEB_CUDA(cudaStreamSynchronize(H.s));
   H.pool.free(col);
@@ -2473,8 +2711,8 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   for (int i = 0; i < nc; ++i)
     for (int j = 0; j < nc; ++j) Es[(size_t)i * nc + j] = 0.5 * (Ec[(size_t)i * nc + j] + Ec[(size_t)j * nc + i]);
   std::vector<double> Ei = sym_pinv(Es, nc);
-  FEB_TRY(H.pool.upload(&H.Einv, Ei.data(), Ei.size()));
-  H.has_rigid = true;
+  if (const int cst = g_staging.copy(H.Einv, Ei.data(), Ei.size() * sizeof(double), H.s); cst != FEB_OK)
+    return undo(cst);
   return H.sync_out();
 }
 
@@ -2490,6 +2728,7 @@ int feb_solve(FebHandle* h, const double* f, const double* x0, double* xout, Feb
   FebHandle& H = *h;
   if (H.coarsest < 0) { set_last_error("feb_solve: handle built with max_levels = 0 (operator only)"); return FEB_ERR_ARG; }
   const int64_t n = 3 * H.ntotal;
+  FEB_TRY(H.settle());
   FEB_TRY(H.sync_in());
   H.launches = 0;
   FebInfo inf{};
@@ -2616,6 +2855,7 @@ int feb_solve_batch(FebHandle* const* hs, int32_t n, const double* const* f, con
     for (int j = 0; j < i; ++j)
       if (hs[j] == hs[i]) { set_last_error("feb_solve_batch: handle %d given twice", i); return FEB_ERR_ARG; }
   }
+  for (int i = 0; i < n; ++i) FEB_TRY(hs[i]->settle());
   FebHandle& H0 = *hs[0];
   const long long before = g_launches.load();
   cudaGraph_t G = nullptr;
@@ -2677,6 +2917,7 @@ int feb_solve_batch(FebHandle* const* hs, int32_t n, const double* const* f, con
 int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y) {
   if (!h || !u || !y) { set_last_error("feb_apply: null argument"); return FEB_ERR_ARG; }
   FEB_TRY(h->sync_in());
+  FEB_TRY(h->wait_fine());
   if (prec == 0) h->apply<double>(0, (const double*)u, (double*)y, nullptr);
   else h->apply<float>(0, (const float*)u, (float*)y, nullptr);
   FEB_CUDA(cudaGetLastError());
@@ -2686,6 +2927,7 @@ int feb_apply(FebHandle* h, int32_t prec, const void* u, void* y) {
 int feb_precondition(FebHandle* h, const double* r, double* z) {
   if (!h || !r || !z) { set_last_error("feb_precondition: null argument"); return FEB_ERR_ARG; }
   if (h->coarsest < 0) { set_last_error("feb_precondition: handle built with max_levels = 0 (operator only)"); return FEB_ERR_ARG; }
+  FEB_TRY(h->settle());
   FEB_TRY(h->sync_in());
   h->precondition<double>(r, z, nullptr);
   FEB_CUDA(cudaGetLastError());
@@ -2715,6 +2957,7 @@ int64_t feb_launch_count(void) { return g_launches.load(); }
 
 int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms) {
   if (!h || !u || !y || nrep < 1 || !ms) { set_last_error("feb_benchmark_apply: bad argument"); return FEB_ERR_ARG; }
+  FEB_TRY(h->settle());     // the timed products run alone
   FEB_TRY(h->sync_in());
   FEB_CUDA(cudaEventRecord(h->ev0, h->s));
   for (int i = 0; i < nrep; ++i) {
@@ -2738,6 +2981,7 @@ int feb_benchmark_apply_set(FebHandle* h, int32_t prec, int32_t nbuf, const void
   }
   for (int b = 0; b < nbuf; ++b)
     if (!u[b] || !y[b]) { set_last_error("feb_benchmark_apply_set: null buffer %d", b); return FEB_ERR_ARG; }
+  FEB_TRY(h->settle());     // the timed products run alone
   FEB_TRY(h->sync_in());
   FEB_CUDA(cudaEventRecord(h->ev0, h->s));
   for (int i = 0; i < nrep; ++i) {

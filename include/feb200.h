@@ -90,7 +90,10 @@ typedef struct FebOptions {
   uint64_t seed;                 /* power-iteration start vectors */
   int32_t x0_mode;               /* start value x0: 0 as given; 1 its energy-optimal multiple; 2 (default) x0 + M (f -
                                     K x0) (one preconditioner application), then its energy-optimal multiple */
-  int32_t pad_;
+  int32_t level_kernel;          /* coarse-level stencil products (one node per thread, the 14 block slots over 4
+                                    warps): 0 (default) slot index a compile-time constant in FP32 products and a
+                                    run-time value in FP64 products (the faster form of each); 1 run-time in both;
+                                    2 compile-time in both */
 } FebOptions;
 
 typedef struct FebInfo {
@@ -99,7 +102,8 @@ typedef struct FebInfo {
   int32_t levels;                /* multigrid levels incl. the coarsest */
   int32_t sweeps;                /* refinement sweeps (1 for FP64 / MIXED) */
   double relres;                 /* FP64 ||f - K x|| / ||f|| of the returned x */
-  double t_setup_ms;             /* device time of feb_create's multigrid set-up */
+  double t_setup_ms;             /* device time of feb_create's multigrid set-up, from its start to the end of
+                                    the last set-up chain (some finish after feb_create returns) */
   double t_solve_ms;             /* device time of feb_solve */
   int64_t ndof;                  /* 3 x used nodes */
   int64_t level_dofs[8];
@@ -108,8 +112,11 @@ typedef struct FebInfo {
   int32_t kernel_launches;       /* kernels launched by feb_solve */
   int32_t ku_shape[4];           /* autotuned fine K.u launch shape: FP32 (warps per CTA, 0 = tensor cores;
                                     node planes per CTA), FP64 (warps, planes) */
-  double t_stage_ms[8];          /* feb_create stages: cells, penalties/extra, diagonal blocks, K.u tuning,
-                                    Galerkin hierarchy, power iterations, dense coarse level, (spare) */
+  double t_stage_ms[8];          /* feb_create stages (device time): cells, penalties/extra, diagonal blocks,
+                                    K.u tuning, Galerkin hierarchy, work vectors and power-iteration launch, then
+                                    the deferred tail (dense coarse level beside the power iterations, measured
+                                    from the launch's end to the slowest chain's end); [7] host time of feb_create
+                                    before the device-timed set-up (pool reservation, handle) */
   int32_t x0_used;               /* 1: the solve started from the caller's x0 (as FebOptions.x0_mode prepares it); 0:
                                     from zero (no x0, or a start s with s.f <= 0: the fallback of a warm start) */
   float x0_scale;                /* the energy-optimal multiple a = s.f / s.K s applied to the start (1 in mode 0) */
@@ -123,7 +130,12 @@ FEB_API void feb_default_options(FebOptions* opt);
 
 /* Builds the operator and the multigrid hierarchy on the device (replaces the CPU/SciPy assembly,
  * fe/solver.py:137-162, rb/splitfe.py:72-91, rb/gpusolve.py:306-346, and the hierarchy set-up,
- * fe/gmg.py:79-102, rb/gpusolve.py:39-171).  `stream` is a cudaStream_t (NULL = default). */
+ * fe/gmg.py:79-102, rb/gpusolve.py:39-171).  `stream` is a cudaStream_t (NULL = default).
+ * The last set-up steps (the dense coarsest level's inverse, the smoothers' eigenvalue estimates) are still
+ * running on the handle's side streams when feb_create returns, so that the caller's next steps
+ * (feb_set_rigid_groups, loads, a start value) overlap them; feb_solve, feb_solve_batch, feb_precondition and the
+ * benchmark calls wait for them, and a coarsest-level matrix that is not positive definite is reported there
+ * (FEB_ERR_COARSE, on that call and every later one). */
 FEB_API int feb_create(const FebGrid* grid, const FebOperator* op, const FebOptions* opt, void* stream, FebHandle** out);
 
 /* Per-group rigid-body modes for the additive coarse correction Z pinv(Z^T K Z) Z^T
