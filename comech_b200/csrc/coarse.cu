@@ -69,8 +69,10 @@ __global__ void k_csr_add(int nrow, const int* __restrict__ row_dof, const int* 
 
 template <typename T>
 __global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __restrict__ rf, T* __restrict__ rc,
-                                const int* __restrict__ skip) {
+                                const int* __restrict__ skip, T* __restrict__ zero, int nzero) {
   if (skip && *skip) return;
+  if (nzero && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+    for (int e = threadIdx.x; e < nzero; e += blockDim.x) zero[e] = T(0);
   const int cnx = P.ax[0].nc, cny = P.ax[1].nc;
   const int jx = blockIdx.x * blockDim.x + threadIdx.x, jy = blockIdx.y, jz = blockIdx.z;
   if (jx >= cnx) return;
@@ -93,8 +95,10 @@ __global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __rest
 // weight 1 (a = 0) or 1/2 (a = +-1)
 template <typename T>
 __global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, const T* __restrict__ rf,
-                                T* __restrict__ rc, const int* __restrict__ skip) {
+                                T* __restrict__ rc, const int* __restrict__ skip, T* __restrict__ zero, int nzero) {
   if (skip && *skip) return;
+  if (nzero && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+    for (int e = threadIdx.x; e < nzero; e += blockDim.x) zero[e] = T(0);
   const int jx = blockIdx.x * blockDim.x + threadIdx.x, jy = blockIdx.y, jz = blockIdx.z;
   if (jx >= cnx) return;
   T s0 = 0, s1 = 0, s2 = 0;
@@ -124,7 +128,8 @@ __global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, con
 // one the mean of its two neighbours
 template <typename T>
 __global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, const uint8_t* __restrict__ used,
-                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
+                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip,
+                               TermAcc<T> acc) {
   if (skip && *skip) return;
   const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
   if (pi >= fnx) return;
@@ -141,6 +146,7 @@ __global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, const uint8_t
         s0 += w * xc[3 * K]; s1 += w * xc[3 * K + 1]; s2 += w * xc[3 * K + 2];
       }
   xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+  term_acc(acc, n, s0, s1, s2);
 }
 
 template <typename T>
@@ -186,7 +192,8 @@ __device__ __forceinline__ void prolong_at(const TransferDev& P, int pi, int pj,
 
 template <typename T>
 __global__ void k_prolong_grid(TransferDev P, int fnx, int fny, const uint8_t* __restrict__ used,
-                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip) {
+                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip,
+                               TermAcc<T> acc) {
   if (skip && *skip) return;
   const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
   if (pi >= fnx) return;
@@ -195,6 +202,7 @@ __global__ void k_prolong_grid(TransferDev P, int fnx, int fny, const uint8_t* _
   T s0, s1, s2;
   prolong_at(P, pi, pj, pk, xc, s0, s1, s2);
   xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+  term_acc(acc, n, s0, s1, s2);
 }
 
 template <typename T>
@@ -694,7 +702,7 @@ template <typename T, int EPI, bool CMP, bool CT>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
       T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
-      const int* __restrict__ skip) {
+      const int* __restrict__ skip, TermAcc<T> acc) {
   if (skip && *skip) return;
   __shared__ T red[4][3][32];
   __shared__ T spat[2][CMP ? 126 : 1];
@@ -829,17 +837,24 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
     r[3 * n + c] = rc;
     d_out[3 * n + c] = e;
     x[3 * n + c] = xc + e;
+    term_acc1(acc, n, c, e);
   }
 }
 
 }  // namespace
 
 template <typename T>
-void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
-                const LevelParams* lp, int k, const int* skip, cudaStream_t s) {
-  const dim3 g(div_up(L.nx, 32), L.ny, L.nz), blk(32, 4);
+void launch_sym(const SymView<T>& L0, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
+                const LevelParams* lp, int k, const int* skip, cudaStream_t s, const T* tdot_in,
+                const TermAcc<T>& acc) {
+  const dim3 g(div_up(L0.nx, 32), L0.ny, L0.nz), blk(32, 4);
+  SymView<T> L = L0;
   if (L.tn_ptr && L.nterms > 0) {
-    k_term_dots<T><<<div_up(L.nterms, 8), 256, 0, s>>>(L, L.nterms, u, skip); note_launch();
+    if (tdot_in) {
+      L.tdot = const_cast<T*>(tdot_in);
+    } else {
+      k_term_dots<T><<<div_up(L.nterms, 8), 256, 0, s>>>(L, L.nterms, u, skip); note_launch();
+    }
   }
   if (126 * L.np >= (int64_t)INT32_MAX) {  // stencil-plane offsets are 32-bit; never reached by a coarse level
     fprintf(stderr, "launch_sym: level of %lld nodes exceeds the 32-bit stencil offsets\n", (long long)L.n);
@@ -847,7 +862,7 @@ void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r
   }
   const bool cmp = L.tag != nullptr;
   const bool ct = L.slots == 2 || (L.slots == 0 && std::is_same<T, float>::value);
-#define FEB_SYM(E, C, CT_) k_sym<T, E, C, CT_><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip)
+#define FEB_SYM(E, C, CT_) k_sym<T, E, C, CT_><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip, acc)
 #define FEB_SYM2(E, C) do { if (ct) FEB_SYM(E, C, true); else FEB_SYM(E, C, false); } while (0)
   if (epi == EPI_APPLY) {
     if (cmp) FEB_SYM2(EPI_APPLY, true); else FEB_SYM2(EPI_APPLY, false);
@@ -868,9 +883,11 @@ void launch_stencil_to_sym(const double* A, int nx, int ny, int nz, T* S, cudaSt
 }
 
 template void launch_sym<float>(const SymView<float>&, int, const float*, float*, const float*, float*, float*,
-                                float*, const LevelParams*, int, const int*, cudaStream_t);
+                                float*, const LevelParams*, int, const int*, cudaStream_t, const float*,
+                                const TermAcc<float>&);
 template void launch_sym<double>(const SymView<double>&, int, const double*, double*, const double*, double*,
-                                 double*, double*, const LevelParams*, int, const int*, cudaStream_t);
+                                 double*, double*, const LevelParams*, int, const int*, cudaStream_t, const double*,
+                                 const TermAcc<double>&);
 void launch_galerkin_axis(const AxisDev& ax, int d, const double* Ain, int inx, int iny, int inz, double* Aout,
                           int onx, int ony, int onz, cudaStream_t s) {
   const int64_t no = (int64_t)onx * ony * onz;
@@ -896,12 +913,14 @@ void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int*
 
 template <typename T>
 void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
-                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s) {
+                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s, T* zero, int nzero) {
+  if (!zero) nzero = 0;
   if (P.even) {
     k_restrict_even<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(
-        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, rf, rc, skip); note_launch();
+        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, rf, rc, skip, zero, nzero); note_launch();
   } else {
-    k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip); note_launch();
+    k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip,
+                                                                                         zero, nzero); note_launch();
   }
   if (fntotal > fnnode)
     k_restrict_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
@@ -912,12 +931,12 @@ void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fn
 template <typename T>
 void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
-                        cudaStream_t s) {
+                        cudaStream_t s, const TermAcc<T>& acc) {
   if (P.even) {
     k_prolong_even<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P.ax[0].nc, P.ax[1].nc, fnx, fny, used, xc, xf,
-                                                                     skip); note_launch();
+                                                                     skip, acc); note_launch();
   } else {
-    k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip); note_launch();
+    k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip, acc); note_launch();
   }
   if (fntotal > fnnode) {
     k_prolong_copies<T><<<div_up(fntotal - fnnode, kThreads), kThreads, 0, s>>>(P, fnx, fny, fnnode, fntotal,
@@ -1006,13 +1025,15 @@ template void launch_csr_add<float>(int, const int*, const int*, const int*, con
 template void launch_csr_add<double>(int, const int*, const int*, const int*, const double*, const double*, double*,
                                      const int*, cudaStream_t);
 template void launch_restrict<float>(const TransferDev&, int, int, int, int64_t, int64_t, const int*, const float*,
-                                     float*, const int*, cudaStream_t);
+                                     float*, const int*, cudaStream_t, float*, int);
 template void launch_restrict<double>(const TransferDev&, int, int, int, int64_t, int64_t, const int*, const double*,
-                                      double*, const int*, cudaStream_t);
+                                      double*, const int*, cudaStream_t, double*, int);
 template void launch_prolong_add<float>(const TransferDev&, int, int, int, int64_t, int64_t, const int*,
-                                        const uint8_t*, const float*, float*, const int*, cudaStream_t);
+                                        const uint8_t*, const float*, float*, const int*, cudaStream_t,
+                                        const TermAcc<float>&);
 template void launch_prolong_add<double>(const TransferDev&, int, int, int, int64_t, int64_t, const int*,
-                                         const uint8_t*, const double*, double*, const int*, cudaStream_t);
+                                         const uint8_t*, const double*, double*, const int*, cudaStream_t,
+                                         const TermAcc<double>&);
 template void launch_galerkin_cells<MAT_ISO_SRI>(const FineView<double>&, const double*, const TransferDev&, double*,
                                                  double*, int, int, int, cudaStream_t);
 template void launch_galerkin_cells<MAT_ISO_FULL>(const FineView<double>&, const double*, const TransferDev&, double*,

@@ -3,6 +3,7 @@
 #pragma once
 #include "common.cuh"
 #include "fine.cuh"
+#include "vec.cuh"
 
 namespace feb {
 
@@ -82,9 +83,12 @@ struct SymView {
 // directions: t = A d_in, r -= t, d_out = a1 d_in + a2 Dinv r, x += d_out.
 enum SymEpi : int { EPI_APPLY = 0, EPI_RESID = 1, EPI_CHEB = 2 };
 struct LevelParams;
+// tdot_in: the rank-1 term dots of u, formed by u's producer (TermAcc); null: a k_term_dots pass forms them
+// first.  acc (EPI_CHEB): the dots of the new direction d_out are accumulated for the next product.
 template <typename T>
 void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r, T* d_out, T* x,
-                const LevelParams* lp, int k, const int* skip, cudaStream_t s);
+                const LevelParams* lp, int k, const int* skip, cudaStream_t s, const T* tdot_in = nullptr,
+                const TermAcc<T>& acc = TermAcc<T>());
 // full [243][n] FP64 stencil of an nx x ny x nz level -> row-padded half storage in T ([126][sym_np])
 template <typename T>
 void launch_stencil_to_sym(const double* A, int nx, int ny, int nz, T* S, cudaStream_t s);
@@ -94,15 +98,18 @@ void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int*
                     const int* skip, cudaStream_t s);
 
 // r_c = P^T r_f.  Fine level given by its grid dims; copies (ids >= nnode) are folded through `orig`.
+// zero[0 .. nzero): cleared by the same launch (the coarse level's term-dot buffers of this V-cycle).
 template <typename T>
 void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
-                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s);
+                     const int* orig_copy, const T* rf, T* rc, const int* skip, cudaStream_t s, T* zero = nullptr,
+                     int nzero = 0);
 
 // x_f += P x_c on used fine nodes (copies take their grid node's value).
+// acc: the term dots of the added P x_c (the fine level's iterate changes by it) are accumulated
 template <typename T>
 void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
-                        cudaStream_t s);
+                        cudaStream_t s, const TermAcc<T>& acc = TermAcc<T>());
 
 // One axis pass of the separable Galerkin product P^T A P of a [243][n] stencil: axis d of the input grid
 // (inx, iny, inz) coarsened by ax to the output grid (onx, ony, onz).

@@ -86,6 +86,7 @@ void set_last_error(const char* fmt, ...) {
 namespace {
 
 constexpr int kMaxLevels = 8;
+constexpr int kTermDotBufs = 2 * 9 - 1;   // V-cycle term-dot buffers of a level for Chebyshev degrees <= 9
 
 // ------------------------------------------------------------------------------------------------ memory
 // Set-up uploads go through one process-wide pinned staging ring: a host copy into pinned memory, then an
@@ -664,6 +665,11 @@ struct Level {
   float* Dinv32 = nullptr;
   double* tdot64 = nullptr;               // per-term dots of the current product (rank-1 terms)
   float* tdot32 = nullptr;
+  // the V-cycle's term dots, formed by the kernels that write the level's vectors (TermAcc): buffer 0 the
+  // iterate x, 1 .. deg-1 the pre-smoothing directions, deg .. 2 deg - 2 the post-smoothing directions;
+  // kTermDotBufs x nterms, cleared by the restriction into the level at the start of each V-cycle
+  double* tdb64 = nullptr;
+  float* tdb32 = nullptr;
   uint8_t* tag = nullptr;                 // compressed stencil (level 1): material tag per node, 0 = stored
   double *pat64 = nullptr, *tmat64 = nullptr;
   float *pat32 = nullptr, *tmat32 = nullptr;
@@ -736,6 +742,8 @@ int upload_terms(Pool& pool, const Terms& T, int64_t nnode, Level& V) {
   FEB_TRY(pool.upload(&V.tn_coef32, coef32.data(), coef32.size()));
   FEB_TRY(pool.alloc(&V.tdot64, T.size()));
   FEB_TRY(pool.alloc(&V.tdot32, T.size()));
+  FEB_TRY(pool.zeros(&V.tdb64, kTermDotBufs * T.size()));
+  FEB_TRY(pool.zeros(&V.tdb32, kTermDotBufs * T.size()));
   return FEB_OK;
 }
 
@@ -1043,7 +1051,7 @@ struct FebHandle {
     SymView<T> S;
     S.nx = V.nx; S.ny = V.ny; S.nz = V.nz; S.n = V.nnode;
     S.nxp = sym_nxp(V.nx); S.np = sym_np(V.nx, V.ny, V.nz);
-    S.slots = opt.level_kernel;
+    S.slots = opt.level_kernel & 3;
     S.S = symS<T>(V);
     S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
     S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
@@ -1070,6 +1078,19 @@ struct FebHandle {
   template <typename T> static T* vr(Level& V);
   template <typename T> static T* vd(Level& V);
   template <typename T> static T* vt(Level& V);
+  template <typename T> T* tdb(Level& V) const {
+    if (!V.nterms || (opt.level_kernel & 4)) return nullptr;   // bit 2: a dot pass before every product instead
+    if constexpr (std::is_same<T, double>::value) return V.tdb64; else return V.tdb32;
+  }
+  // the V-cycle's term-dot accumulation at level V into dot buffers a, b (either may be null)
+  template <typename T>
+  static TermAcc<T> term_acc(Level& V, T* a, T* b) {
+    TermAcc<T> A;
+    if (!V.nterms || (!a && !b)) return A;
+    A.tn_ptr = V.tn_ptr; A.tn_term = V.tn_term; A.tn_coef = tcoef<T>(V); A.t_lam = tlam<T>(V);
+    A.dot_a = a; A.dot_b = b;
+    return A;
+  }
 
   // ---------------------------------------------------------------------------------------------- V-cycle
   template <typename T>
@@ -1079,14 +1100,24 @@ struct FebHandle {
       const SymView<T> SV = symview<T>(V);
       T *r = vr<T>(V), *d = vd<T>(V), *e = ve<T>(V);
       const T* D = dinv<T>(V);
+      // term dots of each product's input come from the kernel that wrote it (no dot pass): the iterate's
+      // (buffer 0) while pre-smoothing, whose result the residual reads; each step's direction but the last's
+      T* B = tdb<T>(V);
+      const int deg = opt.cheb_degree, base = zero_start ? 1 : deg;
+      auto buf = [&](int i) { return B ? B + (size_t)i * V.nterms : nullptr; };
+      T* tdx = buf(0);
       if (zero_start) {
-        launch_cheb_first<T>(b, r, d, x, D, lp + l, V.ntotal, skip, s);
+        launch_cheb_first<T>(b, r, d, x, D, lp + l, V.ntotal, skip, s,
+                             term_acc<T>(V, deg > 1 ? buf(base) : nullptr, tdx));
       } else {
-        launch_sym<T>(SV, EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s);
-        launch_cheb_from_r<T>(r, d, x, D, lp + l, V.ntotal, skip, s);
+        launch_sym<T>(SV, EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s, tdx);
+        launch_cheb_from_r<T>(r, d, x, D, lp + l, V.ntotal, skip, s,
+                              term_acc<T>(V, deg > 1 ? buf(base) : nullptr, nullptr));
       }
-      for (int k = 0; k + 1 < opt.cheb_degree; ++k) {
-        launch_sym<T>(SV, EPI_CHEB, d, nullptr, nullptr, r, e, x, lp + l, k, skip, s);
+      for (int k = 0; k + 1 < deg; ++k) {
+        const bool last = k + 2 == deg;
+        launch_sym<T>(SV, EPI_CHEB, d, nullptr, nullptr, r, e, x, lp + l, k, skip, s, buf(base + k),
+                      term_acc<T>(V, last ? nullptr : buf(base + k + 1), zero_start ? tdx : nullptr));
         std::swap(d, e);
       }
       return;
@@ -1129,7 +1160,8 @@ struct FebHandle {
       A.r_in = (deg == 1) ? b : r; A.r_out = r;
       pair_run<T>(d, nullptr, &A, skip);
     }
-    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s);
+    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s, tdb<T>(C),
+                       kTermDotBufs * C.nterms);
     vcycle<T>(1, vb<T>(C), vx<T>(C), skip);
     launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), xs, skip, s);
     {
@@ -1163,15 +1195,18 @@ struct FebHandle {
     Level& C = L[l + 1];
     smooth<T>(l, b, x, true, skip);
     T *t = vt<T>(V), *r = vr<T>(V);
+    T* tdx = tdb<T>(V);   // level l's iterate dots (buffer 0; null at level 0 and on levels without terms)
     if (l > 0) {
-      launch_sym<T>(symview<T>(V), EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s);
+      launch_sym<T>(symview<T>(V), EPI_RESID, x, nullptr, b, r, nullptr, nullptr, nullptr, 0, skip, s, tdx);
     } else {
       apply<T>(l, x, t, skip);
       launch_residual<T>(b, t, r, 3 * V.ntotal, skip, s);
     }
-    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s);
+    launch_restrict<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, r, vb<T>(C), skip, s, tdb<T>(C),
+                       kTermDotBufs * C.nterms);
     vcycle<T>(l + 1, vb<T>(C), vx<T>(C), skip);
-    launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), x, skip, s);
+    launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), x, skip, s,
+                          term_acc<T>(V, nullptr, tdx));
     smooth<T>(l, b, x, false, skip);
   }
 
@@ -2410,11 +2445,16 @@ void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) want = std::min<uint64_t>(want, have + free_b / 2);
   if (have >= want) return;
   void* p = nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
   if (cudaMallocAsync(&p, want - have, caller) == cudaSuccess) {
     cudaFreeAsync(p, caller);
     cudaStreamSynchronize(caller);      // the block is free for the handle's own stream from here on
   }
   cudaGetLastError();                   // a failed reservation is not an error: set-up grows the pool as needed
+  if (std::getenv("FEB_POOL_LOG"))      // FEB_POOL_LOG=1: every growth on stderr (diagnostics)
+    std::fprintf(stderr, "feb pool: reserved %.2f -> %.2f GB (used peak %.2f GB) in %.2f ms\n", have / 1e9,
+                 want / 1e9, high / 1e9,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
 }
 
 int env_flag(const char* name) {

@@ -196,7 +196,7 @@ __device__ __forceinline__ void bj(const T* __restrict__ D, int64_t nn, int64_t 
 template <typename T>
 __global__ void k_cheb_first(const T* __restrict__ b, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
                              const T* __restrict__ D, const LevelParams* __restrict__ lp, int64_t nn,
-                             const int* __restrict__ skip) {
+                             const int* __restrict__ skip, TermAcc<T> acc) {
   if (skip && *skip) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nn) return;
@@ -207,6 +207,7 @@ __global__ void k_cheb_first(const T* __restrict__ b, T* __restrict__ r, T* __re
   z0 *= c; z1 *= c; z2 *= c;
   d[3 * i] = z0; d[3 * i + 1] = z1; d[3 * i + 2] = z2;
   x[3 * i] = z0; x[3 * i + 1] = z1; x[3 * i + 2] = z2;
+  term_acc(acc, i, z0, z1, z2);
 }
 
 template <typename T>
@@ -243,7 +244,8 @@ __global__ void k_cheb_step(const T* __restrict__ Ad, T* __restrict__ r, T* __re
 
 template <typename T>
 __global__ void k_cheb_from_r(const T* __restrict__ r, T* __restrict__ d, T* __restrict__ x, const T* __restrict__ D,
-                              const LevelParams* __restrict__ lp, int64_t nn, const int* __restrict__ skip) {
+                              const LevelParams* __restrict__ lp, int64_t nn, const int* __restrict__ skip,
+                              TermAcc<T> acc) {
   if (skip && *skip) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nn) return;
@@ -253,6 +255,7 @@ __global__ void k_cheb_from_r(const T* __restrict__ r, T* __restrict__ d, T* __r
   z0 *= c; z1 *= c; z2 *= c;
   d[3 * i] = z0; d[3 * i + 1] = z1; d[3 * i + 2] = z2;
   x[3 * i] += z0; x[3 * i + 1] += z1; x[3 * i + 2] += z2;
+  term_acc(acc, i, z0, z1, z2);
 }
 
 template <typename T>
@@ -388,8 +391,8 @@ void launch_dot_finalize(int kind, const Ta* a, const Tb* b, int64_t n, double* 
 
 template <typename T>
 void launch_cheb_first(const T* b, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
-                       const int* skip, cudaStream_t s) {
-  k_cheb_first<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, r, d, x, Dinv, lp, nn, skip); note_launch();
+                       const int* skip, cudaStream_t s, const TermAcc<T>& acc) {
+  k_cheb_first<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(b, r, d, x, Dinv, lp, nn, skip, acc); note_launch();
 }
 
 template <typename T>
@@ -406,8 +409,8 @@ void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelP
 
 template <typename T>
 void launch_cheb_from_r(const T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn, const int* skip,
-                        cudaStream_t s) {
-  k_cheb_from_r<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(r, d, x, Dinv, lp, nn, skip); note_launch();
+                        cudaStream_t s, const TermAcc<T>& acc) {
+  k_cheb_from_r<T><<<div_up(nn, kThreads), kThreads, 0, s>>>(r, d, x, Dinv, lp, nn, skip, acc); note_launch();
 }
 
 template <typename T>
@@ -464,14 +467,14 @@ void launch_mask_vector(double* v, const uint8_t* used, int64_t nn, double fill,
   template void launch_update_xr<T>(const T*, const T*, T*, T*, const CgState*, int64_t, double*, const int*,   \
                                     cudaStream_t);                                                             \
   template void launch_cheb_first<T>(const T*, T*, T*, T*, const T*, const LevelParams*, int64_t, const int*,   \
-                                     cudaStream_t);                                                            \
+                                     cudaStream_t, const TermAcc<T>&);                                         \
   template void launch_cheb_init<T>(const T*, const T*, T*, T*, T*, const T*, const LevelParams*, int64_t,      \
                                     const int*, cudaStream_t);                                                 \
   template void launch_cheb_step<T>(const T*, T*, T*, T*, const T*, const LevelParams*, int, int64_t,           \
                                     const int*, cudaStream_t);                                                 \
   template void launch_residual<T>(const T*, const T*, T*, int64_t, const int*, cudaStream_t);                 \
   template void launch_cheb_from_r<T>(const T*, T*, T*, const T*, const LevelParams*, int64_t, const int*,      \
-                                      cudaStream_t);                                                           \
+                                      cudaStream_t, const TermAcc<T>&);                                        \
   template void launch_axpy_dev<T>(const T*, T*, int64_t, const int*, cudaStream_t);
 INST_T(float)
 INST_T(double)

@@ -16,6 +16,44 @@ struct CgState {
   double rtrue;  // ||f - K x||^2 of the result (FIN_TRUE)
 };
 
+// Rank-1 term dots formed by the kernel that writes a coarse-level vector, instead of a dot pass before every
+// stencil product that reads it: for each node the kernel writes that some term touches (tn_ptr), the term's
+// lam_t v_t(node) . delta(node) is added atomically to dot_a[t] and dot_b[t] (either may be null; both zeroed
+// beforehand), delta being the written direction or the change of the iterate.  tn_ptr null: nothing to do.
+template <typename T>
+struct TermAcc {
+  const int* tn_ptr = nullptr;
+  const int* tn_term = nullptr;
+  const T* tn_coef = nullptr;    // v_t at the node, 3 components per (node, term) pair
+  const T* t_lam = nullptr;
+  T* dot_a = nullptr;
+  T* dot_b = nullptr;
+};
+
+template <typename T>
+__device__ __forceinline__ void term_acc(const TermAcc<T>& A, int64_t n, T v0, T v1, T v2) {
+  if (!A.tn_ptr) return;
+  const int pe = A.tn_ptr[n + 1];
+  for (int p = A.tn_ptr[n]; p < pe; ++p) {
+    const int t = A.tn_term[p];
+    const T c = A.t_lam[t] * (A.tn_coef[3 * p] * v0 + A.tn_coef[3 * p + 1] * v1 + A.tn_coef[3 * p + 2] * v2);
+    if (A.dot_a) atomicAdd(A.dot_a + t, c);
+    if (A.dot_b) atomicAdd(A.dot_b + t, c);
+  }
+}
+// one component `comp` of the node's delta (a kernel whose threads own single components)
+template <typename T>
+__device__ __forceinline__ void term_acc1(const TermAcc<T>& A, int64_t n, int comp, T v) {
+  if (!A.tn_ptr) return;
+  const int pe = A.tn_ptr[n + 1];
+  for (int p = A.tn_ptr[n]; p < pe; ++p) {
+    const int t = A.tn_term[p];
+    const T c = A.t_lam[t] * A.tn_coef[3 * p + comp] * v;
+    if (A.dot_a) atomicAdd(A.dot_a + t, c);
+    if (A.dot_b) atomicAdd(A.dot_b + t, c);
+  }
+}
+
 // Per-level smoother parameters written by the power iteration.
 struct LevelParams {
   double lam, lmax, lmin;
@@ -55,7 +93,7 @@ void launch_dot_finalize(int kind, const Ta* a, const Tb* b, int64_t n, double* 
 // Chebyshev smoother pieces (Dinv SoA [9][nn], vectors AoS [3 nn])
 template <typename T>
 void launch_cheb_first(const T* b, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
-                       const int* skip, cudaStream_t s);
+                       const int* skip, cudaStream_t s, const TermAcc<T>& acc = TermAcc<T>());
 template <typename T>
 void launch_cheb_init(const T* b, const T* Ax, T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn,
                       const int* skip, cudaStream_t s);
@@ -65,7 +103,7 @@ void launch_cheb_step(const T* Ad, T* r, T* d, T* x, const T* Dinv, const LevelP
 // d = (1/theta) Dinv r, x += d  (Chebyshev start from a given residual)
 template <typename T>
 void launch_cheb_from_r(const T* r, T* d, T* x, const T* Dinv, const LevelParams* lp, int64_t nn, const int* skip,
-                        cudaStream_t s);
+                        cudaStream_t s, const TermAcc<T>& acc = TermAcc<T>());
 template <typename T>
 void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, cudaStream_t s);
 

@@ -91,9 +91,11 @@ typedef struct FebOptions {
   int32_t x0_mode;               /* start value x0: 0 as given; 1 its energy-optimal multiple; 2 (default) x0 + M (f -
                                     K x0) (one preconditioner application), then its energy-optimal multiple */
   int32_t level_kernel;          /* coarse-level stencil products (one node per thread, the 14 block slots over 4
-                                    warps): 0 (default) slot index a compile-time constant in FP32 products and a
-                                    run-time value in FP64 products (the faster form of each); 1 run-time in both;
-                                    2 compile-time in both */
+                                    warps), bits 0-1: 0 (default) slot index a compile-time constant in FP32
+                                    products and a run-time value in FP64 products (the faster form of each); 1
+                                    run-time in both; 2 compile-time in both.  Bit 2 (+4): the V-cycle's rank-1 term
+                                    dots by a dot pass before every product, instead of accumulated by the kernels
+                                    that write the vectors */
 } FebOptions;
 
 typedef struct FebInfo {

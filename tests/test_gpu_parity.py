@@ -428,28 +428,34 @@ def test_deferred_setup_is_joined_before_use(golden):
     assert rel(x2[ok].cpu().numpy(), x1[ok].cpu().numpy()) < 1e-7
 
 
+@pytest.mark.parametrize("kernels", [(1, 2), (0, 4)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_level_kernels_agree(golden, precision):
-    """The coarse-level stencil products with the slot index a run-time value (level_kernel 1) and a compile-time
-    constant (level_kernel 2) give the same preconditioner: z = M r agrees to 1e-12 (FP64 V-cycle) / 1e-4 (FP32
-    V-cycle: the products round in other orders) relative, and the solves take the same iterations (+-1) to the
-    same solution."""
+def test_level_kernels_agree(golden, precision, kernels):
+    """Forms of the coarse-level products give the same preconditioner: the slot index a run-time value
+    (level_kernel 1) or a compile-time constant (2); the rank-1 term dots accumulated by the kernels that write
+    the vectors (0) or formed by a dot pass before each product (4).  z = M r agrees to 1e-12 (FP64 V-cycle) /
+    1e-4 (FP32 V-cycle: sums round in other orders) relative, and the solves take the same iterations (+-1) to
+    the same solution."""
     import torch
     z, g = _hindfoot(golden)
     args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
             [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z))
     ntotal = len(z["orig"])
     r = torch.randn(3 * ntotal, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    levels = []
     out = {}
-    for lk in (1, 2):
-        ctx = engine.prepare_cn(*args, tol=1e-10, precision=precision, options=dict(level_kernel=lk))
+    for lk in kernels:
+        # min_dofs 300: levels 1 and 2 of the 24 x 18 x 16 grid are stencil levels carrying the springs' terms
+        ctx = engine.prepare_cn(*args, tol=1e-10, precision=precision, options=dict(level_kernel=lk, min_dofs=300))
         try:
             zr = ctx["P"].precondition(r).cpu().numpy()
             x, info = ctx["P"].solve(ctx["f"], ctx["x0"])
             out[lk] = (zr, x.cpu().numpy(), info.iters, info.flag)
+            levels.append(int(info.levels))
         finally:
             ctx["P"].close()
-    (z1, x1, it1, f1), (z2, x2, it2, f2) = out[1], out[2]
+    assert min(levels) >= 4              # two stencil levels below the fine level and above the dense one
+    (z1, x1, it1, f1), (z2, x2, it2, f2) = out[kernels[0]], out[kernels[1]]
     assert f1 == 0 and f2 == 0 and abs(it1 - it2) <= 1
     assert rel(z2, z1) < (1e-12 if precision == "fp64" else 1e-4)
     assert rel(x2, x1) < 1e-8
