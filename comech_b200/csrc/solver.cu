@@ -554,45 +554,57 @@ __global__ void k_axpy_inplace(double* x, const double* y, int64_t n, double a) 
   if (i < n) x[i] += a * y[i];
 }
 
-// Rigid groups: per group (one CTA each) the number of its nodes that are used; a node id out of range sets
-// *bad.  Then the used nodes of the kept groups are compacted in their given order (one CTA per group, a
-// block-wide scan per chunk of 1024 entries).
+// Rigid groups, filtered on the device.  Group g's entries are cut into chunks of 1024 (one CTA per chunk and
+// group): the count pass writes each chunk's number of used nodes and adds it to the group's count (a node id
+// out of range sets *bad); the compaction pass writes the used nodes of the kept groups in their given order,
+// each chunk at the group's destination offset plus the counts of the group's earlier chunks.
 __global__ void __launch_bounds__(1024)
 k_group_count(const int64_t* __restrict__ nodes, const int64_t* __restrict__ off, const uint8_t* __restrict__ used,
-              int64_t ntotal, int* __restrict__ count, int* __restrict__ bad) {
-  const int g = blockIdx.x;
-  int c = 0;
-  for (int64_t e = off[g] + threadIdx.x; e < off[g + 1]; e += blockDim.x) {
-    const int64_t n = nodes[e];
-    if (n < 0 || n >= ntotal) { atomicExch(bad, 1); continue; }
-    c += used[n] ? 1 : 0;
+              int64_t ntotal, int ngroups, int nchunk, int* __restrict__ chunk_cnt, int* __restrict__ count,
+              int* __restrict__ bad) {
+  for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
+    const int64_t e = off[g] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int c = 0;
+    if (e < off[g + 1]) {
+      const int64_t n = nodes[e];
+      if (n < 0 || n >= ntotal) atomicExch(bad, 1);
+      else c = used[n] ? 1 : 0;
+    }
+    c = block_sum(c);
+    if (threadIdx.x == 0) {
+      chunk_cnt[(size_t)g * nchunk + blockIdx.x] = c;
+      if (c) atomicAdd(count + g, c);
+    }
+    __syncthreads();   // block_sum's shared scratch is reused by the next group
   }
-  c = block_sum(c);
-  if (threadIdx.x == 0) count[g] = c;
 }
 
 __global__ void __launch_bounds__(1024)
 k_group_compact(const int64_t* __restrict__ nodes, const int64_t* __restrict__ off, const uint8_t* __restrict__ used,
-                const int* __restrict__ dst_off, int64_t* __restrict__ out) {
-  const int g = blockIdx.x;
-  if (dst_off[g] < 0) return;           // dropped group
+                int ngroups, int nchunk, const int* __restrict__ chunk_cnt, const int* __restrict__ dst_off,
+                int64_t* __restrict__ out) {
   __shared__ int warp_tot[32];
-  __shared__ int base;
-  if (threadIdx.x == 0) base = dst_off[g];
-  __syncthreads();
+  __shared__ int prior_s;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int64_t e0 = off[g]; e0 < off[g + 1]; e0 += blockDim.x) {
+  for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
+    if (dst_off[g] < 0) continue;       // dropped group (uniform over the CTA)
+    const int64_t e0 = off[g] + (int64_t)blockIdx.x * blockDim.x;
+    if (e0 >= off[g + 1]) continue;     // past the group's end (uniform)
+    int prior = 0;                      // used nodes in the group's earlier chunks
+    for (int q = threadIdx.x; q < (int)blockIdx.x; q += blockDim.x) prior += chunk_cnt[(size_t)g * nchunk + q];
+    prior = block_sum(prior);
+    if (threadIdx.x == 0) prior_s = prior;
+    __syncthreads();
+    prior = prior_s;
     const int64_t e = e0 + threadIdx.x;
     const bool keep = e < off[g + 1] && used[nodes[e]];
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     const int before = __popc(m & ((1u << lane) - 1u));
     if (lane == 0) warp_tot[w] = __popc(m);
     __syncthreads();
-    int prefix = 0, total = 0;
-    for (int q = 0; q < nw; ++q) { prefix += q < w ? warp_tot[q] : 0; total += warp_tot[q]; }
-    if (keep) out[base + prefix + before] = nodes[e];
-    __syncthreads();
-    if (threadIdx.x == 0) base += total;
+    int prefix = 0;
+    for (int q = 0; q < w && q < nw; ++q) prefix += warp_tot[q];
+    if (keep) out[dst_off[g] + prior + prefix + before] = nodes[e];
     __syncthreads();
   }
 }
@@ -2673,11 +2685,20 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   // keep used nodes of every group, drop groups with fewer than 4 (rb/splitfe.py:105-112); the filtering and
   // the compaction run on the device, the host sees the per-group counts only
   std::vector<int64_t> off_in(offsets, offsets + ngroups + 1);
+  int64_t maxlen = 0;
+  for (int g = 0; g < ngroups; ++g) {
+    if (off_in[g + 1] < off_in[g]) { set_last_error("feb_set_rigid_groups: offsets decrease at group %d", g); return FEB_ERR_ARG; }
+    maxlen = std::max(maxlen, off_in[g + 1] - off_in[g]);
+  }
+  const int nchunk = (int)std::max<int64_t>(1, (maxlen + 1023) / 1024);
+  const dim3 ggrid(nchunk, std::min(ngroups, 65535));
   int64_t* d_off_in = nullptr;
-  int *d_count = nullptr, *d_dst = nullptr;
+  int *d_count = nullptr, *d_dst = nullptr, *d_chunk = nullptr;
   FEB_TRY(H.pool.upload(&d_off_in, off_in.data(), off_in.size()));
   FEB_TRY(H.pool.zeros(&d_count, (size_t)ngroups + 1));     // counts, then the out-of-range flag
-  k_group_count<<<ngroups, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, H.ntotal, d_count, d_count + ngroups);
+  FEB_TRY(H.pool.alloc(&d_chunk, (size_t)ngroups * nchunk));
+  k_group_count<<<ggrid, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, H.ntotal, ngroups, nchunk, d_chunk, d_count,
+                                         d_count + ngroups);
   note_launch();
   std::vector<int> cnt(ngroups + 1);
   FEB_CUDA(cudaMemcpyAsync(cnt.data(), d_count, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, H.s));
@@ -2698,7 +2719,7 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   FEB_TRY(H.pool.upload(&d_dst, dst.data(), dst.size()));
   FEB_TRY(H.pool.upload(&doff, off.data(), off.size()));
   FEB_TRY(H.pool.alloc(&dnodes, (size_t)nkept));
-  k_group_compact<<<ngroups, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, d_dst, dnodes);
+  k_group_compact<<<ggrid, 1024, 0, H.s>>>(nodes, d_off_in, H.L[0].used, ngroups, nchunk, d_chunk, d_dst, dnodes);
   note_launch();
   FEB_TRY(H.pool.alloc(&cen, 3 * (size_t)G));
   RigidView& Z = H.Z;
@@ -2747,6 +2768,7 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   H.pool.free(d_off_in);
   H.pool.free(d_count);
   H.pool.free(d_dst);
+  H.pool.free(d_chunk);
   std::vector<double> Es((size_t)nc * nc);
   for (int i = 0; i < nc; ++i)
     for (int j = 0; j < nc; ++j) Es[(size_t)i * nc + j] = 0.5 * (Ec[(size_t)i * nc + j] + Ec[(size_t)j * nc + i]);
