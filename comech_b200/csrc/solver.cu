@@ -2456,9 +2456,14 @@ void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) want = std::min<uint64_t>(want, have + free_b / 2);
   if (have >= want) return;
+  // the pool serves a request from its free reserved memory first: to hold `want` it must be asked for all of it
+  // beyond what is in use now
+  uint64_t used = 0;
+  cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemCurrent, &used);
+  if (used >= want) return;
   void* p = nullptr;
   const auto t0 = std::chrono::steady_clock::now();
-  if (cudaMallocAsync(&p, want - have, caller) == cudaSuccess) {
+  if (cudaMallocAsync(&p, want - used, caller) == cudaSuccess) {
     cudaFreeAsync(p, caller);
     cudaStreamSynchronize(caller);      // the block is free for the handle's own stream from here on
   }
