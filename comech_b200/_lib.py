@@ -17,7 +17,7 @@ PREC = {"fp64": 0, "mixed": 1, "refine": 2}
 
 EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_solve", "feb_solve_batch", "feb_apply", "feb_precondition",
            "feb_export_solution", "feb_used_nodes", "feb_destroy", "feb_accumulate_nodal", "feb_cell_stress",
-           "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_benchmark_apply_set", "feb_launch_count", "feb_last_error",
+           "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_benchmark_apply_set", "feb_launch_count", "feb_pool_stats", "feb_last_error",
            "feb_region_forces", "feb_rigid_fit", "feb_relative_displacement", "feb_sample_cells",
            "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
            "feb_mix_materials", "feb_net_conv", "feb_net_wgrad", "feb_net_colsum", "feb_net_weights", "feb_net_head",
@@ -135,6 +135,7 @@ def load():
     lib.feb_net_head_grad.argtypes = [P, C.c_int32, C.c_int64, P, P, P, C.c_int32, P, P, P]
     lib.feb_net_loss.argtypes = [FebNetGrid, P, P, P, P, C.c_float, C.c_float, C.c_float, P, P, P]
     lib.feb_net_energy_loss.argtypes = [FebNetGrid, P, P, P, P, P, C.c_float, P, P, P]
+    lib.feb_pool_stats.argtypes = [P, P, P]
     lib.feb_launch_count.argtypes = []
     lib.feb_launch_count.restype = C.c_int64
     lib.feb_last_error.argtypes = []

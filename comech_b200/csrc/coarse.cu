@@ -126,18 +126,13 @@ __global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, con
 
 // x_f += P x_c on used fine nodes for even coarsening: per axis an even fine node takes its coarse node, an odd
 // one the mean of its two neighbours
+// even coarsening: the interpolated coarse value at fine grid position (pi, pj, pk)
 template <typename T>
-__global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, const uint8_t* __restrict__ used,
-                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip,
-                               TermAcc<T> acc) {
-  if (skip && *skip) return;
-  const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
-  if (pi >= fnx) return;
-  const int64_t n = pi + (int64_t)fnx * (pj + (int64_t)fny * pk);
-  if (!used[n]) return;
+__device__ __forceinline__ void even_interp(int cnx, int cny, int pi, int pj, int pk, const T* __restrict__ xc,
+                                            T& s0, T& s1, T& s2) {
   const int ni = (pi & 1) + 1, nj = (pj & 1) + 1, nk = (pk & 1) + 1;
   const T wi = T(ni == 2 ? 0.5 : 1.0), wj = T(nj == 2 ? 0.5 : 1.0), wk = T(nk == 2 ? 0.5 : 1.0);
-  T s0 = 0, s1 = 0, s2 = 0;
+  s0 = 0; s1 = 0; s2 = 0;
   for (int c = 0; c < nk; ++c)
     for (int b = 0; b < nj; ++b)
       for (int a = 0; a < ni; ++a) {
@@ -145,6 +140,33 @@ __global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, const uint8_t
         const T w = wi * wj * wk;
         s0 += w * xc[3 * K]; s1 += w * xc[3 * K + 1]; s2 += w * xc[3 * K + 2];
       }
+}
+
+// x_f += P x_c for even coarsening; grid (x blocks of 64, fny, fnz + extra): the z layers past fnz take the
+// split copies (ids fnnode .. fnnode + ncopy), which receive their grid position's value
+template <typename T>
+__global__ void k_prolong_even(int cnx, int cny, int fnx, int fny, int fnz, const uint8_t* __restrict__ used,
+                               const T* __restrict__ xc, T* __restrict__ xf, const int* __restrict__ skip,
+                               TermAcc<T> acc, int64_t fnnode, int64_t ncopy, const int* __restrict__ orig_copy) {
+  if (skip && *skip) return;
+  if ((int)blockIdx.z >= fnz) {
+    const int64_t c = ((int64_t)(blockIdx.z - fnz) * gridDim.y + blockIdx.y) * ((int64_t)gridDim.x * blockDim.x) +
+                      blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncopy) return;
+    const int o = orig_copy[c];
+    const int pi = o % fnx, pj = (o / fnx) % fny, pk = o / (fnx * fny);
+    T s0, s1, s2;
+    even_interp(cnx, cny, pi, pj, pk, xc, s0, s1, s2);
+    const int64_t n = fnnode + c;
+    xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
+    return;
+  }
+  const int pi = blockIdx.x * blockDim.x + threadIdx.x, pj = blockIdx.y, pk = blockIdx.z;
+  if (pi >= fnx) return;
+  const int64_t n = pi + (int64_t)fnx * (pj + (int64_t)fny * pk);
+  if (!used[n]) return;
+  T s0, s1, s2;
+  even_interp(cnx, cny, pi, pj, pk, xc, s0, s1, s2);
   xf[3 * n] += s0; xf[3 * n + 1] += s1; xf[3 * n + 2] += s2;
   term_acc(acc, n, s0, s1, s2);
 }
@@ -932,9 +954,12 @@ template <typename T>
 void launch_prolong_add(const TransferDev& P, int fnx, int fny, int fnz, int64_t fnnode, int64_t fntotal,
                         const int* orig_copy, const uint8_t* used, const T* xc, T* xf, const int* skip,
                         cudaStream_t s, const TermAcc<T>& acc) {
-  if (P.even) {
-    k_prolong_even<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P.ax[0].nc, P.ax[1].nc, fnx, fny, used, xc, xf,
-                                                                     skip, acc); note_launch();
+  if (P.even) {   // the copies ride in extra z layers of the same launch
+    const int64_t ncopy = fntotal - fnnode, layer = (int64_t)div_up(fnx, 64) * 64 * fny;
+    const int extra = (int)((ncopy + layer - 1) / layer);
+    k_prolong_even<T><<<dim3(div_up(fnx, 64), fny, fnz + extra), 64, 0, s>>>(
+        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, used, xc, xf, skip, acc, fnnode, ncopy, orig_copy); note_launch();
+    return;
   } else {
     k_prolong_grid<T><<<dim3(div_up(fnx, 64), fny, fnz), 64, 0, s>>>(P, fnx, fny, used, xc, xf, skip, acc); note_launch();
   }

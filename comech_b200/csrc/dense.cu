@@ -155,36 +155,26 @@ __global__ void k_gj_finish(double* __restrict__ M, int nd, int k0, int bs, cons
   }
 }
 
+// x = Minv b on the coarsest level in one launch: blocks [0, brows) take 8 rows each (warp per row, b gathered
+// through klist on the fly, the row's result written straight to its node); the remaining blocks zero the
+// entries of nodes outside the dense system (cmap < 0), a disjoint set.
 template <typename T>
-__global__ void k_dense_gather(const T* __restrict__ b, const int* __restrict__ cidx_list, int nk,
-                               double* __restrict__ bd, const int* __restrict__ skip) {
+__global__ void k_dense_solve(const double* __restrict__ Minv, int nd, const int* __restrict__ klist,
+                              const int* __restrict__ cmap, int64_t n, const T* __restrict__ b, T* __restrict__ x,
+                              int brows, const int* __restrict__ skip) {
   if (skip && *skip) return;
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= 3 * nk) return;
-  bd[e] = double(b[3 * (int64_t)cidx_list[e / 3] + e % 3]);
-}
-
-// warp per row
-__global__ void k_dense_gemv(const double* __restrict__ Minv, const double* __restrict__ x, double* __restrict__ y,
-                             int nd, const int* __restrict__ skip) {
-  if (skip && *skip) return;
-  int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
-  if (row >= nd) return;
-  const double* m = Minv + (size_t)row * nd;
-  double s = 0.0;
-  for (int j = lane; j < nd; j += 32) s += m[j] * x[j];
-  s = warp_sum(s);
-  if (lane == 0) y[row] = s;
-}
-
-template <typename T>
-__global__ void k_dense_scatter(const double* __restrict__ yd, const int* __restrict__ cmap, int64_t n,
-                                T* __restrict__ x, const int* __restrict__ skip) {
-  if (skip && *skip) return;
-  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= 3 * n) return;
-  int c = cmap[e / 3];
-  x[e] = c < 0 ? T(0) : T(yd[3 * c + e % 3]);
+  if ((int)blockIdx.x < brows) {
+    const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (row >= nd) return;
+    const double* m = Minv + (size_t)row * nd;
+    double acc = 0.0;
+    for (int j = lane; j < nd; j += 32) acc += m[j] * double(b[3 * (int64_t)klist[j / 3] + j % 3]);
+    acc = warp_sum(acc);
+    if (lane == 0) x[3 * (int64_t)klist[row / 3] + row % 3] = T(acc);
+    return;
+  }
+  const int64_t e = (int64_t)(blockIdx.x - brows) * blockDim.x + threadIdx.x;
+  if (e < 3 * n && cmap[e / 3] < 0) x[e] = T(0);
 }
 
 }  // namespace
@@ -241,16 +231,15 @@ size_t dense_scratch_doubles(int nd) { return (size_t)GJ_B * GJ_B + 2 * (size_t)
 
 template <typename T>
 void launch_dense_solve(const double* Minv, int nd, const int* klist, const int* cmap, int64_t n, const T* b, T* x,
-                        double* bd, double* xd, const int* skip, cudaStream_t s) {
-  int nk = nd / 3;
-  k_dense_gather<T><<<div_up(nd, kThreads), kThreads, 0, s>>>(b, klist, nk, bd, skip); note_launch();
-  k_dense_gemv<<<div_up(nd, 8), 256, 0, s>>>(Minv, bd, xd, nd, skip); note_launch();
-  k_dense_scatter<T><<<div_up(3 * n, kThreads), kThreads, 0, s>>>(xd, cmap, n, x, skip); note_launch();
+                        const int* skip, cudaStream_t s) {
+  const int brows = div_up(nd, 8);
+  k_dense_solve<T><<<brows + (int)div_up(3 * n, 256), 256, 0, s>>>(Minv, nd, klist, cmap, n, b, x, brows, skip);
+  note_launch();
 }
 
 template void launch_dense_solve<float>(const double*, int, const int*, const int*, int64_t, const float*, float*,
-                                        double*, double*, const int*, cudaStream_t);
+                                        const int*, cudaStream_t);
 template void launch_dense_solve<double>(const double*, int, const int*, const int*, int64_t, const double*, double*,
-                                         double*, double*, const int*, cudaStream_t);
+                                         const int*, cudaStream_t);
 
 }  // namespace feb

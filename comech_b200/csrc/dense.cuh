@@ -15,9 +15,10 @@ void launch_dense_add_entries(int nent, const int* rdof, const int* cdof, const 
 // non-positive pivot.
 void launch_dense_invert(double* M, int nd, double* scratch, int* status, cudaStream_t s);
 size_t dense_scratch_doubles(int nd);
-// x = Minv b on the kept nodes (klist: node of compact index, cmap: compact index of node or -1)
+// x = Minv b on the kept nodes (klist: node of compact index, cmap: compact index of node or -1; x is zeroed on
+// the other nodes), one launch
 template <typename T>
 void launch_dense_solve(const double* Minv, int nd, const int* klist, const int* cmap, int64_t n, const T* b, T* x,
-                        double* bd, double* xd, const int* skip, cudaStream_t s);
+                        const int* skip, cudaStream_t s);
 
 }  // namespace feb

@@ -81,8 +81,10 @@ struct SmoothArgs {
   const T* x_in = nullptr;
   T* x_out = nullptr;
   T* d_out = nullptr;
+  double* x_out64 = nullptr;   // the new iterate in FP64 (instead of, or besides, x_out): the V-cycle's result
   const LevelParams* lp = nullptr;
   int k = -1;
+  __host__ __device__ bool updates() const { return d_out || x_out || x_out64; }
 };
 
 struct PairConfig {

@@ -155,7 +155,7 @@ __device__ __forceinline__ void load_node_ops(const PairView<T>& F, const Smooth
     o.x[c] = S.x_in ? S.x_in[3 * n + c] : T(0);
     o.d[c] = need_dir ? u[3 * n + c] : T(0);
   }
-  if (S.d_out || S.x_out) {
+  if (S.updates()) {
     const T* D = F.dinv6 + n;
 #pragma unroll
     for (int q = 0; q < 6; ++q) o.D[q] = D[(size_t)q * F.ntotal];
@@ -173,7 +173,7 @@ __device__ __forceinline__ void node_update(const SmoothArgs<T>& S, T a1, T a2, 
 #pragma unroll
     for (int c = 0; c < 3; ++c) S.r_out[3 * n + c] = r[c];
   }
-  if (!S.d_out && !S.x_out) return;
+  if (!S.updates()) return;
   T z[3];
   z[0] = o.D[0] * r[0] + o.D[3] * r[1] + o.D[4] * r[2];
   z[1] = o.D[3] * r[0] + o.D[1] * r[1] + o.D[5] * r[2];
@@ -188,6 +188,10 @@ __device__ __forceinline__ void node_update(const SmoothArgs<T>& S, T a1, T a2, 
   if (S.x_out) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) S.x_out[3 * n + c] = o.x[c] + dn[c];
+  }
+  if (S.x_out64) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S.x_out64[3 * n + c] = double(o.x[c] + dn[c]);
   }
 }
 
@@ -217,7 +221,7 @@ k_fine_pair(PairView<T> F, const T* __restrict__ u, T* __restrict__ y, SmoothArg
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   T a1 = T(0), a2 = T(0);
   if constexpr (SMOOTH) {   // the Chebyshev coefficients (a residual-only step carries no parameters)
-    if (S.lp && (S.d_out || S.x_out)) {
+    if (S.lp && S.updates()) {
       a1 = S.k < 0 ? T(0) : T(S.lp->a1[S.k]);
       a2 = S.k < 0 ? T(S.lp->c_init) : T(S.lp->a2[S.k]);
     }

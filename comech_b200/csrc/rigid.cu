@@ -215,6 +215,19 @@ void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, doub
   if (Einv) k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip); note_launch();
 }
 
+template <typename T>
+void launch_rigid_coef(const RigidView& Z, const T* r, double* part, double* zr, double* coef, const double* Einv,
+                       const int* skip, cudaStream_t s, unsigned int* ctr) {
+  dim3 g(rigid_blocks(Z), Z.ngroups);
+  k_ztr_fused<T><<<g, kThreads, 0, s>>>(Z, r, part, Einv, zr, coef, ctr, skip); note_launch();
+}
+
+template <typename T>
+void launch_rigid_scatter(const RigidView& Z, const double* coef, T* z, const int* skip, cudaStream_t s) {
+  dim3 g(rigid_blocks(Z), Z.ngroups);
+  k_z_scatter<T><<<g, kThreads, 0, s>>>(Z, coef, z, skip); note_launch();
+}
+
 void launch_rigid_rho(const RigidView& Z, double* rho, cudaStream_t s) {
   dim3 g(rigid_blocks(Z), Z.ngroups);
   k_rigid_rho<<<g, kThreads, 0, s>>>(Z, rho); note_launch();
@@ -236,5 +249,11 @@ template void launch_rigid_apply<float>(const RigidView&, const float*, float*, 
                                         const double*, const int*, cudaStream_t, unsigned int*);
 template void launch_rigid_apply<double>(const RigidView&, const double*, double*, double*, double*, double*,
                                          const double*, const int*, cudaStream_t, unsigned int*);
+template void launch_rigid_coef<float>(const RigidView&, const float*, double*, double*, double*, const double*,
+                                       const int*, cudaStream_t, unsigned int*);
+template void launch_rigid_coef<double>(const RigidView&, const double*, double*, double*, double*, const double*,
+                                        const int*, cudaStream_t, unsigned int*);
+template void launch_rigid_scatter<float>(const RigidView&, const double*, float*, const int*, cudaStream_t);
+template void launch_rigid_scatter<double>(const RigidView&, const double*, double*, const int*, cudaStream_t);
 
 }  // namespace feb

@@ -27,6 +27,13 @@ void launch_centroids(const RigidView& Z, double* cen, double* part, cudaStream_
 template <typename T>
 void launch_rigid_apply(const RigidView& Z, const T* r, T* z, double* part, double* zr, double* coef,
                         const double* Einv, const int* skip, cudaStream_t s, unsigned int* ctr = nullptr);
+// the two halves of launch_rigid_apply (with ctr): coef = Einv Z^T r (reads r only, so it may run beside
+// whatever forms z), then z += Z coef
+template <typename T>
+void launch_rigid_coef(const RigidView& Z, const T* r, double* part, double* zr, double* coef, const double* Einv,
+                       const int* skip, cudaStream_t s, unsigned int* ctr);
+template <typename T>
+void launch_rigid_scatter(const RigidView& Z, const double* coef, T* z, const int* skip, cudaStream_t s);
 // zr = Z^T r
 void launch_ztr(const RigidView& Z, const double* r, double* part, double* zr, cudaStream_t s);
 // v += column col of Z

@@ -897,7 +897,7 @@ struct FebHandle {
   int coarsest = 0;
   // dense coarsest level
   int nd = 0;
-  double *Minv = nullptr, *bd = nullptr, *xd = nullptr;
+  double *Minv = nullptr;
   int *klist = nullptr, *cmap = nullptr;
   // scalars
   LevelParams* lp = nullptr;
@@ -997,7 +997,14 @@ struct FebHandle {
     return FEB_OK;
   }
 
+  // the rigid-mode coefficients' stream (set with the rigid groups) and its fork / join events
+  cudaStream_t rs = nullptr;
+  cudaEvent_t rs_fork = nullptr, rs_join = nullptr;
+
   ~FebHandle() {
+    if (rs) { cudaStreamSynchronize(rs); g_streams.give(rs); }
+    g_streams.give(rs_fork);
+    g_streams.give(rs_join);
     if (dense_s) { cudaStreamSynchronize(dense_s); g_streams.give(dense_s); }
     g_streams.give(dense_ev);
     g_pinned.give(dense_st_h);
@@ -1153,8 +1160,9 @@ struct FebHandle {
   // Level-0 V-cycle leg with the smoother fused into the paired K.u (same arithmetic as smooth() +
   // residual + transfers): pre-smoothing from zero keeps x = d0 + d1 + ... and the residual of the smoothed
   // iterate is r - K d_last; post-smoothing starts from xs and writes the result into x.
+  // x64 (optional): the last post-smoothing step writes the result there in FP64 instead of into x
   template <typename T>
-  void vcycle0_pair(const T* b, T* x, const int* skip) {
+  void vcycle0_pair(const T* b, T* x, const int* skip, double* x64 = nullptr) {
     Level& V = L[0];
     Level& C = L[1];
     T *r = vr<T>(V), *d = vd<T>(V), *e = ve<T>(V), *xs = vt<T>(V);
@@ -1178,14 +1186,16 @@ struct FebHandle {
     launch_prolong_add<T>(V.P, V.nx, V.ny, V.nz, V.nnode, V.ntotal, orig_copy, V.used, vx<T>(C), xs, skip, s);
     {
       SmoothArgs<T> A;
-      A.r_in = b; A.r_out = deg > 1 ? r : nullptr; A.x_in = xs; A.x_out = x; A.d_out = deg > 1 ? d : nullptr;
+      A.r_in = b; A.r_out = deg > 1 ? r : nullptr; A.x_in = xs; A.d_out = deg > 1 ? d : nullptr;
+      if (deg == 1 && x64) A.x_out64 = x64; else A.x_out = x;
       A.lp = lp; A.k = -1;
       pair_run<T>(xs, nullptr, &A, skip);
     }
     for (int k = 1; k < deg; ++k) {
       const bool last = (k == deg - 1);
       SmoothArgs<T> A;
-      A.r_in = r; A.r_out = last ? nullptr : r; A.x_in = x; A.x_out = x; A.d_out = last ? nullptr : e; A.lp = lp;
+      A.r_in = r; A.r_out = last ? nullptr : r; A.x_in = x; A.d_out = last ? nullptr : e; A.lp = lp;
+      if (last && x64) A.x_out64 = x64; else A.x_out = x;
       A.k = k - 1;
       pair_run<T>(d, nullptr, &A, skip);
       std::swap(d, e);
@@ -1200,7 +1210,7 @@ struct FebHandle {
     }
     if (l == coarsest) {
       Level& V = L[l];
-      launch_dense_solve<T>(Minv, nd, klist, cmap, V.ntotal, b, x, bd, xd, skip, s);
+      launch_dense_solve<T>(Minv, nd, klist, cmap, V.ntotal, b, x, skip, s);
       return;
     }
     Level& V = L[l];
@@ -1227,18 +1237,33 @@ struct FebHandle {
   template <typename T>
   void precondition(const T* r_, T* z_, const int* skip, bool rf_ready = false) {
     const int64_t n = 3 * ntotal;
+    if (has_rigid && rs) {   // Einv Z^T r reads r only: it runs on the rigid-mode stream beside the V-cycle
+      cudaEventRecord(rs_fork, s);
+      cudaStreamWaitEvent(rs, rs_fork, 0);
+      launch_rigid_coef<T>(Z, r_, zpart, zr, zcoef, Einv, skip, rs, ctr + 1);
+      cudaEventRecord(rs_join, rs);
+    }
     if constexpr (std::is_same<T, double>::value) {
       if (opt.precision == FEB_PREC_FP64) {
         vcycle<double>(0, r_, z_, skip);
       } else {
         if (!rf_ready) launch_convert<double, float>(r_, rf, n, skip, s);
-        vcycle<float>(0, rf, zf, skip);
-        launch_convert<float, double>(zf, z_, n, skip, s);
+        if (coarsest > 0 && pair_on<float>()) {
+          vcycle0_pair<float>(rf, zf, skip, z_);   // its last smoothing step writes z in FP64
+        } else {
+          vcycle<float>(0, rf, zf, skip);
+          launch_convert<float, double>(zf, z_, n, skip, s);
+        }
       }
     } else {
       vcycle<float>(0, r_, z_, skip);
     }
-    if (has_rigid) launch_rigid_apply<T>(Z, r_, z_, zpart, zr, zcoef, Einv, skip, s, ctr + 1);
+    if (has_rigid && rs) {
+      cudaStreamWaitEvent(s, rs_join, 0);
+      launch_rigid_scatter<T>(Z, zcoef, z_, skip, s);
+    } else if (has_rigid) {
+      launch_rigid_apply<T>(Z, r_, z_, zpart, zr, zcoef, Einv, skip, s, ctr + 1);
+    }
   }
 
   // one CG iteration (SciPy order: z = M r, beta, p, q = A p, alpha, x, r, convergence)
@@ -2191,8 +2216,6 @@ int build_dense(FebHandle* h) {
   FEB_TRY(H.pool.upload(&H.cmap, cmap.data(), cmap.size()));
   FEB_TRY(H.pool.upload(&H.klist, klist.data(), klist.size()));
   FEB_TRY(H.pool.zeros(&H.Minv, (size_t)H.nd * H.nd));
-  FEB_TRY(H.pool.alloc(&H.bd, H.nd));
-  FEB_TRY(H.pool.alloc(&H.xd, H.nd));
   int *dr = nullptr, *dc = nullptr;
   double* dv = nullptr;
   if (H.coarsest > 0 && V.sparse.size()) {
@@ -2441,6 +2464,8 @@ int check_tc_status(FebHandle* h) {
 // used-memory peak drifts a little from one set-up to the next (whether a block freed on one stream is
 // reused by another depends on timing), so the pool is grown only on a real shortage, reserved memory below
 // 1.25 x that peak or below the size estimate, not whenever the peak passes half of the reservation.
+std::atomic<int> g_pool_grows{0};
+
 void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   int dev = 0;
   cudaMemPool_t mp;
@@ -2466,6 +2491,10 @@ void reserve_pool(int64_t nnode, int64_t nnode_total, cudaStream_t caller) {
   if (cudaMallocAsync(&p, want - used, caller) == cudaSuccess) {
     cudaFreeAsync(p, caller);
     cudaStreamSynchronize(caller);      // the block is free for the handle's own stream from here on
+    // the reservation itself must not count as a set-up's peak (the next handle would double it again)
+    uint64_t reset = 0;
+    cudaMemPoolSetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &reset);
+    g_pool_grows.fetch_add(1);
   }
   cudaGetLastError();                   // a failed reservation is not an error: set-up grows the pool as needed
   if (std::getenv("FEB_POOL_LOG"))      // FEB_POOL_LOG=1: every growth on stderr (diagnostics)
@@ -2747,6 +2776,12 @@ int feb_set_rigid_groups(FebHandle* h, int32_t ngroups, const int64_t* offsets, 
   FEB_TRY(H.pool.alloc(&kcol, 3 * (size_t)H.ntotal));
   FEB_TRY(H.pool.alloc(&Ecd, (size_t)nc * nc));
   FEB_TRY(H.wait_fine());
+  if (!H.rs) {
+    H.rs = g_streams.stream();
+    if (!H.rs_fork) H.rs_fork = g_streams.event();
+    if (!H.rs_join) H.rs_join = g_streams.event();
+    if (!H.rs || !H.rs_fork || !H.rs_join) { set_last_error("feb_set_rigid_groups: stream / event creation failed"); return FEB_ERR_CUDA; }
+  }
   for (int c = 0; c < nc; ++c) {
     FEB_CUDA(cudaMemsetAsync(col, 0, 3 * (size_t)H.ntotal * sizeof(double), H.s));
     launch_z_column(Z, c, col, H.s);
@@ -3021,6 +3056,20 @@ int feb_used_nodes(FebHandle* h, int64_t* nused, uint8_t* mask) {
 }
 
 int64_t feb_launch_count(void) { return g_launches.load(); }
+
+int feb_pool_stats(int64_t* reserved, int64_t* used_peak, int32_t* grow_events) {
+  int dev = 0;
+  cudaMemPool_t mp;
+  FEB_CUDA(cudaGetDevice(&dev));
+  FEB_CUDA(cudaDeviceGetDefaultMemPool(&mp, dev));
+  uint64_t have = 0, high = 0;
+  FEB_CUDA(cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &have));
+  FEB_CUDA(cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &high));
+  if (reserved) *reserved = (int64_t)have;
+  if (used_peak) *used_peak = (int64_t)high;
+  if (grow_events) *grow_events = g_pool_grows.load();
+  return FEB_OK;
+}
 
 int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void* y, int32_t nrep, float* ms) {
   if (!h || !u || !y || nrep < 1 || !ms) { set_last_error("feb_benchmark_apply: bad argument"); return FEB_ERR_ARG; }

@@ -465,6 +465,10 @@ FEB_API int feb_benchmark_apply_set(FebHandle* h, int32_t prec, int32_t nbuf, co
 /* Kernels launched by this library since it was loaded (graph launches count their kernel nodes). */
 FEB_API int64_t feb_launch_count(void);
 
+/* The current device's default memory pool, which serves every handle: bytes reserved, the used-memory peak
+   since the last reservation, and how many times feb_create has grown the reservation in this process. */
+FEB_API int feb_pool_stats(int64_t* reserved, int64_t* used_peak, int32_t* grow_events);
+
 FEB_API const char* feb_last_error(void);
 
 #ifdef __cplusplus

@@ -459,3 +459,28 @@ def test_level_kernels_agree(golden, precision, kernels):
     assert f1 == 0 and f2 == 0 and abs(it1 - it2) <= 1
     assert rel(z2, z1) < (1e-12 if precision == "fp64" else 1e-4)
     assert rel(x2, x1) < 1e-8
+
+
+def test_pool_reservation_settles(golden):
+    """Handles come and go on one device pool: after the first handle of a problem, creating and closing more of
+    the same size grows the reservation no further (a reservation that counted itself as a set-up's peak would
+    double at every handle)."""
+    import ctypes as C
+    z, g = _hindfoot(golden)
+    args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
+            [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z))
+    lib = _lib.load()
+
+    def stats():
+        res, peak, grows = C.c_int64(), C.c_int64(), C.c_int32()
+        _lib.check(lib.feb_pool_stats(C.byref(res), C.byref(peak), C.byref(grows)))
+        return res.value, grows.value
+
+    engine.prepare_cn(*args, tol=1e-8, precision="mixed")["P"].close()
+    engine.prepare_cn(*args, tol=1e-8, precision="mixed")["P"].close()
+    before = stats()
+    for _ in range(4):
+        ctx = engine.prepare_cn(*args, tol=1e-8, precision="mixed")
+        ctx["P"].solve(ctx["f"], ctx["x0"])
+        ctx["P"].close()
+    assert stats() == before
