@@ -52,14 +52,17 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    """nvidia-smi sampler.  It is started before the warm-up steps, so that nvidia-smi's own start-up (NVML
+    initialisation over every GPU of the node, which holds the driver's locks for a while) is over before timing
+    begins; only the samples inside the timed window (`window`) are summarised."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -69,6 +72,9 @@ class Clocks:
         except Exception:
             self.proc = None
         return self
+
+    def window(self, t0, t1):
+        self.t0, self.t1 = t0, t1
 
     def __exit__(self, *a):
         self.rows = []
@@ -81,10 +87,22 @@ class Clocks:
         except Exception:
             self.proc.kill()
             out = ""
+        import datetime
+        rows = []
         for line in out.strip().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                self.rows.append(f)
+            if len(f) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                ts = None
+            rows.append((ts, f[1:]))
+        if self.t0 is not None:   # the timed window, widened by one sampling period so that it holds a sample
+            inside = [r for ts, r in rows if ts is not None and self.t0 - 0.2 <= ts <= self.t1 + 0.2]
+            self.rows = inside or [r for _, r in rows]
+        else:
+            self.rows = [r for _, r in rows]
 
     def summary(self):
         if not getattr(self, "rows", None):
@@ -95,7 +113,6 @@ class Clocks:
         reasons = sorted({names[i] for r in self.rows for i, v in enumerate(r[5:9]) if v.lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
-
 
 def rank_seed(rank):
     """Seed of the instance a rank solves (independent instances, weak scaling)."""
@@ -376,15 +393,22 @@ def run_ours(args, rank, world, dist):
     info_of = lambda out: (round(out[2].t_setup_ms, 2), round(out[2].t_solve_ms, 2), int(out[2].iters),
                            getattr(device_solve, "host_ms", None), round(out[2].t_stage_ms[7], 2))
     for name, pr_, w_ in arms:
+        clk = Clocks(dev) if name == "headline" else None
+        if clk:
+            clk.__enter__()      # before the warm-up: nvidia-smi's start-up is over when timing begins
         for _ in range(args.warmup):
             device_solve(P, d, pr_, warm=w_)
         torch.cuda.synchronize()
         launches0 = lib.feb_launch_count()
         timed_steps.details = []
         if name == "headline":
-            with Clocks(dev) as clk:
+            try:
+                t_a = time.time()
                 ms, out = timed_steps(lambda: device_solve(P, d, pr_, warm=w_), args.steps, flush, dist,
                                       per_step=info_of)
+                clk.window(t_a, time.time())
+            finally:
+                clk.__exit__(None, None, None)
             clk_summary = clk.summary()
             launches = (lib.feb_launch_count() - launches0) // max(args.steps, 1)
         else:

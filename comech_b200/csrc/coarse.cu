@@ -95,7 +95,9 @@ __global__ void k_restrict_grid(TransferDev P, int fnx, int fny, const T* __rest
 // weight 1 (a = 0) or 1/2 (a = +-1)
 template <typename T>
 __global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, const T* __restrict__ rf,
-                                T* __restrict__ rc, const int* __restrict__ skip, T* __restrict__ zero, int nzero) {
+                                T* __restrict__ rc, const int* __restrict__ skip, T* __restrict__ zero, int nzero,
+                                const int* __restrict__ cp_ptr, const int* __restrict__ cp_copy,
+                                const double* __restrict__ cp_w, int64_t fnnode) {
   if (skip && *skip) return;
   if (nzero && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
     for (int e = threadIdx.x; e < nzero; e += blockDim.x) zero[e] = T(0);
@@ -121,6 +123,13 @@ __global__ void k_restrict_even(int cnx, int cny, int fnx, int fny, int fnz, con
     }
   }
   const int64_t J = jx + (int64_t)cnx * (jy + (int64_t)cny * jz);
+  if (cp_ptr) {   // split copies restricting into J, in ascending copy order
+    for (int e = cp_ptr[J]; e < cp_ptr[J + 1]; ++e) {
+      const int64_t f = fnnode + cp_copy[e];
+      const T w = T(cp_w[e]);
+      s0 += w * rf[3 * f]; s1 += w * rf[3 * f + 1]; s2 += w * rf[3 * f + 2];
+    }
+  }
   rc[3 * J] = s0; rc[3 * J + 1] = s1; rc[3 * J + 2] = s2;
 }
 
@@ -939,7 +948,9 @@ void launch_restrict(const TransferDev& P, int fnx, int fny, int fnz, int64_t fn
   if (!zero) nzero = 0;
   if (P.even) {
     k_restrict_even<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(
-        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, rf, rc, skip, zero, nzero); note_launch();
+        P.ax[0].nc, P.ax[1].nc, fnx, fny, fnz, rf, rc, skip, zero, nzero, P.cp_ptr, P.cp_copy, P.cp_w, fnnode);
+    note_launch();
+    if (P.cp_ptr) return;   // the copies were gathered
   } else {
     k_restrict_grid<T><<<dim3(div_up(P.ax[0].nc, 64), P.ax[1].nc, P.ax[2].nc), 64, 0, s>>>(P, fnx, fny, rf, rc, skip,
                                                                                          zero, nzero); note_launch();

@@ -21,6 +21,11 @@ struct TransferDev {
   AxisDev ax[3];
   int even = 0;   // 1: every axis coarsens 2 n - 1 -> n nodes with weights 1 and 1/2 (uniform spacing, even cell
                   // counts); the transfers then index directly instead of reading the axis tables
+  // even coarsening of a level with split copies: per coarse node J the copies that restrict into it,
+  // entries cp_ptr[J] .. cp_ptr[J+1] of (copy index, weight), so that the restriction gathers them (no atomics)
+  const int* cp_ptr = nullptr;
+  const int* cp_copy = nullptr;
+  const double* cp_w = nullptr;
 };
 
 // Structured level (>= 1): nodes nx*ny*nz (x fastest), stencil A[o*9 + 3r + c][n], o = (dx+1) + 3(dy+1) + 9(dz+1)

@@ -1507,6 +1507,36 @@ int upload_transfer(Pool& pool, Level& V) {
   return FEB_OK;
 }
 
+// the split copies' restriction as a gather per coarse node (even coarsening): copy c sits at fine grid
+// position orig_copy[c] and restricts with the weights of that position
+int upload_copy_gather(Pool& pool, Level& V, const std::vector<int64_t>& orig_copy) {
+  if (!V.P.even || orig_copy.empty()) return FEB_OK;
+  const int fnx = V.nx, fny = V.ny, cnx = V.ax[0].nc, cny = V.ax[1].nc, cnz = V.ax[2].nc;
+  const int64_t nc = (int64_t)cnx * cny * cnz;
+  std::vector<int> cnt(nc + 1, 0);
+  auto each = [&](int64_t o, auto&& f) {
+    const int pi = int(o % fnx), pj = int((o / fnx) % fny), pk = int(o / ((int64_t)fnx * fny));
+    const int ni = (pi & 1) + 1, nj = (pj & 1) + 1, nk = (pk & 1) + 1;
+    const double w = (ni == 2 ? 0.5 : 1.0) * (nj == 2 ? 0.5 : 1.0) * (nk == 2 ? 0.5 : 1.0);
+    for (int c = 0; c < nk; ++c)
+      for (int b = 0; b < nj; ++b)
+        for (int a = 0; a < ni; ++a) f((pi >> 1) + a + (int64_t)cnx * ((pj >> 1) + b + (int64_t)cny * ((pk >> 1) + c)), w);
+  };
+  for (size_t c = 0; c < orig_copy.size(); ++c) each(orig_copy[c], [&](int64_t J, double) { cnt[J + 1]++; });
+  for (int64_t J = 0; J < nc; ++J) cnt[J + 1] += cnt[J];
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1), copy(cnt[nc]);
+  std::vector<double> w(cnt[nc]);
+  for (size_t c = 0; c < orig_copy.size(); ++c)      // ascending copy index within each coarse node
+    each(orig_copy[c], [&](int64_t J, double wt) { const int at = fill[J]++; copy[at] = (int)c; w[at] = wt; });
+  int *ptr, *cp;
+  double* wd;
+  FEB_TRY(pool.upload(&ptr, cnt.data(), cnt.size()));
+  FEB_TRY(pool.upload(&cp, copy.data(), copy.size()));
+  FEB_TRY(pool.upload(&wd, w.data(), w.size()));
+  V.P.cp_ptr = ptr; V.P.cp_copy = cp; V.P.cp_w = wd;
+  return FEB_OK;
+}
+
 // 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients, in precision T.
 // (on h->s, with the reduction scratch `part`)
 template <typename T>
@@ -2273,6 +2303,7 @@ int build_hierarchy(FebHandle* h) {
     // transfer l -> l+1
     for (int d = 0; d < 3; ++d) V.ax[d] = make_axis(V.coord[d]);
     FEB_TRY(upload_transfer(H.pool, V));
+    if (l == 0) FEB_TRY(upload_copy_gather(H.pool, V, H.orig_copy_h));
     g_prof.mark("Lk transfer", H.s);
     H.L.emplace_back();
     Level& C = H.L.back();

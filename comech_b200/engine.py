@@ -48,6 +48,20 @@ def _dev(a, dtype):
     return t.to("cuda", non_blocking=False)
 
 
+def _dev_cat(arrays, dtype):
+    """One device tensor of the arrays' concatenation, uploaded piece by piece (no host-side concatenation);
+    the copies are asynchronous from page-locked sources, which the caller keeps until its stream is synchronised."""
+    torch = _torch()
+    parts = [a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=dtype).ravel())
+             for a in arrays]
+    out = torch.empty(sum(int(p.numel()) for p in parts), dtype=getattr(torch, _TDT[dtype]), device="cuda")
+    at = 0
+    for p in parts:
+        out[at:at + p.numel()].copy_(p.reshape(-1), non_blocking=True)
+        at += p.numel()
+    return out
+
+
 def _host(*ts):
     """NumPy copies of device tensors through page-locked buffers (torch's caching host allocator reuses them
     once the arrays are released), one stream synchronisation for all of them."""
@@ -271,7 +285,7 @@ def prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_grou
         return np.unique(np.asarray(cn)[np.flatnonzero(active)])
 
     coo = _extra_entries(extra, used_nodes, ntotal)
-    mat = np.concatenate([np.asarray(lam, np.float64).ravel(), np.asarray(mu, np.float64).ravel()])
+    mat = _dev_cat((lam, mu), np.float64)
     stamps.append(("host_inputs", time.perf_counter()))
     P = Problem(g, _lib.MAT_ISO_SRI, mat, active, cn=cn, orig=orig, pen_node=fn, pen_k=pen_k, extra_coo=coo,
                 precision=precision, tol=tol, maxiter=maxiter, options=options)
@@ -286,7 +300,8 @@ def prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_grou
             from . import warmnet
             net = warmnet.default_net() if warm_start is True else warm_start
             ln, lz = warmnet.load_z(loads)
-            x0d = net.predict_x0(g, lam, mu, active, orig, fn, ln, lz, ntotal, orig_dev=P.orig)
+            nc = g.nx * g.ny * g.nz       # the operator's device copies of lam, mu and active serve the network too
+            x0d = net.predict_x0(g, P.mat[:nc], P.mat[nc:], P.active, orig, fn, ln, lz, ntotal, orig_dev=P.orig)
             stamps.append(("warm_start", time.perf_counter()))
         else:
             x0d = None
