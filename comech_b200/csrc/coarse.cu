@@ -681,9 +681,15 @@ __global__ void k_term_dots(SymView<T> L, int nterms, const T* __restrict__ u, c
 // to the node itself and their u zeroed, so the loads carry no branches.  Q is a compile-time constant: the
 // offsets, the bounds tests and the plane offsets fold.  CMP: blocks of tagged (single-material) nodes are
 // formed from the patterns sp[2][126] and the material table sm[128][2] (shared memory) instead of read.
+// sym_load gathers a slot's operands, sym_acc applies them.
+template <typename T>
+struct SlotVals {
+  T f[9], g[9], uf[3], ub[3];
+};
+
 template <typename T, bool CMP, int Q>
-__device__ __forceinline__ void sym_slot(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
-                                         int k, int tn, const T* sp, const T* sm, T& a0, T& a1, T& a2) {
+__device__ __forceinline__ void sym_load(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
+                                         int k, int tn, const T* sp, const T* sm, SlotVals<T>& v) {
   constexpr int o = 13 + Q;
   constexpr int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
   const int nx = L.nx, ny = L.ny, nz = L.nz, nxp = L.nxp, NP = (int)L.np;
@@ -696,34 +702,48 @@ __device__ __forceinline__ void sym_slot(const SymView<T>& L, const T* __restric
   if constexpr (dy < 0) { vf = vf && j >= 1; vb = vb && j + 1 < ny; }
   if constexpr (dz > 0) { vf = vf && k + 1 < nz; vb = vb && k >= 1; }
   const int mf = vf ? n + off : n;
-  T uf0 = u[3 * mf], uf1 = u[3 * mf + 1], uf2 = u[3 * mf + 2];
-  if (!vf) { uf0 = 0; uf1 = 0; uf2 = 0; }
-  T fv[9];
-  auto stored = [&](int m, T (&v)[9]) {     // m: padded position
 #pragma unroll
-    for (int t = 0; t < 9; ++t) v[t] = B[(size_t)t * NP + m];
+  for (int c = 0; c < 3; ++c) v.uf[c] = u[3 * mf + c];
+  if (!vf) { v.uf[0] = 0; v.uf[1] = 0; v.uf[2] = 0; }
+  auto stored = [&](int m, T (&w)[9]) {     // m: padded position
+#pragma unroll
+    for (int t = 0; t < 9; ++t) w[t] = B[(size_t)t * NP + m];
   };
-  auto formed = [&](int tg, T (&v)[9]) {
+  auto formed = [&](int tg, T (&w)[9]) {
     const T lam = sm[2 * tg], mu = sm[2 * tg + 1];
 #pragma unroll
-    for (int t = 0; t < 9; ++t) v[t] = lam * sp[9 * Q + t] + mu * sp[126 + 9 * Q + t];
+    for (int t = 0; t < 9; ++t) w[t] = lam * sp[9 * Q + t] + mu * sp[126 + 9 * Q + t];
   };
-  if constexpr (CMP) { if (tn) formed(tn, fv); else stored(pn, fv); }
-  else stored(pn, fv);
-  a0 += fv[0] * uf0 + fv[1] * uf1 + fv[2] * uf2;
-  a1 += fv[3] * uf0 + fv[4] * uf1 + fv[5] * uf2;
-  a2 += fv[6] * uf0 + fv[7] * uf1 + fv[8] * uf2;
+  if constexpr (CMP) { if (tn) formed(tn, v.f); else stored(pn, v.f); }
+  else stored(pn, v.f);
   if constexpr (Q > 0) {
     const int mb = vb ? n - off : n, pb = vb ? pn - offp : pn;
-    T ub0 = u[3 * mb], ub1 = u[3 * mb + 1], ub2 = u[3 * mb + 2];
-    if (!vb) { ub0 = 0; ub1 = 0; ub2 = 0; }
-    T gv[9];
-    if constexpr (CMP) { const int tm = L.tag[mb]; if (tm) formed(tm, gv); else stored(pb, gv); }
-    else stored(pb, gv);
-    a0 += gv[0] * ub0 + gv[3] * ub1 + gv[6] * ub2;
-    a1 += gv[1] * ub0 + gv[4] * ub1 + gv[7] * ub2;
-    a2 += gv[2] * ub0 + gv[5] * ub1 + gv[8] * ub2;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.ub[c] = u[3 * mb + c];
+    if (!vb) { v.ub[0] = 0; v.ub[1] = 0; v.ub[2] = 0; }
+    if constexpr (CMP) { const int tm = L.tag[mb]; if (tm) formed(tm, v.g); else stored(pb, v.g); }
+    else stored(pb, v.g);
   }
+}
+
+template <typename T, int Q>
+__device__ __forceinline__ void sym_acc(const SlotVals<T>& v, T& a0, T& a1, T& a2) {
+  a0 += v.f[0] * v.uf[0] + v.f[1] * v.uf[1] + v.f[2] * v.uf[2];
+  a1 += v.f[3] * v.uf[0] + v.f[4] * v.uf[1] + v.f[5] * v.uf[2];
+  a2 += v.f[6] * v.uf[0] + v.f[7] * v.uf[1] + v.f[8] * v.uf[2];
+  if constexpr (Q > 0) {
+    a0 += v.g[0] * v.ub[0] + v.g[3] * v.ub[1] + v.g[6] * v.ub[2];
+    a1 += v.g[1] * v.ub[0] + v.g[4] * v.ub[1] + v.g[7] * v.ub[2];
+    a2 += v.g[2] * v.ub[0] + v.g[5] * v.ub[1] + v.g[8] * v.ub[2];
+  }
+}
+
+template <typename T, bool CMP, int Q>
+__device__ __forceinline__ void sym_slot(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
+                                         int k, int tn, const T* sp, const T* sm, T& a0, T& a1, T& a2) {
+  SlotVals<T> v;
+  sym_load<T, CMP, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, v);
+  sym_acc<T, Q>(v, a0, a1, a2);
 }
 
 // CMP: the level carries the compressed single-material blocks (tags); without them the pattern code is not
