@@ -484,3 +484,20 @@ def test_pool_reservation_settles(golden):
         ctx["P"].solve(ctx["f"], ctx["x0"])
         ctx["P"].close()
     assert stats() == before
+
+
+def test_coarse_failure_is_reported_by_the_solve(golden):
+    """The dense coarsest inverse runs after feb_create has returned, so a coarsest matrix that is not positive
+    definite (here: zero stiffness, no springs, no penalties: the matrix is exactly zero) is reported by the calls
+    that need it, feb_solve and feb_precondition, as FEB_ERR_COARSE, and by every later one."""
+    import torch
+    z, g = _hindfoot(golden)
+    ncell = g.nx * g.ny * g.nz
+    ntotal = len(z["orig"])
+    f = torch.ones(3 * ntotal, dtype=torch.float64, device="cuda")
+    with engine.Problem(g, _lib.MAT_ISO_SRI, np.zeros(2 * ncell), z["active"], cn=z["cn"], orig=z["orig"],
+                        precision="mixed") as P:
+        for call in (lambda: P.solve(f), lambda: P.precondition(f), lambda: P.solve(f)):
+            with pytest.raises(_lib.FebError) as e:
+                call()
+            assert e.value.code == -5 and "not positive definite" in str(e.value)
