@@ -627,7 +627,7 @@ def batch_instance(seed):
 def run_batch(args):
     """64 independent instances of uneven size and seeded action on one GPU: the host thread pool (1, 8 and 16
     whole solve_cn calls in flight) against the batched launch (comech_b200.batch mode "graph": set-up on 16
-    threads, one feb_solve_batch graph launch per chunk of 32 instances while the next chunk is being set up,
+    threads, one feb_solve_batch graph launch per chunk of 16 instances while the next chunks are being set up,
     then the downloads).  Times are
     wall-clock around the whole batch through the public API (host inputs, uploads, set-up, solves, downloads),
     after one warm-up pass."""

@@ -12,8 +12,10 @@ few thousand nodes and every CG iteration is a chain of short launches.
      trip;
   3. finish: U and reactions per instance (engine.finish_cn), on a second thread pool.
 The chunks are pipelined: every instance's set-up is queued on the pool at the start, so while one chunk's
-graph runs the next chunks are being set up (default chunk: half of the items, at least 4: on 64 uneven instances
-four chunks solved in 1.81 s what one launch solves in 1.32 s, so the chunks are kept few), and each chunk's
+graph runs the next chunks are being set up (default chunk: a quarter of the items, at least 4; smaller chunks
+overlap more of the host-bound set-up, larger ones solve more efficiently: on 64 uneven instances four launches
+took 1.81 s where one took 1.32 s, while two chunks left 3.1 s of set-up before the first launch on a box with a
+slower host), and each chunk's
 handles are closed once it is finished, which also bounds device memory.  Mode "threads" keeps the earlier scheme
 (each thread runs a whole ``solve_cn``; up to ``concurrency`` in flight).
 
@@ -47,7 +49,7 @@ def solve_batch(items, precision="mixed", tol=1e-8, maxiter=800, warm_start=None
     if precision == "refine":
         raise ValueError("the batched graph solve runs the fp64 and mixed precisions (refine: mode='threads')")
     n = len(items)
-    chunk = max(4, -(-n // 2)) if not chunk else int(chunk)
+    chunk = max(4, -(-n // 4)) if not chunk else int(chunk)
     return _solve_pipelined(items, precision, tol, maxiter, warm_start, concurrency, options, chunk)
 
 
