@@ -1965,26 +1965,36 @@ class ExtraPrep {
   std::vector<char> taken;       // entries represented by `terms`
   Terms terms;
   char err[160] = {};            // bounds error (empty: none)
+  int err_code = FEB_ERR_ARG;    // FEB_ERR_NOMEM when the worker ran out of host memory
 
   void start(const FebOperator* op, int64_t nnode, int64_t ntotal, int gx, int gy,
              const std::vector<int64_t>* orig_copy) {
     std::shared_future<void> go = ready_.get_future().share();
     th_ = std::thread([this, op, nnode, ntotal, gx, gy, orig_copy, go]() {
-      ex.r.reserve(op->nextra); ex.c.reserve(op->nextra); ex.v.reserve(op->nextra);
-      for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
-        const int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
-        if (rr < 0 || cc < 0 || rr >= 3 * ntotal || cc >= 3 * ntotal) {
-          snprintf(err, sizeof(err), "extra entry (%lld, %lld) out of range", (long long)rr, (long long)cc);
-          return;
-        }
-        ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
+      try {
+        run(op, nnode, ntotal, gx, gy, orig_copy, go);
+      } catch (const std::exception& e) {   // nothing may escape a thread: report it as the set-up's error
+        snprintf(err, sizeof(err), "extra entries: %s", e.what());
+        err_code = FEB_ERR_NOMEM;
       }
-      coo_merge(ex);
-      go.wait();
-      if (!ok_.load(std::memory_order_acquire)) return;
-      classify(nnode, gx, gy, *orig_copy);
-      taken = factor_nonlocal(ex, is_local, terms);
     });
+  }
+  void run(const FebOperator* op, int64_t nnode, int64_t ntotal, int gx, int gy,
+           const std::vector<int64_t>* orig_copy, const std::shared_future<void>& go) {
+    ex.r.reserve(op->nextra); ex.c.reserve(op->nextra); ex.v.reserve(op->nextra);
+    for (int64_t e2 = 0; e2 < op->nextra; ++e2) {
+      const int64_t rr = op->extra_row[e2], cc = op->extra_col[e2];
+      if (rr < 0 || cc < 0 || rr >= 3 * ntotal || cc >= 3 * ntotal) {
+        snprintf(err, sizeof(err), "extra entry (%lld, %lld) out of range", (long long)rr, (long long)cc);
+        return;
+      }
+      ex.r.push_back(rr); ex.c.push_back(cc); ex.v.push_back(op->extra_val[e2]);
+    }
+    coo_merge(ex);
+    go.wait();
+    if (!ok_.load(std::memory_order_acquire)) return;
+    classify(nnode, gx, gy, *orig_copy);
+    taken = factor_nonlocal(ex, is_local, terms);
   }
   // the split copies' positions are in place (called once, on success)
   void ready() {
@@ -2149,7 +2159,7 @@ int setup_level0(FebHandle* h, const FebOperator* op) {
   // device, non-local ones projected through the levels on the host
   g_prof.mark("L0 penalties", s);
   xp.join();
-  if (xp.err[0]) { set_last_error("%s", xp.err); return FEB_ERR_ARG; }
+  if (xp.err[0]) { set_last_error("%s", xp.err); return xp.err_code; }
   Entries& ex = xp.ex;
   std::vector<char>& is_local = xp.is_local;
   std::vector<char>& taken = xp.taken;
