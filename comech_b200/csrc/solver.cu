@@ -1540,18 +1540,19 @@ int upload_copy_gather(Pool& pool, Level& V, const std::vector<int64_t>& orig_co
 // 12 power steps for lambda_max(Dinv A) (fe/gmg.py:47-59) and the Chebyshev coefficients, in precision T.
 // (on h->s, with the reduction scratch `part`)
 template <typename T>
-int power_iteration(FebHandle* h, int l, double* part) {
+int power_iteration(FebHandle* h, int l, double* part, unsigned int* pctr) {
   Level& V = h->L[l];
   const int64_t n = 3 * V.ntotal;
   T *x = FebHandle::vx<T>(V), *t = FebHandle::vt<T>(V), *d = FebHandle::vd<T>(V);
   launch_random_start<T>(x, V.used, V.ntotal, h->opt.seed + 7919ull * (uint64_t)l, h->s);
   launch_dot_partial<T, T>(x, x, n, part, nullptr, h->s);
   launch_finalize(FIN_POWER0, part, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
+  // step: d = Dinv K x / ||previous d|| with x the previous d, unscaled (the 1 / ||d|| of the previous step is
+  // applied after the product, so no scaling pass), and the power step in the norm kernel's last block
   for (int it = 0; it < 12; ++it) {
-    h->apply<T>(l, x, t, nullptr);
-    launch_bj_apply_norm<T>(FebHandle::dinv<T>(V), t, d, V.ntotal, part, h->s);
-    launch_finalize(FIN_POWER, part, nullptr, h->lp + l, h->opt.cheb_degree, nullptr, h->s);
-    launch_scale<T>(d, x, h->lp + l, n, h->s);
+    h->apply<T>(l, it == 0 ? x : d, t, nullptr);
+    launch_bj_apply_norm<T>(FebHandle::dinv<T>(V), t, d, V.ntotal, part, h->s, it == 0 ? nullptr : h->lp + l,
+                            h->lp + l, pctr, h->opt.cheb_degree);
   }
   FEB_CUDA(cudaGetLastError());
   return FEB_OK;
@@ -1567,7 +1568,10 @@ int power_fork(FebHandle* h, double** part) {
   const int nl = H.coarsest;
   *part = nullptr;
   if (nl <= 0) return FEB_OK;
-  FEB_TRY(H.pool.alloc(part, (size_t)kRedBlocks * nl));
+  // kRedBlocks partial sums per level, then one arrival counter per level (zeroed; re-armed by its last block)
+  FEB_TRY(H.pool.alloc(part, (size_t)kRedBlocks * nl + nl));
+  unsigned int* ctrs = reinterpret_cast<unsigned int*>(*part + (size_t)kRedBlocks * nl);
+  FEB_CUDA(cudaMemsetAsync(ctrs, 0, (size_t)nl * sizeof(double), H.s));
   FEB_CUDA(cudaEventRecord(H.ev_sync, H.s));
   cudaStream_t main = H.s;
   int st = FEB_OK;
@@ -1579,7 +1583,7 @@ int power_fork(FebHandle* h, double** part) {
     }
     FEB_CUDA(cudaStreamWaitEvent(H.aux[k], H.ev_sync, 0));
     H.s = H.aux[k];
-    st = power_iteration<T>(h, k, *part + (size_t)kRedBlocks * k);
+    st = power_iteration<T>(h, k, *part + (size_t)kRedBlocks * k, ctrs + 2 * k);
     H.s = main;
     FEB_CUDA(cudaEventRecord(H.aux_ev[k], H.aux[k]));
   }

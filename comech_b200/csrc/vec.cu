@@ -285,27 +285,42 @@ __global__ void k_random_start(T* __restrict__ x, const uint8_t* __restrict__ ma
   x[i] = (mask == nullptr || mask[i / 3]) ? T(g) : T(0);
 }
 
+// y = f Dinv v and its squared norm; f = scale->inv (the previous power step's 1 / ||y||, so that the product
+// that formed v could take the unscaled vector) or 1.  With ctr the last block runs the power step FIN_POWER on
+// fin (no separate finalize launch); each block reads scale->inv before it arrives, the last block writes it after.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_bj_apply_norm(const T* __restrict__ D, const T* __restrict__ v, T* __restrict__ y, int64_t nn,
-                double* __restrict__ partials) {
+                double* __restrict__ partials, const LevelParams* scale, LevelParams* fin, unsigned int* ctr,
+                int deg) {
+  const T f = scale ? T(scale->inv) : T(1);
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < nn; i += (int64_t)gridDim.x * kThreads) {
     T z0, z1, z2;
     bj(D, nn, i, v[3 * i], v[3 * i + 1], v[3 * i + 2], z0, z1, z2);
+    z0 *= f; z1 *= f; z2 *= f;
     y[3 * i] = z0; y[3 * i + 1] = z1; y[3 * i + 2] = z2;
     s += double(z0) * double(z0) + double(z1) * double(z1) + double(z2) * double(z2);
   }
   s = block_sum(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (!ctr) return;
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) t += ((volatile double*)partials)[i];
+  t = block_sum(t);
+  if (threadIdx.x == 0) {
+    finalize_step(FIN_POWER, t, nullptr, fin, deg);
+    *ctr = 0u;
+  }
 }
 
-template <typename T>
-__global__ void k_scale(const T* __restrict__ y, T* __restrict__ x, const LevelParams* __restrict__ lp, int64_t n) {
-  const T inv = T(lp->inv);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    x[i] = y[i] * inv;
-}
 
 template <typename Ts, typename Td>
 __global__ void k_convert(const Ts* __restrict__ a, Td* __restrict__ b, int64_t n, const int* __restrict__ skip) {
@@ -424,20 +439,17 @@ void launch_random_start(T* x, const uint8_t* mask, int64_t nn, uint64_t seed, c
 }
 
 template <typename T>
-void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s) {
-  k_bj_apply_norm<T><<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials); note_launch();
+void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s,
+                          const LevelParams* scale, LevelParams* fin, unsigned int* ctr, int deg) {
+  k_bj_apply_norm<T><<<kRedBlocks, kThreads, 0, s>>>(Dinv, v, y, nn, partials, scale, fin, ctr, deg); note_launch();
 }
 
-template <typename T>
-void launch_scale(const T* y, T* x, const LevelParams* lp, int64_t n, cudaStream_t s) {
-  k_scale<T><<<grid_for(n), kThreads, 0, s>>>(y, x, lp, n); note_launch();
-}
 template void launch_random_start<float>(float*, const uint8_t*, int64_t, uint64_t, cudaStream_t);
 template void launch_random_start<double>(double*, const uint8_t*, int64_t, uint64_t, cudaStream_t);
-template void launch_bj_apply_norm<float>(const float*, const float*, float*, int64_t, double*, cudaStream_t);
-template void launch_bj_apply_norm<double>(const double*, const double*, double*, int64_t, double*, cudaStream_t);
-template void launch_scale<float>(const float*, float*, const LevelParams*, int64_t, cudaStream_t);
-template void launch_scale<double>(const double*, double*, const LevelParams*, int64_t, cudaStream_t);
+template void launch_bj_apply_norm<float>(const float*, const float*, float*, int64_t, double*, cudaStream_t,
+                                          const LevelParams*, LevelParams*, unsigned int*, int);
+template void launch_bj_apply_norm<double>(const double*, const double*, double*, int64_t, double*, cudaStream_t,
+                                           const LevelParams*, LevelParams*, unsigned int*, int);
 
 template <typename Ts, typename Td>
 void launch_convert(const Ts* src, Td* dst, int64_t n, const int* skip, cudaStream_t s) {

@@ -110,10 +110,12 @@ void launch_residual(const T* b, const T* Ax, T* r, int64_t n, const int* skip, 
 // power iteration
 template <typename T>
 void launch_random_start(T* x, const uint8_t* mask, int64_t nn, uint64_t seed, cudaStream_t s);
+// y = f Dinv v (f = scale->inv, or 1 without scale) and partial squared norms; with ctr (a zeroed counter) the last
+// block also runs the power step FIN_POWER on fin
 template <typename T>
-void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s);
-template <typename T>
-void launch_scale(const T* y, T* x, const LevelParams* lp, int64_t n, cudaStream_t s);
+void launch_bj_apply_norm(const T* Dinv, const T* v, T* y, int64_t nn, double* partials, cudaStream_t s,
+                          const LevelParams* scale = nullptr, LevelParams* fin = nullptr, unsigned int* ctr = nullptr,
+                          int deg = 0);
 
 // conversions and small helpers
 template <typename Ts, typename Td>
