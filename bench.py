@@ -396,8 +396,13 @@ def run_ours(args, rank, world, dist):
         clk = Clocks(dev) if name == "headline" else None
         if clk:
             clk.__enter__()      # before the warm-up: nvidia-smi's start-up is over when timing begins
+        # warm-up in the timed loop's form: each step runs while the previous step's results are still held (as
+        # timed_steps holds them), so torch's device cache has its two sets of result buffers before timing; a
+        # first allocation of the second set inside the timed region waited on cudaMalloc (+45-97 ms in one step)
+        prev = None
         for _ in range(args.warmup):
-            device_solve(P, d, pr_, warm=w_)
+            prev = device_solve(P, d, pr_, warm=w_)
+        prev = None
         torch.cuda.synchronize()
         launches0 = lib.feb_launch_count()
         timed_steps.details = []
