@@ -501,3 +501,21 @@ def test_coarse_failure_is_reported_by_the_solve(golden):
             with pytest.raises(_lib.FebError) as e:
                 call()
             assert e.value.code == -5 and "not positive definite" in str(e.value)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_launch_modes_agree(golden, precision):
+    """Direct launches (use_graphs 0), one captured graph per CG iteration (1) and the device-side while loop (2)
+    run the same iteration, the rigid-mode coefficients on their side stream included (a real fork / join in
+    mode 0, captured edges in 1 and 2): iteration counts within 1 (atomic sums round in run-dependent order),
+    the same solution."""
+    z, g = _hindfoot(golden)
+    args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
+            [(z["load_nodes"], z["load_area"], z["load_t"])], _springs(z), _groups(z))
+    out = [engine.solve_cn(*args, tol=1e-10, precision=precision, options=dict(use_graphs=m)) for m in (0, 1, 2)]
+    (U0, i0, _), rest = out[0], out[1:]
+    ok = np.isfinite(U0)
+    for U, info, _ in rest:
+        assert info["flag"] == 0
+        assert abs(info["iters"] - i0["iters"]) <= 1
+        assert rel(U[ok], U0[ok]) < 1e-8
