@@ -225,14 +225,9 @@ ORACLE_FULL_S = 284.3
 def device_solve(P, d, precision, x0=None, warm=None):
     """One solve from device-resident inputs (same work as engine.solve_cn + cell_stress_cn); with ``warm`` (a
     trained warmnet.WarmNet) the network's prediction is the initial guess, computed inside the step."""
-    import torch
     from comech_b200 import engine, _lib
     g = P["grid"]
     t = [time.perf_counter()]          # host time stamps of the phases (no synchronisation added)
-    pending = None
-    if warm is not None and x0 is None:   # the network's start, on a side stream beside the set-up (engine.solve_cn)
-        x0, pending = engine.start_prediction(warm, g, d["mat"], d["active"], P["orig"], P["fixed"][0],
-                                              d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
     pr = engine.Problem(g, _lib.MAT_ISO_SRI, d["mat"], d["active"], cn=d["cn"], orig=d["orig"],
                         pen_node=d["pen_node"], pen_k=d["pen_k"], extra_coo=d["extra"], precision=precision, tol=TOL,
                         maxiter=800, options=SOLVER_OPTIONS)
@@ -241,9 +236,10 @@ def device_solve(P, d, precision, x0=None, warm=None):
         pr.set_rigid_groups(d["g_nodes"], offsets=d["g_off"])
         t.append(time.perf_counter())
         f = pr.rhs([(d["l_nodes"], d["l_vals"])])
-        if pending is not None:
-            torch.cuda.current_stream().wait_event(pending)
-            warm.check_status()
+        if warm is not None and x0 is None:
+            nc = g.nx * g.ny * g.nz
+            x0 = warm.predict_x0(g, d["mat"][:nc], d["mat"][nc:], d["active"], P["orig"], P["fixed"][0],
+                                 d["load_nodes_h"], d["load_z_h"], len(P["orig"]), orig_dev=d["orig"])
         t.append(time.perf_counter())
         x, info = pr.solve(f, x0)
         t.append(time.perf_counter())

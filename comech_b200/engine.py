@@ -16,7 +16,6 @@ Extra keyword-only arguments (not in the reference): ``precision`` ('fp64', 'mix
 (return device tensors in ``info['device']`` for a following stress call without a round trip).
 """
 import ctypes as C
-import threading
 import time
 
 import numpy as np
@@ -61,35 +60,6 @@ def _dev_cat(arrays, dtype):
         out[at:at + p.numel()].copy_(p.reshape(-1), non_blocking=True)
         at += p.numel()
     return out
-
-
-_SIDE = threading.local()
-
-
-def _side_stream():
-    """This thread's side stream (work that overlaps the caller's stream, joined back by an event)."""
-    torch = _torch()
-    if getattr(_SIDE, "stream", None) is None:
-        _SIDE.stream = torch.cuda.Stream()
-    return _SIDE.stream
-
-
-def start_prediction(net, g, mat_dev, active_dev, orig, fixed_nodes, load_nodes, load_z, ntotal, orig_dev=None):
-    """Launches the network's start value on this thread's side stream (after the work queued so far on the
-    current stream) and returns (x0, event); the caller makes its stream wait for the event before it reads x0
-    and then calls net.check_status()."""
-    torch = _torch()
-    cur = torch.cuda.current_stream()
-    side = _side_stream()
-    side.wait_stream(cur)
-    nc = g.nx * g.ny * g.nz
-    with torch.cuda.stream(side):
-        x0 = net.predict_x0(g, mat_dev[:nc], mat_dev[nc:], active_dev, orig, fixed_nodes, load_nodes, load_z, ntotal,
-                            orig_dev=orig_dev, check=False)
-    x0.record_stream(cur)
-    done = torch.cuda.Event()
-    done.record(side)
-    return x0, done
 
 
 def _host(*ts):
@@ -316,21 +286,8 @@ def prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_grou
 
     coo = _extra_entries(extra, used_nodes, ntotal)
     mat = _dev_cat((lam, mu), np.float64)
-    act = _dev(active.view(np.uint8), np.uint8)
-    pending = None
-    if x0 is None and warm_start is not None and warm_start is not False:
-        # the network's start depends on the inputs only: it runs on a side stream beside the operator's set-up,
-        # from the same device copies of lam, mu, active and the node map
-        from . import warmnet
-        net = warmnet.default_net() if warm_start is True else warm_start
-        ln, lz = warmnet.load_z(loads)
-        nnode = (g.nx + 1) * (g.ny + 1) * (g.nz + 1)
-        orig_d = _dev(orig, np.int64) if ntotal > nnode else None
-        x0d, done = start_prediction(net, g, mat, act, orig, fn, ln, lz, ntotal, orig_dev=orig_d)
-        pending = (net, done)
-        orig = orig_d if orig_d is not None else orig
     stamps.append(("host_inputs", time.perf_counter()))
-    P = Problem(g, _lib.MAT_ISO_SRI, mat, act, cn=cn, orig=orig, pen_node=fn, pen_k=pen_k, extra_coo=coo,
+    P = Problem(g, _lib.MAT_ISO_SRI, mat, active, cn=cn, orig=orig, pen_node=fn, pen_k=pen_k, extra_coo=coo,
                 precision=precision, tol=tol, maxiter=maxiter, options=options)
     stamps.append(("create", time.perf_counter()))
     try:
@@ -339,10 +296,12 @@ def prepare_cn(g, lam, mu, active, cn, orig, fixed, loads, extra=None, node_grou
         f = P.rhs(loads)
         if x0 is not None:
             x0d = _dev(np.nan_to_num(np.asarray(x0, np.float64)).ravel(), np.float64)
-        elif pending is not None:
-            net, done = pending
-            _torch().cuda.current_stream().wait_event(done)
-            net.check_status()
+        elif warm_start is not None and warm_start is not False:
+            from . import warmnet
+            net = warmnet.default_net() if warm_start is True else warm_start
+            ln, lz = warmnet.load_z(loads)
+            nc = g.nx * g.ny * g.nz       # the operator's device copies of lam, mu and active serve the network too
+            x0d = net.predict_x0(g, P.mat[:nc], P.mat[nc:], P.active, orig, fn, ln, lz, ntotal, orig_dev=P.orig)
             stamps.append(("warm_start", time.perf_counter()))
         else:
             x0d = None

@@ -374,16 +374,13 @@ class WarmNet:
                                       100.0 / total, _ptr(scratch), _ptr(out), _stream()))
         return out, dict(hn=hn, h=np.asarray(h, np.float64), total_load=total, dims=dims)
 
-    def predict_x0(self, g, lam, mu, active, orig, fixed_nodes, load_nodes, load_z, nnode_total, orig_dev=None,
-                   check=True):
+    def predict_x0(self, g, lam, mu, active, orig, fixed_nodes, load_nodes, load_z, nnode_total, orig_dev=None):
         """Initial guess (full layout, FP64, device) for the solve of these inputs (orig: host node map; orig_dev:
-        the same map already on the device, if any).  check=False leaves the status check (a host synchronisation)
-        to the caller (check_status), so that the prediction can run on a side stream beside other work."""
+        the same map already on the device, if any)."""
         x, meta = self.inputs(g, lam, mu, active, orig, fixed_nodes, load_nodes, load_z)
         self.status.zero_()
         pred = self.forward(x, meta["dims"])
-        if check:
-            self.check_status()              # a network pass whose tensor-core wait ran out gives no start value
+        self.check_status()                  # a network pass whose tensor-core wait ran out gives no start value
         scale = self.u_unit * meta["total_load"] / REF_LOAD
         x0 = self.torch.empty(3 * nnode_total, dtype=self.torch.float64, device="cuda")
         nnode = (g.nx + 1) * (g.ny + 1) * (g.nz + 1)
