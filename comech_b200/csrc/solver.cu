@@ -221,46 +221,87 @@ struct Entries {
   size_t size() const { return v.size(); }
 };
 
-// Sorts entries by (row, col) and sums duplicates: LSD radix sort of the packed key row << 32 | col
-// (dofs < 2^31, feb_create checks 3 nnode_total), 11-bit digits, digits that never vary skipped.
+// Stable LSD radix sort of key[0, n) (idx carried along), 11-bit digits (the histogram stays in L1), digits
+// constant over all keys skipped; k2 / i2 are scratch of the same length.  The result ends in key / idx.
+void radix_range(uint64_t* key, uint32_t* idx, uint64_t* k2, uint32_t* i2, size_t n) {
+  uint64_t any_or = 0, any_and = ~0ull;
+  for (size_t i = 0; i < n; ++i) { any_or |= key[i]; any_and &= key[i]; }
+  constexpr int kBits = 11;
+  constexpr uint64_t kMask = (1u << kBits) - 1;
+  uint32_t cnt[size_t(1) << kBits];
+  uint64_t *ka = key, *kb = k2;
+  uint32_t *ia = idx, *ib = i2;
+  for (int shift = 0; shift < 64; shift += kBits) {
+    if ((((any_or ^ any_and) >> shift) & kMask) == 0) continue;
+    std::fill(cnt, cnt + (size_t(1) << kBits), 0u);
+    for (size_t i = 0; i < n; ++i) cnt[(ka[i] >> shift) & kMask]++;
+    uint32_t sum = 0;
+    for (auto& c : cnt) { const uint32_t t = c; c = sum; sum += t; }
+    for (size_t i = 0; i < n; ++i) {
+      const uint32_t at = cnt[(ka[i] >> shift) & kMask]++;
+      kb[at] = ka[i];
+      ib[at] = ia[i];
+    }
+    std::swap(ka, kb);
+    std::swap(ia, ib);
+  }
+  if (ka != key) {
+    std::copy(ka, ka + n, key);
+    std::copy(ia, ia + n, idx);
+  }
+}
+
+// Sorts entries by (row, col) and sums duplicates (in input order): the packed key row << 32 | col (dofs < 2^31,
+// feb_create checks 3 nnode_total) radix-sorted.  Large inputs are first cut into 4 row ranges (a stable
+// counting pass), sorted on 4 threads; the result is the same as one sort.
 void coo_merge(Entries& E) {
   const size_t n = E.size();
   if (n == 0) return;
   std::vector<uint64_t> key(n), k2(n);
   std::vector<uint32_t> idx(n), i2(n);
-  uint64_t any_or = 0, any_and = ~0ull;
   for (size_t i = 0; i < n; ++i) {
     key[i] = ((uint64_t)E.r[i] << 32) | (uint32_t)E.c[i];
     idx[i] = (uint32_t)i;
-    any_or |= key[i];
-    any_and &= key[i];
   }
-  // LSD radix sort with 11-bit digits (the histogram stays in L1); digits constant over all keys are skipped
-  constexpr int kBits = 11;
-  constexpr uint64_t kMask = (1u << kBits) - 1;
-  std::vector<uint32_t> cnt(size_t(1) << kBits);
-  for (int shift = 0; shift < 64; shift += kBits) {
-    if ((((any_or ^ any_and) >> shift) & kMask) == 0) continue;
-    std::fill(cnt.begin(), cnt.end(), 0u);
-    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> shift) & kMask]++;
-    uint32_t sum = 0;
-    for (auto& c : cnt) { const uint32_t t = c; c = sum; sum += t; }
-    for (size_t i = 0; i < n; ++i) {
-      const uint32_t at = cnt[(key[i] >> shift) & kMask]++;
+  constexpr int kParts = 4;
+  if (n >= 32768 && std::thread::hardware_concurrency() >= (unsigned)kParts) {
+    int64_t rmin = E.r[0], rmax = E.r[0];
+    for (size_t i = 1; i < n; ++i) { rmin = std::min(rmin, E.r[i]); rmax = std::max(rmax, E.r[i]); }
+    const int64_t span = rmax - rmin + 1;
+    auto part = [&](size_t i) { return (int)((E.r[i] - rmin) * kParts / span); };
+    size_t off[kParts + 1] = {};
+    for (size_t i = 0; i < n; ++i) off[part(i) + 1]++;
+    for (int p = 0; p < kParts; ++p) off[p + 1] += off[p];
+    size_t fill[kParts];
+    std::copy(off, off + kParts, fill);
+    for (size_t i = 0; i < n; ++i) {     // stable scatter into the row ranges
+      const size_t at = fill[part(i)]++;
       k2[at] = key[i];
       i2[at] = idx[i];
     }
     key.swap(k2);
     idx.swap(i2);
+    std::vector<std::thread> th;
+    for (int p = 1; p < kParts; ++p)
+      th.emplace_back(radix_range, key.data() + off[p], idx.data() + off[p], k2.data() + off[p], i2.data() + off[p],
+                      off[p + 1] - off[p]);
+    radix_range(key.data(), idx.data(), k2.data(), i2.data(), off[1]);
+    for (auto& t : th) t.join();
+  } else {
+    radix_range(key.data(), idx.data(), k2.data(), i2.data(), n);
   }
-  Entries M;
-  M.r.reserve(n); M.c.reserve(n); M.v.reserve(n);
+  // rows and columns come back out of the sorted keys; only the values are gathered
+  std::vector<double> vals(n);
+  size_t m = 0;
   for (size_t t = 0; t < n; ++t) {
-    const size_t i = idx[t];
-    if (t > 0 && key[t] == key[t - 1]) M.v.back() += E.v[i];
-    else { M.r.push_back(E.r[i]); M.c.push_back(E.c[i]); M.v.push_back(E.v[i]); }
+    const double v = E.v[idx[t]];
+    if (t > 0 && key[t] == key[t - 1]) vals[m - 1] += v;
+    else { k2[m] = key[t]; vals[m++] = v; }
   }
-  E = std::move(M);
+  E.r.resize(m); E.c.resize(m);
+  for (size_t t = 0; t < m; ++t) { E.r[t] = (int64_t)(k2[t] >> 32); E.c[t] = (int64_t)(uint32_t)k2[t]; }
+  vals.resize(m);
+  E.v.swap(vals);
 }
 
 // supports of a node position along each axis
@@ -2019,11 +2060,22 @@ class ExtraPrep {
       x = int(a - q * ugx); z = int(q / ugy); y = int(q - (uint32_t)z * ugy);
     };
     is_local.assign(ex.size(), 0);
-    for (size_t e2 = 0; e2 < ex.size(); ++e2) {
-      int ax, ay, az, bx, by, bz;
-      coords(ex.r[e2] / 3, ax, ay, az);
-      coords(ex.c[e2] / 3, bx, by, bz);
-      is_local[e2] = std::abs(ax - bx) <= 1 && std::abs(ay - by) <= 1 && std::abs(az - bz) <= 1;
+    auto slice = [&](size_t lo, size_t hi) {
+      for (size_t e2 = lo; e2 < hi; ++e2) {
+        int ax, ay, az, bx, by, bz;
+        coords(ex.r[e2] / 3, ax, ay, az);
+        coords(ex.c[e2] / 3, bx, by, bz);
+        is_local[e2] = std::abs(ax - bx) <= 1 && std::abs(ay - by) <= 1 && std::abs(az - bz) <= 1;
+      }
+    };
+    const size_t n = ex.size();
+    if (n >= 32768 && std::thread::hardware_concurrency() >= 4) {   // independent entries: 4 slices
+      std::vector<std::thread> th;
+      for (int p = 1; p < 4; ++p) th.emplace_back(slice, n * p / 4, n * (p + 1) / 4);
+      slice(0, n / 4);
+      for (auto& t : th) t.join();
+    } else {
+      slice(0, n);
     }
   }
 
