@@ -252,8 +252,8 @@ void radix_range(uint64_t* key, uint32_t* idx, uint64_t* k2, uint32_t* i2, size_
 }
 
 // Sorts entries by (row, col) and sums duplicates (in input order): the packed key row << 32 | col (dofs < 2^31,
-// feb_create checks 3 nnode_total) radix-sorted.  Large inputs are first cut into 4 row ranges (a stable
-// counting pass), sorted on 4 threads; the result is the same as one sort.
+// feb_create checks 3 nnode_total) radix-sorted.  Large inputs are first cut into 4 key ranges (splitters from
+// the quartiles of a sample; a stable counting pass), sorted on 4 threads; the result is the same as one sort.
 void coo_merge(Entries& E) {
   const size_t n = E.size();
   if (n == 0) return;
@@ -265,10 +265,14 @@ void coo_merge(Entries& E) {
   }
   constexpr int kParts = 4;
   if (n >= 32768 && std::thread::hardware_concurrency() >= (unsigned)kParts) {
-    int64_t rmin = E.r[0], rmax = E.r[0];
-    for (size_t i = 1; i < n; ++i) { rmin = std::min(rmin, E.r[i]); rmax = std::max(rmax, E.r[i]); }
-    const int64_t span = rmax - rmin + 1;
-    auto part = [&](size_t i) { return (int)((E.r[i] - rmin) * kParts / span); };
+    // key ranges of about equal size from the quartiles of a sample (equal keys share a range)
+    std::vector<uint64_t> smp;
+    const size_t step = std::max<size_t>(1, n / 4096);
+    for (size_t i = 0; i < n; i += step) smp.push_back(key[i]);
+    std::sort(smp.begin(), smp.end());
+    uint64_t split[kParts - 1];
+    for (int p = 1; p < kParts; ++p) split[p - 1] = smp[smp.size() * p / kParts];
+    auto part = [&](size_t i) { return (int)(std::upper_bound(split, split + kParts - 1, key[i]) - split); };
     size_t off[kParts + 1] = {};
     for (size_t i = 0; i < n; ++i) off[part(i) + 1]++;
     for (int p = 0; p < kParts; ++p) off[p + 1] += off[p];
