@@ -17,7 +17,7 @@ PREC = {"fp64": 0, "mixed": 1, "refine": 2}
 
 EXPORTS = ["feb_default_options", "feb_create", "feb_set_rigid_groups", "feb_solve", "feb_solve_batch", "feb_apply", "feb_precondition",
            "feb_export_solution", "feb_used_nodes", "feb_destroy", "feb_accumulate_nodal", "feb_cell_stress",
-           "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_benchmark_apply_set", "feb_launch_count", "feb_pool_stats", "feb_last_error",
+           "feb_element_forces", "feb_cell_stress_noalloc", "feb_benchmark_apply", "feb_benchmark_apply_set", "feb_benchmark_smooth_set", "feb_launch_count", "feb_pool_stats", "feb_last_error",
            "feb_region_forces", "feb_rigid_fit", "feb_relative_displacement", "feb_sample_cells",
            "feb_nearest_active", "feb_sample_nodes", "feb_split_connectivity",
            "feb_mix_materials", "feb_net_conv", "feb_net_wgrad", "feb_net_colsum", "feb_net_weights", "feb_net_head",
@@ -111,6 +111,9 @@ def load():
     lib.feb_benchmark_apply.argtypes = [P, C.c_int32, P, P, C.c_int32, C.POINTER(C.c_float)]
     lib.feb_benchmark_apply_set.argtypes = [P, C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                             C.c_int32, C.POINTER(C.c_float)]
+    lib.feb_benchmark_smooth_set.argtypes = [P, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                             C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32,
+                                             C.POINTER(C.c_float)]
     lib.feb_region_forces.argtypes = [C.POINTER(FebGrid), P, P, P, P, P, P, C.c_int32, C.c_int32, C.c_int64, P, P, P]
     lib.feb_rigid_fit.argtypes = [P, P, C.c_int64, P, P]
     lib.feb_relative_displacement.argtypes = [C.POINTER(FebGrid), P, C.c_int64, P, P, P, P]

@@ -3156,6 +3156,41 @@ int feb_used_nodes(FebHandle* h, int64_t* nused, uint8_t* mask) {
   return FEB_OK;
 }
 
+int feb_benchmark_smooth_set(FebHandle* h, int32_t nbuf, void* const* d, void* const* r, void* const* x,
+                             void* const* e, int32_t nrep, float* ms) {
+  if (!h || nbuf < 1 || !d || !r || !x || !e || nrep < 1 || !ms) {
+    set_last_error("feb_benchmark_smooth_set: bad argument");
+    return FEB_ERR_ARG;
+  }
+  for (int b = 0; b < nbuf; ++b)
+    if (!d[b] || !r[b] || !x[b] || !e[b]) { set_last_error("feb_benchmark_smooth_set: null buffer %d", b); return FEB_ERR_ARG; }
+  if (h->coarsest < 1 || !h->pair_on<float>()) {
+    set_last_error("feb_benchmark_smooth_set: needs a hierarchy and the paired level-0 kernel");
+    return FEB_ERR_ARG;
+  }
+  FEB_TRY(h->settle());     // the Chebyshev coefficients come from the power iteration
+  FEB_TRY(h->sync_in());
+  FEB_TRY(h->tune_events());
+  auto step = [&](int i) {
+    const int b = i % nbuf;
+    SmoothArgs<float> A;
+    A.r_in = (const float*)r[b]; A.r_out = (float*)r[b];
+    A.x_in = (const float*)x[b]; A.x_out = (float*)x[b];
+    A.d_out = (float*)e[b];
+    A.lp = h->lp; A.k = 0;
+    h->pair_run<float>((const float*)d[b], nullptr, &A, nullptr);
+  };
+  step(0);
+  FEB_CUDA(cudaEventRecord(h->tev0, h->s));
+  for (int i = 0; i < nrep; ++i) step(i);
+  FEB_CUDA(cudaEventRecord(h->tev1, h->s));
+  FEB_CUDA(cudaEventSynchronize(h->tev1));
+  float t = 0.f;
+  FEB_CUDA(cudaEventElapsedTime(&t, h->tev0, h->tev1));
+  *ms = t / nrep;
+  return h->sync_out();
+}
+
 int64_t feb_launch_count(void) { return g_launches.load(); }
 
 int feb_pool_stats(int64_t* reserved, int64_t* used_peak, int32_t* grow_events) {

@@ -462,6 +462,13 @@ FEB_API int feb_benchmark_apply(FebHandle* h, int32_t prec, const void* u, void*
 FEB_API int feb_benchmark_apply_set(FebHandle* h, int32_t prec, int32_t nbuf, const void* const* u, void* const* y,
                                     int32_t nrep, float* ms);
 
+/* Benchmark hook: the level-0 smoother step as the V-cycle runs it (the paired K.u with the fused Chebyshev
+   update r -= K d, d' = a1 d + a2 D^-1 r, x += d', FP32), over nbuf sets of (d, r, x, d') buffers used in turn,
+   each 3 nnode_total floats on the device; the handle needs its hierarchy (the level's Chebyshev
+   coefficients).  ms: the average step. */
+FEB_API int feb_benchmark_smooth_set(FebHandle* h, int32_t nbuf, void* const* d, void* const* r, void* const* x,
+                                     void* const* e, int32_t nrep, float* ms);
+
 /* Kernels launched by this library since it was loaded (graph launches count their kernel nodes). */
 FEB_API int64_t feb_launch_count(void);
 

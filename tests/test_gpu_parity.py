@@ -519,3 +519,26 @@ def test_launch_modes_agree(golden, precision):
         assert info["flag"] == 0
         assert abs(info["iters"] - i0["iters"]) <= 1
         assert rel(U[ok], U0[ok]) < 1e-8
+
+
+def test_benchmark_smooth_set(golden):
+    """feb_benchmark_smooth_set times the level-0 smoother step (paired K.u with the fused Chebyshev update) over
+    rotating buffer sets; a handle without a hierarchy (no Chebyshev coefficients) is an argument error."""
+    import ctypes as C
+    import torch
+    z, g = _hindfoot(golden)
+    ntotal = len(z["orig"])
+    mat = np.concatenate([z["lam"], z["mu"]])
+    sets = [[torch.randn(3 * ntotal, dtype=torch.float32, device="cuda") for _ in range(4)] for _ in range(2)]
+    ptr = [(C.c_void_p * 2)(*[st[q].data_ptr() for st in sets]) for q in range(4)]
+    lib = _lib.load()
+    ms = C.c_float()
+    with engine.Problem(g, _lib.MAT_ISO_SRI, mat, z["active"], cn=z["cn"], orig=z["orig"],
+                        pen_node=np.asarray(z["fixed_nodes"], np.int64),
+                        pen_k=np.repeat((np.asarray(z["fixed_area"]) * engine.K_GROUND)[:, None], 3, axis=1),
+                        precision="mixed") as P:
+        _lib.check(lib.feb_benchmark_smooth_set(P.h, 2, ptr[0], ptr[1], ptr[2], ptr[3], 4, C.byref(ms)))
+        assert ms.value > 0
+    with engine.Problem(g, _lib.MAT_ISO_SRI, mat, z["active"], cn=z["cn"], orig=z["orig"],
+                        options=dict(max_levels=0)) as P:
+        assert lib.feb_benchmark_smooth_set(P.h, 2, ptr[0], ptr[1], ptr[2], ptr[3], 4, C.byref(ms)) == -1
