@@ -875,7 +875,8 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=None, help="refinement: FP32 sweep tolerance")
     ap.add_argument("--use-graphs", type=int, default=None, help="0 direct, 1 graph per iteration, 2 device loop")
     ap.add_argument("--level-kernel", type=int, default=None,
-                    help="coarse-level stencil slots: 0 auto, 1 run-time slot index, 2 compile-time slot index")
+                    help="coarse-level stencil slots: 0 auto, 1 run-time slot index, 2 compile-time slot index; "
+                         "+4 term-dot passes; +8 FP32 stencil copies instead of FP16")
     ap.add_argument("--warm", choices=["auto", "on", "off"], default="auto",
                     help="learned warm start (auto: when the packaged network is present)")
     args = ap.parse_args()

@@ -1,4 +1,6 @@
 // Coarse-level kernels: stencil products, structured restriction / prolongation, Galerkin on the device.
+#include <algorithm>
+
 #include "coarse.cuh"
 #include "vec.cuh"
 
@@ -654,6 +656,27 @@ __global__ void k_stencil_to_sym(const double* __restrict__ A, int nx, int nxp, 
       S[(size_t)(q * 9 + t) * np + p] = i < nx ? T(A[(size_t)((q + 13) * 9 + t) * n + m]) : T(0);
 }
 
+// largest |entry| of the FP64 half storage into *amax (float bits; non-negative floats order as unsigned ints)
+__global__ void k_sym_absmax(const double* __restrict__ S, int64_t m, unsigned* __restrict__ amax) {
+  float v = 0.f;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+    v = fmaxf(v, (float)fabs(S[e]));
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(amax, __float_as_uint(v));
+}
+
+// Sh = S / 2^e as FP16 with 2^e the smallest power of two above amax / 2^15 (so |Sh| < 2^15 < 65504); the
+// scale itself goes to hscale[0]
+__global__ void k_sym_to_half(const double* __restrict__ S, int64_t m, const unsigned* __restrict__ amax,
+                              float* __restrict__ hscale, __half* __restrict__ Sh) {
+  int e = 0;
+  frexpf(__uint_as_float(*amax), &e);            // amax < 2^e
+  const double inv = ldexp(1.0, 15 - e);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i == 0) *hscale = ldexpf(1.f, e - 15);
+  if (i < m) Sh[i] = __float2half_rn((float)(S[i] * inv));
+}
+
 // Stencil product of a symmetric half-stored level with a fused epilogue.
 //
 // A CTA of 32 x 4 threads takes 32 consecutive nodes of one x-row.  The 14 stored block slots
@@ -687,7 +710,7 @@ struct SlotVals {
   T f[9], g[9], uf[3], ub[3];
 };
 
-template <typename T, bool CMP, int Q>
+template <typename T, bool CMP, bool H, int Q>
 __device__ __forceinline__ void sym_load(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
                                          int k, int tn, const T* sp, const T* sm, SlotVals<T>& v) {
   constexpr int o = 13 + Q;
@@ -706,8 +729,14 @@ __device__ __forceinline__ void sym_load(const SymView<T>& L, const T* __restric
   for (int c = 0; c < 3; ++c) v.uf[c] = u[3 * mf + c];
   if (!vf) { v.uf[0] = 0; v.uf[1] = 0; v.uf[2] = 0; }
   auto stored = [&](int m, T (&w)[9]) {     // m: padded position
+    if constexpr (H) {
+      const __half* __restrict__ Bh = L.Sh + (size_t)Q * 9 * NP;
 #pragma unroll
-    for (int t = 0; t < 9; ++t) w[t] = B[(size_t)t * NP + m];
+      for (int t = 0; t < 9; ++t) w[t] = T(__half2float(Bh[(size_t)t * NP + m]));
+    } else {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) w[t] = B[(size_t)t * NP + m];
+    }
   };
   auto formed = [&](int tg, T (&w)[9]) {
     const T lam = sm[2 * tg], mu = sm[2 * tg + 1];
@@ -738,18 +767,19 @@ __device__ __forceinline__ void sym_acc(const SlotVals<T>& v, T& a0, T& a1, T& a
   }
 }
 
-template <typename T, bool CMP, int Q>
+template <typename T, bool CMP, bool H, int Q>
 __device__ __forceinline__ void sym_slot(const SymView<T>& L, const T* __restrict__ u, int n, int pn, int ic, int j,
                                          int k, int tn, const T* sp, const T* sm, T& a0, T& a1, T& a2) {
   SlotVals<T> v;
-  sym_load<T, CMP, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, v);
+  sym_load<T, CMP, H, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, v);
   sym_acc<T, Q>(v, a0, a1, a2);
 }
 
 // CMP: the level carries the compressed single-material blocks (tags); without them the pattern code is not
 // compiled into the kernel at all.  Offsets within the stencil planes are 32-bit (126 x the padded node count
-// < 2^31 is checked at launch).
-template <typename T, int EPI, bool CMP, bool CT>
+// < 2^31 is checked at launch).  H (with CT, FP32): the stored blocks are read from the 16-bit copy Sh and the
+// slot sums scaled by hscale before the entries and terms are added.
+template <typename T, int EPI, bool CMP, bool CT, bool H>
 __global__ void __launch_bounds__(128)
 k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restrict__ b, T* __restrict__ r,
       T* __restrict__ d_out, T* __restrict__ x, const LevelParams* __restrict__ lp, int kstep,
@@ -780,7 +810,7 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
   const T* sm = CMP ? &smat[0][0] : nullptr;
   if constexpr (CT) {
     // the 14 slots over the 4 warps (warp-uniform switch): 0 4 8 12 | 1 5 9 13 | 2 6 10 | 3 7 11
-#define FEB_SLOT(Q) sym_slot<T, CMP, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, a0, a1, a2)
+#define FEB_SLOT(Q) sym_slot<T, CMP, H, Q>(L, u, n, pn, ic, j, k, tn, sp, sm, a0, a1, a2)
     switch (w) {
       case 0: FEB_SLOT(0); FEB_SLOT(4); FEB_SLOT(8); FEB_SLOT(12); break;
       case 1: FEB_SLOT(1); FEB_SLOT(5); FEB_SLOT(9); FEB_SLOT(13); break;
@@ -788,6 +818,10 @@ k_sym(SymView<T> L, const T* __restrict__ u, T* __restrict__ y, const T* __restr
       default: FEB_SLOT(3); FEB_SLOT(7); FEB_SLOT(11); break;
     }
 #undef FEB_SLOT
+    if constexpr (H) {
+      const T sc = T(*L.hscale);
+      a0 *= sc; a1 *= sc; a2 *= sc;
+    }
   } else {
     // the same slots with the slot index a run-time value (the loop keeps every slot's loads in flight together)
 #pragma unroll
@@ -913,8 +947,19 @@ void launch_sym(const SymView<T>& L0, int epi, const T* u, T* y, const T* b, T* 
   }
   const bool cmp = L.tag != nullptr;
   const bool ct = L.slots == 2 || (L.slots == 0 && std::is_same<T, float>::value);
-#define FEB_SYM(E, C, CT_) k_sym<T, E, C, CT_><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip, acc)
+#define FEB_SYM(E, C, CT_) k_sym<T, E, C, CT_, false><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip, acc)
 #define FEB_SYM2(E, C) do { if (ct) FEB_SYM(E, C, true); else FEB_SYM(E, C, false); } while (0)
+  if constexpr (std::is_same<T, float>::value) {
+    if (L.Sh) {   // 16-bit storage: uncompressed levels, compile-time slots (the builder sets it only then)
+#define FEB_SYMH(E) k_sym<T, E, false, true, true><<<g, blk, 0, s>>>(L, u, y, b, r, d_out, x, lp, k, skip, acc)
+      if (epi == EPI_APPLY) FEB_SYMH(EPI_APPLY);
+      else if (epi == EPI_RESID) FEB_SYMH(EPI_RESID);
+      else FEB_SYMH(EPI_CHEB);
+#undef FEB_SYMH
+      note_launch();
+      return;
+    }
+  }
   if (epi == EPI_APPLY) {
     if (cmp) FEB_SYM2(EPI_APPLY, true); else FEB_SYM2(EPI_APPLY, false);
   } else if (epi == EPI_RESID) {
@@ -925,6 +970,14 @@ void launch_sym(const SymView<T>& L0, int epi, const T* u, T* y, const T* b, T* 
 #undef FEB_SYM2
 #undef FEB_SYM
   note_launch();
+}
+
+void launch_sym_to_half(const double* S64, int nx, int ny, int nz, unsigned* amax, float* hscale, __half* Sh,
+                        cudaStream_t s) {
+  const int64_t m = 126 * sym_np(nx, ny, nz);
+  cudaMemsetAsync(amax, 0, sizeof(unsigned), s);
+  k_sym_absmax<<<std::min<int64_t>(div_up(m, kThreads), 4 * 148), kThreads, 0, s>>>(S64, m, amax); note_launch();
+  k_sym_to_half<<<div_up(m, kThreads), kThreads, 0, s>>>(S64, m, amax, hscale, Sh); note_launch();
 }
 
 template <typename T>

@@ -1,6 +1,8 @@
 // Coarse multigrid levels: 27-point 3x3-block stencils on structured node grids, structured transfers,
 // and the Galerkin products P^T A P built on the device.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "fine.cuh"
 #include "vec.cuh"
@@ -82,6 +84,11 @@ struct SymView {
   const uint8_t* tag = nullptr;
   const T* tmat = nullptr;  // [128][2]
   const T* pat = nullptr;   // [2][126]
+  // 16-bit storage (FP32 products only): Sh[i] = S[i] / hscale[0] as FP16, hscale a power of two chosen so that
+  // the level's largest entry lands below 2^15; the product accumulates in FP32 and is scaled once.  Sh ==
+  // nullptr: S is read.
+  const __half* Sh = nullptr;
+  const float* hscale = nullptr;
 };
 
 // Fused level kernels: EPI_APPLY y = A u; EPI_RESID r = b - A u; EPI_CHEB Chebyshev step with ping-pong
@@ -97,6 +104,10 @@ void launch_sym(const SymView<T>& L, int epi, const T* u, T* y, const T* b, T* r
 // full [243][n] FP64 stencil of an nx x ny x nz level -> row-padded half storage in T ([126][sym_np])
 template <typename T>
 void launch_stencil_to_sym(const double* A, int nx, int ny, int nz, T* S, cudaStream_t s);
+// FP64 half storage S64 ([126][sym_np]) -> FP16 scaled by a power of two: amax[0] (a scratch word) gets the
+// largest |entry|, hscale[0] the scale 2^e with amax < 2^(e + 15), Sh the entries divided by it
+void launch_sym_to_half(const double* S64, int nx, int ny, int nz, unsigned* amax, float* hscale, __half* Sh,
+                        cudaStream_t s);
 
 template <typename T>
 void launch_csr_add(int nrow, const int* row_dof, const int* row_ptr, const int* col, const T* val, const T* u, T* y,

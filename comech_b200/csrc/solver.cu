@@ -706,6 +706,8 @@ struct Level {
   double* A64 = nullptr;                  // full stencil [243][n] (levels >= 1, set-up only)
   double* S64 = nullptr;                  // symmetric half storage [126][n] (levels >= 1)
   float* S32 = nullptr;
+  __half* S16 = nullptr;                  // 16-bit copy for the FP32 products (instead of S32), and its scale
+  float* hscale = nullptr;                // [2]: the scale, then the largest |entry| (as bits) it was formed from
   int* node_ptr = nullptr;                // per-node CSR of the entries the stencil cannot hold
   int8_t* ent_r = nullptr;
   int* ent_col = nullptr;
@@ -1117,6 +1119,7 @@ struct FebHandle {
     S.nxp = sym_nxp(V.nx); S.np = sym_np(V.nx, V.ny, V.nz);
     S.slots = opt.level_kernel & 3;
     S.S = symS<T>(V);
+    if constexpr (std::is_same<T, float>::value) { S.Sh = V.S16; S.hscale = V.hscale; }
     S.node_ptr = V.node_ptr; S.ent_r = V.ent_r; S.ent_col = V.ent_col; S.ent_v = entv<T>(V);
     S.tn_ptr = V.nterms ? V.tn_ptr : nullptr; S.tn_term = V.tn_term; S.tn_coef = tcoef<T>(V);
     S.t_ptr = V.t_ptr; S.t_dof = V.t_dof; S.t_val = tval<T>(V); S.t_lam = tlam<T>(V);
@@ -2466,7 +2469,12 @@ int build_hierarchy(FebHandle* h) {
       }
       FEB_CUDA(cudaGetLastError());
     }
-    if (f32) {
+    // FP16 copy scaled by a power of two (the compile-time-slot product reads it), else an FP32 copy
+    if (f32 && !(H.opt.level_kernel & 8) && (H.opt.level_kernel & 3) != 1 && !C.tag) {
+      FEB_TRY(H.pool.alloc(&C.S16, 126 * (size_t)sym_np(C.nx, C.ny, C.nz)));
+      FEB_TRY(H.pool.alloc(&C.hscale, 2));
+      launch_sym_to_half(C.S64, C.nx, C.ny, C.nz, reinterpret_cast<unsigned*>(C.hscale + 1), C.hscale, C.S16, H.s);
+    } else if (f32) {
       FEB_TRY(H.pool.alloc(&C.S32, 126 * (size_t)sym_np(C.nx, C.ny, C.nz)));
       launch_stencil_to_sym<float>(C.A64, C.nx, C.ny, C.nz, C.S32, H.s);
     }

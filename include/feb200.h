@@ -95,7 +95,9 @@ typedef struct FebOptions {
                                     products and a run-time value in FP64 products (the faster form of each); 1
                                     run-time in both; 2 compile-time in both.  Bit 2 (+4): the V-cycle's rank-1 term
                                     dots by a dot pass before every product, instead of accumulated by the kernels
-                                    that write the vectors */
+                                    that write the vectors.  FP32 products with compile-time slots read a 16-bit
+                                    copy of the stencil (FP16 scaled by a power of two, FP32 sums) on levels
+                                    without compressed blocks; bit 3 (+8) gives them an FP32 copy instead */
 } FebOptions;
 
 typedef struct FebInfo {

@@ -428,14 +428,16 @@ def test_deferred_setup_is_joined_before_use(golden):
     assert rel(x2[ok].cpu().numpy(), x1[ok].cpu().numpy()) < 1e-7
 
 
-@pytest.mark.parametrize("kernels", [(1, 2), (0, 4)])
+@pytest.mark.parametrize("kernels", [(9, 10), (8, 12), (8, 0)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_level_kernels_agree(golden, precision, kernels):
-    """Forms of the coarse-level products give the same preconditioner: the slot index a run-time value
-    (level_kernel 1) or a compile-time constant (2); the rank-1 term dots accumulated by the kernels that write
-    the vectors (0) or formed by a dot pass before each product (4).  z = M r agrees to 1e-12 (FP64 V-cycle) /
-    1e-4 (FP32 V-cycle: sums round in other orders) relative, and the solves take the same iterations (+-1) to
-    the same solution."""
+    """Forms of the coarse-level products give the same preconditioner (FP32 stencil copies: +8): the slot index
+    a run-time value (level_kernel 9) or a compile-time constant (10); the rank-1 term dots accumulated by the
+    kernels that write the vectors (8) or formed by a dot pass before each product (12).  z = M r agrees to
+    1e-12 (FP64 V-cycle) / 1e-4 (FP32 V-cycle: sums round in other orders) relative, and the solves take the
+    same iterations (+-1) to the same solution.  The default FP16 stencil copies (0 against 8; FP32 V-cycle
+    only) perturb the coarse operators by the FP16 rounding (2^-12 relative per entry): z agrees to 1e-2, the
+    iterations to +-2, the solution to 1e-8."""
     import torch
     z, g = _hindfoot(golden)
     args = (g, z["lam"], z["mu"], z["active"], z["cn"], z["orig"], (z["fixed_nodes"], z["fixed_area"]),
@@ -456,8 +458,9 @@ def test_level_kernels_agree(golden, precision, kernels):
             ctx["P"].close()
     assert min(levels) >= 4              # two stencil levels below the fine level and above the dense one
     (z1, x1, it1, f1), (z2, x2, it2, f2) = out[kernels[0]], out[kernels[1]]
-    assert f1 == 0 and f2 == 0 and abs(it1 - it2) <= 1
-    assert rel(z2, z1) < (1e-12 if precision == "fp64" else 1e-4)
+    half = kernels[1] == 0 and precision == "mixed"
+    assert f1 == 0 and f2 == 0 and abs(it1 - it2) <= (2 if half else 1)
+    assert rel(z2, z1) < (1e-12 if precision == "fp64" else (1e-2 if half else 1e-4))
     assert rel(x2, x1) < 1e-8
 
 
