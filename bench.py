@@ -573,6 +573,8 @@ def run_ours(args, rank, world, dist):
                                else "zero (no trained network found)"),
                 "tol": TOL, "iters": int(hinfo.iters), "sweeps": int(hinfo.sweeps), "relres": hinfo.relres,
                 "levels": int(hinfo.levels), "ku_kernel": ["per-cell", "paired-row", "tensor-core"][int(hinfo.ku_kind)],
+                "coarse_stencils": ("f64" if prec == "fp64" else
+                                    "f32" if SOLVER_OPTIONS.get("level_kernel", 0) & 8 else "f16 scaled, f32 sums"),
                 "l2": "flushed (256 MB write) before every step", "parallelism": f"independent solves x{world}"},
         arms_s_per_solve={k: round(v, 5) for k, v in mean_s.items()},
         arms_step_ms={k: [round(x, 2) for x in v["ms"]] for k, v in res.items()},
